@@ -1,0 +1,10 @@
+"""B200-native interpolated mode summation for FastEMRIWaveforms.
+
+Drop-in for ``few.summation.interpolatedmodesum.InterpolatedModeSum`` and its
+``CubicSplineInterpolant``: Python host code over hand-written sm_100a CUDA
+kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
+"""
+from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBase
+from .utility import get_mismatch, get_overlap
+
+__all__ = ["CubicSplineInterpolant", "InterpolatedModeSum", "SummationBase", "get_mismatch", "get_overlap"]

@@ -1,0 +1,58 @@
+// Host-side internals shared by the translation units of libfew_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "few_b200.h"
+
+namespace few {
+
+// Records the message of a failed call for few_last_error() and returns code.
+int fail(int code, const char *fmt, ...);
+
+// Clears the message at the start of a call.
+void clear_error();
+
+// Checks a CUDA runtime result; on failure records it and returns FEW_ERR_CUDA.
+#define FEW_CUDA_TRY(expr)                                                                   \
+    do {                                                                                     \
+        cudaError_t few_err_ = (expr);                                                       \
+        if (few_err_ != cudaSuccess)                                                         \
+            return ::few::fail(FEW_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,                 \
+                               cudaGetErrorString(few_err_), __FILE__, __LINE__);            \
+    } while (0)
+
+// After a kernel launch: report launch-configuration errors.
+#define FEW_LAUNCH_CHECK(name)                                                               \
+    do {                                                                                     \
+        cudaError_t few_err_ = cudaGetLastError();                                           \
+        if (few_err_ != cudaSuccess)                                                         \
+            return ::few::fail(FEW_ERR_CUDA, "launch of %s failed: %s", name,                 \
+                               cudaGetErrorString(few_err_));                                \
+    } while (0)
+
+// Host-side fold plan and segment plan (plan.cpp), also used by the
+// reference-shaped entry point.
+int fold_plan(const int *m, const int *k, const int *n, int K, int max_rows, int max_keys, int *row_m,
+              int *row_k, int *dims, int *key_ptr, int *key_list);
+int segment_plan(const double *h_t, const double *phase_t, int init_len, int out_len, double dt,
+                 int chunk, int max_units, int *seg_start, double *seg_info, int *units, int *counts);
+
+// Kernel launchers (no argument validation beyond what the kernels need).
+int launch_spline_build(const double *t, long long t_rs, const double *y, long long sk, long long sp,
+                        int split, long long off2, int ni, int N, double *out, int layout,
+                        cudaStream_t st);
+int launch_fold(const double *coeffs, const double2 *ylms, const int *key_ptr, const int *key_list,
+                int K, int N, int nseg, int R, int NN, double2 *W, cudaStream_t st);
+int launch_sum_folded(double2 *wf, const double2 *W, const double *pc, int N, const double *seg_info,
+                      const int *units, int nunits, const int *row_m, const int *row_k, int R,
+                      int nlo, int NN, double dt, int mode, int use_theta, cudaStream_t st);
+
+constexpr int kMaxRows = 256;        // distinct (m', k') rows of a fold plan
+constexpr int kDefaultChunk = 1024;  // output samples per work unit of the sum
+
+}  // namespace few

@@ -1,0 +1,299 @@
+// Folded FP64 mode sum.
+//
+// The reference (src/few/cutils/interpolate.cu:444-689) evaluates, for every
+// output sample and every mode, a complex exponential of the rounded phase
+// fl(m*Phi_phi + k*Phi_theta + n*Phi_r), the cubic amplitude, and two complex
+// products, one launch per knot segment with FP64 atomics.
+//
+// Here the sum is regrouped without changing its value:
+//   * Fold.  The phase of a term depends on its key (m', k', n') only, so per
+//     knot segment s every amplitude term sharing a key is summed once:
+//     W[s][key][c] = sum Y+_j a_c(j) (the +m term of mode j) and
+//     sum Y-_j conj(a_c(j)) for the -m term, whose key is (-m, -k, -n) because
+//     conj(exp(-i fl(phase))) = exp(-i fl(-phase)).  (k_fold_coeffs)
+//   * Phasors by recurrence.  Per sample, e^{-i Phi_phi}, e^{-i Phi_r}
+//     (and e^{-i Phi_theta} if used) come from one FP64 sincos each; every key
+//     phasor is built from them by complex multiplication: rows (m', k') by
+//     binary powering, columns n' by a running product along the n' grid.
+//   * Rounding replay (FEW_SUM_FAITHFUL).  The reference rounds the combined
+//     phase; the recurrence does not.  The exact difference is recovered with
+//     error-free transformations: m'*Phi = p + e exactly (e = fma(m', Phi, -p)),
+//     and a + b = fl(a+b) + TwoSum error.  With eps the sum of the five errors,
+//     e^{-i fl(phase)} = e^{-i phase} e^{+i eps}, and |eps| < 1e-8 rad, so the
+//     factor is applied as (1 + i eps).  Row-only and column-only errors are
+//     folded into the row and column phasors; the one error that depends on
+//     both (rounding fl(s12 + p3)) costs one TwoSum per key and sample.
+//   * Per sample: h = sum_{n'} v_{n'} sum_{r} u_r (sum_c x^c W[r][n'][c]),
+//     10 DFMA per key in FEW_SUM_EXACT, 18 FP64 operations per key in
+//     FEW_SUM_FAITHFUL.
+// One CTA owns a run of at most `chunk` samples of one segment (a work unit),
+// stages that segment's W block in shared memory (broadcast reads), and each
+// thread writes its own samples: no atomics, deterministic, coalesced stores.
+#include <algorithm>
+
+#include "few_common.cuh"
+#include "few_internal.h"
+
+namespace few {
+
+namespace {
+
+constexpr int kSumThreads = 256;
+constexpr int kRowBlock = 8;                   // rows held in registers at once
+constexpr int kSmemBudget = 200 * 1024;        // dynamic shared memory for W per CTA
+
+// ---------------------------------------------------------------------------
+// Fold: thread per (segment, key), contributors in mode order (deterministic).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_fold_coeffs(const double *__restrict__ coeffs,
+                                                     const double2 *__restrict__ ylms,
+                                                     const int *__restrict__ key_ptr,
+                                                     const int *__restrict__ key_list, int K, int N,
+                                                     int nseg, int nkeys, double2 *__restrict__ W)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nseg * nkeys) return;
+    const int s = (int)(idx / nkeys);
+    const int q = (int)(idx - (long long)s * nkeys);
+    const long long plane = (long long)N * 2 * K;
+    const double *cs = coeffs + (long long)s * 2 * K;
+    double2 acc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] = make_double2(0.0, 0.0);
+    const int b = key_ptr[q], e = key_ptr[q + 1];
+    for (int it = b; it < e; ++it) {
+        const int code = key_list[it];
+        const int j = code >> 1;
+        const bool minus = code & 1;
+        const double2 Y = minus ? ylms[K + j] : ylms[j];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double ar = cs[c * plane + j];
+            const double ai = minus ? -cs[c * plane + K + j] : cs[c * plane + K + j];
+            acc[c].x = fma(Y.x, ar, fma(-Y.y, ai, acc[c].x));
+            acc[c].y = fma(Y.x, ai, fma(Y.y, ar, acc[c].y));
+        }
+    }
+    double2 *w = W + idx * 4;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) w[c] = acc[c];
+}
+
+// ---------------------------------------------------------------------------
+// Sum.
+// ---------------------------------------------------------------------------
+struct SumArgs {
+    double2 *wf;
+    const double2 *W;
+    const double *pc;  // (8, N-1, 3)
+    const double *seg_info;
+    const int *units;
+    const int *row_m;
+    const int *row_k;
+    int N, R, nlo, NN;
+    int rows_per_pass;
+    int use_theta;
+    double dt;
+};
+
+template <int RB, bool FAITHFUL>
+__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *sW = reinterpret_cast<double2 *>(smem_raw);
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+
+    const int u = blockIdx.x;
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const int R = a.R, NN = a.NN, nlo = a.nlo;
+    const long long nps = (long long)(a.N - 1) * 3;
+
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        s_rm[r] = a.row_m[r];
+        s_rk[r] = a.row_k[r];
+    }
+    if (threadIdx.x < 24) {
+        const int q = threadIdx.x >> 3, c = threadIdx.x & 7;  // q: 0 phi, 1 theta, 2 r
+        s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+
+    for (int r0 = 0; r0 < R; r0 += a.rows_per_pass) {
+        const int nrp = min(a.rows_per_pass, R - r0);
+        __syncthreads();  // previous pass finished reading sW
+        {
+            const double2 *src = a.W + ((long long)seg * R + r0) * NN * 4;
+            const int count = nrp * NN * 4;
+            for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
+        }
+        __syncthreads();
+
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            // Sample time and phases exactly as interpolate.cu:626-644.
+            const double t = rmul(a.dt, (double)i);
+            const double x = rsub(t, t0);
+            const double s = __ddiv_rn(rsub(t, pt0), pw);
+            const double s1 = rsub(1.0, s);
+            const double Pp = phase_poly(s_pc, s, s1);
+            const double Pr = phase_poly(s_pc + 16, s, s1);
+            const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
+            double sn, cs;
+            sincos(Pp, &sn, &cs);
+            const double2 Ep = make_double2(cs, -sn);
+            sincos(Pr, &sn, &cs);
+            const double2 Er = make_double2(cs, -sn);
+            double2 Et = make_double2(1.0, 0.0);
+            if (a.use_theta) {
+                sincos(Pt, &sn, &cs);
+                Et = make_double2(cs, -sn);
+            }
+            const double2 V0 = cpow_int(Er, nlo);
+            double2 h = make_double2(0.0, 0.0);
+
+            for (int rb = 0; rb < nrp; rb += RB) {
+                double2 U[RB];
+                double S12[RB];
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    U[q] = make_double2(0.0, 0.0);
+                    S12[q] = 0.0;
+                    if (rb + q < nrp) {
+                        const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
+                        double2 uu = cpow_int(Ep, mm);
+                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
+                        if (FAITHFUL) {
+                            const double dm = (double)mm, dk = (double)kk;
+                            const double p1 = rmul(dm, Pp);
+                            const double e1 = fma(dm, Pp, -p1);
+                            const double p2 = rmul(dk, Pt);
+                            const double e2 = fma(dk, Pt, -p2);
+                            const double s12 = radd(p1, p2);
+                            const double e12 = two_sum_err(p1, p2, s12);
+                            uu = crot_small(uu, (e1 + e2) + e12);
+                            S12[q] = s12;
+                        }
+                        U[q] = uu;
+                    }
+                }
+                double2 v = V0;
+                const double2 *wrow = sW + (long long)rb * NN * 4;
+                for (int c = 0; c < NN; ++c) {
+                    double2 vv = v;
+                    double p3 = 0.0;
+                    if (FAITHFUL) {
+                        const double dn = (double)(nlo + c);
+                        p3 = rmul(dn, Pr);
+                        vv = crot_small(v, fma(dn, Pr, -p3));
+                    }
+                    double2 T = make_double2(0.0, 0.0);
+                    const double2 *wc = wrow + c * 4;
+#pragma unroll
+                    for (int q = 0; q < RB; ++q) {
+                        if (rb + q < nrp) {
+                            const double2 *w = wc + (long long)q * NN * 4;
+                            const double2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+                            double2 Wx;
+                            Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
+                            Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
+                            if (FAITHFUL) {
+                                const double sp = radd(S12[q], p3);
+                                Wx = crot_small(Wx, two_sum_err(S12[q], p3, sp));
+                            }
+                            T.x = fma(U[q].x, Wx.x, fma(-U[q].y, Wx.y, T.x));
+                            T.y = fma(U[q].x, Wx.y, fma(U[q].y, Wx.x, T.y));
+                        }
+                    }
+                    h.x = fma(vv.x, T.x, fma(-vv.y, T.y, h.x));
+                    h.y = fma(vv.x, T.y, fma(vv.y, T.x, h.y));
+                    v = cmul(v, Er);
+                }
+            }
+            double2 o = a.wf[i];
+            o.x += h.x;
+            o.y += h.y;
+            a.wf[i] = o;
+        }
+    }
+}
+
+template <int RB, bool F>
+int launch_sum_t(const SumArgs &a, int nunits, size_t smem, cudaStream_t st)
+{
+    // Per-device attribute; cheap, so set on every launch (one process may drive several devices).
+    FEW_CUDA_TRY(cudaFuncSetAttribute(k_sum_folded<RB, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kSmemBudget));
+    k_sum_folded<RB, F><<<nunits, kSumThreads, smem, st>>>(a);
+    FEW_LAUNCH_CHECK("k_sum_folded");
+    return FEW_OK;
+}
+
+}  // namespace
+
+int launch_fold(const double *coeffs, const double2 *ylms, const int *key_ptr, const int *key_list, int K, int N,
+                int nseg, int R, int NN, double2 *W, cudaStream_t st)
+{
+    const int nkeys = R * NN;
+    const long long total = (long long)nseg * nkeys;
+    if (total == 0) return FEW_OK;
+    const int threads = 256;
+    const long long blocks = (total + threads - 1) / threads;
+    k_fold_coeffs<<<(unsigned)blocks, threads, 0, st>>>(coeffs, ylms, key_ptr, key_list, K, N, nseg, nkeys, W);
+    FEW_LAUNCH_CHECK("k_fold_coeffs");
+    return FEW_OK;
+}
+
+int launch_sum_folded(double2 *wf, const double2 *W, const double *pc, int N, const double *seg_info,
+                      const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo, int NN,
+                      double dt, int mode, int use_theta, cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    SumArgs a;
+    a.wf = wf;
+    a.W = W;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const long long row_bytes = (long long)NN * 4 * sizeof(double2);
+    int rpp = (int)std::min<long long>(R, kSmemBudget / row_bytes);
+    if (rpp < 1) return fail(FEW_ERR_SIZE, "few_sum_folded: NN=%d too large for one row in shared memory", NN);
+    a.rows_per_pass = rpp;
+    const size_t smem = (size_t)rpp * row_bytes;
+    if (mode == FEW_SUM_FAITHFUL) return launch_sum_t<kRowBlock, true>(a, nunits, smem, st);
+    return launch_sum_t<kRowBlock, false>(a, nunits, smem, st);
+}
+
+}  // namespace few
+
+extern "C" int few_fold_coeffs(const double *coeffs, const void *ylms, const int *key_ptr, const int *key_list,
+                               int K, int N, int nseg, int R, int NN, void *W, void *stream)
+{
+    few::clear_error();
+    if (!coeffs || !ylms || !key_ptr || !key_list || !W) return few::fail(FEW_ERR_ARG, "few_fold_coeffs: null pointer");
+    if (K < 1 || N < 2 || nseg < 0 || nseg > N - 1 || R < 1 || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_fold_coeffs: bad sizes");
+    return few::launch_fold(coeffs, (const double2 *)ylms, key_ptr, key_list, K, N, nseg, R, NN, (double2 *)W,
+                            (cudaStream_t)stream);
+}
+
+extern "C" int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, int N, const double *seg_info,
+                              const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo,
+                              int NN, double dt, int mode, int use_theta, void *stream)
+{
+    few::clear_error();
+    if (!wf || !W || !phase_coeffs || !seg_info || !units || !row_m || !row_k)
+        return few::fail(FEW_ERR_ARG, "few_sum_folded: null pointer");
+    if (N < 2 || nunits < 0 || R < 1 || R > few::kMaxRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_sum_folded: bad sizes (R must be <= %d)", few::kMaxRows);
+    if (mode != FEW_SUM_FAITHFUL && mode != FEW_SUM_EXACT) return few::fail(FEW_ERR_ARG, "few_sum_folded: bad mode");
+    return few::launch_sum_folded((double2 *)wf, (const double2 *)W, phase_coeffs, N, seg_info, units, nunits, row_m,
+                                  row_k, R, nlo, NN, dt, mode, use_theta, (cudaStream_t)stream);
+}

@@ -1,0 +1,266 @@
+// Batched not-a-knot cubic splines: build (tridiagonal solve) and evaluation.
+//
+// Build.  The reference fills the not-a-knot rows (src/few/cutils/interpolate.cu:48-145),
+// solves every system with a pivoting tridiagonal solver (cuSPARSE gtsv2StridedBatch
+// on the GPU, LAPACK dgtsv on the CPU, interpolate.cu:201-239) and then derives
+// the cubic coefficients (interpolate.cu:29-43, 149-198, 241-280) in three more
+// launches with host synchronisations between them.
+//
+// Here one thread owns one interpolant and does all of it in one launch:
+//   * The first and last not-a-knot rows are not diagonally dominant, so they
+//     are eliminated up front.  Row 0 reads h1*s0 + (x2-x0)*s1 = b0 and row 1
+//     has h1 as its s0 coefficient, so row1 - row0 removes s0 with an exact
+//     factor of 1 (the same elimination a pivoting solver makes at that step);
+//     the last row is removed from row N-2 the same way.  Rows 1..N-2 are then
+//     strictly diagonally dominant and a Thomas sweep without pivoting is
+//     stable.
+//   * The forward sweep writes its two running values (c'_i, r'_i) into the
+//     c2/c3 output rows of knot i; the backward sweep reads them back, forms the
+//     slope s_i and immediately overwrites knot i with the final coefficients,
+//     so no scratch memory is used.
+//   * The coefficient formulas are those of fill_coefficients and
+//     fill_final_derivs (the last knot carries the derivative-extrapolated
+//     c1, c2, c3 of the last segment).
+// y is read through a strided view, so the (N, K) complex Teukolsky amplitudes
+// are splined in place (real parts as interpolants 0..K-1, imaginary parts as
+// K..2K-1) with no (2K, N) copy.  Output layout (4, N, ninterps) makes every
+// store of a warp one contiguous run.
+//
+// Evaluation restates CubicSplineInterpolant.__call__
+// (src/few/summation/interpolatedmodesum.py:118-257): interval by
+// searchsorted(side="right") - 1 with the last knot mapped to the last interval,
+// y + c1 x + c2 x^2 + c3 x^3 (or a derivative), edge values outside the range.
+#include "few_common.cuh"
+#include "few_internal.h"
+
+namespace few {
+
+namespace {
+
+struct SplineArgs {
+    const double *t;
+    long long t_rs;
+    const double *y;
+    long long sk, sp, off2;
+    int split;
+    int ni, N;
+    double *out;
+    long long os_i, os_p;  // output stride per knot / per interpolant inside one plane
+};
+
+__device__ __forceinline__ void write_segment(double *o1, double *o2, double *o3, long long off, double s_i,
+                                              double s_ip1, double y_i, double y_ip1, double dx)
+{
+    // fill_coefficients (interpolate.cu:29-43)
+    double slope = (y_ip1 - y_i) / dx;
+    double tt = (s_i + s_ip1 - 2 * slope) / dx;
+    o1[off] = s_i;
+    o2[off] = (slope - s_i) / dx - tt;
+    o3[off] = tt / dx;
+}
+
+__global__ void __launch_bounds__(128) k_spline_build(SplineArgs a)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.ni) return;
+    const int N = a.N;
+    const double *x = a.t + (long long)p * a.t_rs;
+    const double *yb = (p < a.split) ? a.y + (long long)p * a.sp : a.y + a.off2 + (long long)(p - a.split) * a.sp;
+    const long long sk = a.sk;
+    const long long plane = (long long)N * a.ni, oi = a.os_i;
+    double *o0 = a.out + (long long)p * a.os_p;
+    double *o1 = o0 + plane;
+    double *o2 = o1 + plane;
+    double *o3 = o2 + plane;
+
+    // First not-a-knot row (interpolate.cu:71-86).
+    const double x0 = x[0], x1 = x[1], x2 = x[2];
+    const double y0 = yb[0], y1 = yb[sk], y2 = yb[2 * sk];
+    const double h0 = x1 - x0, h1 = x2 - x1, d0 = x2 - x0;
+    const double b0 = ((h0 + 2 * d0) * h1 * ((y1 - y0) / h0) + h0 * h0 * ((y2 - y1) / h1)) / d0;
+    // Last not-a-knot row (interpolate.cu:56-69).
+    const double xa = x[N - 3], xb = x[N - 2], xc = x[N - 1];
+    const double ya = yb[(long long)(N - 3) * sk], yv = yb[(long long)(N - 2) * sk], yc = yb[(long long)(N - 1) * sk];
+    const double hA = xb - xa, hB = xc - xb, dE = xc - xa;
+    const double bE = (hB * hB * ((yv - ya) / hA) + (2 * dE + hB) * hA * ((yc - yv) / hB)) / dE;
+
+    // Forward sweep over rows 1..N-2 (interior rows of interpolate.cu:88-101).
+    double cprev = 0.0, rprev = 0.0;
+    double xm = x0, xi = x1, ym = y0, yi = y1;
+    for (int i = 1; i <= N - 2; ++i) {
+        const double xn = x[i + 1];
+        const double yn = yb[(long long)(i + 1) * sk];
+        const double hl = xi - xm, hr = xn - xi;
+        double lo = hr, dg = 2 * (hl + hr), up = hl;
+        double rhs = 3.0 * (hr * ((yi - ym) / hl) + hl * ((yn - yi) / hr));
+        if (i == 1) {  // row 1 - row 0
+            dg -= d0;
+            rhs -= b0;
+            lo = 0.0;
+        }
+        if (i == N - 2) {  // row N-2 - row N-1
+            dg -= dE;
+            rhs -= bE;
+            up = 0.0;
+        }
+        const double den = dg - lo * cprev;
+        const double cp = up / den;
+        const double rp = (rhs - lo * rprev) / den;
+        o2[i * oi] = cp;
+        o3[i * oi] = rp;
+        cprev = cp;
+        rprev = rp;
+        xm = xi;
+        xi = xn;
+        ym = yi;
+        yi = yn;
+    }
+
+    // Backward sweep.  s_{N-2} = r'_{N-2}; s_{N-1} from the last row.
+    double s_ip1 = rprev;
+    const double s_last = (bE - dE * s_ip1) / hA;
+    {
+        const long long off = (long long)(N - 2) * oi;
+        write_segment(o1, o2, o3, off, s_ip1, s_last, yv, yc, hB);
+        o0[off] = yv;
+        // fill_final_derivs (interpolate.cu:241-280)
+        const double c1 = o1[off], c2 = o2[off], c3 = o3[off];
+        const double xx = hB, x2v = xx * xx;
+        const long long offe = (long long)(N - 1) * oi;
+        o0[offe] = yc;
+        o1[offe] = c1 + 2 * c2 * xx + 3 * c3 * x2v;
+        o2[offe] = (2. * c2 + 6. * c3 * xx) / 2.;
+        o3[offe] = c3;
+    }
+    double xr = xb, yr = yv;  // knot i+1
+    for (int i = N - 3; i >= 1; --i) {
+        const long long off = (long long)i * oi;
+        const double cp = o2[off], rp = o3[off];
+        const double s_i = rp - cp * s_ip1;
+        const double xl = x[i];
+        const double yl = yb[(long long)i * sk];
+        write_segment(o1, o2, o3, off, s_i, s_ip1, yl, yr, xr - xl);
+        o0[off] = yl;
+        s_ip1 = s_i;
+        xr = xl;
+        yr = yl;
+    }
+    // s_0 from the first row.
+    const double s0 = (b0 - d0 * s_ip1) / h1;
+    write_segment(o1, o2, o3, 0, s0, s_ip1, y0, y1, h0);
+    o0[0] = y0;
+}
+
+__global__ void k_spline_eval(const double *__restrict__ t, long long t_rs, const double *__restrict__ coeffs,
+                              int ni, int N, const double *__restrict__ tnew, long long tn_rs, int M, int deriv,
+                              double *__restrict__ out, int *__restrict__ flags)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)ni * M) return;
+    const int p = (int)(idx / M);
+    const int j = (int)(idx - (long long)p * M);
+    const double *x = t + (long long)p * t_rs;
+    const double tv = tnew[(long long)p * tn_rs + j];
+    // searchsorted(x, tv, side="right") - 1
+    int lo = 0, hi = N;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (x[mid] <= tv) lo = mid + 1;
+        else hi = mid;
+    }
+    int ind = lo - 1;
+    if (tv == x[N - 1]) ind = N - 2;
+    const bool left = tv < x[0];
+    const bool right = tv > x[N - 1];
+    if (left) atomicOr(&flags[0], 1);
+    if (right) atomicOr(&flags[1], 1);
+    if (ind < 0) ind = 0;  // only reached when left; value replaced below
+    const long long plane = (long long)N * ni;
+    const long long o = (long long)ind * ni + p;
+    const double xx = tv - x[ind];
+    const double y = coeffs[o], c1 = coeffs[plane + o], c2 = coeffs[2 * plane + o], c3 = coeffs[3 * plane + o];
+    double v;
+    if (deriv == 0) {
+        const double x2 = xx * xx, x3 = x2 * xx;
+        v = y + c1 * xx + c2 * x2 + c3 * x3;
+        if (left) v = coeffs[p];
+        if (right) v = coeffs[(long long)(N - 1) * ni + p];
+    } else if (deriv == 1) {
+        v = c1 + 2 * c2 * xx + 3 * c3 * (xx * xx);
+    } else if (deriv == 2) {
+        v = 2 * c2 + 6 * c3 * xx;
+    } else {
+        v = 6 * c3;
+    }
+    out[idx] = v;
+}
+
+}  // namespace
+
+int launch_spline_build(const double *t, long long t_rs, const double *y, long long sk, long long sp, int split,
+                        long long off2, int ni, int N, double *out, int layout, cudaStream_t st)
+{
+    SplineArgs a;
+    a.t = t;
+    a.t_rs = t_rs;
+    a.y = y;
+    a.sk = sk;
+    a.sp = sp;
+    a.off2 = off2;
+    a.split = split;
+    a.ni = ni;
+    a.N = N;
+    a.out = out;
+    if (layout == FEW_LAYOUT_KNOT_MAJOR) {
+        a.os_i = ni;
+        a.os_p = 1;
+    } else {
+        a.os_i = 1;
+        a.os_p = N;
+    }
+    const int threads = 128;
+    const int blocks = (ni + threads - 1) / threads;
+    k_spline_build<<<blocks, threads, 0, st>>>(a);
+    FEW_LAUNCH_CHECK("k_spline_build");
+    return FEW_OK;
+}
+
+}  // namespace few
+
+extern "C" int few_spline_build(const double *t, long long t_row_stride, const double *y, long long y_knot_stride,
+                                long long y_interp_stride, int y_split, long long y_split_offset, int ninterps,
+                                int length, double *coeffs, int layout, void *stream)
+{
+    few::clear_error();
+    if (!t || !y || !coeffs) return few::fail(FEW_ERR_ARG, "few_spline_build: null pointer");
+    if (ninterps < 1) return few::fail(FEW_ERR_SIZE, "few_spline_build: ninterps=%d < 1", ninterps);
+    if (length < 4)
+        return few::fail(FEW_ERR_SIZE, "few_spline_build: length=%d; not-a-knot splines need at least 4 knots",
+                         length);
+    if (layout != FEW_LAYOUT_KNOT_MAJOR && layout != FEW_LAYOUT_INTERP_MAJOR)
+        return few::fail(FEW_ERR_ARG, "few_spline_build: unknown layout %d", layout);
+    if (y_split < 0 || y_split > ninterps) return few::fail(FEW_ERR_ARG, "few_spline_build: bad y_split");
+    if ((long long)ninterps * length * 4 > (1LL << 40)) return few::fail(FEW_ERR_SIZE, "few_spline_build: too large");
+    return few::launch_spline_build(t, t_row_stride, y, y_knot_stride, y_interp_stride, y_split, y_split_offset,
+                                    ninterps, length, coeffs, layout, (cudaStream_t)stream);
+}
+
+extern "C" int few_spline_eval(const double *t, long long t_row_stride, const double *coeffs, int ninterps,
+                               int length, const double *tnew, long long tnew_row_stride, int M, int deriv_order,
+                               double *out, int *flags, void *stream)
+{
+    few::clear_error();
+    if (!t || !coeffs || !tnew || !out || !flags) return few::fail(FEW_ERR_ARG, "few_spline_eval: null pointer");
+    if (ninterps < 1 || length < 2 || M < 0) return few::fail(FEW_ERR_SIZE, "few_spline_eval: bad sizes");
+    if (deriv_order < 0 || deriv_order > 3)
+        return few::fail(FEW_ERR_ARG, "deriv_order must be within 0 <= deriv_order <= 3.");
+    if (M == 0) return FEW_OK;
+    const long long total = (long long)ninterps * M;
+    const int threads = 256;
+    const long long blocks = (total + threads - 1) / threads;
+    if (blocks > 0x7fffffffLL) return few::fail(FEW_ERR_SIZE, "few_spline_eval: too many points");
+    few::k_spline_eval<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        t, t_row_stride, coeffs, ninterps, length, tnew, tnew_row_stride, M, deriv_order, out, flags);
+    FEW_LAUNCH_CHECK("k_spline_eval");
+    return FEW_OK;
+}

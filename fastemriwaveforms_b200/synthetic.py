@@ -1,0 +1,278 @@
+"""Seeded synthetic EMRI-like inputs for the interpolated mode sum.
+
+No public dataset is involved in this path: the inputs of
+``InterpolatedModeSum`` (``src/few/summation/interpolatedmodesum.py:283-375``)
+are a trajectory's knot times, Teukolsky amplitudes at those knots, spherical
+harmonics and DOPR853-style phase coefficients.  This module draws them from
+fixed generators with the shapes and value ranges of a FastEMRIWaveforms
+trajectory, seeded with ``numpy.random.default_rng``.
+
+Workloads (sizes are part of the benchmark definition):
+
+* ``plain_small``  -- K=200 modes (l=2..4, m=0..l, n=-10..10, truncated),
+  N=100 knots on [0, 1e6] s, dt=10 s, 100,001 samples.
+* ``plain_full``   -- K=3843 modes (l=2..10, m=0..l, n=-30..30), N=1000 knots
+  on [0, 3.15e7] s, dt=10 s, 3,150,001 samples (one year at 10 s cadence).
+* ``adjoint``      -- K=1000 (prefix of the full list), N=500 knots,
+  1,000,000 samples.
+* ``batch``        -- many waveforms with uneven T, N and K.
+
+Phases are closed-form integrals of a chirping frequency
+f(t) = 1e-3 (1 - t/t_c)^(-3/8) Hz:
+Phi_phi = int 2 pi f dt and Phi_r = int 0.78 * 2 pi f (1 + 0.1 t/S) dt.
+They are fitted with not-a-knot cubic splines and written in the 8-term
+dense-output basis the sum kernel evaluates (``interpolate.cu:637-644``): a
+cubic y0 + A1 s + A2 s^2 + A3 s^3 in s = (t - t_j)/h is exactly the basis
+vector (y0, A1+A2+A3, -A2-A3, -A3, 0, 0, 0, 0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+YRSID_SI = 31558149.763545595  # seconds per sidereal year (src/few/cutils/global.h:23)
+
+
+@dataclass
+class ModeSumInputs:
+    """Arguments of ``InterpolatedModeSum.__call__`` for one waveform."""
+
+    t: np.ndarray              # (N,) knot times, s
+    teuk_modes: np.ndarray     # (N, K) complex amplitudes at the knots
+    ylms: np.ndarray           # (2K,) complex: +m harmonics, then -m harmonics
+    phase_t: np.ndarray        # (N,) knot times of the phase polynomials
+    phase_coeffs: np.ndarray   # (N-1, 3, 8) [Phi_phi, Phi_theta, Phi_r] basis coefficients
+    l: np.ndarray              # (K,) int
+    m: np.ndarray
+    k: np.ndarray
+    n: np.ndarray
+    dt: float
+    T: float                   # observation time in years (SummationBase.__call__)
+    phase_knots: np.ndarray = field(default=None)  # (3, N) phase values at the knots
+    name: str = ""
+    seed: int = 0
+
+    @property
+    def num_modes(self) -> int:
+        return int(self.teuk_modes.shape[1])
+
+    @property
+    def num_knots(self) -> int:
+        return int(self.t.shape[0])
+
+    @property
+    def out_len(self) -> int:
+        """Output length as SummationBase.__call__ computes it (no padding)."""
+        return output_length(self.t, self.T, self.dt)[0]
+
+    def call_args(self):
+        return (self.t, self.teuk_modes, self.ylms, self.phase_t, self.phase_coeffs,
+                self.l, self.m, self.k, self.n)
+
+
+def output_length(t, T: float, dt: float, pad_output: bool = False, odd_len: bool = False):
+    """(num_pts, num_pts_pad) exactly as ``SummationBase.__call__``
+    (``src/few/summation/base.py:87-124``)."""
+    n_pts = int(T * YRSID_SI / dt)
+    Tsec = n_pts * dt
+    t0 = float(t[0])
+    t1 = float(t[-1])
+    if Tsec < t1:
+        num_pts = int((Tsec - t0) / dt) + 1
+        num_pts_pad = 0
+    else:
+        num_pts = int((t1 - t0) / dt) + 1
+        num_pts_pad = int((Tsec - t0) / dt) + 1 - num_pts if pad_output else 0
+    if odd_len and (num_pts + num_pts_pad) % 2 == 0:
+        num_pts_pad += 1
+    return num_pts, num_pts_pad
+
+
+def mode_list(lmax: int, nmax: int, count: int | None = None):
+    """(l, m, k, n) in product order l=2..lmax, m=0..l, n=-nmax..nmax, k=0."""
+    ls, ms, ns = [], [], []
+    for l in range(2, lmax + 1):
+        for m in range(0, l + 1):
+            for n in range(-nmax, nmax + 1):
+                ls.append(l)
+                ms.append(m)
+                ns.append(n)
+    ls = np.asarray(ls, dtype=np.int32)
+    ms = np.asarray(ms, dtype=np.int32)
+    ns = np.asarray(ns, dtype=np.int32)
+    if count is not None:
+        ls, ms, ns = ls[:count], ms[:count], ns[:count]
+    return ls, ms, np.zeros_like(ms), ns
+
+
+def knot_times(rng, N: int, span: float, min_gap: float) -> np.ndarray:
+    """N sorted knots on [0, span]: endpoints fixed, N-2 uniform draws
+    conditioned on every gap being >= min_gap (spacing transform of sorted
+    uniforms, equal in law to redrawing until the condition holds)."""
+    free = span - (N - 1) * min_gap
+    if free <= 0:
+        raise ValueError("min_gap too large for the span")
+    u = np.sort(rng.uniform(0.0, free, N - 2))
+    t = np.empty(N)
+    t[0] = 0.0
+    t[-1] = span
+    t[1:-1] = u + min_gap * np.arange(1, N - 1)
+    return t
+
+
+def phase_values(t, t_c: float, scale: float, f0: float = 1e-3):
+    """Closed-form Phi_phi(t), Phi_r(t) of the chirp f = f0 (1 - t/t_c)^(-3/8)."""
+    w = 1.0 - np.asarray(t, dtype=np.float64) / t_c
+    a = 0.1 * t_c / scale
+    phi = 2.0 * np.pi * f0 * t_c * 1.6 * (1.0 - w ** 0.625)
+    phr = 2.0 * np.pi * 0.78 * f0 * t_c * ((1.0 + a) * 1.6 * (1.0 - w ** 0.625)
+                                           - a * (8.0 / 13.0) * (1.0 - w ** 1.625))
+    return phi, phr
+
+
+def cubic_to_basis(y0, c1, c2, c3, h):
+    """Map cubic segments y0 + c1 x + c2 x^2 + c3 x^3 (x = t - t_j, width h)
+    onto the 8-term basis y + s(b1 + s1(b2 + s(b3 + s1(...)))) of
+    ``interpolate.cu:637-644`` with s = x/h, s1 = 1 - s.  Returns (..., 8)."""
+    A1 = c1 * h
+    A2 = c2 * h * h
+    A3 = c3 * h * h * h
+    out = np.zeros(np.shape(y0) + (8,))
+    out[..., 0] = y0
+    out[..., 1] = A1 + A2 + A3
+    out[..., 2] = -A2 - A3
+    out[..., 3] = -A3
+    return out
+
+
+def not_a_knot_coeffs(t, y):
+    """Not-a-knot cubic spline coefficients (y, c1, c2, c3) per segment, each
+    (..., N-1), via scipy (same boundary conditions as the reference spline)."""
+    from scipy.interpolate import CubicSpline
+
+    cs = CubicSpline(t, y, axis=-1, bc_type="not-a-knot")
+    c = cs.c  # (4, N-1, ...) highest power first
+    c = np.moveaxis(c, 1, -1) if c.ndim == 3 else c
+    return c[3], c[2], c[1], c[0]
+
+
+def phase_basis_from_knots(t, phase_knots):
+    """(N-1, 3, 8) phase coefficients from (3, N) phase knot values, through
+    not-a-knot cubic splines."""
+    N = len(t)
+    h = np.diff(t)
+    out = np.zeros((N - 1, 3, 8))
+    for q in range(3):
+        if not np.any(phase_knots[q]):
+            continue
+        y0, c1, c2, c3 = not_a_knot_coeffs(t, phase_knots[q])
+        out[:, q, :] = cubic_to_basis(y0, c1, c2, c3, h)
+    return out
+
+
+def make_inputs(K: int, N: int, span: float, t_c: float, lmax: int, nmax: int, seed: int,
+                dt: float = 10.0, scale: float | None = None, name: str = "",
+                min_gap: float | None = None) -> ModeSumInputs:
+    rng = np.random.default_rng(seed)
+    scale = span if scale is None else scale
+    if min_gap is None:
+        # 1e3 s at N=100 on [0, 1e6] s, rescaled with the mean gap elsewhere
+        min_gap = 0.099 * span / (N - 1)
+    t = knot_times(rng, N, span, min_gap)
+    l, m, k, n = mode_list(lmax, nmax, K)
+    K = len(l)
+    phi, phr = phase_values(t, t_c, scale)
+    phase_knots = np.stack([phi, np.zeros_like(phi), phr])
+    phase_coeffs = phase_basis_from_knots(t, phase_knots)
+
+    a = (rng.standard_normal(K) + 1j * rng.standard_normal(K)) / np.sqrt(2.0)
+    a *= np.exp(-np.abs(n) / 4.0) / (l.astype(np.float64) ** 2)
+    omega = rng.uniform(0.0, 1e-6, K)
+    teuk = a[None, :] * (1.0 + 0.5 * t[:, None] / scale) * np.exp(1j * omega[None, :] * t[:, None])
+
+    # one (+m, -m) harmonic pair per (l, m)
+    lm_keys = sorted(set(zip(l.tolist(), m.tolist())))
+    yp = {}
+    for key in lm_keys:
+        z = (rng.standard_normal(4)) / np.sqrt(2.0)
+        yp[key] = (z[0] + 1j * z[1], z[2] + 1j * z[3])
+    ylms = np.empty(2 * K, dtype=np.complex128)
+    for j in range(K):
+        p, q = yp[(int(l[j]), int(m[j]))]
+        ylms[j] = p
+        ylms[K + j] = q
+
+    T = (span + dt) / YRSID_SI
+    return ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
+                         phase_coeffs=phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=T,
+                         phase_knots=phase_knots, name=name, seed=seed)
+
+
+def plain_small(seed: int = 1) -> ModeSumInputs:
+    """K=200, N=100 on [0, 1e6] s, t_c=1.2e6 s, S=1e6 s, dt=10 s, 100,001 samples."""
+    return make_inputs(K=200, N=100, span=1e6, t_c=1.2e6, lmax=4, nmax=10, seed=seed,
+                       scale=1e6, name="plain_small", min_gap=1e3)
+
+
+def plain_full(seed: int = 2) -> ModeSumInputs:
+    """K=3843, N=1000 on [0, 3.15e7] s, t_c=3.2e7 s, S=span, dt=10 s, 3,150,001 samples."""
+    return make_inputs(K=3843, N=1000, span=3.15e7, t_c=3.2e7, lmax=10, nmax=30, seed=seed,
+                       name="plain_full")
+
+
+def adjoint_case(seed: int = 4) -> ModeSumInputs:
+    """K=1000 (prefix of the full list), N=500, 1,000,000 samples (span 1e7 s)."""
+    return make_inputs(K=1000, N=500, span=1e7 - 10.0, t_c=1.1e7, lmax=10, nmax=30, seed=seed,
+                       name="adjoint")
+
+
+def batch_cases(count: int = 256, seed: int = 5):
+    """Waveforms with T ~ logU[1e5, 3.15e6] samples, N ~ U[50, 2000], K ~ U[200, 3843]
+    (prefixes of the full mode list), independent seeds."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for w in range(count):
+        T_samples = int(np.exp(rng.uniform(np.log(1e5), np.log(3.15e6))))
+        N = int(rng.integers(50, 2001))
+        K = int(rng.integers(200, 3844))
+        span = (T_samples - 1) * 10.0
+        out.append(make_inputs(K=K, N=N, span=span, t_c=span * 1.02, lmax=10, nmax=30,
+                               seed=int(rng.integers(1 << 31)), name=f"batch{w}"))
+    return out
+
+
+def small_case(K: int = 10, N: int = 20, out_len: int = 4000, seed: int = 7, dt: float = 10.0,
+               theta: bool = True, high_order: bool = True) -> ModeSumInputs:
+    """A small case in the style of the reference's own summation test
+    (tests/test_mode_summation.py:64-151): random m in [2,4], k in {0,1},
+    n in [-4,3], arbitrary 8-term phase polynomials (all coefficients set,
+    Phi_theta included), linear-ramp amplitudes."""
+    rng = np.random.default_rng(seed)
+    span = (out_len - 1) * dt
+    t = knot_times(rng, N, span, 0.2 * span / (N - 1))
+    l = rng.integers(2, 5, K).astype(np.int32)
+    m = rng.integers(2, 5, K).astype(np.int32)
+    k = (rng.integers(0, 2, K) if theta else np.zeros(K)).astype(np.int32)
+    n = rng.integers(-4, 4, K).astype(np.int32)
+    # phase polynomials: smooth growth plus small high-order terms
+    phase_coeffs = np.zeros((N - 1, 3, 8))
+    rates = np.array([2e-3, 1.3e-3, 0.9e-3]) * 2 * np.pi
+    for q in range(3):
+        base = rates[q] * t
+        h = np.diff(t)
+        phase_coeffs[:, q, 0] = base[:-1]
+        phase_coeffs[:, q, 1] = rates[q] * h
+        if high_order:
+            phase_coeffs[:, q, 2:] = rng.normal(0, 1e-3, (N - 1, 6))
+    if not theta:
+        phase_coeffs[:, 1, :] = 0.0
+    lo = rng.uniform(-1, 1, (2, K))
+    hi = rng.uniform(-1, 1, (2, K))
+    frac = (t / span)[:, None]
+    teuk = (lo[0] + (hi[0] - lo[0]) * frac) + 1j * (lo[1] + (hi[1] - lo[1]) * frac)
+    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    T = (span + dt) / YRSID_SI
+    return ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
+                         phase_coeffs=phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=T,
+                         name="small", seed=seed)

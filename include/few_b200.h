@@ -1,0 +1,189 @@
+/*
+ * few_b200.h -- C ABI of the B200-native interpolated mode sum
+ * (libfew_b200.so, built from fastemriwaveforms_b200/csrc).
+ *
+ * The reference reaches its native code through a Cython pointer shim
+ * (src/few/cutils/pyinterp.pyx:25-61) that passes raw addresses to
+ * interpolate_arrays and get_waveform (src/few/cutils/interpolate.hh:27-31).
+ * This header is the replacement boundary: plain pointers and sizes, no
+ * Python or torch types.  Differences from the reference's functions:
+ *   - every entry point returns an int status (FEW_OK or a negative FEW_ERR_*)
+ *     instead of calling exit() on a CUDA error (global.h:49-57);
+ *     few_last_error() gives the message of the last failure on this thread;
+ *   - every device entry point takes the CUDA stream to run on (void *, a
+ *     cudaStream_t; NULL is the legacy default stream) and returns without
+ *     synchronising, unless its comment says otherwise;
+ *   - pointers marked [device] are device memory, [host] host memory.
+ * Complex arrays are interleaved (re, im) double pairs, i.e. complex128.
+ */
+#ifndef FEW_B200_H
+#define FEW_B200_H
+
+#if defined(__GNUC__)
+#define FEW_API __attribute__((visibility("default")))
+#else
+#define FEW_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEW_OK 0
+#define FEW_ERR_ARG (-1)      /* null pointer or invalid argument value          */
+#define FEW_ERR_SIZE (-2)     /* size out of the supported range                 */
+#define FEW_ERR_CUDA (-3)     /* a CUDA runtime call failed                      */
+#define FEW_ERR_KNOTS (-4)    /* knots unusable (see the function's comment)     */
+#define FEW_ERR_NOMEM (-5)    /* host or device allocation failed                */
+
+/* Sum precision modes (few_sum_folded `mode`). */
+#define FEW_SUM_FAITHFUL 0 /* FP64; replays the reference's rounding of m*Phi_phi+k*Phi_theta+n*Phi_r */
+#define FEW_SUM_EXACT 1    /* FP64; mode phasors by recurrence, the combined phase never rounded     */
+
+/* Coefficient layouts of few_spline_build. */
+#define FEW_LAYOUT_KNOT_MAJOR 0   /* (4, length, ninterps): CubicSplineInterpolant.interp_array */
+#define FEW_LAYOUT_INTERP_MAJOR 1 /* (4, ninterps, length): interpolate_arrays' in-place layout */
+
+/* Message of the last failed call on the calling thread ("" if none). */
+FEW_API const char *few_last_error(void);
+
+/* ABI version, bumped on any signature change. */
+FEW_API int few_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Reference-shaped entry points                                            */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces interpolate_arrays (src/few/cutils/interpolate.hh:27,
+ * interpolate.cu:284-325): not-a-knot cubic splines of `ninterps` series.
+ * t_arr [device] (ninterps*length): knots, one row per interpolant.
+ * interp_array [device] (4, ninterps, length): row 0 holds y on entry; rows
+ * 1..3 receive c1, c2, c3 (and row 0 is rewritten with the same y).
+ * B, upper_diag, diag, lower_diag [device]: the reference's caller scratch;
+ * accepted for signature compatibility and not touched.
+ * Requires length >= 4 (the reference reads out of bounds at length 2 and its
+ * system is singular at length 3); knots strictly increasing. */
+FEW_API int few_interpolate_arrays(const double *t_arr, double *interp_array, int ninterps, int length,
+                           double *B, double *upper_diag, double *diag, double *lower_diag,
+                           void *stream);
+
+/* Replaces get_waveform (src/few/cutils/interpolate.hh:29-31,
+ * interpolate.cu:726-797): accumulates the interpolated mode sum into
+ * d_waveform.
+ * d_waveform [device] (out_len,) complex: h[i] += sum over modes (caller zeroes).
+ * interp_array [device] (4, init_len, 2K): CubicSplineInterpolant.interp_array.
+ * phase_interp_t [host] (init_len,); h_t [host] (init_len,): knot times, read
+ * on the host as in the reference.
+ * phase_interp_coeffs [device] (8, init_len-1, 3) flat.
+ * d_m, d_k, d_n [device] (K,) int32; d_Ylms [device] (2K,) complex, the -m
+ * half already multiplied by (-1)^l.  dev: the CUDA device to use.
+ * This entry point copies m, k, n to the host and synchronises `stream`
+ * before it returns (the reference synchronises after every launch).
+ * Uses FEW_SUM_FAITHFUL.  FEW_ERR_KNOTS when no knot reaches the last
+ * output sample (undefined in the reference). */
+FEW_API int few_get_waveform(void *d_waveform, const double *interp_array, const double *phase_interp_t,
+                     const double *phase_interp_coeffs, const int *d_m, const int *d_k,
+                     const int *d_n, int init_len, int out_len, int num_teuk_modes,
+                     const void *d_Ylms, double delta_t, const double *h_t, int dev, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Spline build and evaluation (CubicSplineInterpolant)                     */
+/* ------------------------------------------------------------------------ */
+
+/* Not-a-knot cubic splines of ninterps series of `length` knots
+ * (CubicSplineInterpolant.__init__, src/few/summation/interpolatedmodesum.py:35-107).
+ * t [device]: knots; interpolant p uses t + p*t_row_stride (0 = shared knots).
+ * y [device]: value i of interpolant p is
+ *     y[i*y_knot_stride + p*y_interp_stride]                         for p <  y_split,
+ *     y[y_split_offset + i*y_knot_stride + (p-y_split)*y_interp_stride] for p >= y_split
+ *   (a (ninterps, length) array: strides (1, length), y_split = ninterps; the
+ *   real/imaginary halves of a (length, K) complex array: strides (2K, 2),
+ *   y_split = K, y_split_offset = 1).
+ * coeffs [device]: (4, ...) in `layout`; must not overlap y.
+ * Requires length >= 4; knots strictly increasing. */
+FEW_API int few_spline_build(const double *t, long long t_row_stride, const double *y, long long y_knot_stride,
+                     long long y_interp_stride, int y_split, long long y_split_offset, int ninterps,
+                     int length, double *coeffs, int layout, void *stream);
+
+/* Spline evaluation (CubicSplineInterpolant.__call__, interpolatedmodesum.py:161-257).
+ * t [device]: knots, interpolant p uses t + p*t_row_stride (0 = shared).
+ * coeffs [device] (4, length, ninterps).  tnew [device]: point j of
+ * interpolant p is tnew[p*tnew_row_stride + j] (0 = shared points).
+ * out [device] (ninterps, M).  flags [device] int[2]: flags[0] is set to 1 if
+ * any point lies left of the first knot, flags[1] if right of the last
+ * (deriv_order 0 fills those with the edge values; the caller raises for
+ * derivatives, as the reference does).  deriv_order 0..3. */
+FEW_API int few_spline_eval(const double *t, long long t_row_stride, const double *coeffs, int ninterps,
+                    int length, const double *tnew, long long tnew_row_stride, int M, int deriv_order,
+                    double *out, int *flags, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Host planners (pure host code, no GPU)                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Fold plan of the mode list.  Term (+) of mode j has phase key
+ * (m_j, k_j, n_j); term (-) (m_j != 0) has key (-m_j, -k_j, -n_j).  Keys are
+ * laid on a dense grid: rows = distinct (m', k') pairs sorted ascending,
+ * columns n' = nlo .. nlo+NN-1.
+ * Outputs: row_m, row_k [host] (max_rows,): the rows; dims [host] int[3] =
+ * {R, nlo, NN}; key_ptr [host] (max_rows*NN_max+1 -- pass max_keys+1 entries)
+ * and key_list [host] (2K,): contributors of key q are
+ * key_list[key_ptr[q] .. key_ptr[q+1]), each 2*j (+ term) or 2*j+1 (- term),
+ * in mode order.  FEW_ERR_SIZE if R > max_rows or R*NN > max_keys. */
+FEW_API int few_fold_plan(const int *m, const int *k, const int *n, int K, int max_rows, int max_keys,
+                  int *row_m, int *row_k, int *dims, int *key_ptr, int *key_list);
+
+/* Segment plan (find_start_inds, interpolate.cu:694-723) and work units.
+ * h_t, phase_t [host] (init_len,).  Segment j owns output samples
+ * [seg_start[j], seg_start[j+1]).  seg_start [host] (init_len,);
+ * seg_info [host] (3*(init_len-1),): per segment {h_t[j], phase_t[j],
+ * phase_t[j+1]-phase_t[j]}; units [host] (3*max_units,): {segment, first
+ * sample, end sample} for runs of at most `chunk` samples; counts [host]
+ * int[2] = {segments used, units}.  FEW_ERR_KNOTS when no knot reaches the
+ * last output sample; FEW_ERR_SIZE when max_units is too small
+ * (init_len + out_len/chunk + 1 always suffices). */
+FEW_API int few_segment_plan(const double *h_t, const double *phase_t, int init_len, int out_len, double dt,
+                     int chunk, int max_units, int *seg_start, double *seg_info, int *units,
+                     int *counts);
+
+/* ------------------------------------------------------------------------ */
+/* Mode-sum kernels                                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Folds the amplitude splines over the modes sharing a phase key, per segment:
+ * W[s][r][c'][c] = sum over contributors of Y+_j a_c(j)  (+ term)
+ *                                       or Y-_j conj(a_c(j)) (- term),
+ * a_c(j) = coeffs[c][s][j] + i coeffs[c][s][K+j] (spline coefficient c of
+ * mode j at knot s).  coeffs [device] (4, N, 2K); ylms [device] (2K,) complex
+ * (-m half times (-1)^l); key_ptr, key_list [device] from few_fold_plan;
+ * W [device] (nseg, R, NN, 4) complex. */
+FEW_API int few_fold_coeffs(const double *coeffs, const void *ylms, const int *key_ptr, const int *key_list,
+                    int K, int N, int nseg, int R, int NN, void *W, void *stream);
+
+/* Accumulates the folded sum into wf [device] (out_len,) complex:
+ * wf[i] += sum_{r,c'} (sum_c x^c W[s][r][c'][c]) exp(-i phase_{r,c'}(t_i)),
+ * t_i = i*dt, x = t_i - seg_info[s].t0, phases from the 8-term polynomials
+ * phase_coeffs [device] (8, N-1, 3) at s = (t_i - pt0)/pw.
+ * seg_info [device] (3*(N-1),), units [device] (3*nunits,) from
+ * few_segment_plan; row_m, row_k [device] (R,); nlo, NN: the n' grid.
+ * mode: FEW_SUM_FAITHFUL or FEW_SUM_EXACT.  use_theta: nonzero if any row
+ * has k' != 0 (Phi_theta is then evaluated). */
+FEW_API int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, int N, const double *seg_info,
+                   const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo,
+                   int NN, double dt, int mode, int use_theta, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Measurement                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* FP64 FMA throughput probe (no counterpart in the reference): `blocks` CTAs
+ * of 256 threads, each thread 8 independent FMA chains of `iters` steps,
+ * 16*iters flops per thread.  out [device] (blocks*256,) receives the chain
+ * sums.  Used to measure the FP64 pipe peak that bounds the sum kernels. */
+FEW_API int few_probe_fp64_fma(double *out, int blocks, int iters, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEW_B200_H */

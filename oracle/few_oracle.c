@@ -1,0 +1,332 @@
+/*
+ * few_oracle.c -- CPU restatement of the FastEMRIWaveforms time-domain
+ * interpolated mode sum.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is checked
+ * against.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg may load it; the product path (fastemriwaveforms_b200) never does.
+ *
+ * Parity pin: the restatement is checked against the reference itself, built
+ * from its own sources by oracle/Makefile into oracle/_ref, and against the
+ * golden vectors under tests/golden (made by tests/golden/make_golden.py from
+ * that build) plus scipy.interpolate.CubicSpline for the spline build.
+ *
+ * Reference functions restated (paths inside the FastEMRIWaveforms project):
+ *   src/few/cutils/interpolate.cu:29-43    fill_coefficients
+ *   src/few/cutils/interpolate.cu:48-102   prep_splines (not-a-knot rows)
+ *   src/few/cutils/interpolate.cu:201-239  fit_wrap (CPU branch: LAPACK dgtsv)
+ *   src/few/cutils/interpolate.cu:241-280  fill_final_derivs
+ *   src/few/cutils/interpolate.cu:284-325  interpolate_arrays
+ *   src/few/cutils/interpolate.cu:444-689  make_waveform (CPU branch)
+ *   src/few/cutils/interpolate.cu:694-723  find_start_inds
+ *   src/few/cutils/interpolate.cu:726-797  get_waveform
+ *
+ * Build with -ffp-contract=off: every a*b+c in the reference source is two
+ * rounded operations here, in the order the source writes them.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------- */
+/* Spline build                                                              */
+/* ------------------------------------------------------------------------- */
+
+/* Not-a-knot row i of the slope system for one interpolant
+ * (interpolate.cu:48-102).  Row i reads lower*s[i-1] + diag*s[i] + upper*s[i+1]. */
+static void oracle_row(int i, int n, const double *x, const double *y,
+                       double *b, double *ud, double *dg, double *ld)
+{
+    double dx1, dx2, d, slope1, slope2;
+    if (i == n - 1) {
+        dx1 = x[n - 2] - x[n - 3];
+        dx2 = x[n - 1] - x[n - 2];
+        d = x[n - 1] - x[n - 3];
+        slope1 = (y[n - 2] - y[n - 3]) / dx1;
+        slope2 = (y[n - 1] - y[n - 2]) / dx2;
+        b[i] = ((dx2 * dx2 * slope1 + (2 * d + dx2) * dx1 * slope2) / d);
+        dg[i] = dx1;
+        ld[i] = d;
+        ud[i] = 0.0;
+    } else if (i == 0) {
+        dx1 = x[1] - x[0];
+        dx2 = x[2] - x[1];
+        d = x[2] - x[0];
+        slope1 = (y[1] - y[0]) / dx1;
+        slope2 = (y[2] - y[1]) / dx2;
+        b[0] = ((dx1 + 2 * d) * dx2 * slope1 + dx1 * dx1 * slope2) / d;
+        dg[0] = dx2;
+        ud[0] = d;
+        ld[0] = 0.0;
+    } else {
+        dx1 = x[i] - x[i - 1];
+        dx2 = x[i + 1] - x[i];
+        slope1 = (y[i] - y[i - 1]) / dx1;
+        slope2 = (y[i + 1] - y[i]) / dx2;
+        b[i] = 3.0 * (dx2 * slope1 + dx1 * slope2);
+        dg[i] = 2 * (dx1 + dx2);
+        ud[i] = dx1;
+        ld[i] = dx2;
+    }
+}
+
+/* Tridiagonal solve by Gaussian elimination with partial (row) pivoting, the
+ * published algorithm of LAPACK xGTSV that fit_wrap calls on the CPU
+ * (interpolate.cu:231-236).  sub[i] = A[i+1][i] (n-1 entries), dg[i] = A[i][i],
+ * sup[i] = A[i][i+1] (n-1 entries).  A row swap moves a second superdiagonal
+ * entry into sup2.  b is overwritten with the solution.  Returns 0, or i+1 when
+ * pivot i is exactly zero. */
+static int oracle_gtsv(int n, double *sub, double *dg, double *sup, double *b, double *sup2)
+{
+    for (int i = 0; i < n - 1; ++i) {
+        if (fabs(dg[i]) >= fabs(sub[i])) {
+            if (dg[i] == 0.0) return i + 1;
+            double f = sub[i] / dg[i];
+            dg[i + 1] = dg[i + 1] - f * sup[i];
+            b[i + 1] = b[i + 1] - f * b[i];
+            sup2[i] = 0.0;
+        } else {
+            /* the next row becomes the pivot row */
+            double f = dg[i] / sub[i];
+            double old_d1 = dg[i + 1];
+            double old_u1 = (i < n - 2) ? sup[i + 1] : 0.0;
+            dg[i] = sub[i];
+            dg[i + 1] = sup[i] - f * old_d1;
+            sup[i] = old_d1;
+            sup2[i] = old_u1;
+            if (i < n - 2) sup[i + 1] = -f * old_u1;
+            double bi = b[i];
+            b[i] = b[i + 1];
+            b[i + 1] = bi - f * b[i];
+        }
+    }
+    if (dg[n - 1] == 0.0) return n;
+    b[n - 1] = b[n - 1] / dg[n - 1];
+    if (n > 1) b[n - 2] = (b[n - 2] - sup[n - 2] * b[n - 1]) / dg[n - 2];
+    for (int i = n - 3; i >= 0; --i)
+        b[i] = (b[i] - sup[i] * b[i + 1] - sup2[i] * b[i + 2]) / dg[i];
+    return 0;
+}
+
+/* interpolate_arrays (interpolate.cu:284-325), CPU branch.
+ * t_arr: (ninterps, length) knots, one row per interpolant.
+ * interp_array: (4, ninterps, length); row 0 holds y on entry, rows 1..3
+ * receive c1, c2, c3.  B/upper/diag/lower: (ninterps*length) scratch, as in
+ * the reference.  Returns 0, or a negative code on bad sizes, or the first
+ * failing pivot of the first singular system. */
+int oracle_interpolate_arrays(const double *t_arr, double *interp_array, int ninterps, int length,
+                              double *B, double *upper_diag, double *diag, double *lower_diag)
+{
+    if (ninterps < 1 || length < 3) return -1;
+    double *sup2 = (double *)malloc(sizeof(double) * (size_t)length);
+    if (!sup2) return -2;
+    const size_t plane = (size_t)ninterps * (size_t)length;
+    int status = 0;
+    for (int p = 0; p < ninterps; ++p) {
+        const size_t lead = (size_t)p * (size_t)length;
+        const double *x = t_arr + lead;
+        double *y = interp_array + lead;
+        for (int i = 0; i < length; ++i)
+            oracle_row(i, length, x, y, B + lead, upper_diag + lead, diag + lead, lower_diag + lead);
+        /* fit_wrap passes dl = &lower[j*m+1]: sub-diagonal entry i is row i+1's lower coefficient */
+        int info = oracle_gtsv(length, lower_diag + lead + 1, diag + lead, upper_diag + lead, B + lead, sup2);
+        if (info != 0 && status == 0) status = info;
+        double *c1 = interp_array + plane + lead;
+        double *c2 = interp_array + 2 * plane + lead;
+        double *c3 = interp_array + 3 * plane + lead;
+        const double *dydx = B + lead;
+        /* fill_coefficients (interpolate.cu:29-43) */
+        for (int i = 0; i < length - 1; ++i) {
+            double dx = x[i + 1] - x[i];
+            double slope = (y[i + 1] - y[i]) / dx;
+            double dydx_i = dydx[i];
+            double tt = (dydx_i + dydx[i + 1] - 2 * slope) / dx;
+            c1[i] = dydx_i;
+            c2[i] = (slope - dydx_i) / dx - tt;
+            c3[i] = tt / dx;
+        }
+        /* fill_final_derivs (interpolate.cu:241-280) */
+        {
+            double a1 = c1[length - 2], a2 = c2[length - 2], a3 = c3[length - 2];
+            double xx = x[length - 1] - x[length - 2];
+            double x2 = xx * xx;
+            c1[length - 1] = a1 + 2 * a2 * xx + 3 * a3 * x2;
+            c2[length - 1] = (2. * a2 + 6. * a3 * xx) / 2.;
+            c3[length - 1] = a3;
+        }
+    }
+    free(sup2);
+    return status;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Mode sum                                                                  */
+/* ------------------------------------------------------------------------- */
+
+/* find_start_inds (interpolate.cu:694-723).  Segment j owns output samples
+ * [start[j], start[j+1]).  Returns the number of usable segments, or -1 when
+ * no knot reaches the end of the output (a case the reference leaves
+ * undefined; this restatement refuses it). */
+int oracle_find_start_inds(int *start, const double *h_t, double dt, int length, int out_len)
+{
+    double T = (out_len - 1) * dt;
+    start[0] = 0;
+    for (int i = 1; i < length; ++i) {
+        double t = h_t[i];
+        if (t < T) {
+            start[i] = (int)ceil(t / dt);
+        } else {
+            start[i] = out_len;
+            return i; /* segments 0..i-1 */
+        }
+    }
+    return -1;
+}
+
+/* The sum body of make_waveform (interpolate.cu:618-686) for the samples
+ * [i_lo, i_hi) of segment `seg`, double precision, operation order as written
+ * in the reference.  wf: interleaved complex, absolute sample index. */
+static void oracle_segment_f64(double *wf, const double *interp, const double *pc,
+                               const int *m_arr, const int *k_arr, const int *n_arr, int K,
+                               const double *ylm, double dt, double start_t, int seg,
+                               int i_lo, int i_hi, int init_len, double pt0, double pwidth)
+{
+    const size_t num_base = (size_t)init_len * (size_t)(2 * K);
+    const size_t nps = (size_t)(init_len - 1) * 3;
+    double pp[8], pt[8], pr[8];
+    for (int c = 0; c < 8; ++c) {
+        pp[c] = pc[c * nps + (size_t)seg * 3 + 0];
+        pt[c] = pc[c * nps + (size_t)seg * 3 + 1];
+        pr[c] = pc[c * nps + (size_t)seg * 3 + 2];
+    }
+    const double *cr[4], *ci[4];
+    for (int c = 0; c < 4; ++c) {
+        cr[c] = interp + c * num_base + (size_t)seg * (2 * K);
+        ci[c] = cr[c] + K;
+    }
+    for (int i = i_lo; i < i_hi; ++i) {
+        double t = dt * i;
+        double x = t - start_t;
+        double x2 = x * x;
+        double x3 = x * x2;
+        double s = (t - pt0) / pwidth;
+        double s1 = 1.0 - s;
+        double Pp = pp[0] + s * (pp[1] + s1 * (pp[2] + s * (pp[3] + s1 * (pp[4] + s * (pp[5] + s1 * (pp[6] + s * pp[7]))))));
+        double Pt = pt[0] + s * (pt[1] + s1 * (pt[2] + s * (pt[3] + s1 * (pt[4] + s * (pt[5] + s1 * (pt[6] + s * pt[7]))))));
+        double Pr = pr[0] + s * (pr[1] + s1 * (pr[2] + s * (pr[3] + s1 * (pr[4] + s * (pr[5] + s1 * (pr[6] + s * pr[7]))))));
+        double tr = 0.0, ti = 0.0;
+        for (int j = 0; j < K; ++j) {
+            int m = m_arr[j], k = k_arr[j], n = n_arr[j];
+            double phase = m * Pp + k * Pt + n * Pr;
+            double ang = -phase;                 /* imag part of -i*phase */
+            double er = cos(ang), ei = sin(ang); /* exp(0 + i*ang) */
+            double re = cr[0][j] + cr[1][j] * x + cr[2][j] * x2 + cr[3][j] * x3;
+            double im = ci[0][j] + ci[1][j] * x + ci[2][j] * x2 + ci[3][j] * x3;
+            double qr = er * re - ei * im;       /* exp * amplitude */
+            double qi = er * im + ei * re;
+            double ypr = ylm[2 * j], ypi = ylm[2 * j + 1];
+            double tpr = qr * ypr - qi * ypi;
+            double tpi = qr * ypi + qi * ypr;
+            double tmr = 0.0, tmi = 0.0;
+            if (m != 0) {
+                double ymr = ylm[2 * (K + j)], ymi = ylm[2 * (K + j) + 1];
+                double nqi = -qi;                /* conj(partial_mode) */
+                tmr = qr * ymr - nqi * ymi;
+                tmi = qr * ymi + nqi * ymr;
+            }
+            tr = tr + tmr + tpr;
+            ti = ti + tmi + tpi;
+        }
+        wf[2 * (size_t)i] += tr;
+        wf[2 * (size_t)i + 1] += ti;
+    }
+}
+
+/* The same sum in 80-bit extended arithmetic after the phase polynomials:
+ * Phi is evaluated exactly as the reference does (double), then the mode phase
+ * m*Phi_phi + k*Phi_theta + n*Phi_r, its sine/cosine, the amplitude and the
+ * products are formed in long double.  This is the accuracy reference for the
+ * recurrence form, which does not round the combined mode phase. */
+static void oracle_segment_ext(double *wf, const double *interp, const double *pc,
+                               const int *m_arr, const int *k_arr, const int *n_arr, int K,
+                               const double *ylm, double dt, double start_t, int seg,
+                               int i_lo, int i_hi, int init_len, double pt0, double pwidth)
+{
+    const size_t num_base = (size_t)init_len * (size_t)(2 * K);
+    const size_t nps = (size_t)(init_len - 1) * 3;
+    double pp[8], pt[8], pr[8];
+    for (int c = 0; c < 8; ++c) {
+        pp[c] = pc[c * nps + (size_t)seg * 3 + 0];
+        pt[c] = pc[c * nps + (size_t)seg * 3 + 1];
+        pr[c] = pc[c * nps + (size_t)seg * 3 + 2];
+    }
+    const double *cr[4], *ci[4];
+    for (int c = 0; c < 4; ++c) {
+        cr[c] = interp + c * num_base + (size_t)seg * (2 * K);
+        ci[c] = cr[c] + K;
+    }
+    for (int i = i_lo; i < i_hi; ++i) {
+        double t = dt * i;
+        double x = t - start_t;
+        double s = (t - pt0) / pwidth;
+        double s1 = 1.0 - s;
+        double Pp = pp[0] + s * (pp[1] + s1 * (pp[2] + s * (pp[3] + s1 * (pp[4] + s * (pp[5] + s1 * (pp[6] + s * pp[7]))))));
+        double Pt = pt[0] + s * (pt[1] + s1 * (pt[2] + s * (pt[3] + s1 * (pt[4] + s * (pt[5] + s1 * (pt[6] + s * pt[7]))))));
+        double Pr = pr[0] + s * (pr[1] + s1 * (pr[2] + s * (pr[3] + s1 * (pr[4] + s * (pr[5] + s1 * (pr[6] + s * pr[7]))))));
+        long double X = x;
+        long double tr = 0.0L, ti = 0.0L;
+        for (int j = 0; j < K; ++j) {
+            int m = m_arr[j], k = k_arr[j], n = n_arr[j];
+            long double phase = (long double)m * Pp + (long double)k * Pt + (long double)n * Pr;
+            long double er = cosl(phase), ei = -sinl(phase);
+            long double re = ((cr[3][j] * X + cr[2][j]) * X + cr[1][j]) * X + cr[0][j];
+            long double im = ((ci[3][j] * X + ci[2][j]) * X + ci[1][j]) * X + ci[0][j];
+            long double qr = er * re - ei * im;
+            long double qi = er * im + ei * re;
+            long double ypr = ylm[2 * j], ypi = ylm[2 * j + 1];
+            tr += qr * ypr - qi * ypi;
+            ti += qr * ypi + qi * ypr;
+            if (m != 0) {
+                long double ymr = ylm[2 * (K + j)], ymi = ylm[2 * (K + j) + 1];
+                tr += qr * ymr + qi * ymi;
+                ti += qr * ymi - qi * ymr;
+            }
+        }
+        wf[2 * (size_t)i] += (double)tr;
+        wf[2 * (size_t)i + 1] += (double)ti;
+    }
+}
+
+/* get_waveform (interpolate.cu:726-797), CPU branch, restricted to the output
+ * samples [s_lo, s_hi) (pass 0 and out_len for the whole waveform).
+ * wf: (out_len,) complex128 as interleaved doubles, accumulated with +=.
+ * interp_array: (4, init_len, 2K); phase_coeffs: (8, init_len-1, 3);
+ * ylm: (2K,) complex with the -m half already multiplied by (-1)^l.
+ * extended = 0: double precision in the reference's operation order;
+ * extended = 1: the long double restatement above.
+ * Returns 0, or a negative code when the knots do not reach the output end. */
+int oracle_get_waveform(double *wf, const double *interp_array, const double *phase_interp_t,
+                        const double *phase_interp_coeffs, const int *m_arr, const int *k_arr,
+                        const int *n_arr, int init_len, int out_len, int K, const double *ylm,
+                        double dt, const double *h_t, int s_lo, int s_hi, int extended)
+{
+    if (init_len < 2 || out_len < 1 || K < 1) return -1;
+    int *start = (int *)malloc(sizeof(int) * (size_t)init_len);
+    if (!start) return -2;
+    int nseg = oracle_find_start_inds(start, h_t, dt, init_len, out_len);
+    if (nseg < 0) { free(start); return -3; }
+    for (int j = 0; j < nseg; ++j) {
+        int a = start[j] > s_lo ? start[j] : s_lo;
+        int b = start[j + 1] < s_hi ? start[j + 1] : s_hi;
+        if (a >= b) continue;
+        double pt0 = phase_interp_t[j], pw = phase_interp_t[j + 1] - phase_interp_t[j];
+        if (extended)
+            oracle_segment_ext(wf, interp_array, phase_interp_coeffs, m_arr, k_arr, n_arr, K, ylm,
+                               dt, h_t[j], j, a, b, init_len, pt0, pw);
+        else
+            oracle_segment_f64(wf, interp_array, phase_interp_coeffs, m_arr, k_arr, n_arr, K, ylm,
+                               dt, h_t[j], j, a, b, init_len, pt0, pw);
+    }
+    free(start);
+    return 0;
+}

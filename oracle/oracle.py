@@ -1,0 +1,261 @@
+"""ctypes front end for the oracle (test infrastructure only).
+
+Two CPU implementations of the reference's time-domain interpolated mode sum:
+
+* ``impl="oracle"`` -- ``few_oracle.c``, the C restatement in this folder;
+* ``impl="ref"``    -- the reference's own CPU path
+  (``src/few/cutils/interpolate.cu`` compiled as C++ by ``make -C oracle ref``
+  into ``oracle/_ref``; present only where the reference sources were).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker.  The product package never imports it.
+
+The host-side preprocessing mirrors ``InterpolatedModeSum.sum``
+(``src/few/summation/interpolatedmodesum.py:331-375``) and
+``CubicSplineInterpolant.__init__`` (``interpolatedmodesum.py:35-107``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
+LIB_REF = os.path.join(HERE, "_ref", "libfew_ref.so")
+REFERENCE_ROOT = "/root/reference"
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_libs: dict = {}
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile the C restatement, and the reference's CPU path when its
+    sources are present (``ref=None``: only if they exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref is None:
+        ref = os.path.isfile(os.path.join(REFERENCE_ROOT, "src/few/cutils/interpolate.cu"))
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_ROOT}"], check=True)
+
+
+def have_ref() -> bool:
+    return os.path.isfile(LIB_REF)
+
+
+def _lib(impl: str):
+    if impl in _libs:
+        return _libs[impl]
+    if impl == "oracle":
+        if not os.path.isfile(LIB_ORACLE):
+            build(ref=False)
+        lib = ctypes.CDLL(LIB_ORACLE)
+        lib.oracle_interpolate_arrays.restype = ctypes.c_int
+        lib.oracle_interpolate_arrays.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]
+        lib.oracle_get_waveform.restype = ctypes.c_int
+        lib.oracle_get_waveform.argtypes = [_dp, _dp, _dp, _dp, _ip, _ip, _ip, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _dp, ctypes.c_double, _dp, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int]
+        lib.oracle_find_start_inds.restype = ctypes.c_int
+        lib.oracle_find_start_inds.argtypes = [_ip, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    elif impl == "ref":
+        if not os.path.isfile(LIB_REF):
+            raise FileNotFoundError("reference CPU build missing: make -C oracle ref")
+        lib = ctypes.CDLL(LIB_REF)
+        lib.few_ref_interpolate_arrays.restype = None
+        lib.few_ref_interpolate_arrays.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]
+        lib.few_ref_get_waveform.restype = None
+        lib.few_ref_get_waveform.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _ip, _ip, _ip, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
+                                             _dp, ctypes.c_int]
+    else:
+        raise ValueError(impl)
+    _libs[impl] = lib
+    return lib
+
+
+def _p(a, typ=_dp):
+    return a.ctypes.data_as(typ)
+
+
+def interpolate_arrays(t, y_all, impl: str = "oracle") -> np.ndarray:
+    """Spline coefficients in the reference's native layout (4, ninterps, N):
+    ``interpolate_arrays`` applied as ``CubicSplineInterpolant.__init__`` does
+    before its final transpose (``interpolatedmodesum.py:52-97``)."""
+    y_all = np.atleast_2d(np.asarray(y_all, dtype=np.float64))
+    ninterps, length = y_all.shape
+    t = np.asarray(t, dtype=np.float64)
+    if t.ndim == 1:
+        t_full = np.ascontiguousarray(np.tile(t, (ninterps, 1)).reshape(-1))
+    else:
+        t_full = np.ascontiguousarray(t.reshape(-1))
+    interp = np.zeros((4, ninterps, length))
+    interp[0] = y_all
+    interp = np.ascontiguousarray(interp.reshape(-1))
+    B = np.zeros(ninterps * length)
+    up, dg, lo = np.zeros_like(B), np.zeros_like(B), np.zeros_like(B)
+    lib = _lib(impl)
+    if impl == "oracle":
+        st = lib.oracle_interpolate_arrays(_p(t_full), _p(interp), ninterps, length, _p(B), _p(up), _p(dg), _p(lo))
+        if st != 0:
+            raise ValueError(f"oracle spline build failed with status {st}")
+    else:
+        lib.few_ref_interpolate_arrays(_p(t_full), _p(interp), ninterps, length, _p(B), _p(up), _p(dg), _p(lo))
+    return interp.reshape(4, ninterps, length)
+
+
+def spline_coeffs(t, y_all, impl: str = "oracle") -> np.ndarray:
+    """``CubicSplineInterpolant.interp_array`` reshaped to (4, N, ninterps)."""
+    return np.ascontiguousarray(np.transpose(interpolate_arrays(t, y_all, impl), (0, 2, 1)))
+
+
+def spline_eval(t, coeffs, tnew, deriv_order: int = 0) -> np.ndarray:
+    """``CubicSplineInterpolant.__call__`` (``interpolatedmodesum.py:118-257``)
+    for 1-D knots t and coefficients (4, N, ninterps) -> (ninterps, M)."""
+    t = np.asarray(t, dtype=np.float64)
+    tnew = np.atleast_1d(np.asarray(tnew, dtype=np.float64))
+    inds = np.searchsorted(t, tnew, side="right") - 1
+    inds[tnew == t[-1]] = len(t) - 2
+    bad_l = tnew < t[0]
+    bad_r = tnew > t[-1]
+    inds = np.clip(inds, 0, len(t) - 1)
+    x = tnew - t[inds]
+    y, c1, c2, c3 = (coeffs[c][inds].T for c in range(4))
+    if deriv_order == 0:
+        out = y + c1 * x + c2 * (x * x) + c3 * (x * x * x)
+        out[:, bad_l] = coeffs[0][0][:, None]
+        out[:, bad_r] = coeffs[0][-1][:, None]
+    else:
+        if bad_l.any() or bad_r.any():
+            raise ValueError("x points outside of the domain of the spline are not supported when taking derivatives.")
+        if deriv_order == 1:
+            out = c1 + 2 * c2 * x + 3 * c3 * (x * x)
+        elif deriv_order == 2:
+            out = 2 * c2 + 6 * c3 * x
+        elif deriv_order == 3:
+            out = 6 * c3 * np.ones_like(x)
+        else:
+            raise ValueError("deriv_order must be within 0 <= deriv_order <= 3.")
+    return out
+
+
+def prepare_sum(inp):
+    """The preprocessing of ``InterpolatedModeSum.sum``
+    (``interpolatedmodesum.py:321-358``): y_all = [Re; Im] of teuk_modes.T,
+    phase coefficients (N-1,3,8) -> flat (8,N-1,3), ylms[K:] *= (-1)^l."""
+    K = inp.teuk_modes.shape[1]
+    y_all = np.concatenate([inp.teuk_modes.T.real, inp.teuk_modes.T.imag], axis=0)
+    pc = np.ascontiguousarray(np.transpose(np.asarray(inp.phase_coeffs, dtype=np.float64), (2, 0, 1)).reshape(-1))
+    ylms = np.array(inp.ylms, dtype=np.complex128, copy=True)
+    ylms[K:] *= (-1.0) ** np.asarray(inp.l)
+    return y_all, pc, ylms
+
+
+def mode_sum(inp, impl: str = "oracle", extended: bool = False, window=None,
+             coeffs: np.ndarray | None = None, out_len: int | None = None) -> np.ndarray:
+    """The waveform of ``InterpolatedModeSum.__call__`` on the CPU.
+
+    impl="oracle": the C restatement (``extended`` selects the long double
+    form; ``window=(lo, hi)`` computes only those output samples, the rest
+    stay zero).  impl="ref": the reference's own get_waveform (whole output).
+    ``coeffs`` optionally supplies amplitude spline coefficients (4, N, 2K)."""
+    from fastemriwaveforms_b200.synthetic import output_length
+
+    K = inp.teuk_modes.shape[1]
+    N = len(inp.t)
+    if out_len is None:
+        out_len = output_length(inp.t, inp.T, inp.dt)[0]
+    y_all, pc, ylms = prepare_sum(inp)
+    if coeffs is None:
+        coeffs = spline_coeffs(inp.t, y_all, impl=impl)
+    interp = np.ascontiguousarray(coeffs.reshape(-1))
+    m = np.ascontiguousarray(inp.m, dtype=np.int32)
+    k = np.ascontiguousarray(inp.k, dtype=np.int32)
+    n = np.ascontiguousarray(inp.n, dtype=np.int32)
+    h_t = np.ascontiguousarray(inp.t, dtype=np.float64)
+    pt = np.ascontiguousarray(inp.phase_t, dtype=np.float64)
+    ylm_flat = np.ascontiguousarray(ylms).view(np.float64)
+    wf = np.zeros(out_len, dtype=np.complex128)
+    lib = _lib(impl)
+    if impl == "oracle":
+        lo, hi = (0, out_len) if window is None else window
+        st = lib.oracle_get_waveform(_p(wf.view(np.float64)), _p(interp), _p(pt), _p(pc), _p(m, _ip), _p(k, _ip),
+                                     _p(n, _ip), N, out_len, K, _p(ylm_flat), float(inp.dt), _p(h_t),
+                                     int(lo), int(hi), 1 if extended else 0)
+        if st != 0:
+            raise ValueError(f"oracle mode sum failed with status {st}")
+    else:
+        if window is not None or extended:
+            raise ValueError("the reference build computes the whole waveform in double precision")
+        lib.few_ref_get_waveform(wf.ctypes.data, _p(interp), _p(pt), _p(pc), _p(m, _ip), _p(k, _ip), _p(n, _ip),
+                                 N, out_len, K, ylm_flat.ctypes.data, float(inp.dt), _p(h_t), 0)
+    return wf
+
+
+def find_start_inds(t, dt: float, out_len: int):
+    """Segment starts of ``find_start_inds`` (``interpolate.cu:694-723``);
+    returns (start (nseg+1,), nseg)."""
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    start = np.zeros(len(t), dtype=np.int32)
+    nseg = _lib("oracle").oracle_find_start_inds(_p(start, _ip), _p(t), float(dt), len(t), int(out_len))
+    if nseg < 0:
+        raise ValueError("knots do not reach the end of the output")
+    return start[: nseg + 1], nseg
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def mismatch(a, b) -> float:
+    """1 - overlap, as ``get_mismatch`` (``src/few/utils/utility.py:16-95``)."""
+    fa = np.fft.fft(np.asarray(a))
+    fb = np.fft.fft(np.asarray(b))
+    ac = np.vdot(fa, fb) / np.sqrt(np.vdot(fa, fa) * np.vdot(fb, fb))
+    return float(1.0 - ac.real)
+
+
+def window_problem(inp, coeffs, j0: int, samples: int):
+    """Arguments of the reference's get_waveform for `samples` output samples
+    starting at the first sample of knot segment j0, as a problem of its own:
+    knots from j0 on, shifted by that sample's time so that it becomes sample
+    0, with the same spline and phase coefficients (sliced).  Used to spread a
+    CPU baseline over processes; the values differ from the whole-waveform call
+    only by the rounding of the shifted times."""
+    K = inp.teuk_modes.shape[1]
+    start = int(np.ceil(inp.t[j0] / inp.dt)) if j0 > 0 else 0
+    shift = start * inp.dt
+    t_sub = np.ascontiguousarray(inp.t[j0:] - shift)
+    pt_sub = np.ascontiguousarray(inp.phase_t[j0:] - shift)
+    c_sub = np.ascontiguousarray(coeffs[:, j0:, :])
+    _, pc, ylms = prepare_sum(inp)
+    N = len(inp.t)
+    pc_sub = np.ascontiguousarray(pc.reshape(8, N - 1, 3)[:, j0:, :].reshape(-1))
+    return dict(t=t_sub, phase_t=pt_sub, coeffs=c_sub, pc=pc_sub, ylms=ylms, K=K, out_len=int(samples),
+                m=np.ascontiguousarray(inp.m, dtype=np.int32), k=np.ascontiguousarray(inp.k, dtype=np.int32),
+                n=np.ascontiguousarray(inp.n, dtype=np.int32), dt=float(inp.dt))
+
+
+def run_window(prob, impl: str = "ref") -> np.ndarray:
+    """Runs a window_problem through the reference's get_waveform (or the
+    restatement) and returns its output."""
+    lib = _lib(impl)
+    wf = np.zeros(prob["out_len"], dtype=np.complex128)
+    N = len(prob["t"])
+    interp = prob["coeffs"].reshape(-1)
+    ylm = np.ascontiguousarray(prob["ylms"]).view(np.float64)
+    args = (_p(interp), _p(prob["phase_t"]), _p(prob["pc"]), _p(prob["m"], _ip), _p(prob["k"], _ip),
+            _p(prob["n"], _ip), N, prob["out_len"], prob["K"])
+    if impl == "ref":
+        lib.few_ref_get_waveform(wf.ctypes.data, *args, ylm.ctypes.data, prob["dt"], _p(prob["t"]), 0)
+    else:
+        st = lib.oracle_get_waveform(_p(wf.view(np.float64)), *args, _p(ylm), prob["dt"], _p(prob["t"]), 0,
+                                     prob["out_len"], 0)
+        if st != 0:
+            raise ValueError(f"oracle mode sum failed with status {st}")
+    return wf

@@ -1,0 +1,24 @@
+// C-linkage entry points into the reference's own CPU implementation
+// (src/few/cutils/interpolate.hh:27-31), so the oracle tests can call it
+// through ctypes.  Built only by oracle/Makefile into oracle/_ref; test
+// infrastructure, never part of the product path.
+#include "interpolate.hh"
+
+extern "C" {
+
+void few_ref_interpolate_arrays(double *t_arr, double *interp_array, int ninterps, int length,
+                                double *B, double *upper_diag, double *diag, double *lower_diag)
+{
+    interpolate_arrays(t_arr, interp_array, ninterps, length, B, upper_diag, diag, lower_diag);
+}
+
+void few_ref_get_waveform(void *d_waveform, double *interp_array, double *phase_interp_t,
+                          double *phase_interp_coeffs, int *d_m, int *d_k, int *d_n, int init_len,
+                          int out_len, int num_teuk_modes, void *d_Ylms, double delta_t, double *h_t,
+                          int dev)
+{
+    get_waveform((cmplx *)d_waveform, interp_array, phase_interp_t, phase_interp_coeffs, d_m, d_k,
+                 d_n, init_len, out_len, num_teuk_modes, (cmplx *)d_Ylms, delta_t, h_t, dev);
+}
+
+}

@@ -1,0 +1,93 @@
+"""Generates the golden vectors in tests/golden from the reference itself.
+
+The reference's CPU path (src/few/cutils/interpolate.cu, built as C++ from the
+reference sources by ``make -C oracle ref`` into oracle/_ref) is run on small
+seeded inputs and its outputs are stored next to those inputs.  The reference
+ships no golden files of its own; its tests pin the spline against
+scipy.interpolate.CubicSpline (tests/test_mode_summation.py:23-52) and the sum
+against a direct numpy sum (tests/test_mode_summation.py:64-151), which the
+tests here restate as well.
+
+    python tests/golden/make_golden.py      (needs the reference sources)
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from fastemriwaveforms_b200 import synthetic as S  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def inputs_digest(inp) -> str:
+    h = hashlib.sha256()
+    for a in (inp.t, inp.teuk_modes, inp.ylms, inp.phase_t, inp.phase_coeffs, inp.l, inp.m, inp.k, inp.n):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def save_case(name, inp, wf, extra=None):
+    d = dict(t=inp.t, teuk_modes=inp.teuk_modes, ylms=inp.ylms, phase_t=inp.phase_t,
+             phase_coeffs=inp.phase_coeffs, l=inp.l, m=inp.m, k=inp.k, n=inp.n, dt=inp.dt, T=inp.T,
+             waveform=wf)
+    if extra:
+        d.update(extra)
+    np.savez_compressed(os.path.join(HERE, name), **d)
+
+
+def main():
+    O.build(ref=True)
+    rng = np.random.default_rng(2024)
+
+    # 1. the reference spline test's inputs: cos/sin on 1000 uniform knots
+    t = np.linspace(0, 100, 1000)
+    y = np.vstack((np.cos(t), np.sin(t)))
+    np.savez_compressed(os.path.join(HERE, "spline_cos_sin.npz"), t=t, y=y,
+                        coeffs=O.interpolate_arrays(t, y, impl="ref"))
+
+    # 2. per-interpolant knots (2-D t), uneven spacing, 5 series of 37 knots
+    t2 = np.sort(rng.uniform(0, 50, (5, 37)), axis=1)
+    t2[:, 0] = 0.0
+    y2 = rng.standard_normal((5, 37)).cumsum(axis=1)
+    np.savez_compressed(os.path.join(HERE, "spline_rows2d.npz"), t=t2, y=y2,
+                        coeffs=O.interpolate_arrays(t2, y2, impl="ref"))
+
+    # 3. small sums in the style of the reference's summation test
+    for name, kw in (("sum_small_theta.npz", dict(K=10, N=20, out_len=4000, seed=7, theta=True)),
+                     ("sum_small_m0.npz", dict(K=40, N=33, out_len=6001, seed=8, theta=False))):
+        inp = S.small_case(**kw)
+        if name == "sum_small_m0.npz":
+            inp.m[:8] = 0  # m = 0 modes: no -m term
+        wf = O.mode_sum(inp, impl="ref")
+        save_case(name, inp, wf)
+
+    # 4. observation shorter than the trajectory: the knot loop stops early
+    inp = S.small_case(K=12, N=25, out_len=5000, seed=9)
+    inp.T = 0.6 * (4999 * inp.dt) / S.YRSID_SI
+    wf = O.mode_sum(inp, impl="ref")
+    save_case("sum_small_truncated.npz", inp, wf)
+
+    # 5. the K=200, N=100, 100,001-sample workload: the reference's output on
+    #    the first 3000 samples and around three knots, plus whole-output norms
+    inp = S.plain_small()
+    wf = O.mode_sum(inp, impl="ref")
+    start, nseg = O.find_start_inds(inp.t, inp.dt, len(wf))
+    picks = [np.arange(0, 3000)]
+    for j in (17, 50, 98):
+        picks.append(np.arange(max(start[j] - 200, 0), min(start[j] + 200, len(wf))))
+    idx = np.unique(np.concatenate(picks))
+    np.savez_compressed(os.path.join(HERE, "plain_small_ref.npz"), idx=idx, values=wf[idx],
+                        norm=np.linalg.norm(wf), sum=wf.sum(), out_len=len(wf),
+                        digest=inputs_digest(inp), seed=inp.seed)
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

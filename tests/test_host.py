@@ -1,0 +1,148 @@
+"""Host-side logic, no GPU: the C ABI's planners, the output-length contract,
+the synthetic workloads and the cubic -> 8-term phase basis map."""
+import numpy as np
+import pytest
+
+from fastemriwaveforms_b200 import _lib
+from fastemriwaveforms_b200 import synthetic as S
+
+
+def fold_plan_host(m, k, n, max_rows=256):
+    m, k, n = (np.ascontiguousarray(a, dtype=np.int32) for a in (m, k, n))
+    K = len(m)
+    nmax = int(np.abs(n).max())
+    max_keys = max_rows * (2 * nmax + 1)
+    row_m = np.zeros(max_rows, np.int32)
+    row_k = np.zeros(max_rows, np.int32)
+    dims = np.zeros(3, np.int32)
+    key_ptr = np.zeros(max_keys + 1, np.int32)
+    key_list = np.zeros(2 * K, np.int32)
+    _lib.call("few_fold_plan", m.ctypes.data, k.ctypes.data, n.ctypes.data, K, max_rows, max_keys,
+              row_m.ctypes.data, row_k.ctypes.data, dims.ctypes.data, key_ptr.ctypes.data, key_list.ctypes.data)
+    R, nlo, NN = dims.tolist()
+    return row_m[:R], row_k[:R], nlo, NN, key_ptr[: R * NN + 1], key_list
+
+
+def test_fold_plan_covers_every_term_once():
+    l, m, k, n = S.mode_list(10, 30)
+    row_m, row_k, nlo, NN, key_ptr, key_list = fold_plan_host(m, k, n)
+    assert len(row_m) == 21 and nlo == -30 and NN == 61
+    assert list(row_m) == list(range(-10, 11)) and not row_k.any()
+    nterms = len(m) + int(np.count_nonzero(m))
+    assert key_ptr[-1] == nterms
+    codes = key_list[:nterms]
+    assert len(np.unique(codes)) == nterms
+    # every contributor sits under the key of its phase
+    for q in range(len(row_m) * NN):
+        r, c = divmod(q, NN)
+        for code in codes[key_ptr[q]:key_ptr[q + 1]]:
+            j, minus = divmod(int(code), 2)
+            sgn = -1 if minus else 1
+            assert (sgn * m[j], sgn * k[j], sgn * n[j]) == (row_m[r], row_k[r], nlo + c)
+
+
+def test_fold_plan_sparse_modes_with_theta():
+    m = np.array([2, 3, 4, 0, 2])
+    k = np.array([0, 1, 1, 1, 0])
+    n = np.array([-4, 3, 0, 2, -4])
+    row_m, row_k, nlo, NN, key_ptr, key_list = fold_plan_host(m, k, n)
+    assert sorted(zip(row_m.tolist(), row_k.tolist())) == list(zip(row_m.tolist(), row_k.tolist()))
+    assert (0, 1) in zip(row_m.tolist(), row_k.tolist())
+    assert nlo == -4 and NN == 9
+    assert key_ptr[-1] == 5 + 4
+    # modes 0 and 4 share the key (2, 0, -4): listed in mode order
+    q = list(zip(row_m.tolist(), row_k.tolist())).index((2, 0)) * NN + (-4 - nlo)
+    assert key_list[key_ptr[q]:key_ptr[q + 1]].tolist() == [0, 8]
+
+
+def test_fold_plan_limits():
+    m = np.arange(0, 300) % 300
+    with pytest.raises(ValueError):
+        fold_plan_host(m, np.zeros(300), np.zeros(300), max_rows=256)
+
+
+def segment_plan_host(h_t, phase_t, out_len, dt, chunk):
+    h_t = np.ascontiguousarray(h_t, np.float64)
+    phase_t = np.ascontiguousarray(phase_t, np.float64)
+    N = len(h_t)
+    max_units = N + out_len // chunk + 1
+    seg_start = np.zeros(N, np.int32)
+    seg_info = np.zeros(3 * (N - 1))
+    units = np.zeros(3 * max_units, np.int32)
+    counts = np.zeros(2, np.int32)
+    _lib.call("few_segment_plan", h_t.ctypes.data, phase_t.ctypes.data, N, out_len, dt, chunk, max_units,
+              seg_start.ctypes.data, seg_info.ctypes.data, units.ctypes.data, counts.ctypes.data)
+    nseg, nu = counts.tolist()
+    return seg_start[: nseg + 1], seg_info[: 3 * nseg].reshape(-1, 3), units[: 3 * nu].reshape(-1, 3)
+
+
+def test_segment_plan_matches_find_start_inds(oracle):
+    inp = S.plain_small()
+    out_len = inp.out_len
+    start, info, units = segment_plan_host(inp.t, inp.phase_t, out_len, inp.dt, 1024)
+    ostart, nseg = oracle.find_start_inds(inp.t, inp.dt, out_len)
+    assert start.tolist() == ostart.tolist()
+    # units tile [0, out_len) exactly, in order, within their segments, <= chunk long
+    assert units[0, 1] == 0 and units[-1, 2] == out_len
+    assert (units[1:, 1] == units[:-1, 2]).all()
+    assert ((units[:, 2] - units[:, 1]) <= 1024).all()
+    assert (units[:, 1] >= start[units[:, 0]]).all() and (units[:, 2] <= start[units[:, 0] + 1]).all()
+    np.testing.assert_array_equal(info[:, 0], inp.t[:nseg])
+    np.testing.assert_array_equal(info[:, 2], np.diff(inp.phase_t)[:nseg])
+
+
+def test_segment_plan_truncated_and_errors():
+    t = np.array([0.0, 15.0, 30.0, 45.5, 70.0])
+    start, info, units = segment_plan_host(t, t, 6, 10.0, 4)
+    assert start.tolist() == [0, 2, 3, 5, 6]
+    assert units.tolist() == [[0, 0, 2], [1, 2, 3], [2, 3, 5], [3, 5, 6]]
+    with pytest.raises(ValueError):  # knots never reach the last sample
+        segment_plan_host(t, t, 20, 10.0, 4)
+    with pytest.raises(ValueError):  # not increasing
+        segment_plan_host(np.array([0.0, 20.0, 10.0, 70.0]), t[:4], 6, 10.0, 4)
+
+
+def test_output_length_contract():
+    t = np.array([0.0, 1e3, 1e6])
+    # T beyond the trajectory: output ends at the last knot
+    assert S.output_length(t, 2e6 / S.YRSID_SI, 10.0) == (100001, 0)
+    assert S.output_length(t, 2e6 / S.YRSID_SI, 10.0, pad_output=True)[1] > 0
+    # T inside the trajectory
+    n, pad = S.output_length(t, 5e5 / S.YRSID_SI, 10.0)
+    assert pad == 0 and n in (50000, 50001)
+    n, pad = S.output_length(t, 2e6 / S.YRSID_SI, 10.0, odd_len=True)
+    assert (n + pad) % 2 == 1
+
+
+def test_synthetic_workloads():
+    a = S.plain_small()
+    assert a.num_modes == 200 and a.num_knots == 100 and a.out_len == 100001
+    assert np.diff(a.t).min() >= 1e3 - 1e-6
+    l, m, k, n = S.mode_list(10, 30)
+    assert len(l) == 3843
+    inp = S.make_inputs(K=300, N=60, span=3e6, t_c=3.2e6, lmax=10, nmax=30, seed=3)
+    assert inp.phase_coeffs.shape == (59, 3, 8) and not inp.phase_coeffs[:, 1].any()
+
+
+def test_cubic_to_basis_reproduces_cubic():
+    rng = np.random.default_rng(0)
+    y0, c1, c2, c3 = rng.standard_normal(4)
+    h = 3.7
+    b = S.cubic_to_basis(y0, c1, c2, c3, h)
+    for x in np.linspace(0, h, 7):
+        s = x / h
+        s1 = 1 - s
+        v = b[0] + s * (b[1] + s1 * (b[2] + s * (b[3] + s1 * (b[4] + s * (b[5] + s1 * (b[6] + s * b[7]))))))
+        assert abs(v - (y0 + c1 * x + c2 * x * x + c3 * x ** 3)) < 1e-12
+
+
+def test_mismatch_known_answer():
+    # tests/test_few.py:232-245 of the reference
+    from fastemriwaveforms_b200 import get_mismatch, get_overlap
+
+    t = np.arange(10000) * 1.0
+    x0 = np.sin(t) + 1j * np.sin(t)
+    x2 = np.sin(t) + 1j * np.cos(t)
+    assert abs(get_overlap(x0, x0) - 1.0) < 1e-12
+    assert abs(get_overlap(x0, x2) - 0.499981442642142) < 1e-7
+    assert abs(get_mismatch(x0, x0)) < 1e-12

@@ -1,0 +1,87 @@
+"""The oracle pinned against the reference: golden vectors made by the
+reference's own CPU build, scipy's CubicSpline (the reference's spline test,
+tests/test_mode_summation.py:23-52) and, where the reference sources are
+present, the reference build itself."""
+import os
+
+import numpy as np
+import pytest
+from scipy.interpolate import CubicSpline
+
+from conftest import GOLDEN, load_case
+from fastemriwaveforms_b200 import synthetic as S
+
+
+def test_spline_matches_golden_bitwise(oracle):
+    d = np.load(os.path.join(GOLDEN, "spline_cos_sin.npz"))
+    got = oracle.interpolate_arrays(d["t"], d["y"])
+    assert np.array_equal(got, d["coeffs"])
+    d = np.load(os.path.join(GOLDEN, "spline_rows2d.npz"))
+    got = oracle.interpolate_arrays(d["t"], d["y"])
+    assert np.array_equal(got, d["coeffs"])
+
+
+def test_spline_matches_scipy_like_reference_test(oracle):
+    # tests/test_mode_summation.py:23-52 with its rtol 1e-10
+    t = np.linspace(0, 100, 1000)
+    f = np.vstack((np.cos(t), np.sin(t)))
+    coeffs = oracle.spline_coeffs(t, f)
+    cs = CubicSpline(t, f, axis=-1)
+    np.testing.assert_allclose(oracle.spline_eval(t, coeffs, t), f, rtol=1e-10)
+    for nu in range(1, 4):
+        np.testing.assert_allclose(oracle.spline_eval(t, coeffs, t, nu), cs(t, nu=nu), rtol=1e-10)
+    te = np.linspace(0, 100, 1852)
+    for nu in range(4):
+        np.testing.assert_allclose(oracle.spline_eval(t, coeffs, te, nu), cs(te, nu=nu), rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["sum_small_theta.npz", "sum_small_m0.npz", "sum_small_truncated.npz"])
+def test_mode_sum_matches_golden_bitwise(oracle, name):
+    inp, ref = load_case(name)
+    got = oracle.mode_sum(inp)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
+
+
+def test_extended_oracle_within_reference_rounding(oracle):
+    inp, ref = load_case("sum_small_theta.npz")
+    ext = oracle.mode_sum(inp, extended=True)
+    # the reference rounds each mode phase; at |phase| ~ 1e2 rad that is ~1e-14
+    assert oracle.rel_l2(ext, ref) < 1e-12
+
+
+def test_plain_small_inputs_and_reference_values(oracle):
+    d = np.load(os.path.join(GOLDEN, "plain_small_ref.npz"))
+    inp = S.plain_small(int(d["seed"]))
+    from golden.make_golden import inputs_digest
+
+    assert inputs_digest(inp) == str(d["digest"]), "synthetic generator drifted from the golden inputs"
+    idx = d["idx"]
+    wf = oracle.mode_sum(inp, window=(0, int(idx.max()) + 1))
+    assert np.array_equal(wf[idx], d["values"])
+
+
+def test_window_is_a_restriction(oracle):
+    inp, ref = load_case("sum_small_m0.npz")
+    part = oracle.mode_sum(inp, window=(1000, 2500))
+    assert np.array_equal(part[1000:2500], ref[1000:2500])
+    assert not part[:1000].any() and not part[2500:].any()
+
+
+def test_find_start_inds_semantics(oracle):
+    t = np.array([0.0, 15.0, 30.0, 45.5, 70.0])
+    start, nseg = oracle.find_start_inds(t, 10.0, 6)  # T = 50: knot 70 closes the plan
+    assert nseg == 4
+    assert start.tolist() == [0, 2, 3, 5, 6]
+    with pytest.raises(ValueError):
+        oracle.find_start_inds(t, 10.0, 20)  # no knot reaches T = 190
+
+
+@pytest.mark.skipif(not os.path.isfile(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "libfew_ref.so")),
+                    reason="reference build absent (sources not on this machine)")
+def test_restatement_equals_reference_build(oracle):
+    inp = S.small_case(K=25, N=30, out_len=7000, seed=11)
+    assert np.array_equal(oracle.mode_sum(inp), oracle.mode_sum(inp, impl="ref"))
+    t = np.sort(np.random.default_rng(3).uniform(0, 10, 64))
+    y = np.random.default_rng(4).standard_normal((7, 64))
+    assert np.array_equal(oracle.interpolate_arrays(t, y), oracle.interpolate_arrays(t, y, impl="ref"))
