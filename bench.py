@@ -25,7 +25,6 @@ import datetime
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -49,6 +48,8 @@ def parse():
                     help="output samples of the bounded single-core reference run (cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only run warmup + steps forward calls (for ncu captures); prints no JSON line")
     return ap.parse_args()
 
 
@@ -75,50 +76,67 @@ def config_of(inp, args, extra=None):
 # clocks
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled through NVML (read-only) every
+    5 ms on a background thread while the timed region runs."""
 
-    def __init__(self, gpu_index: int):
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device):
+        import threading
+
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._thread = None
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-i", str(gpu_index), "-lms", "200"], stdout=self.fh,
-                                         stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            h = None
+            bus = getattr(torch.cuda.get_device_properties(device), "pci_bus_id", None)
+            if bus is not None:
+                try:
+                    busid = "%08x:%02x:%02x.0" % (getattr(torch.cuda.get_device_properties(device), "pci_domain_id", 0),
+                                                  bus, getattr(torch.cuda.get_device_properties(device),
+                                                               "pci_device_id", 0))
+                    h = nv.nvmlDeviceGetHandleByPciBusId(busid)
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(device.index or 0)
+            self.nv, self.h = nv, h
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self._get_reasons = get_reasons
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
         except Exception:
-            self.proc = None
+            self._thread = None
+
+    def _run(self):
+        nv, h = self.nv, self.h
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                bits = int(self._get_reasons(h))
+                for bit, name in self.REASONS.items():
+                    if bits & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.005)
 
     def stop(self):
-        if self.proc is None:
+        if self._thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.fh.close()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                p = [x.strip() for x in line.split(",")]
-                if len(p) < 9:
-                    continue
-                try:
-                    sm.append(float(p[1]))
-                    smax = float(p[2])
-                except ValueError:
-                    continue
-                for name, v in zip(names, p[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(name)
-        if not sm:
+        self._stop.set()
+        self._thread.join(timeout=2)
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 5 ms"}
 
 
 # ------------------------------------------------------------------------------------------
@@ -289,6 +307,12 @@ def main():
     pc_d = torch.from_numpy(inp.phase_coeffs).to(dev)
     call_args = (inp.t, teuk_d, ylms_d, inp.phase_t, pc_d, inp.l, inp.m, inp.k, inp.n)
 
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            ims(*call_args, T=inp.T, dt=inp.dt)
+        torch.cuda.synchronize()
+        return 0
+
     fp64_tflops = fp64_peak(dev)
 
     for _ in range(max(args.warmup, 3)):
@@ -297,7 +321,7 @@ def main():
 
     # ---- device-resident timed region -------------------------------------------------
     ims.record_stages = True
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev)
     stage_events = []
     barrier()
     torch.cuda.synchronize()
