@@ -41,6 +41,8 @@ SIGNATURES = {
     "few_sum_folded": [_vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
                        _c_int, _vp],
     "few_probe_fp64_fma": [_vp, _c_int, _c_int, _vp],
+    "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
+                                 _c_int, _vp],
 }
 _RESTYPE = {"few_last_error": ctypes.c_char_p}
 

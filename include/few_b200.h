@@ -86,6 +86,33 @@ FEW_API int few_get_waveform(void *d_waveform, const double *interp_array, const
                      const int *d_n, int init_len, int out_len, int num_teuk_modes,
                      const void *d_Ylms, double delta_t, const double *h_t, int dev, void *stream);
 
+/* Size of the fixed device scratch of few_get_waveform_noalloc. */
+#define FEW_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/* few_get_waveform without any device memory allocation.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc (or
+ * cudaMallocAsync) -- a host framework that owns all device memory through
+ * its own pool, an application held to a fixed device memory budget, or a
+ * pipeline that must not let the CUDA driver block or synchronise inside an
+ * allocation.  Arguments, layouts and results are those of few_get_waveform.
+ * Its scratch is one device array of FEW_NOALLOC_SCRATCH_BYTES (8 MiB) inside
+ * the library, which every GPU that loads the library holds until the process
+ * exits; the waveform is built in batches of knot segments that fit it.
+ * Sizes where a single knot segment's folded coefficients do not fit
+ * (R * NN * 64 bytes plus the fold tables, R the (m, k) rows and NN the n
+ * range of the mode list) are rejected with FEW_ERR_SIZE and a message.
+ * The first call on each device looks up the array's device address (with
+ * that device made current); make that first call before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * (other threads, other streams) race and must be serialised by the caller;
+ * each call writes every scratch byte it reads, so nothing needs clearing.
+ * Synchronises `stream` before returning, like few_get_waveform. */
+FEW_API int few_get_waveform_noalloc(void *d_waveform, const double *interp_array, const double *phase_interp_t,
+                                     const double *phase_interp_coeffs, const int *d_m, const int *d_k,
+                                     const int *d_n, int init_len, int out_len, int num_teuk_modes,
+                                     const void *d_Ylms, double delta_t, const double *h_t, int dev,
+                                     void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Spline build and evaluation (CubicSplineInterpolant)                     */
 /* ------------------------------------------------------------------------ */
