@@ -41,6 +41,12 @@ SIGNATURES = {
     "few_sum_folded": [_vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
                        _c_int, _vp],
     "few_probe_fp64_fma": [_vp, _c_int, _c_int, _vp],
+    "few_adjoint_phase": [_vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
+                          _vp, _vp],
+    "few_adjoint_phase_reduce": [_vp, _vp, _c_int, _vp, _vp],
+    "few_adjoint_G": [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp, _vp],
+    "few_unfold": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_spline_adjoint": [_vp, _c_ll, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
 }

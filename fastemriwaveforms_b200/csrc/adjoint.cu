@@ -1,0 +1,675 @@
+// Adjoint of the interpolated mode sum: dL/d(amplitude knots) and
+// dL/d(phase coefficients) for L = Re sum_i g_i h_i, with g supplied.
+//
+// The forward map is  knots y --spline--> coefficients a --fold--> W --sum--> h,
+// phases Phi(s) = sum_q b_q(s) coef_q (the 8-term basis of
+// src/few/cutils/interpolate.cu:642-644).  Its adjoint runs the chain backwards:
+//
+//   k_adj_phase   per sample, the forward-like sums dh/dPhi_phi, dh/dPhi_r,
+//                 dh/dPhi_theta (phasors recomputed, not stored), projected on
+//                 the basis b_q(s) and reduced per work unit; k_adj_phase_reduce
+//                 adds the unit partials per segment in unit order.
+//   k_adj_G       per segment, G[key][c] = sum_i g_i x_i^c P_key(t_i): one CTA
+//                 per segment, per-sample phasor tables staged in shared memory,
+//                 each thread owning a few keys (deterministic, no atomics).
+//   k_unfold      the transpose of the fold: dL/da per mode and coefficient.
+//   k_spline_adjoint  the transpose of the spline build: solves with A^T, the
+//                 transposed not-a-knot matrix.  With M the row operations that
+//                 remove the two non-dominant rows (row1 -= row0,
+//                 row[N-2] -= row[N-1]) and M A = A~, A^{-T} = M^T A~^{-T}: the
+//                 first and last columns of A~ each hold one entry, and the
+//                 interior block is the transpose of a row-dominant tridiagonal
+//                 matrix (column-dominant), so elimination without pivoting is
+//                 stable there too.
+//
+// With torch's convention the upstream gradient of a complex output is
+// G = dL/dRe h + i dL/dIm h, so g = conj(G).  Gradients with respect to real
+// inputs are plain derivatives; for complex inputs d/dRe + i d/dIm.
+#include "few_common.cuh"
+#include "few_internal.h"
+
+namespace few {
+
+namespace {
+
+constexpr int kAdjThreads = 256;
+constexpr int kRowBlock = 8;
+constexpr int kSmemBudget = 200 * 1024;
+
+struct AdjPhaseArgs {
+    const double2 *grad;  // (out_len,) torch upstream gradient G; g = conj(G)
+    const double2 *W;
+    const double *pc;     // (8, N-1, 3)
+    const double *seg_info;
+    const int *units;
+    const int *row_m;
+    const int *row_k;
+    double *partial;      // (nunits, 24): unit partials of dL/dcoef[field][q], field 0 phi, 1 theta, 2 r
+    int N, R, nlo, NN, rows_per_pass, use_theta;
+    double dt;
+};
+
+// dL/dPhi at every sample of the unit, projected on the phase basis.
+template <int RB>
+__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *sW = reinterpret_cast<double2 *>(smem_raw);
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    __shared__ double s_red[kAdjThreads / 32][24];
+
+    const int u = blockIdx.x;
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const int R = a.R, NN = a.NN, nlo = a.nlo;
+    const long long nps = (long long)(a.N - 1) * 3;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        s_rm[r] = a.row_m[r];
+        s_rk[r] = a.row_k[r];
+    }
+    if (threadIdx.x < 24) {
+        const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
+        s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    double acc[24];
+#pragma unroll
+    for (int q = 0; q < 24; ++q) acc[q] = 0.0;
+
+    for (int r0 = 0; r0 < R; r0 += a.rows_per_pass) {
+        const int nrp = min(a.rows_per_pass, R - r0);
+        __syncthreads();
+        {
+            const double2 *src = a.W + ((long long)seg * R + r0) * NN * 4;
+            const int count = nrp * NN * 4;
+            for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
+        }
+        __syncthreads();
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            const double t = rmul(a.dt, (double)i);
+            const double x = rsub(t, t0);
+            const double s = __ddiv_rn(rsub(t, pt0), pw);
+            const double s1 = rsub(1.0, s);
+            const double Pp = phase_poly(s_pc, s, s1);
+            const double Pr = phase_poly(s_pc + 16, s, s1);
+            const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
+            double sn, cs;
+            sincos(Pp, &sn, &cs);
+            const double2 Ep = make_double2(cs, -sn);
+            sincos(Pr, &sn, &cs);
+            const double2 Er = make_double2(cs, -sn);
+            double2 Et = make_double2(1.0, 0.0);
+            if (a.use_theta) {
+                sincos(Pt, &sn, &cs);
+                Et = make_double2(cs, -sn);
+            }
+            const double2 V0 = cpow_int(Er, nlo);
+            double2 Dp = make_double2(0.0, 0.0), Dr = Dp, Dt = Dp;
+            for (int rb = 0; rb < nrp; rb += RB) {
+                double2 U[RB];
+                double Mq[RB], Kq[RB];
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    U[q] = make_double2(0.0, 0.0);
+                    Mq[q] = 0.0;
+                    Kq[q] = 0.0;
+                    if (rb + q < nrp) {
+                        const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
+                        double2 uu = cpow_int(Ep, mm);
+                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
+                        U[q] = uu;
+                        Mq[q] = (double)mm;
+                        Kq[q] = (double)kk;
+                    }
+                }
+                double2 v = V0;
+                const double2 *wrow = sW + (long long)rb * NN * 4;
+                for (int c = 0; c < NN; ++c) {
+                    double2 T = make_double2(0.0, 0.0), Tm = T, Tk = T;
+                    const double2 *wc = wrow + c * 4;
+#pragma unroll
+                    for (int q = 0; q < RB; ++q) {
+                        if (rb + q < nrp) {
+                            const double2 *w = wc + (long long)q * NN * 4;
+                            const double2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+                            double2 Wx;
+                            Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
+                            Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
+                            const double2 P = cmul(U[q], Wx);
+                            T.x += P.x;
+                            T.y += P.y;
+                            Tm.x = fma(Mq[q], P.x, Tm.x);
+                            Tm.y = fma(Mq[q], P.y, Tm.y);
+                            Tk.x = fma(Kq[q], P.x, Tk.x);
+                            Tk.y = fma(Kq[q], P.y, Tk.y);
+                        }
+                    }
+                    const double dn = (double)(nlo + c);
+                    const double2 vT = cmul(v, T);
+                    const double2 vTm = cmul(v, Tm);
+                    Dp.x += vTm.x;
+                    Dp.y += vTm.y;
+                    Dr.x = fma(dn, vT.x, Dr.x);
+                    Dr.y = fma(dn, vT.y, Dr.y);
+                    if (a.use_theta) {
+                        const double2 vTk = cmul(v, Tk);
+                        Dt.x += vTk.x;
+                        Dt.y += vTk.y;
+                    }
+                    v = cmul(v, Er);
+                }
+            }
+            // dh/dPhi = -i D; dL/dPhi = Re(g (-i D)) = Im(g D) with g = conj(G)
+            const double2 G = a.grad[i];
+            const double ep = G.x * Dp.y - G.y * Dp.x;
+            const double er = G.x * Dr.y - G.y * Dr.x;
+            const double et = G.x * Dt.y - G.y * Dt.x;
+            // basis b_q(s): 1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3, s^4 s1^3
+            double b[8];
+            b[0] = 1.0;
+            b[1] = s;
+            b[2] = s * s1;
+            b[3] = b[2] * s;
+            b[4] = b[3] * s1;
+            b[5] = b[4] * s;
+            b[6] = b[5] * s1;
+            b[7] = b[6] * s;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                acc[q] = fma(ep, b[q], acc[q]);
+                acc[8 + q] = fma(et, b[q], acc[8 + q]);
+                acc[16 + q] = fma(er, b[q], acc[16 + q]);
+            }
+        }
+    }
+    // block reduction in a fixed order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 24; ++q) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) s_red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 24) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_red[w][threadIdx.x];
+        a.partial[(long long)u * 24 + threadIdx.x] = v;
+    }
+}
+
+// Sum the unit partials of each segment (units of a segment are consecutive) into
+// grad_pc (N-1, 3, 8) (the layout of phase_interp_coeffs).
+__global__ void k_adj_phase_reduce(const double *__restrict__ partial, const int *__restrict__ seg_units, int nseg,
+                                   double *__restrict__ grad_pc)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nseg * 24) return;
+    const int s = idx / 24, e = idx - s * 24;
+    double v = 0.0;
+    for (int u = seg_units[s]; u < seg_units[s + 1]; ++u) v += partial[(long long)u * 24 + e];
+    grad_pc[idx] = v;  // (s, field, q) with e = field*8 + q
+}
+
+// G[s][key][c] = sum_{i in segment s} g_i x_i^c P_key(t_i).
+struct AdjGArgs {
+    const double2 *grad;
+    const double *pc;
+    const double *seg_info;
+    const int *seg_start;  // (nseg+1,) first output sample of each segment (clamped)
+    const int *row_m;
+    const int *row_k;
+    double2 *G;            // (nseg, R, NN, 4)
+    int N, R, nlo, NN, use_theta, key_base, nkeys_pass;
+    double dt;
+};
+
+constexpr int kGTile = 32;    // samples per shared-memory tile
+constexpr int kGKeys = 6;     // keys per thread per pass (256*6 = 1536 keys per pass)
+
+__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_G(AdjGArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int R = a.R, NN = a.NN;
+    double2 *s_gu = reinterpret_cast<double2 *>(smem_raw);  // [kGTile][R]   g_i u_r(t_i)
+    double2 *s_v = s_gu + kGTile * R;                         // [kGTile][NN]  v_{n'}(t_i)
+    double *s_x = reinterpret_cast<double *>(s_v + kGTile * NN);  // [kGTile][4] x^0..x^3
+    double2 *s_E = reinterpret_cast<double2 *>(s_x + kGTile * 4);  // [kGTile][4] Ep, Er, Et, g
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+
+    const int seg = blockIdx.x;
+    const int lo = a.seg_start[seg], hi = a.seg_start[seg + 1];
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const long long nps = (long long)(a.N - 1) * 3;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        s_rm[r] = a.row_m[r];
+        s_rk[r] = a.row_k[r];
+    }
+    if (threadIdx.x < 24) {
+        const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
+        s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    double2 acc[kGKeys][4];
+#pragma unroll
+    for (int k = 0; k < kGKeys; ++k)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[k][c] = make_double2(0.0, 0.0);
+    int kr[kGKeys], kc[kGKeys];
+#pragma unroll
+    for (int k = 0; k < kGKeys; ++k) {
+        const int key = a.key_base + threadIdx.x + k * kAdjThreads;
+        kr[k] = key / NN;
+        kc[k] = key - kr[k] * NN;
+        if (threadIdx.x + k * kAdjThreads >= a.nkeys_pass) kr[k] = -1;
+    }
+    __syncthreads();
+
+    for (int i0 = lo; i0 < hi; i0 += kGTile) {
+        const int ns = min(kGTile, hi - i0);
+        // per-sample scalars
+        if (threadIdx.x < ns) {
+            const int i = i0 + threadIdx.x;
+            const double t = rmul(a.dt, (double)i);
+            const double x = rsub(t, t0);
+            const double s = __ddiv_rn(rsub(t, pt0), pw);
+            const double s1 = rsub(1.0, s);
+            double sn, cs;
+            sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+            s_E[threadIdx.x * 4 + 0] = make_double2(cs, -sn);
+            sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+            s_E[threadIdx.x * 4 + 1] = make_double2(cs, -sn);
+            if (a.use_theta) {
+                sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+                s_E[threadIdx.x * 4 + 2] = make_double2(cs, -sn);
+            } else {
+                s_E[threadIdx.x * 4 + 2] = make_double2(1.0, 0.0);
+            }
+            const double2 G = a.grad[i];
+            s_E[threadIdx.x * 4 + 3] = make_double2(G.x, -G.y);  // g = conj(G)
+            s_x[threadIdx.x * 4 + 0] = 1.0;
+            s_x[threadIdx.x * 4 + 1] = x;
+            s_x[threadIdx.x * 4 + 2] = x * x;
+            s_x[threadIdx.x * 4 + 3] = x * x * x;
+        }
+        __syncthreads();
+        // tables: g u_r (rows) and v_{n'} (columns, runs of 8 by recurrence)
+        for (int w = threadIdx.x; w < ns * R; w += blockDim.x) {
+            const int j = w / R, r = w - j * R;
+            double2 uu = cpow_int(s_E[j * 4 + 0], s_rm[r]);
+            if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[j * 4 + 2], s_rk[r]));
+            s_gu[j * R + r] = cmul(s_E[j * 4 + 3], uu);
+        }
+        const int runs = (NN + 7) / 8;
+        for (int w = threadIdx.x; w < ns * runs; w += blockDim.x) {
+            const int j = w / runs, b = w - j * runs;
+            const double2 Er = s_E[j * 4 + 1];
+            double2 v = cpow_int(Er, a.nlo + 8 * b);
+            const int cend = min(NN, 8 * b + 8);
+            for (int c = 8 * b; c < cend; ++c) {
+                s_v[j * NN + c] = v;
+                v = cmul(v, Er);
+            }
+        }
+        __syncthreads();
+        for (int j = 0; j < ns; ++j) {
+            const double x1 = s_x[j * 4 + 1], x2 = s_x[j * 4 + 2], x3 = s_x[j * 4 + 3];
+#pragma unroll
+            for (int k = 0; k < kGKeys; ++k) {
+                if (kr[k] >= 0) {
+                    const double2 z = cmul(s_gu[j * R + kr[k]], s_v[j * NN + kc[k]]);
+                    acc[k][0].x += z.x;
+                    acc[k][0].y += z.y;
+                    acc[k][1].x = fma(x1, z.x, acc[k][1].x);
+                    acc[k][1].y = fma(x1, z.y, acc[k][1].y);
+                    acc[k][2].x = fma(x2, z.x, acc[k][2].x);
+                    acc[k][2].y = fma(x2, z.y, acc[k][2].y);
+                    acc[k][3].x = fma(x3, z.x, acc[k][3].x);
+                    acc[k][3].y = fma(x3, z.y, acc[k][3].y);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const long long nkeys = (long long)R * NN;
+#pragma unroll
+    for (int k = 0; k < kGKeys; ++k) {
+        if (kr[k] >= 0) {
+            const long long key = a.key_base + threadIdx.x + k * kAdjThreads;
+            double2 *g = a.G + ((long long)seg * nkeys + key) * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) g[c] = acc[k][c];
+        }
+    }
+}
+
+// Transpose of the fold: dL/d coefficient (4, N, 2K); knots >= nseg get 0.
+__global__ void k_unfold(const double2 *__restrict__ G, const double2 *__restrict__ ylms,
+                         const int *__restrict__ key_plus, const int *__restrict__ key_minus, int K, int N, int nseg,
+                         int nkeys, double *__restrict__ gcoef)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)N * K) return;
+    const int s = (int)(idx / K), j = (int)(idx - (long long)s * K);
+    const long long plane = (long long)N * 2 * K;
+    double gre[4] = {0.0, 0.0, 0.0, 0.0}, gim[4] = {0.0, 0.0, 0.0, 0.0};
+    if (s < nseg) {
+        const double2 Yp = ylms[j];
+        const double2 *gp = G + ((long long)s * nkeys + key_plus[j]) * 4;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double2 z = cmul(gp[c], Yp);
+            gre[c] = z.x;    // dL/dRe a = Re(G Y+)
+            gim[c] = -z.y;   // dL/dIm a = -Im(G Y+)
+        }
+        if (key_minus[j] >= 0) {
+            const double2 Ym = ylms[K + j];
+            const double2 *gm = G + ((long long)s * nkeys + key_minus[j]) * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double2 z = cmul(gm[c], Ym);
+                gre[c] += z.x;   // Re(G Y-)
+                gim[c] += z.y;   // +Im(G Y-)
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        gcoef[c * plane + (long long)s * 2 * K + j] = gre[c];
+        gcoef[c * plane + (long long)s * 2 * K + K + j] = gim[c];
+    }
+}
+
+// Transpose of k_spline_build for one series per thread.  gc (4, N, ni) knot
+// major is consumed (overwritten as scratch); gy receives dL/dy through the same
+// strided view the build reads y with (accumulated with += when `accumulate`).
+struct SplineAdjArgs {
+    const double *t;
+    long long t_rs;
+    double *gc;
+    double *gy;
+    long long sk, sp, off2;
+    int split, ni, N, accumulate;
+};
+
+__global__ void __launch_bounds__(128) k_spline_adjoint(SplineAdjArgs a)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.ni) return;
+    const int N = a.N;
+    const double *x = a.t + (long long)p * a.t_rs;
+    double *gyb = (p < a.split) ? a.gy + (long long)p * a.sp : a.gy + a.off2 + (long long)(p - a.split) * a.sp;
+    const long long sk = a.sk, ni = a.ni;
+    const long long plane = (long long)N * ni;
+    double *g0 = a.gc + p;
+    double *g1 = g0 + plane;
+    double *g2 = g1 + plane;
+    double *g3 = g2 + plane;
+
+    const double x0 = x[0], x1 = x[1], x2 = x[2];
+    const double h0 = x1 - x0, h1 = x2 - x1, d0 = x2 - x0;
+    const double xa = x[N - 3], xb = x[N - 2], xc = x[N - 1];
+    const double hA = xb - xa, hB = xc - xb, dE = xc - xa;
+
+    // gradient of the extrapolated last-knot coefficients, folded into segment N-2
+    const long long oE = (long long)(N - 1) * ni;
+    const double gE1 = g1[oE], gE2 = g2[oE], gE3 = g3[oE];
+    const double gy_last0 = g0[oE];
+
+    // Pass F: slopes' gradient gs_i and the forward sweep of A~^T (interior block).
+    // Stored at knot i: g1 <- c'_i, g2 <- r'_i, g3 <- direct dL/d delta_i.
+    double gs_carry = 0.0;  // contribution to gs_i from segment i-1
+    double w0 = 0.0, wE = 0.0;
+    double cprev = 0.0, rprev = 0.0;
+    for (int i = 0; i <= N - 2; ++i) {
+        const long long o = (long long)i * ni;
+        const double h = x[i + 1] - x[i];
+        double a1 = g1[o], a2 = g2[o], a3 = g3[o];
+        if (i == N - 2) {
+            a1 += gE1;
+            a2 += 2 * h * gE1 + gE2;
+            a3 += 3 * h * h * gE1 + 3 * h * gE2 + gE3;
+        }
+        const double gtt = -a2 + a3 / h;
+        const double gdel = a2 / h - 2.0 * gtt / h;
+        const double gs_i = gs_carry + a1 - a2 / h + gtt / h;
+        gs_carry = gtt / h;
+        g3[o] = gdel;
+        if (i == 0) {
+            w0 = gs_i / h1;
+        } else {
+            // row i of A~^T restricted to the interior block
+            double rhs = gs_i;
+            if (i == 1) rhs -= d0 * w0;
+            if (i == N - 2) {
+                wE = gs_carry / hA;  // gs_{N-1} is complete: only segment N-2 feeds it
+                rhs -= dE * wE;
+            }
+            const double dg = 2 * (x[i] - x[i - 1] + h) - (i == 1 ? d0 : 0.0) - (i == N - 2 ? dE : 0.0);
+            const double lo = (i >= 2) ? (x[i - 1] - x[i - 2]) : 0.0;  // A~^T[i][i-1] = h_{i-2}
+            const double up = (i <= N - 3) ? (x[i + 2] - x[i + 1]) : 0.0;  // A~^T[i][i+1] = h_{i+1}
+            const double den = dg - lo * cprev;
+            const double cp = up / den;
+            const double rp = (rhs - lo * rprev) / den;
+            g1[o] = cp;
+            g2[o] = rp;
+            cprev = cp;
+            rprev = rp;
+        }
+    }
+
+    // Pass B: w (= z on the interior), z_0 = w0 - w1, z_{N-1} = wE - w_{N-2};
+    // gb = z feeds d delta; then dL/dy.
+    const double w_last = rprev;              // w_{N-2}
+    const double zE = wE - w_last;            // z_{N-1}
+    // row N-1 of b: delta_{N-3} and delta_{N-2}
+    const double rE_a = zE * hB * hB / dE;
+    const double rE_b = zE * (2 * dE + hB) * hA / dE;
+    double w_ip1 = 0.0;           // w_{i+1}
+    double gdel_ip1 = 0.0;        // final d delta_{i+1}
+    double pend_from_next = 0.0;  // row i+1's contribution 3 h_{i+1} z_{i+1} to d delta_i
+    auto put = [&](long long knot, double v) {
+        double *dst = gyb + knot * sk;
+        *dst = a.accumulate ? *dst + v : v;
+    };
+    for (int i = N - 2; i >= 1; --i) {
+        const long long o = (long long)i * ni;
+        const double w_i = (i == N - 2) ? w_last : (g2[o] - g1[o] * w_ip1);
+        const double hl = x[i] - x[i - 1];  // h_{i-1}
+        const double hr = x[i + 1] - x[i];  // h_i
+        // d delta_i: direct + row i (3 h_{i-1} z_i) + row i+1 + boundary rows
+        double gdel_i = g3[o] + 3.0 * hl * w_i + pend_from_next;
+        if (i == N - 2) gdel_i += rE_b;
+        if (i == N - 3) gdel_i += rE_a;
+        if (i == 1) gdel_i += (w0 - w_i) * h0 * h0 / d0;
+        // dL/dy_{i+1} = c0 gradient + d delta_i / h_i - d delta_{i+1} / h_{i+1}
+        double gy_ip1 = ((i + 1 == N - 1) ? gy_last0 : g0[o + ni]) + gdel_i / hr;
+        if (i + 1 <= N - 2) gy_ip1 -= gdel_ip1 / (x[i + 2] - x[i + 1]);
+        put(i + 1, gy_ip1);
+        pend_from_next = 3.0 * hr * w_i;
+        gdel_ip1 = gdel_i;
+        w_ip1 = w_i;
+        if (i == 1) {
+            // delta_0: direct + row 1 + row 0 (z_0 = w_0 - w_1); then y_1 and y_0
+            const double z0 = w0 - w_i;
+            const double gdel0 = g3[0] + pend_from_next + z0 * (h0 + 2 * d0) * h1 / d0;
+            put(1, g0[ni] + gdel0 / h0 - gdel_i / hr);
+            put(0, g0[0] - gdel0 / h0);
+        }
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+int launch_adj_phase(const double2 *grad, const double2 *W, const double *pc, int N, const double *seg_info,
+                     const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo, int NN,
+                     double dt, int use_theta, double *partial, cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    AdjPhaseArgs a;
+    a.grad = grad;
+    a.W = W;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.partial = partial;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const long long row_bytes = (long long)NN * 4 * sizeof(double2);
+    const int rpp = (int)std::min<long long>(R, kSmemBudget / row_bytes);
+    if (rpp < 1) return fail(FEW_ERR_SIZE, "adjoint: NN=%d too large for one row in shared memory", NN);
+    a.rows_per_pass = rpp;
+    FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kSmemBudget));
+    k_adj_phase<kRowBlock><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
+    FEW_LAUNCH_CHECK("k_adj_phase");
+    return FEW_OK;
+}
+
+int launch_adj_phase_reduce(const double *partial, const int *seg_units, int nseg, double *grad_pc, cudaStream_t st)
+{
+    if (nseg == 0) return FEW_OK;
+    const int threads = 256;
+    k_adj_phase_reduce<<<(nseg * 24 + threads - 1) / threads, threads, 0, st>>>(partial, seg_units, nseg, grad_pc);
+    FEW_LAUNCH_CHECK("k_adj_phase_reduce");
+    return FEW_OK;
+}
+
+int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg_info, const int *seg_start, int nseg,
+                 const int *row_m, const int *row_k, int R, int nlo, int NN, double dt, int use_theta, double2 *G,
+                 cudaStream_t st)
+{
+    if (nseg == 0) return FEW_OK;
+    const size_t smem = (size_t)kGTile * (R + NN) * sizeof(double2) + (size_t)kGTile * 4 * sizeof(double) +
+                        (size_t)kGTile * 4 * sizeof(double2);
+    if (smem > (size_t)kSmemBudget) return fail(FEW_ERR_SIZE, "adjoint: R + NN too large for the G tiles");
+    FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_G, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    const int nkeys = R * NN;
+    const int per_pass = kAdjThreads * kGKeys;
+    for (int base = 0; base < nkeys; base += per_pass) {
+        AdjGArgs a;
+        a.grad = grad;
+        a.pc = pc;
+        a.seg_info = seg_info;
+        a.seg_start = seg_start;
+        a.row_m = row_m;
+        a.row_k = row_k;
+        a.G = G;
+        a.N = N;
+        a.R = R;
+        a.nlo = nlo;
+        a.NN = NN;
+        a.use_theta = use_theta;
+        a.key_base = base;
+        a.nkeys_pass = std::min(per_pass, nkeys - base);
+        a.dt = dt;
+        k_adj_G<<<nseg, kAdjThreads, smem, st>>>(a);
+        FEW_LAUNCH_CHECK("k_adj_G");
+    }
+    return FEW_OK;
+}
+
+int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, const int *key_minus, int K, int N,
+                  int nseg, int nkeys, double *gcoef, cudaStream_t st)
+{
+    const long long total = (long long)N * K;
+    const int threads = 256;
+    k_unfold<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(G, ylms, key_plus, key_minus, K, N, nseg,
+                                                                             nkeys, gcoef);
+    FEW_LAUNCH_CHECK("k_unfold");
+    return FEW_OK;
+}
+
+int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *gy, long long sk, long long sp,
+                          int split, long long off2, int ni, int N, int accumulate, cudaStream_t st)
+{
+    SplineAdjArgs a;
+    a.t = t;
+    a.t_rs = t_rs;
+    a.gc = gc;
+    a.gy = gy;
+    a.sk = sk;
+    a.sp = sp;
+    a.off2 = off2;
+    a.split = split;
+    a.ni = ni;
+    a.N = N;
+    a.accumulate = accumulate;
+    const int threads = 128;
+    k_spline_adjoint<<<(ni + threads - 1) / threads, threads, 0, st>>>(a);
+    FEW_LAUNCH_CHECK("k_spline_adjoint");
+    return FEW_OK;
+}
+
+}  // namespace few
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int few_adjoint_phase(const void *grad, const void *W, const double *phase_coeffs, int N,
+                                 const double *seg_info, const int *units, int nunits, const int *row_m,
+                                 const int *row_k, int R, int nlo, int NN, double dt, int use_theta, double *partial,
+                                 void *stream)
+{
+    few::clear_error();
+    if (!grad || !W || !phase_coeffs || !seg_info || !units || !row_m || !row_k || !partial)
+        return few::fail(FEW_ERR_ARG, "few_adjoint_phase: null pointer");
+    if (N < 2 || nunits < 0 || R < 1 || R > few::kMaxRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase: bad sizes");
+    return few::launch_adj_phase((const double2 *)grad, (const double2 *)W, phase_coeffs, N, seg_info, units, nunits,
+                                 row_m, row_k, R, nlo, NN, dt, use_theta, partial, (cudaStream_t)stream);
+}
+
+extern "C" int few_adjoint_phase_reduce(const double *partial, const int *seg_units, int nseg, double *grad_pc,
+                                        void *stream)
+{
+    few::clear_error();
+    if (!partial || !seg_units || !grad_pc) return few::fail(FEW_ERR_ARG, "few_adjoint_phase_reduce: null pointer");
+    if (nseg < 0) return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_reduce: bad sizes");
+    return few::launch_adj_phase_reduce(partial, seg_units, nseg, grad_pc, (cudaStream_t)stream);
+}
+
+extern "C" int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, const double *seg_info,
+                             const int *seg_start, int nseg, const int *row_m, const int *row_k, int R, int nlo, int NN,
+                             double dt, int use_theta, void *G, void *stream)
+{
+    few::clear_error();
+    if (!grad || !phase_coeffs || !seg_info || !seg_start || !row_m || !row_k || !G)
+        return few::fail(FEW_ERR_ARG, "few_adjoint_G: null pointer");
+    if (N < 2 || nseg < 0 || nseg > N - 1 || R < 1 || R > few::kMaxRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_G: bad sizes");
+    return few::launch_adj_G((const double2 *)grad, phase_coeffs, N, seg_info, seg_start, nseg, row_m, row_k, R, nlo,
+                             NN, dt, use_theta, (double2 *)G, (cudaStream_t)stream);
+}
+
+extern "C" int few_unfold(const void *G, const void *ylms, const int *key_plus, const int *key_minus, int K, int N,
+                          int nseg, int nkeys, double *gcoef, void *stream)
+{
+    few::clear_error();
+    if (!G || !ylms || !key_plus || !key_minus || !gcoef) return few::fail(FEW_ERR_ARG, "few_unfold: null pointer");
+    if (K < 1 || N < 2 || nseg < 0 || nseg > N - 1 || nkeys < 1) return few::fail(FEW_ERR_SIZE, "few_unfold: bad sizes");
+    return few::launch_unfold((const double2 *)G, (const double2 *)ylms, key_plus, key_minus, K, N, nseg, nkeys, gcoef,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int few_spline_adjoint(const double *t, long long t_row_stride, double *gcoeffs, double *gy,
+                                  long long y_knot_stride, long long y_interp_stride, int y_split,
+                                  long long y_split_offset, int ninterps, int length, int accumulate, void *stream)
+{
+    few::clear_error();
+    if (!t || !gcoeffs || !gy) return few::fail(FEW_ERR_ARG, "few_spline_adjoint: null pointer");
+    if (ninterps < 1) return few::fail(FEW_ERR_SIZE, "few_spline_adjoint: ninterps=%d < 1", ninterps);
+    if (length < 4) return few::fail(FEW_ERR_SIZE, "few_spline_adjoint: length=%d < 4", length);
+    if (y_split < 0 || y_split > ninterps) return few::fail(FEW_ERR_ARG, "few_spline_adjoint: bad y_split");
+    return few::launch_spline_adjoint(t, t_row_stride, gcoeffs, gy, y_knot_stride, y_interp_stride, y_split,
+                                      y_split_offset, ninterps, length, accumulate, (cudaStream_t)stream);
+}

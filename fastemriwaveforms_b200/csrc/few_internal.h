@@ -52,6 +52,18 @@ int launch_sum_folded(double2 *wf, const double2 *W, const double *pc, int N, co
                       const int *units, int nunits, const int *row_m, const int *row_k, int R,
                       int nlo, int NN, double dt, int mode, int use_theta, cudaStream_t st);
 
+int launch_adj_phase(const double2 *grad, const double2 *W, const double *pc, int N, const double *seg_info,
+                     const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo, int NN,
+                     double dt, int use_theta, double *partial, cudaStream_t st);
+int launch_adj_phase_reduce(const double *partial, const int *seg_units, int nseg, double *grad_pc, cudaStream_t st);
+int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg_info, const int *seg_start, int nseg,
+                 const int *row_m, const int *row_k, int R, int nlo, int NN, double dt, int use_theta, double2 *G,
+                 cudaStream_t st);
+int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, const int *key_minus, int K, int N,
+                  int nseg, int nkeys, double *gcoef, cudaStream_t st);
+int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *gy, long long sk, long long sp,
+                          int split, long long off2, int ni, int N, int accumulate, cudaStream_t st);
+
 constexpr int kMaxRows = 256;        // distinct (m', k') rows of a fold plan
 constexpr int kDefaultChunk = 1024;  // output samples per work unit of the sum
 

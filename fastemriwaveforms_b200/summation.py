@@ -251,13 +251,25 @@ class _FoldPlan:
         self.key_ptr = key_ptr[: nkeys + 1].copy()
         self.key_list = key_list[: int(self.key_ptr[-1])].copy()
         self.K = K
-        host = np.concatenate([self.row_m, self.row_k, self.key_ptr, self.key_list]).astype(np.int32)
+        # key of each mode's + term and - term (-1: m = 0 has no - term)
+        self.key_plus = np.full(K, -1, np.int32)
+        self.key_minus = np.full(K, -1, np.int32)
+        for q in range(nkeys):
+            for code in self.key_list[self.key_ptr[q]:self.key_ptr[q + 1]]:
+                if code & 1:
+                    self.key_minus[code >> 1] = q
+                else:
+                    self.key_plus[code >> 1] = q
+        host = np.concatenate([self.row_m, self.row_k, self.key_ptr, self.key_list, self.key_plus,
+                               self.key_minus]).astype(np.int32)
         self.table = torch.from_numpy(host).to(device)
         o = 0
         self.d_row_m = self.table[o:o + self.R]; o += self.R
         self.d_row_k = self.table[o:o + self.R]; o += self.R
         self.d_key_ptr = self.table[o:o + nkeys + 1]; o += nkeys + 1
-        self.d_key_list = self.table[o:o + len(self.key_list)]
+        self.d_key_list = self.table[o:o + len(self.key_list)]; o += len(self.key_list)
+        self.d_key_plus = self.table[o:o + K]; o += K
+        self.d_key_minus = self.table[o:o + K]
 
 
 class _SegmentPlan:
@@ -279,6 +291,42 @@ class _SegmentPlan:
         self.d_seg_info = torch.from_numpy(self.seg_info_host.copy()).pin_memory().to(device, non_blocking=True)
         self.d_units = torch.from_numpy(self.units_host.copy() if self.nunits else np.zeros(3, np.int32)).pin_memory() \
             .to(device, non_blocking=True)
+        self._device = device
+
+    def backward_tables(self):
+        """Device (seg_start, seg_units), each (nseg+1,) int32, for the adjoint kernels."""
+        if not hasattr(self, "_bwd"):
+            seg_units = np.zeros(self.nseg + 1, np.int32)
+            useg = self.units_host.reshape(-1, 3)[:, 0] if self.nunits else np.zeros(0, np.int32)
+            seg_units[1:] = np.cumsum(np.bincount(useg, minlength=self.nseg)[: self.nseg])
+            host = np.concatenate([self.seg_start.astype(np.int32), seg_units])
+            t = torch.from_numpy(host).to(self._device)
+            self._bwd = (t[: self.nseg + 1], t[self.nseg + 1:])
+        return self._bwd
+
+
+class _Prepared:
+    """Inputs, plans and device tensors of one call (kept for the backward)."""
+
+
+class _ModeSumFunction(torch.autograd.Function):
+    """h = InterpolatedModeSum(teuk_modes, phase_interp_coeffs; fixed t, ylms, modes).
+
+    Backward: the adjoint kernels (phasors recomputed from the phase
+    polynomials, not stored; the folded coefficients W of the forward are kept)."""
+
+    @staticmethod
+    def forward(ctx, teuk, pc, module, prep, total):
+        out = torch.zeros(total, dtype=torch.complex128, device=prep.dev)
+        module._launch(prep, out)
+        prep.teuk_in = prep.pc_in = None  # do not keep the autograd inputs alive through ctx
+        ctx.prep = prep
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        g_teuk, g_pc = InterpolatedModeSum._backward(ctx.prep, grad, ctx.needs_input_grad[0], ctx.needs_input_grad[1])
+        return g_teuk, g_pc, None, None, None
 
 
 class InterpolatedModeSum(SummationBase):
@@ -315,9 +363,27 @@ class InterpolatedModeSum(SummationBase):
 
     def sum(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, *args,
             dt: float = 10.0, integrate_backwards: bool = False, **kwargs):
-        """Interpolated summation into ``self.waveform`` (``interpolatedmodesum.py:283-375``)."""
+        """Interpolated summation into ``self.waveform`` (``interpolatedmodesum.py:283-375``).
+
+        If ``teuk_modes`` or ``phase_interp_coeffs`` is a torch tensor that
+        requires grad (and grad mode is on), the waveform is the output of a
+        ``torch.autograd.Function`` whose backward runs the adjoint kernels."""
+        needs_grad = torch.is_grad_enabled() and any(
+            isinstance(x, torch.Tensor) and x.requires_grad for x in (teuk_modes, phase_interp_coeffs))
+        prep = self._prepare(t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr,
+                             dt, integrate_backwards, keep=needs_grad)
+        if needs_grad:
+            total = self.waveform.shape[0]
+            self.waveform = _ModeSumFunction.apply(prep.teuk_in, prep.pc_in, self, prep, total)
+        else:
+            self._launch(prep, self.waveform)
+        return self.waveform
+
+    def _prepare(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, dt,
+                 integrate_backwards, keep=False):
+        """Validates the inputs, makes the host plans and the device tensors."""
         dev = self.device
-        st = _stream(dev)
+        p = _Prepared()
         h_t = _to_host(t, np.float64)
         phase_t = _to_host(phase_interp_t, np.float64)
         if h_t.ndim != 1:
@@ -329,7 +395,9 @@ class InterpolatedModeSum(SummationBase):
             raise ValueError("t must increase strictly.")
         if len(phase_t) != N:
             raise ValueError("phase_interp_t must have the same length as t.")
-        teuk = _to_device(teuk_modes, torch.complex128, dev)
+        teuk_in = teuk_modes.to(device=dev, dtype=torch.complex128) if isinstance(teuk_modes, torch.Tensor) \
+            else _to_device(teuk_modes, torch.complex128, dev)
+        teuk = teuk_in.detach().contiguous()
         if teuk.ndim != 2 or teuk.shape[0] != N:
             raise ValueError("teuk_modes must have shape (len(t), num_teuk_modes).")
         K = int(teuk.shape[1])
@@ -341,49 +409,85 @@ class InterpolatedModeSum(SummationBase):
             raise ValueError("l_arr, m_arr, k_arr, n_arr must have num_teuk_modes entries.")
         if tuple(np.shape(ylms)) != (2 * K,):
             raise ValueError("ylms must have shape (2 * num_teuk_modes,).")
-        pcs = tuple(phase_interp_coeffs.shape)
-        if pcs != (N - 1, 3, 8):
+        if tuple(phase_interp_coeffs.shape) != (N - 1, 3, 8):
             raise ValueError("phase_interp_coeffs must have shape (len(t) - 1, 3, 8).")
-
         if integrate_backwards:
             # align the knots with t=0 as the reference does (interpolatedmodesum.py:341-345)
             offset = h_t[-1] - int(h_t[-1] / dt) * dt
             h_t = h_t - offset
             phase_t = phase_t - offset
-        t_dev = torch.from_numpy(h_t).to(dev)
-
+        pc_in = phase_interp_coeffs.to(device=dev, dtype=torch.float64) \
+            if isinstance(phase_interp_coeffs, torch.Tensor) else _to_device(phase_interp_coeffs, torch.float64, dev)
+        p.dev, p.st, p.N, p.K, p.dt = dev, _stream(dev), N, K, float(dt)
+        p.teuk, p.teuk_in, p.pc_in = teuk, (teuk_in if keep else None), (pc_in if keep else None)
+        p.t_dev = torch.from_numpy(h_t).to(dev)
         # ylms[K:] *= (-1)^l (interpolatedmodesum.py:357-358)
         sign = np.where(l_h % 2 == 0, 1.0, -1.0)
         ylm = _to_device(ylms, torch.complex128, dev).clone()
         ylm[K:] *= torch.from_numpy(sign).to(dev)
+        p.ylm = ylm
         # (N-1, 3, 8) -> (8, N-1, 3) (interpolatedmodesum.py:352-354)
-        pc = _to_device(phase_interp_coeffs, torch.float64, dev).permute(2, 0, 1).contiguous()
-        fold = self._fold_plan(m_h, k_h, n_h, dev)
-        seg = _SegmentPlan(h_t, phase_t, self.num_pts, dt, self.chunk, dev)
-        coeffs = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
-        W = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
+        p.pc = pc_in.detach().permute(2, 0, 1).contiguous()
+        p.fold = self._fold_plan(m_h, k_h, n_h, dev)
+        p.seg = _SegmentPlan(h_t, phase_t, self.num_pts, dt, self.chunk, dev)
+        p.out_len = int(self.num_pts)
+        return p
 
+    def _launch(self, p, out):
+        """Spline build, fold and sum into `out` (three launches on the current stream)."""
+        fold, seg, N, K, st = p.fold, p.seg, p.N, p.K, p.st
+        coeffs = torch.empty((4, N, 2 * K), dtype=torch.float64, device=p.dev)
+        W = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=p.dev)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if self.record_stages else None
         if ev:
             ev[0].record()
         # amplitude splines straight from the (N, K) complex array: real parts are
         # interpolants 0..K-1, imaginary parts K..2K-1 (interpolatedmodesum.py:331-337)
-        _lib.call("few_spline_build", _ptr(t_dev), 0, _ptr(teuk), 2 * K, 2, K, 1, 2 * K, N, _ptr(coeffs),
+        _lib.call("few_spline_build", _ptr(p.t_dev), 0, _ptr(p.teuk), 2 * K, 2, K, 1, 2 * K, N, _ptr(coeffs),
                   _lib.FEW_LAYOUT_KNOT_MAJOR, st)
         if ev:
             ev[1].record()
-        _lib.call("few_fold_coeffs", _ptr(coeffs), _ptr(ylm), _ptr(fold.d_key_ptr), _ptr(fold.d_key_list), K, N,
+        _lib.call("few_fold_coeffs", _ptr(coeffs), _ptr(p.ylm), _ptr(fold.d_key_ptr), _ptr(fold.d_key_list), K, N,
                   seg.nseg, fold.R, fold.NN, _ptr(W), st)
         if ev:
             ev[2].record()
-        _lib.call("few_sum_folded", _ptr(self.waveform), _ptr(W), _ptr(pc), N, _ptr(seg.d_seg_info),
+        _lib.call("few_sum_folded", _ptr(out), _ptr(W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
                   _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN,
-                  float(dt), _PRECISIONS[self.precision], fold.use_theta, st)
+                  p.dt, _PRECISIONS[self.precision], fold.use_theta, st)
         if ev:
             ev[3].record()
             self._stage_events = ev
         self._last_plan = (fold, seg)
-        return self.waveform
+        p.W = W
+        return out
+
+    @staticmethod
+    def _backward(p, grad, need_teuk=True, need_pc=True):
+        """Adjoint kernels: (dL/d teuk_modes (N, K) complex, dL/d phase_interp_coeffs (N-1, 3, 8))."""
+        fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
+        grad = grad[: p.out_len].to(torch.complex128).contiguous()
+        g_teuk = g_pc = None
+        if need_teuk:
+            seg_start, _ = seg.backward_tables()
+            G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
+            _lib.call("few_adjoint_G", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg_start), seg.nseg,
+                      _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta,
+                      _ptr(G), st)
+            gcoef = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
+            _lib.call("few_unfold", _ptr(G), _ptr(p.ylm), _ptr(fold.d_key_plus), _ptr(fold.d_key_minus), K, N,
+                      seg.nseg, fold.R * fold.NN, _ptr(gcoef), st)
+            g_teuk = torch.empty((N, K), dtype=torch.complex128, device=dev)
+            _lib.call("few_spline_adjoint", _ptr(p.t_dev), 0, _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N, 0,
+                      st)
+        if need_pc:
+            _, seg_units = seg.backward_tables()
+            partial = torch.empty((max(seg.nunits, 1), 24), dtype=torch.float64, device=dev)
+            _lib.call("few_adjoint_phase", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                      fold.NN, p.dt, fold.use_theta, _ptr(partial), st)
+            g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
+            _lib.call("few_adjoint_phase_reduce", _ptr(partial), _ptr(seg_units), seg.nseg, _ptr(g_pc), st)
+        return g_teuk, g_pc
 
     def stage_times(self) -> dict:
         """Kernel times (ms) of the last call with ``record_stages`` set:

@@ -200,6 +200,48 @@ FEW_API int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, 
                    int NN, double dt, int mode, int use_theta, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Adjoint (no counterpart in the reference: it has no gradients)           */
+/* ------------------------------------------------------------------------ */
+/* For L = Re sum_i g_i h_i.  `grad` [device] (out_len,) complex is torch's
+ * upstream gradient of the waveform, G = dL/dRe h + i dL/dIm h (so g = conj(G)).
+ * Phasors are recomputed from the phase polynomials, not stored.  All other
+ * arguments are the forward's. */
+
+/* dL/d(phase coefficients), per work unit: partial [device] (nunits, 24) =
+ * sum over the unit's samples of dL/dPhi_f(t_i) b_q(s_i), f = phi, theta, r,
+ * b_q the 8-term basis (1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3, s^4 s1^3). */
+FEW_API int few_adjoint_phase(const void *grad, const void *W, const double *phase_coeffs, int N,
+                              const double *seg_info, const int *units, int nunits, const int *row_m,
+                              const int *row_k, int R, int nlo, int NN, double dt, int use_theta, double *partial,
+                              void *stream);
+
+/* Sums the unit partials per segment in unit order: seg_units [device]
+ * (nseg+1,) = first unit of each segment; grad_pc [device] (nseg, 3, 8), the
+ * layout of phase_interp_coeffs. */
+FEW_API int few_adjoint_phase_reduce(const double *partial, const int *seg_units, int nseg, double *grad_pc,
+                                     void *stream);
+
+/* G [device] (nseg, R, NN, 4) complex: G[s][key][c] = sum over segment s's
+ * samples of g_i x_i^c exp(-i phase_key(t_i)).  seg_start [device] (nseg+1,). */
+FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, const double *seg_info,
+                          const int *seg_start, int nseg, const int *row_m, const int *row_k, int R, int nlo, int NN,
+                          double dt, int use_theta, void *G, void *stream);
+
+/* Transpose of few_fold_coeffs: gcoef [device] (4, N, 2K) = dL/d(spline
+ * coefficients) (zero at knots >= nseg).  key_plus, key_minus [device] (K,):
+ * key index of each mode's + and - term (-1: none). */
+FEW_API int few_unfold(const void *G, const void *ylms, const int *key_plus, const int *key_minus, int K, int N,
+                       int nseg, int nkeys, double *gcoef, void *stream);
+
+/* Transpose of few_spline_build (knot-major coefficients): gcoeffs [device]
+ * (4, length, ninterps) = dL/d(coefficients), overwritten as scratch; gy
+ * [device] receives dL/dy through the y view of few_spline_build (written, or
+ * added to when accumulate != 0). */
+FEW_API int few_spline_adjoint(const double *t, long long t_row_stride, double *gcoeffs, double *gy,
+                               long long y_knot_stride, long long y_interp_stride, int y_split,
+                               long long y_split_offset, int ninterps, int length, int accumulate, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */
 
