@@ -47,10 +47,14 @@ SIGNATURES = {
     "few_adjoint_G": [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp, _vp],
     "few_unfold": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
     "few_spline_adjoint": [_vp, _c_ll, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
+    "few_mixed_operand_bytes": [_c_int, _c_int, _c_int],
+    "few_fold_mixed": [_vp, _vp, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_sum_mixed": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
+                      _vp, _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
 }
-_RESTYPE = {"few_last_error": ctypes.c_char_p}
+_RESTYPE = {"few_last_error": ctypes.c_char_p, "few_mixed_operand_bytes": ctypes.c_longlong}
 
 _lock = threading.Lock()
 _lib = None

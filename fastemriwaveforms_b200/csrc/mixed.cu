@@ -1,0 +1,495 @@
+// Mixed-precision mode sum on the 5th-generation tensor cores (tcgen05).
+//
+// Per knot segment s the folded sum is a dense complex contraction
+//     Y[i, r] = sum_{c, n'} X[i, (c, n')] W'[(c, n'), r],   h_i = sum_r u_r(t_i) Y[i, r]
+// with X[i, (c, n')] = tau_i^c v_{n'}(t_i), tau = (t - t_s)/h_s in [0, 1),
+// W'[c] = W[c] h_s^c (the folded coefficients rescaled so every X entry has
+// modulus <= 1), v_{n'} = exp(-i n' Phi_r), u_r = exp(-i (m' Phi_phi + k' Phi_theta)).
+//
+// Precision plan:
+//   * FP64: the phase polynomials, the per-sample anchors exp(-i Phi) and the
+//     anchors of the n' recurrence (every 32 steps), each reduced mod 2 pi;
+//   * FP32: the phasor recurrence between anchors, the row phasors u_r, the
+//     epilogue sum over rows;
+//   * tensor cores: the contraction as a real GEMM
+//       [Re X | Im X interleaved] (128 x 2*4*NNp)  x  B (2*4*NNp x NB)
+//     in split BF16 (x = hi + lo, three products hi*hi + hi*lo + lo*hi) with
+//     FP32 accumulation in TMEM.  B's columns are (Re Y_r, Im Y_r) pairs,
+//     column 2r and 2r+1, padded to NB.
+//
+// Layout: A and B tiles are K-major, no swizzle: 8x8 bf16 core matrices of
+// 128 contiguous bytes; stride 128 B between the two K halves of a K=16 step
+// (LBO) and 256 B between 8-row groups (SBO).  One CTA of 128 threads owns a
+// work unit (<= 1024 samples of one segment); each thread owns one sample row of
+// a 128-sample tile.  Per 64-wide K chunk: threads write the chunk of A, copy
+// the segment's precomputed B chunk, one thread issues 12 tcgen05.mma (4 K-steps
+// x 3 split products) and commits to an mbarrier; every wait is bounded and a
+// timeout sets an error word and ends the kernel after freeing TMEM.
+#include <cuda_bf16.h>
+
+#include "few_common.cuh"
+#include "few_internal.h"
+
+namespace few {
+
+namespace {
+
+constexpr int kMT = 128;   // samples per tile (MMA M)
+constexpr int kKC = 64;    // real K per chunk
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s of global time per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait; false if the phase did not complete within kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (global_ns() - t0 < kWaitLimitNs)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100; base offset 0; no swizzle
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Byte offset of element (row, k) of a K-major, no-swizzle tile whose K-steps
+// of 16 hold `groups` 8-row groups: K-step stride groups*256, 8-row group
+// stride (SBO) 256, K-half stride (LBO) 128, row 16, element 2.
+__host__ __device__ __forceinline__ uint32_t tile_off(int row, int k, int groups)
+{
+    return (uint32_t)((k >> 4) * groups * 256 + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// x = hi + lo with hi, lo bf16, packed two complex numbers (re, im, re, im) at a time.
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    float2 hf = __bfloat1622float2(h);
+    __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<uint32_t *>(&h);
+    lo = *reinterpret_cast<uint32_t *>(&l);
+}
+
+__device__ __forceinline__ float2 fcmul(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 fcpow(float2 z, int p)
+{
+    if (p < 0) {
+        z.y = -z.y;
+        p = -p;
+    }
+    float2 r = make_float2(1.f, 0.f);
+    while (p) {
+        if (p & 1) r = fcmul(r, z);
+        p >>= 1;
+        if (p) z = fcmul(z, z);
+    }
+    return r;
+}
+
+// exp(-i phi) in FP64 with the argument reduced mod 2 pi first, rounded to FP32.
+__device__ __forceinline__ float2 anchor(double phi)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    const double k = rint(phi / two_pi);
+    const double red = fma(-k, two_pi, phi);
+    double s, c;
+    sincos(red, &s, &c);
+    return make_float2((float)c, (float)-s);
+}
+
+// ---------------------------------------------------------------------------
+// B operand: per segment and K chunk, hi and lo bf16 tiles in the smem layout.
+// ---------------------------------------------------------------------------
+__global__ void k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots, int nseg, int R,
+                             int NN, int NNp, int NB, int nchunks, __nv_bfloat16 *__restrict__ Bpk)
+{
+    const long long per_chunk = (long long)NB * kKC;
+    const long long total = (long long)nseg * nchunks * per_chunk;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int s = (int)(idx / (nchunks * per_chunk));
+    const long long rem = idx - (long long)s * nchunks * per_chunk;
+    const int ch = (int)(rem / per_chunk);
+    const int e = (int)(rem - (long long)ch * per_chunk);
+    const int j = e / kKC, kk = e - j * kKC;
+    const int kappa = ch * (kKC / 2) + (kk >> 1);
+    const int part = kk & 1;  // 0: multiplies Re X, 1: Im X
+    const int c = kappa / NNp, nidx = kappa - c * NNp;
+    double val = 0.0;
+    if (j < 2 * R && nidx < NN) {
+        const int r = j >> 1;
+        const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r
+        const double h = t_knots[s + 1] - t_knots[s];
+        const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
+        const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
+        const double wr = w.x * hc, wi = w.y * hc;
+        if (part == 0) val = im_col ? wi : wr;     // Re Y += Re X Re W ; Im Y += Re X Im W
+        else val = im_col ? wr : -wi;              // Re Y -= Im X Im W ; Im Y += Im X Re W
+    }
+    const float f = (float)val;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(f);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+    const uint32_t off = tile_off(j, kk, NB / 8) / 2;  // in elements
+    __nv_bfloat16 *base = Bpk + (((long long)s * nchunks + ch) * 2) * per_chunk;
+    base[off] = hi;
+    base[per_chunk + off] = lo;
+}
+
+struct MixedArgs {
+    double2 *wf;
+    const __nv_bfloat16 *Bpk;
+    const double *pc;
+    const double *seg_info;
+    const double *t_knots;
+    const int *units;
+    const int *row_m;
+    const int *row_k;
+    int *err;
+    int N, R, nlo, NN, NNp, NB, nchunks, use_theta, tmem_cols;
+    double dt;
+};
+
+__global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int NB = a.NB;
+    unsigned char *sA_hi = smem_raw;                   // 128 x 64 bf16 = 16 KB
+    unsigned char *sA_lo = sA_hi + kMT * kKC * 2;      // 16 KB
+    unsigned char *sB_hi = sA_lo + kMT * kKC * 2;      // NB x 64 bf16
+    unsigned char *sB_lo = sB_hi + NB * kKC * 2;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int u = blockIdx.x;
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
+    const int R = a.R, NN = a.NN, NNp = a.NNp, nlo = a.nlo;
+    const long long nps = (long long)(a.N - 1) * 3;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"((uint32_t)a.tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int r = tid; r < R; r += blockDim.x) {
+        s_rm[r] = a.row_m[r];
+        s_rk[r] = a.row_k[r];
+    }
+    if (tid < 24) {
+        const int q = tid >> 3, c = tid & 7;
+        s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_bf16(kMT, NB);
+    const uint32_t aH = smem_u32(sA_hi), aL = smem_u32(sA_lo), bH = smem_u32(sB_hi), bL = smem_u32(sB_lo);
+    const int halves = NNp / 32;
+    const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * a.nchunks * 2 * NB * kKC;
+    uint32_t phase = 0;
+    bool failed = false;
+
+    for (int base = lo; base < hi && !failed; base += kMT) {
+        const int i = base + tid;
+        const bool valid = i < hi;
+        // FP64 prelude: phases (interpolate.cu:626-644) and anchors
+        const double t = (double)i * a.dt;
+        const double x = t - t0;
+        const float tau = (float)(x / hs);
+        const double s = (t - pt0) / pw;
+        const double s1 = 1.0 - s;
+        const double Pp = phase_poly(s_pc, s, s1);
+        const double Pr = phase_poly(s_pc + 16, s, s1);
+        const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
+        const float2 Ep = anchor(Pp);
+        const float2 Er = anchor(Pr);
+        const float2 Et = a.use_theta ? anchor(Pt) : make_float2(1.f, 0.f);
+        const float taup[4] = {1.f, tau, tau * tau, tau * tau * tau};
+
+        for (int hh = 0; hh < halves && !failed; ++hh) {
+            const int n0 = nlo + 32 * hh;
+            float2 v[32];
+            v[0] = anchor((double)n0 * Pr);
+#pragma unroll
+            for (int q = 1; q < 32; ++q) v[q] = fcmul(v[q - 1], Er);
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                if (!valid || 32 * hh + q >= NN) v[q] = make_float2(0.f, 0.f);
+            for (int c = 0; c < 4 && !failed; ++c) {
+                const int ch = c * halves + hh;
+                const float sc = taup[c];
+                // A chunk, this thread's row: complex q -> real k = 2q (re), 2q+1 (im)
+#pragma unroll
+                for (int g = 0; g < 8; ++g) {  // 8 groups of 4 complex = 8 bf16 = 16 bytes
+                    uint32_t h4[4], l4[4];
+#pragma unroll
+                    for (int e2 = 0; e2 < 4; ++e2) {
+                        const float2 z = v[4 * g + e2];
+                        split2(sc * z.x, sc * z.y, h4[e2], l4[e2]);
+                    }
+                    const uint32_t off = tile_off(tid, 8 * g, kMT / 8);
+                    *reinterpret_cast<uint4 *>(sA_hi + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
+                    *reinterpret_cast<uint4 *>(sA_lo + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
+                }
+                // B chunk (hi then lo, contiguous) from global
+                {
+                    const uint4 *src = reinterpret_cast<const uint4 *>(Bseg + (long long)ch * 2 * NB * kKC);
+                    uint4 *dst = reinterpret_cast<uint4 *>(sB_hi);
+                    const int n16 = 2 * NB * kKC * 2 / 16;
+                    for (int q = tid; q < n16; q += blockDim.x) dst[q] = src[q];
+                }
+                fence_async_smem();
+                __syncthreads();
+                if (tid == 0) {
+                    tc_fence_after();
+#pragma unroll
+                    for (int st = 0; st < kKC / 16; ++st) {
+                        const uint64_t da_h = smem_desc(aH + st * (kMT / 8) * 256, 128, 256);
+                        const uint64_t da_l = smem_desc(aL + st * (kMT / 8) * 256, 128, 256);
+                        const uint64_t db_h = smem_desc(bH + st * (NB / 8) * 256, 128, 256);
+                        const uint64_t db_l = smem_desc(bL + st * (NB / 8) * 256, 128, 256);
+                        mma_bf16(tmem, da_h, db_h, idesc, (ch | st) != 0);
+                        mma_bf16(tmem, da_h, db_l, idesc, 1u);
+                        mma_bf16(tmem, da_l, db_h, idesc, 1u);
+                    }
+                    mma_commit(&s_bar);
+                }
+                const bool ok = mbar_wait_bounded(&s_bar, phase);
+                phase ^= 1u;
+                if (__syncthreads_or(!ok)) {
+                    failed = true;
+                    if (tid == 0) atomicExch(a.err, 1);
+                }
+            }
+        }
+        if (failed) break;
+        // epilogue: this thread's accumulator row (TMEM lane = tid), 8 rows (m', k')
+        // per 16-column load; u_r by one multiplication when m' steps by one
+        tc_fence_after();
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float hr = 0.f, hi_ = 0.f;
+        float2 uu = make_float2(1.f, 0.f);
+        int pm = 0x7fffffff, pk = 0x7fffffff;
+        for (int c0 = 0; c0 < NB; c0 += 16) {
+            float D[16];
+            tmem_ld16(trow + c0, D);
+            tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int r = (c0 >> 1) + q;
+                if (r < R) {
+                    const int mm = s_rm[r], kk = s_rk[r];
+                    if (kk == pk && mm == pm + 1) {
+                        uu = fcmul(uu, Ep);
+                    } else {
+                        uu = fcpow(Ep, mm);
+                        if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                    }
+                    pm = mm;
+                    pk = kk;
+                    const float yr = D[2 * q], yi = D[2 * q + 1];
+                    hr = fmaf(uu.x, yr, fmaf(-uu.y, yi, hr));
+                    hi_ = fmaf(uu.x, yi, fmaf(uu.y, yr, hi_));
+                }
+            }
+        }
+        if (valid) {
+            double2 o = a.wf[i];
+            o.x += (double)hr;
+            o.y += (double)hi_;
+            a.wf[i] = o;
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if (failed) {
+        // let any MMA still in flight finish before TMEM is released
+        if (tid == 0) mbar_wait_bounded(&s_bar, phase);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)a.tmem_cols)
+                     : "memory");
+    }
+}
+
+}  // namespace
+
+int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
+{
+    if (2 * R > 256) return fail(FEW_ERR_SIZE, "mixed sum: %d rows exceed the 128 the tensor-core tile holds", R);
+    *NNp = (NN + 31) / 32 * 32;
+    *NB = std::max(16, (2 * R + 15) / 16 * 16);
+    *nchunks = 4 * (*NNp) / 32;
+    int cols = 32;
+    while (cols < *NB) cols <<= 1;
+    *tmem_cols = cols;
+    return FEW_OK;
+}
+
+size_t mixed_bpk_bytes(int nseg, int R, int NN)
+{
+    int NNp, NB, nch, cols;
+    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols)) return 0;
+    return (size_t)nseg * nch * 2 * NB * kKC * sizeof(__nv_bfloat16);
+}
+
+int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, cudaStream_t st)
+{
+    int NNp, NB, nch, cols;
+    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols);
+    if (rc) return rc;
+    const long long total = (long long)nseg * nch * NB * kKC;
+    if (total == 0) return FEW_OK;
+    const int threads = 256;
+    k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NNp, NB, nch,
+                                                                                 (__nv_bfloat16 *)Bpk);
+    FEW_LAUNCH_CHECK("k_fold_mixed");
+    return FEW_OK;
+}
+
+int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, const double *seg_info,
+                     const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k, int R,
+                     int nlo, int NN, double dt, int use_theta, int *err, cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    MixedArgs a;
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols);
+    if (rc) return rc;
+    a.wf = wf;
+    a.Bpk = (const __nv_bfloat16 *)Bpk;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.t_knots = t_knots;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.err = err;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const size_t smem = (size_t)2 * kMT * kKC * 2 + (size_t)2 * a.NB * kKC * 2;
+    FEW_CUDA_TRY(cudaFuncSetAttribute(k_sum_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_sum_mixed<<<nunits, kMT, smem, st>>>(a);
+    FEW_LAUNCH_CHECK("k_sum_mixed");
+    return FEW_OK;
+}
+
+}  // namespace few
+
+extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream)
+{
+    few::clear_error();
+    if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed: null pointer");
+    if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed: bad sizes");
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, Bpk, (cudaStream_t)stream);
+}
+
+extern "C" long long few_mixed_operand_bytes(int nseg, int R, int NN)
+{
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN);
+}
+
+extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
+                             const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
+                             int R, int nlo, int NN, double dt, int use_theta, int *err, void *stream)
+{
+    few::clear_error();
+    if (!wf || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !err)
+        return few::fail(FEW_ERR_ARG, "few_sum_mixed: null pointer");
+    if (N < 2 || nunits < 0 || R < 1 || R > 128 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_sum_mixed: bad sizes");
+    return few::launch_sum_mixed((double2 *)wf, Bpk, phase_coeffs, N, seg_info, t_knots, units, nunits, row_m, row_k,
+                                 R, nlo, NN, dt, use_theta, err, (cudaStream_t)stream);
+}

@@ -13,7 +13,11 @@ path.  Extra keyword ``precision`` of ``InterpolatedModeSum``:
 * ``"faithful"`` (default) -- FP64, replays the reference's rounding of each
   mode phase, so results match the reference CPU path to ~1e-15 relative L2;
 * ``"exact"`` -- FP64, mode phasors by recurrence with no rounding of the
-  combined phase (more accurate than the reference, ~2x less FP64 work).
+  combined phase (more accurate than the reference, ~2x less FP64 work);
+* ``"mixed"`` -- FP64 phases and anchors, FP32 phasor recurrence, the
+  per-segment contraction on the tcgen05 tensor cores in split BF16 with FP32
+  accumulation (waveform mismatch ~1e-10 against FP64).  Gradients of a mixed
+  forward are computed by the FP64 adjoint.
 """
 from __future__ import annotations
 
@@ -28,7 +32,7 @@ from .synthetic import YRSID_SI, output_length
 
 logger = logging.getLogger("few")
 
-_PRECISIONS = {"faithful": _lib.FEW_SUM_FAITHFUL, "exact": _lib.FEW_SUM_EXACT}
+_PRECISIONS = {"faithful": _lib.FEW_SUM_FAITHFUL, "exact": _lib.FEW_SUM_EXACT, "mixed": -1}
 DEFAULT_CHUNK = 1024  # output samples per work unit of the sum kernel
 
 
@@ -348,6 +352,12 @@ class InterpolatedModeSum(SummationBase):
         self._fold_cache: OrderedDict = OrderedDict()
         self.record_stages = False  # set True to time the kernels of each call with CUDA events
         self._stage_events = None
+        self._mixed_err = None
+
+    def mixed_error(self) -> bool:
+        """True if a tensor-core wait of a mixed-precision call timed out (the
+        kernel then stopped early and its output is incomplete).  Synchronises."""
+        return bool(self._mixed_err is not None and int(self._mixed_err.item()) != 0)
 
     def _fold_plan(self, m, k, n, device) -> _FoldPlan:
         key = (m.tobytes(), k.tobytes(), n.tobytes(), str(device))
@@ -451,9 +461,21 @@ class InterpolatedModeSum(SummationBase):
                   seg.nseg, fold.R, fold.NN, _ptr(W), st)
         if ev:
             ev[2].record()
-        _lib.call("few_sum_folded", _ptr(out), _ptr(W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
-                  _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN,
-                  p.dt, _PRECISIONS[self.precision], fold.use_theta, st)
+        if self.precision == "mixed":
+            nbytes = int(_lib.load().few_mixed_operand_bytes(max(seg.nseg, 1), fold.R, fold.NN))
+            if nbytes <= 0:
+                raise ValueError("precision='mixed' supports at most 128 (m, k) rows")
+            Bpk = torch.empty(nbytes, dtype=torch.uint8, device=p.dev)
+            if self._mixed_err is None or self._mixed_err.device != p.dev:
+                self._mixed_err = torch.zeros(1, dtype=torch.int32, device=p.dev)
+            _lib.call("few_fold_mixed", _ptr(W), _ptr(p.t_dev), seg.nseg, fold.R, fold.NN, _ptr(Bpk), st)
+            _lib.call("few_sum_mixed", _ptr(out), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(p.t_dev),
+                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                      fold.NN, p.dt, fold.use_theta, _ptr(self._mixed_err), st)
+        else:
+            _lib.call("few_sum_folded", _ptr(out), _ptr(W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                      fold.NN, p.dt, _PRECISIONS[self.precision], fold.use_theta, st)
         if ev:
             ev[3].record()
             self._stage_events = ev

@@ -200,6 +200,31 @@ FEW_API int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, 
                    int NN, double dt, int mode, int use_theta, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Mixed-precision sum on tcgen05 tensor cores (no counterpart in the        */
+/* reference, which computes in FP64 only)                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of the tensor-core B operand for nseg segments of an R x NN fold grid
+ * (0 if R > 128). */
+FEW_API long long few_mixed_operand_bytes(int nseg, int R, int NN);
+
+/* Packs the folded coefficients W (few_fold_coeffs) into the split-BF16 B
+ * operand Bpk [device] (few_mixed_operand_bytes bytes): per segment the
+ * coefficients are rescaled by h_s^c (h_s = t_knots[s+1] - t_knots[s]) and laid
+ * out in the tensor-core tile order.  t_knots [device] (N,). */
+FEW_API int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream);
+
+/* Mixed-precision sum into wf [device] (out_len,) complex (accumulated):
+ * FP64 phases, anchors and mod-2pi reduction; FP32 phasor recurrence
+ * re-anchored every 32 n' steps; the per-segment contraction on tcgen05 in
+ * split BF16 with FP32 accumulation.  Arguments as few_sum_folded plus
+ * t_knots [device] (N,) and err [device] int (set to 1 if a tensor-core wait
+ * timed out; the kernel then stops early).  R <= 128. */
+FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
+                          const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
+                          int R, int nlo, int NN, double dt, int use_theta, int *err, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Adjoint (no counterpart in the reference: it has no gradients)           */
 /* ------------------------------------------------------------------------ */
 /* For L = Re sum_i g_i h_i.  `grad` [device] (out_len,) complex is torch's

@@ -1,0 +1,51 @@
+"""The mixed-precision (tcgen05, split-BF16) sum against the FP64 sum:
+waveform mismatch (1 - overlap, src/few/utils/utility.py:16-95) <= 1e-8 and
+relative L2 error <= 1e-4; the max relative error is printed."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_case
+from fastemriwaveforms_b200 import InterpolatedModeSum, get_mismatch
+from fastemriwaveforms_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+MISMATCH_MAX = 1e-8
+REL_L2_MAX = 1e-4
+
+
+def run(inp, precision):
+    ims = InterpolatedModeSum(precision=precision)
+    wf = ims(*inp.call_args(), T=inp.T, dt=inp.dt)
+    torch.cuda.synchronize()
+    if precision == "mixed":
+        assert not ims.mixed_error(), "a tensor-core wait timed out"
+    return wf.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["theta", "m0", "plain_small", "plain_full"])
+def test_mixed_matches_fp64(cuda, case):
+    if case == "theta":
+        inp, _ = load_case("sum_small_theta.npz")
+    elif case == "m0":
+        inp, _ = load_case("sum_small_m0.npz")
+    elif case == "plain_small":
+        inp = S.plain_small()
+    else:
+        inp = S.plain_full()
+    ref = run(inp, "exact")
+    got = run(inp, "mixed")
+    mm = get_mismatch(got, ref)
+    rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    maxrel = float(np.abs(got - ref).max() / np.abs(ref).max())
+    print(f"{case}: mismatch {mm:.3e}, relative L2 {rel:.3e}, max |dh| / max |h| {maxrel:.3e}")
+    assert mm <= MISMATCH_MAX
+    assert rel <= REL_L2_MAX
+
+
+def test_mixed_deterministic(cuda):
+    inp = S.plain_small()
+    a = run(inp, "mixed")
+    b = run(inp, "mixed")
+    assert np.array_equal(a, b)
