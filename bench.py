@@ -269,6 +269,69 @@ def fp64_peak(device) -> float:
     return best
 
 
+def time_forward(ims, call_args, inp, steps, warmup):
+    """Device time per forward (ms) and mean per-stage kernel times."""
+    import torch
+
+    for _ in range(warmup):
+        ims(*call_args, T=inp.T, dt=inp.dt)
+    torch.cuda.synchronize()
+    ims.record_stages = True
+    evs = []
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        ims(*call_args, T=inp.T, dt=inp.dt)
+        evs.append(ims._stage_events)
+    b.record()
+    torch.cuda.synchronize()
+    ims.record_stages = False
+    stage = {name: statistics.mean(ev[i].elapsed_time(ev[i + 1]) for ev in evs)
+             for i, name in enumerate(("spline", "fold", "sum"))}
+    return a.elapsed_time(b) / steps, stage
+
+
+def time_fwd_bwd(precision, inp, dev, steps, warmup):
+    """Forward + backward through torch.autograd (dL/d amplitude knots and
+    dL/d phase coefficients), upstream gradient conj(h_ref + w) with w white,
+    sigma = 0.1 rms(h_ref).  Device time per step (ms)."""
+    import torch
+
+    from fastemriwaveforms_b200 import InterpolatedModeSum
+
+    ims = InterpolatedModeSum(precision=precision)
+    teuk = torch.from_numpy(inp.teuk_modes).to(dev).requires_grad_(True)
+    pc = torch.from_numpy(inp.phase_coeffs).to(dev).requires_grad_(True)
+    ylms = torch.from_numpy(inp.ylms).to(dev)
+    with torch.no_grad():
+        h_ref = InterpolatedModeSum(precision="exact")(inp.t, teuk.detach(), ylms, inp.phase_t, pc.detach(), inp.l,
+                                                       inp.m, inp.k, inp.n, T=inp.T, dt=inp.dt)
+        gen = torch.Generator(device=dev).manual_seed(11)
+        rms = torch.sqrt(torch.mean(torch.abs(h_ref) ** 2))
+        w = torch.complex(torch.randn(h_ref.shape, generator=gen, device=dev, dtype=torch.float64),
+                          torch.randn(h_ref.shape, generator=gen, device=dev, dtype=torch.float64))
+        upstream = torch.conj(h_ref + 0.1 * rms * w / np.sqrt(2.0))
+
+    def step():
+        teuk.grad = None
+        pc.grad = None
+        h = ims(inp.t, teuk, ylms, inp.phase_t, pc, inp.l, inp.m, inp.k, inp.n, T=inp.T, dt=inp.dt)
+        h.backward(upstream)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, teuk.grad.detach().clone(), pc.grad.detach().clone()
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -382,12 +445,58 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(T * 16),
                "ms_per_step": ems / args.steps}
 
+    # ---- the other forms on the same waveform ----------------------------------------
+    from fastemriwaveforms_b200 import get_mismatch
+
+    forms = {}
+    ref_wf = ims(*call_args, T=inp.T, dt=inp.dt).clone()
+    pk, pk_kind = peaks()
+    for prec in ("exact", "mixed"):
+        other = InterpolatedModeSum(precision=prec)
+        ms_o, st_o = time_forward(other, call_args, inp, args.steps, 2)
+        wf_o = other(*call_args, T=inp.T, dt=inp.dt)
+        torch.cuda.synchronize()
+        d = (wf_o - ref_wf)
+        entry = {"ms_per_step": ms_o, "value": world * K * T / (ms_o * 1e-3), "stage_ms": st_o,
+                 "mismatch_vs_faithful": get_mismatch(wf_o, ref_wf),
+                 "rel_l2_vs_faithful": float(torch.linalg.norm(d) / torch.linalg.norm(ref_wf)),
+                 "max_rel_vs_faithful": float(d.abs().max() / ref_wf.abs().max())}
+        if prec == "mixed":
+            f_ = other._last_plan[0]
+            nnp = (f_.NN + 31) // 32 * 32
+            nb = max(16, (2 * f_.R + 15) // 16 * 16)
+            tflop = 2.0 * (8 * nnp) * nb * 3 * T / 1e12
+            entry["mixed_error"] = other.mixed_error()
+            entry["roofline"] = {"bound": "tensor", "kernel": "k_sum_mixed (+ k_fold_mixed)",
+                                 "achieved": tflop / (st_o["sum"] * 1e-3), "peak": pk["bf16_tflops"],
+                                 "unit": "TFLOP/s", "frac": tflop / (st_o["sum"] * 1e-3) / pk["bf16_tflops"],
+                                 "peak_source": f"{pk_kind} bf16_tflops (burst)",
+                                 "algorithmic": f"2 x {8 * nnp} x {nb} x 3 split products per sample"}
+        forms[prec] = entry
+    fb = {}
+    for prec in ("exact", "mixed"):
+        ms_fb, gt, gp = time_fwd_bwd(prec, inp, dev, max(2, args.steps // 2), 1)
+        fb[prec] = {"ms_per_step": ms_fb}
+        if prec == "exact":
+            g_ref = (gt, gp)
+        else:
+            fb[prec]["grad_rel_l2_vs_exact"] = {
+                "amplitude_knots": float(torch.linalg.norm(gt - g_ref[0]) / torch.linalg.norm(g_ref[0])),
+                "phase_coeffs": float(torch.linalg.norm(gp - g_ref[1]) / torch.linalg.norm(g_ref[1]))}
+    del g_ref
+    # the adjoint workload: K=1000, N=500, 1,000,000 samples
+    from fastemriwaveforms_b200 import synthetic as S
+
+    adj = S.adjoint_case(seed=4 + rank)
+    fb_adj = {"workload": f"K={adj.num_modes}, N={adj.num_knots}, T={adj.out_len}"}
+    for prec in ("exact", "mixed"):
+        fb_adj[prec] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1)[0]}
+
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
     flops_per_key_sample = 30 if args.precision == "faithful" else 20
     sum_flops = float(keys) * T * flops_per_key_sample
     achieved = sum_flops / (stage["sum"] * 1e-3) / 1e12
-    pk, pk_kind = peaks()
     spline_bytes = 40.0 * inp.num_knots * 2 * K
     roofline = {"bound": "fp64", "kernel": "k_sum_folded", "achieved": achieved, "peak": fp64_tflops,
                 "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": None,
@@ -411,7 +520,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "cpu_baseline": cpu, "clocks": clk,
+            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "cpu_baseline": cpu, "clocks": clk,
             "device": torch.cuda.get_device_name(dev)}
     print(json.dumps(line), flush=True)
     if world > 1:
