@@ -42,14 +42,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["faithful", "exact"], default="faithful")
+    ap.add_argument("--precision", choices=["faithful", "exact", "mixed"], default="faithful")
     ap.add_argument("--workload", choices=["plain_full", "plain_small"], default="plain_full")
     ap.add_argument("--cpu-samples", type=int, default=60000,
                     help="output samples of the bounded single-core reference run (cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile", action="store_true",
-                    help="only run warmup + steps forward calls (for ncu captures); prints no JSON line")
+                    help="only run warmup + steps calls (for ncu captures); prints no JSON line")
+    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd"], default="forward",
+                    help="with --profile: forward calls, or forward+backward through autograd")
     return ap.parse_args()
 
 
@@ -371,8 +373,11 @@ def main():
     call_args = (inp.t, teuk_d, ylms_d, inp.phase_t, pc_d, inp.l, inp.m, inp.k, inp.n)
 
     if args.profile:
-        for _ in range(args.warmup + args.steps):
-            ims(*call_args, T=inp.T, dt=inp.dt)
+        if args.profile_form == "fwd_bwd":
+            time_fwd_bwd(args.precision, inp, dev, args.steps, args.warmup)
+        else:
+            for _ in range(args.warmup + args.steps):
+                ims(*call_args, T=inp.T, dt=inp.dt)
         torch.cuda.synchronize()
         return 0
 

@@ -24,6 +24,7 @@ FEW_SUM_FAITHFUL = 0
 FEW_SUM_EXACT = 1
 FEW_LAYOUT_KNOT_MAJOR = 0
 FEW_LAYOUT_INTERP_MAJOR = 1
+FEW_FAC_WIDTH = 12
 
 _c_int, _c_ll, _c_dbl, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p
 
@@ -35,6 +36,8 @@ SIGNATURES = {
     "few_get_waveform": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp, _c_int, _vp],
     "few_spline_build": [_vp, _c_ll, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp],
     "few_spline_eval": [_vp, _c_ll, _vp, _c_int, _c_int, _vp, _c_ll, _c_int, _c_int, _vp, _vp, _vp],
+    "few_spline_factor": [_vp, _c_int, _vp],
+    "few_spline_build_factored": [_vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp],
     "few_fold_plan": [_vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp],
     "few_segment_plan": [_vp, _vp, _c_int, _c_int, _c_dbl, _c_int, _c_int, _vp, _vp, _vp, _vp],
     "few_fold_coeffs": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
@@ -46,6 +49,7 @@ SIGNATURES = {
     "few_adjoint_phase_reduce": [_vp, _vp, _c_int, _vp, _vp],
     "few_adjoint_G": [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp, _vp],
     "few_unfold": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_spline_adjoint_factored": [_vp, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
     "few_spline_adjoint": [_vp, _c_ll, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
     "few_mixed_operand_bytes": [_c_int, _c_int, _c_int],
     "few_fold_mixed": [_vp, _vp, _c_int, _c_int, _c_int, _vp, _vp],

@@ -20,29 +20,30 @@ import numpy as np
 import torch
 
 from . import _lib
-from .summation import InterpolatedModeSum, _device, _ptr, _stream, _to_device
+from .summation import InterpolatedModeSum, _device, _ptr, _stream, _to_device, spline_factor_table
 
 
 class _SplineFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, y, t):
+    def forward(ctx, y, fac):
         ni, N = y.shape
         dev = y.device
         coeffs = torch.empty((4, N, ni), dtype=torch.float64, device=dev)
         yc = y.detach().contiguous()
-        _lib.call("few_spline_build", _ptr(t), 0, _ptr(yc), 1, N, ni, 0, ni, N, _ptr(coeffs),
+        _lib.call("few_spline_build_factored", _ptr(fac), _ptr(yc), 1, N, ni, 0, ni, N, _ptr(coeffs),
                   _lib.FEW_LAYOUT_KNOT_MAJOR, _stream(dev))
-        ctx.save_for_backward(t)
+        ctx.save_for_backward(fac)
         ctx.shape = (ni, N)
         return coeffs
 
     @staticmethod
     def backward(ctx, grad):
-        (t,) = ctx.saved_tensors
+        (fac,) = ctx.saved_tensors
         ni, N = ctx.shape
         gc = grad.to(torch.float64).contiguous().clone()  # consumed by the adjoint kernel
         gy = torch.empty((ni, N), dtype=torch.float64, device=grad.device)
-        _lib.call("few_spline_adjoint", _ptr(t), 0, _ptr(gc), _ptr(gy), 1, N, ni, 0, ni, N, 0, _stream(grad.device))
+        _lib.call("few_spline_adjoint_factored", _ptr(fac), _ptr(gc), _ptr(gy), 1, N, ni, 0, ni, N, 0,
+                  _stream(grad.device))
         return gy, None
 
 
@@ -53,10 +54,10 @@ def spline_coefficients(t, y: torch.Tensor) -> torch.Tensor:
     y = y if isinstance(y, torch.Tensor) else _to_device(y, torch.float64, dev)
     if y.ndim == 1:
         y = y[None, :]
-    t_dev = _to_device(t, torch.float64, y.device)
-    if t_dev.ndim != 1 or t_dev.shape[0] != y.shape[1] or y.shape[1] < 4:
+    t_h = t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t, dtype=np.float64)
+    if t_h.ndim != 1 or t_h.shape[0] != y.shape[1] or y.shape[1] < 4:
         raise ValueError("t must be (N,) with N >= 4 matching y's last axis.")
-    return _SplineFunction.apply(y.to(torch.float64), t_dev)
+    return _SplineFunction.apply(y.to(torch.float64), spline_factor_table(t_h, y.device))
 
 
 def phase_coeffs_from_knots(t, phase_knots: torch.Tensor) -> torch.Tensor:

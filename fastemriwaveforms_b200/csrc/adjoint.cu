@@ -224,121 +224,122 @@ struct AdjGArgs {
     double dt;
 };
 
-constexpr int kGTile = 32;    // samples per shared-memory tile
-constexpr int kGKeys = 6;     // keys per thread per pass (256*6 = 1536 keys per pass)
+constexpr int kGTile = 24;  // samples per shared-memory tile
+constexpr int kGCols = 64;  // n' columns per CTA (one per thread of a row block)
+constexpr int kGRowBlocks = kAdjThreads / kGCols;  // 4 row blocks per CTA
 
+// grid (nseg, row groups of 4*RB rows, column groups of 64): thread (row block
+// rb, column c) owns keys (r = group*4*RB + rb*RB + q, n' = c) for q < RB and
+// accumulates their four x^c sums over every sample of the segment.  The column
+// phasor v_{n'}(t_i) is read once per sample and used for RB rows; the row
+// factors g_i u_r(t_i) are warp-wide broadcasts.
+template <int RB>
 __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_G(AdjGArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int R = a.R, NN = a.NN;
-    double2 *s_gu = reinterpret_cast<double2 *>(smem_raw);  // [kGTile][R]   g_i u_r(t_i)
-    double2 *s_v = s_gu + kGTile * R;                         // [kGTile][NN]  v_{n'}(t_i)
-    double *s_x = reinterpret_cast<double *>(s_v + kGTile * NN);  // [kGTile][4] x^0..x^3
-    double2 *s_E = reinterpret_cast<double2 *>(s_x + kGTile * 4);  // [kGTile][4] Ep, Er, Et, g
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    constexpr int RG = kGRowBlocks * RB;  // rows per CTA
+    __shared__ double2 s_gu[kGTile][RG];
+    __shared__ double2 s_v[kGTile][kGCols];
+    __shared__ double s_x[kGTile][4];
+    __shared__ double2 s_E[kGTile][4];  // Ep, Er, Et, g
+    __shared__ int s_rm[RG], s_rk[RG];
     __shared__ double s_pc[24];
 
+    const int R = a.R, NN = a.NN;
     const int seg = blockIdx.x;
+    const int r0 = blockIdx.y * RG, c0 = blockIdx.z * kGCols;
     const int lo = a.seg_start[seg], hi = a.seg_start[seg + 1];
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const long long nps = (long long)(a.N - 1) * 3;
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
-        s_rm[r] = a.row_m[r];
-        s_rk[r] = a.row_k[r];
+    const int tid = threadIdx.x;
+    const int col = tid % kGCols, rb = tid / kGCols;
+    for (int r = tid; r < RG; r += blockDim.x) {
+        s_rm[r] = (r0 + r < R) ? a.row_m[r0 + r] : 0;
+        s_rk[r] = (r0 + r < R) ? a.row_k[r0 + r] : 0;
     }
-    if (threadIdx.x < 24) {
-        const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
-        s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
+    if (tid < 24) {
+        const int q = tid >> 3, c = tid & 7;
+        s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
     }
-    double2 acc[kGKeys][4];
+    double acc[RB][4][2];
 #pragma unroll
-    for (int k = 0; k < kGKeys; ++k)
+    for (int q = 0; q < RB; ++q)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[k][c] = make_double2(0.0, 0.0);
-    int kr[kGKeys], kc[kGKeys];
-#pragma unroll
-    for (int k = 0; k < kGKeys; ++k) {
-        const int key = a.key_base + threadIdx.x + k * kAdjThreads;
-        kr[k] = key / NN;
-        kc[k] = key - kr[k] * NN;
-        if (threadIdx.x + k * kAdjThreads >= a.nkeys_pass) kr[k] = -1;
-    }
+        for (int c = 0; c < 4; ++c) acc[q][c][0] = acc[q][c][1] = 0.0;
     __syncthreads();
 
     for (int i0 = lo; i0 < hi; i0 += kGTile) {
         const int ns = min(kGTile, hi - i0);
-        // per-sample scalars
-        if (threadIdx.x < ns) {
-            const int i = i0 + threadIdx.x;
+        if (tid < ns) {
+            const int i = i0 + tid;
             const double t = rmul(a.dt, (double)i);
             const double x = rsub(t, t0);
             const double s = __ddiv_rn(rsub(t, pt0), pw);
             const double s1 = rsub(1.0, s);
             double sn, cs;
             sincos(phase_poly(s_pc, s, s1), &sn, &cs);
-            s_E[threadIdx.x * 4 + 0] = make_double2(cs, -sn);
+            s_E[tid][0] = make_double2(cs, -sn);
             sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
-            s_E[threadIdx.x * 4 + 1] = make_double2(cs, -sn);
+            s_E[tid][1] = make_double2(cs, -sn);
             if (a.use_theta) {
                 sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
-                s_E[threadIdx.x * 4 + 2] = make_double2(cs, -sn);
+                s_E[tid][2] = make_double2(cs, -sn);
             } else {
-                s_E[threadIdx.x * 4 + 2] = make_double2(1.0, 0.0);
+                s_E[tid][2] = make_double2(1.0, 0.0);
             }
             const double2 G = a.grad[i];
-            s_E[threadIdx.x * 4 + 3] = make_double2(G.x, -G.y);  // g = conj(G)
-            s_x[threadIdx.x * 4 + 0] = 1.0;
-            s_x[threadIdx.x * 4 + 1] = x;
-            s_x[threadIdx.x * 4 + 2] = x * x;
-            s_x[threadIdx.x * 4 + 3] = x * x * x;
+            s_E[tid][3] = make_double2(G.x, -G.y);  // g = conj(G)
+            s_x[tid][0] = 1.0;
+            s_x[tid][1] = x;
+            s_x[tid][2] = x * x;
+            s_x[tid][3] = x * x * x;
         }
         __syncthreads();
-        // tables: g u_r (rows) and v_{n'} (columns, runs of 8 by recurrence)
-        for (int w = threadIdx.x; w < ns * R; w += blockDim.x) {
-            const int j = w / R, r = w - j * R;
-            double2 uu = cpow_int(s_E[j * 4 + 0], s_rm[r]);
-            if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[j * 4 + 2], s_rk[r]));
-            s_gu[j * R + r] = cmul(s_E[j * 4 + 3], uu);
+        // tables: g u_r for this CTA's rows, v_{n'} for its columns (runs of 8 by recurrence)
+        for (int w = tid; w < ns * RG; w += blockDim.x) {
+            const int j = w / RG, r = w - j * RG;
+            double2 uu = cpow_int(s_E[j][0], s_rm[r]);
+            if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[j][2], s_rk[r]));
+            s_gu[j][r] = cmul(s_E[j][3], uu);
         }
-        const int runs = (NN + 7) / 8;
-        for (int w = threadIdx.x; w < ns * runs; w += blockDim.x) {
-            const int j = w / runs, b = w - j * runs;
-            const double2 Er = s_E[j * 4 + 1];
-            double2 v = cpow_int(Er, a.nlo + 8 * b);
-            const int cend = min(NN, 8 * b + 8);
-            for (int c = 8 * b; c < cend; ++c) {
-                s_v[j * NN + c] = v;
+        for (int w = tid; w < ns * (kGCols / 8); w += blockDim.x) {
+            const int j = w / (kGCols / 8), b = w - j * (kGCols / 8);
+            const double2 Er = s_E[j][1];
+            double2 v = cpow_int(Er, a.nlo + c0 + 8 * b);
+#pragma unroll
+            for (int c = 8 * b; c < 8 * b + 8; ++c) {
+                s_v[j][c] = v;
                 v = cmul(v, Er);
             }
         }
         __syncthreads();
         for (int j = 0; j < ns; ++j) {
-            const double x1 = s_x[j * 4 + 1], x2 = s_x[j * 4 + 2], x3 = s_x[j * 4 + 3];
+            const double2 v = s_v[j][col];
+            const double x1 = s_x[j][1], x2 = s_x[j][2], x3 = s_x[j][3];
 #pragma unroll
-            for (int k = 0; k < kGKeys; ++k) {
-                if (kr[k] >= 0) {
-                    const double2 z = cmul(s_gu[j * R + kr[k]], s_v[j * NN + kc[k]]);
-                    acc[k][0].x += z.x;
-                    acc[k][0].y += z.y;
-                    acc[k][1].x = fma(x1, z.x, acc[k][1].x);
-                    acc[k][1].y = fma(x1, z.y, acc[k][1].y);
-                    acc[k][2].x = fma(x2, z.x, acc[k][2].x);
-                    acc[k][2].y = fma(x2, z.y, acc[k][2].y);
-                    acc[k][3].x = fma(x3, z.x, acc[k][3].x);
-                    acc[k][3].y = fma(x3, z.y, acc[k][3].y);
-                }
+            for (int q = 0; q < RB; ++q) {
+                const double2 z = cmul(s_gu[j][rb * RB + q], v);
+                acc[q][0][0] += z.x;
+                acc[q][0][1] += z.y;
+                acc[q][1][0] = fma(x1, z.x, acc[q][1][0]);
+                acc[q][1][1] = fma(x1, z.y, acc[q][1][1]);
+                acc[q][2][0] = fma(x2, z.x, acc[q][2][0]);
+                acc[q][2][1] = fma(x2, z.y, acc[q][2][1]);
+                acc[q][3][0] = fma(x3, z.x, acc[q][3][0]);
+                acc[q][3][1] = fma(x3, z.y, acc[q][3][1]);
             }
         }
         __syncthreads();
     }
-    const long long nkeys = (long long)R * NN;
+    const int n = c0 + col;
+    if (n < NN) {
 #pragma unroll
-    for (int k = 0; k < kGKeys; ++k) {
-        if (kr[k] >= 0) {
-            const long long key = a.key_base + threadIdx.x + k * kAdjThreads;
-            double2 *g = a.G + ((long long)seg * nkeys + key) * 4;
+        for (int q = 0; q < RB; ++q) {
+            const int r = r0 + rb * RB + q;
+            if (r < R) {
+                double2 *g = a.G + (((long long)seg * R + r) * NN + n) * 4;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) g[c] = acc[k][c];
+                for (int c = 0; c < 4; ++c) g[c] = make_double2(acc[q][c][0], acc[q][c][1]);
+            }
         }
     }
 }
@@ -499,7 +500,144 @@ __global__ void __launch_bounds__(128) k_spline_adjoint(SplineAdjArgs a)
     }
 }
 
+// k_spline_adjoint for knots shared by every series, from the host
+// factorization (few_spline_factor, columns 5-9 and the boundary row); loads
+// batched ahead of the two recurrences as in k_spline_build_factored.
+constexpr int kAdjBatch = 8;
+
+__global__ void __launch_bounds__(64) k_spline_adjoint_factored(const double *__restrict__ fac, double *__restrict__ gc,
+                                                              double *__restrict__ gy, long long sk, long long sp,
+                                                              int split, long long off2, int ni, int N, int accumulate)
+{
+    constexpr int W = kFacWidth;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ni) return;
+    double *gyb = (p < split) ? gy + (long long)p * sp : gy + off2 + (long long)(p - split) * sp;
+    const long long nil = ni, plane = (long long)N * ni;
+    double *g0 = gc + p;
+    double *g1 = g0 + plane;
+    double *g2 = g1 + plane;
+    double *g3 = g2 + plane;
+    const double *bnd = fac + (long long)W * N;
+    const double gam0 = __ldg(bnd + 0), gam1 = __ldg(bnd + 1), d0 = __ldg(bnd + 2), h1 = __ldg(bnd + 3);
+    const double e0 = __ldg(bnd + 4), e1 = __ldg(bnd + 5), dE = __ldg(bnd + 6), hA = __ldg(bnd + 7);
+    const long long oE = (long long)(N - 1) * nil;
+    const double gE1 = g1[oE], gE2 = g2[oE], gE3 = g3[oE];
+
+    // Pass F: dL/ds and the forward sweep of the transposed interior block
+    double carry = 0.0, w0 = 0.0, wE = 0.0, rprev = 0.0;
+    for (int i0 = 0; i0 <= N - 2; i0 += kAdjBatch) {
+        double v1[kAdjBatch], v2[kAdjBatch], v3[kAdjBatch], fh[kAdjBatch], fih[kAdjBatch], flt[kAdjBatch],
+            fidt[kAdjBatch];
+#pragma unroll
+        for (int q = 0; q < kAdjBatch; ++q) {
+            const int i = min(i0 + q, N - 2);
+            const long long o = (long long)i * nil;
+            v1[q] = g1[o];
+            v2[q] = g2[o];
+            v3[q] = g3[o];
+            const double *f = fac + (long long)W * i;
+            fh[q] = __ldg(f + 5);
+            fih[q] = __ldg(f + 6);
+            flt[q] = __ldg(f + 7);
+            fidt[q] = __ldg(f + 8);
+        }
+#pragma unroll
+        for (int q = 0; q < kAdjBatch; ++q) {
+            const int i = i0 + q;
+            if (i <= N - 2) {
+                const long long o = (long long)i * nil;
+                double a1 = v1[q], a2 = v2[q], a3 = v3[q];
+                const double h = fh[q], ih = fih[q];
+                if (i == N - 2) {
+                    a1 += gE1;
+                    a2 += 2 * h * gE1 + gE2;
+                    a3 += 3 * h * h * gE1 + 3 * h * gE2 + gE3;
+                }
+                const double gtt = -a2 + a3 * ih;
+                const double gs = carry + a1 - a2 * ih + gtt * ih;
+                carry = gtt * ih;
+                g3[o] = a2 * ih - 2.0 * gtt * ih;  // direct dL/d delta_i
+                if (i == 0) {
+                    w0 = gs / h1;
+                } else {
+                    double rhs = gs;
+                    if (i == 1) rhs -= d0 * w0;
+                    if (i == N - 2) {
+                        wE = carry / hA;
+                        rhs -= dE * wE;
+                    }
+                    const double rp = (rhs - flt[q] * rprev) * fidt[q];
+                    g2[o] = rp;
+                    rprev = rp;
+                }
+            }
+        }
+    }
+
+    // Pass B: back substitution, dL/d delta, dL/dy
+    const double w_last = rprev;
+    const double zE = wE - w_last;
+    const double rE_a = zE * e0, rE_b = zE * e1;
+    double w_ip1 = 0.0, gdel_ip1 = 0.0, pend = 0.0;
+    auto put = [&](long long knot, double v) {
+        double *dst = gyb + knot * sk;
+        *dst = accumulate ? *dst + v : v;
+    };
+    for (int i0 = N - 2; i0 >= 1; i0 -= kAdjBatch) {
+        double vr[kAdjBatch], vd[kAdjBatch], vn[kAdjBatch], fct[kAdjBatch], fhl[kAdjBatch], fhr[kAdjBatch],
+            fihr[kAdjBatch], fihn[kAdjBatch];
+#pragma unroll
+        for (int q = 0; q < kAdjBatch; ++q) {
+            const int i = max(i0 - q, 1);
+            const long long o = (long long)i * nil;
+            vr[q] = g2[o];
+            vd[q] = g3[o];
+            vn[q] = g0[o + nil];
+            fct[q] = __ldg(fac + (long long)W * i + 9);
+            fhl[q] = __ldg(fac + (long long)W * (i - 1) + 5);
+            fhr[q] = __ldg(fac + (long long)W * i + 5);
+            fihr[q] = __ldg(fac + (long long)W * i + 6);
+            fihn[q] = __ldg(fac + (long long)W * (i + 1) + 6);
+        }
+#pragma unroll
+        for (int q = 0; q < kAdjBatch; ++q) {
+            const int i = i0 - q;
+            if (i >= 1) {
+                const double w_i = (i == N - 2) ? w_last : (vr[q] - fct[q] * w_ip1);
+                double gdel_i = vd[q] + 3.0 * fhl[q] * w_i + pend;
+                if (i == N - 2) gdel_i += rE_b;
+                if (i == N - 3) gdel_i += rE_a;
+                if (i == 1) gdel_i += (w0 - w_i) * gam1;
+                double gy_ip1 = vn[q] + gdel_i * fihr[q];
+                if (i + 1 <= N - 2) gy_ip1 -= gdel_ip1 * fihn[q];
+                put(i + 1, gy_ip1);
+                pend = 3.0 * fhr[q] * w_i;
+                gdel_ip1 = gdel_i;
+                w_ip1 = w_i;
+                if (i == 1) {
+                    const double z0 = w0 - w_i;
+                    const double ih0 = __ldg(fac + 6);
+                    const double gdel0 = g3[0] + pend + z0 * gam0;
+                    put(1, g0[nil] + gdel0 * ih0 - gdel_i * fihr[q]);
+                    put(0, g0[0] - gdel0 * ih0);
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
+
+int launch_spline_adjoint_factored(const double *fac, double *gc, double *gy, long long sk, long long sp, int split,
+                                   long long off2, int ni, int N, int accumulate, cudaStream_t st)
+{
+    const int threads = 64;
+    k_spline_adjoint_factored<<<(ni + threads - 1) / threads, threads, 0, st>>>(fac, gc, gy, sk, sp, split, off2, ni,
+                                                                               N, accumulate);
+    FEW_LAUNCH_CHECK("k_spline_adjoint_factored");
+    return FEW_OK;
+}
 
 // ---------------------------------------------------------------------------
 // launchers
@@ -549,32 +687,31 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
                  cudaStream_t st)
 {
     if (nseg == 0) return FEW_OK;
-    const size_t smem = (size_t)kGTile * (R + NN) * sizeof(double2) + (size_t)kGTile * 4 * sizeof(double) +
-                        (size_t)kGTile * 4 * sizeof(double2);
-    if (smem > (size_t)kSmemBudget) return fail(FEW_ERR_SIZE, "adjoint: R + NN too large for the G tiles");
-    FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_G, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
-    const int nkeys = R * NN;
-    const int per_pass = kAdjThreads * kGKeys;
-    for (int base = 0; base < nkeys; base += per_pass) {
-        AdjGArgs a;
-        a.grad = grad;
-        a.pc = pc;
-        a.seg_info = seg_info;
-        a.seg_start = seg_start;
-        a.row_m = row_m;
-        a.row_k = row_k;
-        a.G = G;
-        a.N = N;
-        a.R = R;
-        a.nlo = nlo;
-        a.NN = NN;
-        a.use_theta = use_theta;
-        a.key_base = base;
-        a.nkeys_pass = std::min(per_pass, nkeys - base);
-        a.dt = dt;
-        k_adj_G<<<nseg, kAdjThreads, smem, st>>>(a);
-        FEW_LAUNCH_CHECK("k_adj_G");
+    AdjGArgs a;
+    a.grad = grad;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.seg_start = seg_start;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.G = G;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.key_base = 0;
+    a.nkeys_pass = R * NN;
+    a.dt = dt;
+    const int colg = (NN + kGCols - 1) / kGCols;
+    if (R <= 4 * kGRowBlocks) {
+        dim3 grid(nseg, (R + 4 * kGRowBlocks - 1) / (4 * kGRowBlocks), colg);
+        k_adj_G<4><<<grid, kAdjThreads, 0, st>>>(a);
+    } else {
+        dim3 grid(nseg, (R + 8 * kGRowBlocks - 1) / (8 * kGRowBlocks), colg);
+        k_adj_G<8><<<grid, kAdjThreads, 0, st>>>(a);
     }
+    FEW_LAUNCH_CHECK("k_adj_G");
     return FEW_OK;
 }
 
@@ -659,6 +796,19 @@ extern "C" int few_unfold(const void *G, const void *ylms, const int *key_plus, 
     if (K < 1 || N < 2 || nseg < 0 || nseg > N - 1 || nkeys < 1) return few::fail(FEW_ERR_SIZE, "few_unfold: bad sizes");
     return few::launch_unfold((const double2 *)G, (const double2 *)ylms, key_plus, key_minus, K, N, nseg, nkeys, gcoef,
                               (cudaStream_t)stream);
+}
+
+extern "C" int few_spline_adjoint_factored(const double *fac, double *gcoeffs, double *gy, long long y_knot_stride,
+                                           long long y_interp_stride, int y_split, long long y_split_offset,
+                                           int ninterps, int length, int accumulate, void *stream)
+{
+    few::clear_error();
+    if (!fac || !gcoeffs || !gy) return few::fail(FEW_ERR_ARG, "few_spline_adjoint_factored: null pointer");
+    if (ninterps < 1) return few::fail(FEW_ERR_SIZE, "few_spline_adjoint_factored: ninterps=%d < 1", ninterps);
+    if (length < 4) return few::fail(FEW_ERR_SIZE, "few_spline_adjoint_factored: length=%d < 4", length);
+    if (y_split < 0 || y_split > ninterps) return few::fail(FEW_ERR_ARG, "few_spline_adjoint_factored: bad y_split");
+    return few::launch_spline_adjoint_factored(fac, gcoeffs, gy, y_knot_stride, y_interp_stride, y_split,
+                                               y_split_offset, ninterps, length, accumulate, (cudaStream_t)stream);
 }
 
 extern "C" int few_spline_adjoint(const double *t, long long t_row_stride, double *gcoeffs, double *gy,

@@ -39,6 +39,7 @@ void clear_error();
 // reference-shaped entry point.
 int fold_plan(const int *m, const int *k, const int *n, int K, int max_rows, int max_keys, int *row_m,
               int *row_k, int *dims, int *key_ptr, int *key_list);
+int spline_factor(const double *x, int N, double *fac);
 int segment_plan(const double *h_t, const double *phase_t, int init_len, int out_len, double dt,
                  int chunk, int max_units, int *seg_start, double *seg_info, int *units, int *counts);
 
@@ -64,6 +65,10 @@ int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, co
 int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *gy, long long sk, long long sp,
                           int split, long long off2, int ni, int N, int accumulate, cudaStream_t st);
 
+int launch_spline_adjoint_factored(const double *fac, double *gc, double *gy, long long sk, long long sp, int split,
+                                   long long off2, int ni, int N, int accumulate, cudaStream_t st);
+
+constexpr int kFacWidth = 12;       // doubles per row of the shared spline factorization
 constexpr int kMaxRows = 256;        // distinct (m', k') rows of a fold plan
 constexpr int kDefaultChunk = 1024;  // output samples per work unit of the sum
 

@@ -120,7 +120,89 @@ int segment_plan(const double *h_t, const double *phase_t, int init_len, int out
     return FEW_OK;
 }
 
+// Factorization of the not-a-knot system shared by every series on knots t
+// (the elimination k_spline_build performs per thread, done once), and of the
+// interior block of its transpose for the adjoint (k_spline_adjoint_factored).
+// fac (N+1, kFacWidth = 12), row i:
+//   0 lo_i, 1 1/den_i, 2 c'_i, 3 alpha_i, 4 beta_i  (rows 1..N-2; forward sweep
+//     r'_i = (alpha_i delta_{i-1} + beta_i delta_i - lo_i r'_{i-1}) / den_i, the
+//     two boundary rows' right-hand sides folded into rows 1 and N-2)
+//   5 h_i, 6 1/h_i                                   (rows 0..N-2)
+//   7 lo~_i = h_{i-2}, 8 1/den~_i, 9 c~_i           (rows 1..N-2; transposed block)
+// Row N: gamma0, gamma1 (b0 = gamma0 delta_0 + gamma1 delta_1), d0 = x2 - x0, h1,
+// eps0, eps1 (bE = eps0 delta_{N-3} + eps1 delta_{N-2}), dE = x_{N-1} - x_{N-3},
+// hA = x_{N-2} - x_{N-3}.
+int spline_factor(const double *x, int N, double *fac)
+{
+    const int W = kFacWidth;
+    if (!x || !fac) return fail(FEW_ERR_ARG, "few_spline_factor: null pointer");
+    if (N < 4) return fail(FEW_ERR_SIZE, "few_spline_factor: length=%d; not-a-knot splines need at least 4 knots", N);
+    for (int i = 1; i < N; ++i)
+        if (!(x[i] > x[i - 1])) return fail(FEW_ERR_KNOTS, "few_spline_factor: knots must increase strictly");
+    for (int q = 0; q < W * (N + 1); ++q) fac[q] = 0.0;
+    for (int i = 0; i <= N - 2; ++i) {
+        const double h = x[i + 1] - x[i];
+        fac[W * i + 5] = h;
+        fac[W * i + 6] = 1.0 / h;
+    }
+    const double h0 = x[1] - x[0], h1 = x[2] - x[1], d0 = x[2] - x[0];
+    const double hA = x[N - 2] - x[N - 3], hB = x[N - 1] - x[N - 2], dE = x[N - 1] - x[N - 3];
+    const double g0 = (h0 + 2 * d0) * h1 / d0, g1 = h0 * h0 / d0;
+    const double e0 = hB * hB / dE, e1 = (2 * dE + hB) * hA / dE;
+    double cprev = 0.0, ctprev = 0.0;
+    for (int i = 1; i <= N - 2; ++i) {
+        const double hl = x[i] - x[i - 1], hr = x[i + 1] - x[i];
+        double lo = hr, dg = 2 * (hl + hr), up = hl, alpha = 3.0 * hr, beta = 3.0 * hl;
+        if (i == 1) {
+            dg -= d0;
+            lo = 0.0;
+            alpha -= g0;
+            beta -= g1;
+        }
+        if (i == N - 2) {
+            dg -= dE;
+            up = 0.0;
+            alpha -= e0;
+            beta -= e1;
+        }
+        const double den = dg - lo * cprev;
+        const double cp = up / den;
+        fac[W * i + 0] = lo;
+        fac[W * i + 1] = 1.0 / den;
+        fac[W * i + 2] = cp;
+        fac[W * i + 3] = alpha;
+        fac[W * i + 4] = beta;
+        cprev = cp;
+        // transposed interior block: row i has h_{i-2} left (i >= 2), the same
+        // diagonal, and h_{i+1} right (i <= N-3)
+        const double lot = (i >= 2) ? (x[i - 1] - x[i - 2]) : 0.0;
+        const double upt = (i <= N - 3) ? (x[i + 2] - x[i + 1]) : 0.0;
+        const double dent = dg - lot * ctprev;
+        const double ct = upt / dent;
+        fac[W * i + 7] = lot;
+        fac[W * i + 8] = 1.0 / dent;
+        fac[W * i + 9] = ct;
+        ctprev = ct;
+    }
+    double *b = fac + (size_t)W * N;
+    b[0] = g0;
+    b[1] = g1;
+    b[2] = d0;
+    b[3] = h1;
+    b[4] = e0;
+    b[5] = e1;
+    b[6] = dE;
+    b[7] = hA;
+    return FEW_OK;
+}
+
 }  // namespace few
+
+extern "C" int few_spline_factor(const double *t, int N, double *fac)
+{
+    few::clear_error();
+    return few::spline_factor(t, N, fac);
+}
 
 extern "C" int few_fold_plan(const int *m, const int *k, const int *n, int K, int max_rows, int max_keys, int *row_m,
                              int *row_k, int *dims, int *key_ptr, int *key_list)

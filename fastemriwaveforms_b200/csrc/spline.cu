@@ -151,6 +151,125 @@ __global__ void __launch_bounds__(128) k_spline_build(SplineArgs a)
     o0[0] = y0;
 }
 
+// Shared-knot build from a host factorization (few_spline_factor): per step the
+// forward sweep is r'_i = (alpha_i delta_{i-1} + beta_i delta_i - lo_i r'_{i-1}) / den_i
+// and the backward sweep s_i = r'_i - c'_i s_{i+1}; no division per series and
+// only r' parked in the c3 output row.  Loads are issued kSweepBatch steps
+// ahead of the recurrence (they do not depend on it), so a thread keeps that
+// many in flight instead of waiting on one load per step.
+constexpr int kSweepBatch = 8;
+
+__global__ void __launch_bounds__(64) k_spline_build_factored(const double *__restrict__ fac,
+                                                            const double *__restrict__ y, long long sk, long long sp,
+                                                            int split, long long off2, int ni, int N,
+                                                            double *__restrict__ out, long long os_i, long long os_p)
+{
+    constexpr int W = kFacWidth;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ni) return;
+    const double *yb = (p < split) ? y + (long long)p * sp : y + off2 + (long long)(p - split) * sp;
+    const long long plane = (long long)N * ni;
+    double *o0 = out + (long long)p * os_p;
+    double *o1 = o0 + plane;
+    double *o2 = o1 + plane;
+    double *o3 = o2 + plane;
+    const double *bnd = fac + (long long)W * N;
+    const double g0 = __ldg(bnd + 0), g1 = __ldg(bnd + 1), d0 = __ldg(bnd + 2), h1 = __ldg(bnd + 3);
+    const double e0 = __ldg(bnd + 4), e1 = __ldg(bnd + 5), dE = __ldg(bnd + 6), hA = __ldg(bnd + 7);
+
+    const double y0 = yb[0], y1 = yb[sk], y2 = yb[2 * sk];
+    const double del0 = (y1 - y0) * __ldg(fac + 6);
+    const double del1 = (y2 - y1) * __ldg(fac + W + 6);
+    const double b0 = g0 * del0 + g1 * del1;
+    double ym = y1, dprev = del0, rprev = 0.0, bE = 0.0;
+    for (int i0 = 1; i0 <= N - 2; i0 += kSweepBatch) {
+        double yv[kSweepBatch], fl[kSweepBatch], fi[kSweepBatch], fa[kSweepBatch], fb[kSweepBatch], fh[kSweepBatch];
+#pragma unroll
+        for (int q = 0; q < kSweepBatch; ++q) {
+            const int i = min(i0 + q, N - 2);
+            yv[q] = yb[(long long)(i + 1) * sk];
+            const double *f = fac + (long long)W * i;
+            fl[q] = __ldg(f + 0);
+            fi[q] = __ldg(f + 1);
+            fa[q] = __ldg(f + 3);
+            fb[q] = __ldg(f + 4);
+            fh[q] = __ldg(f + 6);
+        }
+#pragma unroll
+        for (int q = 0; q < kSweepBatch; ++q) {
+            const int i = i0 + q;
+            if (i <= N - 2) {
+                const double del = (yv[q] - ym) * fh[q];
+                const double rp = (fa[q] * dprev + fb[q] * del - fl[q] * rprev) * fi[q];
+                o3[(long long)i * os_i] = rp;
+                if (i == N - 2) bE = e0 * dprev + e1 * del;
+                rprev = rp;
+                dprev = del;
+                ym = yv[q];
+            }
+        }
+    }
+
+    // backward: s_{N-2} = r'_{N-2}, s_{N-1} from the last row, then segments N-2 .. 0
+    double s_ip1 = rprev;
+    const double s_last = (bE - dE * s_ip1) / hA;
+    double yr = yb[(long long)(N - 1) * sk];
+    {
+        const long long i = N - 2;
+        const double yl = yb[i * sk];
+        const double ih = __ldg(fac + W * i + 6), xx = __ldg(fac + W * i + 5);
+        const double dl = (yr - yl) * ih;
+        const double tt = (s_ip1 + s_last - 2 * dl) * ih;
+        const double c1 = s_ip1, c2 = (dl - s_ip1) * ih - tt, c3 = tt * ih;
+        const long long off = i * os_i, offe = (long long)(N - 1) * os_i;
+        o0[off] = yl;
+        o1[off] = c1;
+        o2[off] = c2;
+        o3[off] = c3;
+        o0[offe] = yr;
+        o1[offe] = c1 + 2 * c2 * xx + 3 * c3 * xx * xx;
+        o2[offe] = (2. * c2 + 6. * c3 * xx) / 2.;
+        o3[offe] = c3;
+        yr = yl;
+    }
+    for (int i0 = N - 3; i0 >= 1; i0 -= kSweepBatch) {
+        double yv[kSweepBatch], rv[kSweepBatch], fc[kSweepBatch], fh[kSweepBatch];
+#pragma unroll
+        for (int q = 0; q < kSweepBatch; ++q) {
+            const int i = max(i0 - q, 1);
+            yv[q] = yb[(long long)i * sk];
+            rv[q] = o3[(long long)i * os_i];
+            fc[q] = __ldg(fac + (long long)W * i + 2);
+            fh[q] = __ldg(fac + (long long)W * i + 6);
+        }
+#pragma unroll
+        for (int q = 0; q < kSweepBatch; ++q) {
+            const int i = i0 - q;
+            if (i >= 1) {
+                const long long off = (long long)i * os_i;
+                const double s_i = rv[q] - fc[q] * s_ip1;
+                const double dl = (yr - yv[q]) * fh[q];
+                const double tt = (s_i + s_ip1 - 2 * dl) * fh[q];
+                o0[off] = yv[q];
+                o1[off] = s_i;
+                o2[off] = (dl - s_i) * fh[q] - tt;
+                o3[off] = tt * fh[q];
+                s_ip1 = s_i;
+                yr = yv[q];
+            }
+        }
+    }
+    const double s0 = (b0 - d0 * s_ip1) / h1;
+    {
+        const double ih0 = __ldg(fac + 6);
+        const double tt = (s0 + s_ip1 - 2 * del0) * ih0;
+        o0[0] = y0;
+        o1[0] = s0;
+        o2[0] = (del0 - s0) * ih0 - tt;
+        o3[0] = tt * ih0;
+    }
+}
+
 __global__ void k_spline_eval(const double *__restrict__ t, long long t_rs, const double *__restrict__ coeffs,
                               int ni, int N, const double *__restrict__ tnew, long long tn_rs, int M, int deriv,
                               double *__restrict__ out, int *__restrict__ flags)
@@ -226,6 +345,26 @@ int launch_spline_build(const double *t, long long t_rs, const double *y, long l
 }
 
 }  // namespace few
+
+extern "C" int few_spline_build_factored(const double *fac, const double *y, long long y_knot_stride,
+                                         long long y_interp_stride, int y_split, long long y_split_offset, int ninterps,
+                                         int length, double *coeffs, int layout, void *stream)
+{
+    few::clear_error();
+    if (!fac || !y || !coeffs) return few::fail(FEW_ERR_ARG, "few_spline_build_factored: null pointer");
+    if (ninterps < 1) return few::fail(FEW_ERR_SIZE, "few_spline_build_factored: ninterps=%d < 1", ninterps);
+    if (length < 4) return few::fail(FEW_ERR_SIZE, "few_spline_build_factored: length=%d < 4", length);
+    if (layout != FEW_LAYOUT_KNOT_MAJOR && layout != FEW_LAYOUT_INTERP_MAJOR)
+        return few::fail(FEW_ERR_ARG, "few_spline_build_factored: unknown layout %d", layout);
+    if (y_split < 0 || y_split > ninterps) return few::fail(FEW_ERR_ARG, "few_spline_build_factored: bad y_split");
+    const long long os_i = layout == FEW_LAYOUT_KNOT_MAJOR ? ninterps : 1;
+    const long long os_p = layout == FEW_LAYOUT_KNOT_MAJOR ? 1 : length;
+    const int threads = 64;
+    few::k_spline_build_factored<<<(ninterps + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(
+        fac, y, y_knot_stride, y_interp_stride, y_split, y_split_offset, ninterps, length, coeffs, os_i, os_p);
+    FEW_LAUNCH_CHECK("k_spline_build_factored");
+    return FEW_OK;
+}
 
 extern "C" int few_spline_build(const double *t, long long t_row_stride, const double *y, long long y_knot_stride,
                                 long long y_interp_stride, int y_split, long long y_split_offset, int ninterps,

@@ -71,6 +71,15 @@ def _ptr(t: torch.Tensor) -> int:
     return t.data_ptr()
 
 
+def spline_factor_table(h_t: np.ndarray, device) -> torch.Tensor:
+    """Device copy of the not-a-knot factorization for knots h_t (few_spline_factor)."""
+    h_t = np.ascontiguousarray(h_t, dtype=np.float64)
+    N = len(h_t)
+    fac = np.zeros(_lib.FEW_FAC_WIDTH * (N + 1), np.float64)
+    _lib.call("few_spline_factor", h_t.ctypes.data, N, fac.ctypes.data)
+    return torch.from_numpy(fac).pin_memory().to(device, non_blocking=True)
+
+
 class CubicSplineInterpolant:
     """Multiple not-a-knot cubic splines on the GPU
     (reference: ``interpolatedmodesum.py:12-257``).
@@ -117,8 +126,14 @@ class CubicSplineInterpolant:
         self._t_knots = t_dev
         self._t_rs = t_rs
         coeffs = torch.empty((4, self.length, self.ninterps), dtype=torch.float64, device=dev)
-        _lib.call("few_spline_build", _ptr(t_dev), t_rs, _ptr(y), 1, self.length, self.ninterps, 0,
-                  self.ninterps, self.length, _ptr(coeffs), _lib.FEW_LAYOUT_KNOT_MAJOR, _stream(dev))
+        if t_rs == 0:
+            # shared knots: factor once on the host, sweep per series on the device
+            fac = spline_factor_table(t_dev.cpu().numpy(), dev)
+            _lib.call("few_spline_build_factored", _ptr(fac), _ptr(y), 1, self.length, self.ninterps, 0,
+                      self.ninterps, self.length, _ptr(coeffs), _lib.FEW_LAYOUT_KNOT_MAJOR, _stream(dev))
+        else:
+            _lib.call("few_spline_build", _ptr(t_dev), t_rs, _ptr(y), 1, self.length, self.ninterps, 0,
+                      self.ninterps, self.length, _ptr(coeffs), _lib.FEW_LAYOUT_KNOT_MAJOR, _stream(dev))
         self.interp_array = coeffs.reshape(-1)
         """Flattened array containing all spline coefficients, (4, length, ninterps)."""
         self.reshape_shape = (self.degree + 1, self.length, self.ninterps)
@@ -431,6 +446,7 @@ class InterpolatedModeSum(SummationBase):
         p.dev, p.st, p.N, p.K, p.dt = dev, _stream(dev), N, K, float(dt)
         p.teuk, p.teuk_in, p.pc_in = teuk, (teuk_in if keep else None), (pc_in if keep else None)
         p.t_dev = torch.from_numpy(h_t).to(dev)
+        p.fac = spline_factor_table(h_t, dev)
         # ylms[K:] *= (-1)^l (interpolatedmodesum.py:357-358)
         sign = np.where(l_h % 2 == 0, 1.0, -1.0)
         ylm = _to_device(ylms, torch.complex128, dev).clone()
@@ -453,7 +469,7 @@ class InterpolatedModeSum(SummationBase):
             ev[0].record()
         # amplitude splines straight from the (N, K) complex array: real parts are
         # interpolants 0..K-1, imaginary parts K..2K-1 (interpolatedmodesum.py:331-337)
-        _lib.call("few_spline_build", _ptr(p.t_dev), 0, _ptr(p.teuk), 2 * K, 2, K, 1, 2 * K, N, _ptr(coeffs),
+        _lib.call("few_spline_build_factored", _ptr(p.fac), _ptr(p.teuk), 2 * K, 2, K, 1, 2 * K, N, _ptr(coeffs),
                   _lib.FEW_LAYOUT_KNOT_MAJOR, st)
         if ev:
             ev[1].record()
@@ -499,8 +515,8 @@ class InterpolatedModeSum(SummationBase):
             _lib.call("few_unfold", _ptr(G), _ptr(p.ylm), _ptr(fold.d_key_plus), _ptr(fold.d_key_minus), K, N,
                       seg.nseg, fold.R * fold.NN, _ptr(gcoef), st)
             g_teuk = torch.empty((N, K), dtype=torch.complex128, device=dev)
-            _lib.call("few_spline_adjoint", _ptr(p.t_dev), 0, _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N, 0,
-                      st)
+            _lib.call("few_spline_adjoint_factored", _ptr(p.fac), _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N,
+                      0, st)
         if need_pc:
             _, seg_units = seg.backward_tables()
             partial = torch.empty((max(seg.nunits, 1), 24), dtype=torch.float64, device=dev)

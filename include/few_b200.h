@@ -132,6 +132,23 @@ FEW_API int few_spline_build(const double *t, long long t_row_stride, const doub
                      long long y_interp_stride, int y_split, long long y_split_offset, int ninterps,
                      int length, double *coeffs, int layout, void *stream);
 
+/* Width of a row of few_spline_factor's table. */
+#define FEW_FAC_WIDTH 12
+
+/* Host factorization of the not-a-knot system (and of its transpose) for knots
+ * t [host] (N,), shared by every series on those knots: fac [host]
+ * ((N+1)*FEW_FAC_WIDTH,) (row layout in fastemriwaveforms_b200/csrc/plan.cpp).
+ * FEW_ERR_KNOTS unless t increases strictly. */
+FEW_API int few_spline_factor(const double *t, int N, double *fac);
+
+/* few_spline_build for knots shared by all series, from their factorization
+ * (few_spline_factor, copied to the device: fac [device]).  Same y view,
+ * layouts and results as few_spline_build (to rounding); no division per
+ * series. */
+FEW_API int few_spline_build_factored(const double *fac, const double *y, long long y_knot_stride,
+                                      long long y_interp_stride, int y_split, long long y_split_offset,
+                                      int ninterps, int length, double *coeffs, int layout, void *stream);
+
 /* Spline evaluation (CubicSplineInterpolant.__call__, interpolatedmodesum.py:161-257).
  * t [device]: knots, interpolant p uses t + p*t_row_stride (0 = shared).
  * coeffs [device] (4, length, ninterps).  tnew [device]: point j of
@@ -265,6 +282,12 @@ FEW_API int few_unfold(const void *G, const void *ylms, const int *key_plus, con
 FEW_API int few_spline_adjoint(const double *t, long long t_row_stride, double *gcoeffs, double *gy,
                                long long y_knot_stride, long long y_interp_stride, int y_split,
                                long long y_split_offset, int ninterps, int length, int accumulate, void *stream);
+
+/* few_spline_adjoint for knots shared by every series, from their
+ * factorization (few_spline_factor copied to the device: fac [device]). */
+FEW_API int few_spline_adjoint_factored(const double *fac, double *gcoeffs, double *gy, long long y_knot_stride,
+                                        long long y_interp_stride, int y_split, long long y_split_offset,
+                                        int ninterps, int length, int accumulate, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Measurement                                                              */

@@ -177,3 +177,26 @@ def test_backward_deterministic_and_consistent_with_faithful_forward(cuda):
     assert np.array_equal(outs[1][0], outs[2][0]) and np.array_equal(outs[1][1], outs[2][1])
     for a, b in zip(outs[0], outs[1]):
         assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("N,K", [(4, 3), (9, 5), (1000, 3843)])
+def test_factored_spline_adjoint_matches_generic(cuda, N, K):
+    """Shared-knot adjoint (host factorization) vs the per-series adjoint kernel,
+    on the complex (N, K) view the mode-sum backward uses."""
+    from fastemriwaveforms_b200 import _lib
+    from fastemriwaveforms_b200.summation import spline_factor_table
+
+    rng = np.random.default_rng(N)
+    t = np.cumsum(np.concatenate([[0.0], rng.exponential(1.0, N - 1) + 1e-2]))
+    gc = torch.tensor(rng.standard_normal((4, N, 2 * K)), device=cuda)
+    td = torch.from_numpy(t).to(cuda)
+    st = torch.cuda.current_stream().cuda_stream
+    g_generic = torch.empty((N, K), dtype=torch.complex128, device=cuda)
+    _lib.call("few_spline_adjoint", td.data_ptr(), 0, gc.clone().data_ptr(), g_generic.data_ptr(), 2 * K, 2, K, 1,
+              2 * K, N, 0, st)
+    fac = spline_factor_table(t, cuda)
+    g_fact = torch.empty_like(g_generic)
+    _lib.call("few_spline_adjoint_factored", fac.data_ptr(), gc.clone().data_ptr(), g_fact.data_ptr(), 2 * K, 2, K,
+              1, 2 * K, N, 0, st)
+    a, b = g_fact.cpu().numpy(), g_generic.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-11 * np.abs(b).max()

@@ -84,6 +84,32 @@ def test_complex_strided_input_matches_real_rows(cuda, oracle):
     assert coeff_err(out.cpu().numpy(), ref) < 1e-12
 
 
+@pytest.mark.parametrize("N,ni,seed", [(4, 5, 0), (7, 3, 1), (1000, 7686, 2), (2000, 100, 3)])
+def test_factored_build_matches_generic(cuda, oracle, N, ni, seed):
+    """The shared-knot path (host factorization) agrees with the per-series
+    kernel and the oracle, on the complex (N, K) view InterpolatedModeSum uses."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(np.concatenate([[0.0], rng.exponential(1.0, N - 1) + 1e-2]))
+    K = (ni + 1) // 2
+    teuk = rng.standard_normal((N, K)) + 1j * rng.standard_normal((N, K))
+    td = torch.from_numpy(t).to(cuda)
+    tk = torch.from_numpy(teuk).to(cuda)
+    st = torch.cuda.current_stream().cuda_stream
+    generic = torch.empty((4, N, 2 * K), dtype=torch.float64, device=cuda)
+    _lib.call("few_spline_build", td.data_ptr(), 0, tk.data_ptr(), 2 * K, 2, K, 1, 2 * K, N, generic.data_ptr(),
+              _lib.FEW_LAYOUT_KNOT_MAJOR, st)
+    from fastemriwaveforms_b200.summation import spline_factor_table
+
+    fac = spline_factor_table(t, cuda)
+    fact = torch.empty_like(generic)
+    _lib.call("few_spline_build_factored", fac.data_ptr(), tk.data_ptr(), 2 * K, 2, K, 1, 2 * K, N, fact.data_ptr(),
+              _lib.FEW_LAYOUT_KNOT_MAJOR, st)
+    assert coeff_err(fact.cpu().numpy(), generic.cpu().numpy()) < 1e-11
+    if N <= 1000:
+        y_all = np.concatenate([teuk.T.real, teuk.T.imag])
+        assert coeff_err(fact.cpu().numpy(), oracle.spline_coeffs(t, y_all)) < 1e-11
+
+
 def test_reference_shaped_interpolate_arrays(cuda, oracle):
     rng = np.random.default_rng(6)
     ni, N = 9, 41
