@@ -50,17 +50,18 @@ struct AdjPhaseArgs {
 };
 
 // dL/dPhi at every sample of the unit, projected on the phase basis.
-template <int RB>
-__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
+template <int RB, bool THETA>
+__global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *sW = reinterpret_cast<double2 *>(smem_raw);
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
     __shared__ double s_pc[24];
-    __shared__ double s_red[kAdjThreads / 32][24];
+    __shared__ double s_e[3][1024];  // dL/dPhi_f at each sample of the unit (units hold <= 1024 samples)
 
     const int u = blockIdx.x;
-    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1];
+    const int hi = min(a.units[3 * u + 2], lo + 1024);  // units hold at most 1024 samples (checked on the host)
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const int R = a.R, NN = a.NN, nlo = a.nlo;
     const long long nps = (long long)(a.N - 1) * 3;
@@ -72,9 +73,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
         const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
         s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
     }
-    double acc[24];
-#pragma unroll
-    for (int q = 0; q < 24; ++q) acc[q] = 0.0;
+    for (int q = threadIdx.x; q < hi - lo; q += blockDim.x) s_e[0][q] = s_e[1][q] = s_e[2][q] = 0.0;
 
     for (int r0 = 0; r0 < R; r0 += a.rows_per_pass) {
         const int nrp = min(a.rows_per_pass, R - r0);
@@ -92,14 +91,14 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
             const double s1 = rsub(1.0, s);
             const double Pp = phase_poly(s_pc, s, s1);
             const double Pr = phase_poly(s_pc + 16, s, s1);
-            const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
+            const double Pt = THETA ? phase_poly(s_pc + 8, s, s1) : 0.0;
             double sn, cs;
             sincos(Pp, &sn, &cs);
             const double2 Ep = make_double2(cs, -sn);
             sincos(Pr, &sn, &cs);
             const double2 Er = make_double2(cs, -sn);
             double2 Et = make_double2(1.0, 0.0);
-            if (a.use_theta) {
+            if (THETA) {
                 sincos(Pt, &sn, &cs);
                 Et = make_double2(cs, -sn);
             }
@@ -107,19 +106,14 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
             double2 Dp = make_double2(0.0, 0.0), Dr = Dp, Dt = Dp;
             for (int rb = 0; rb < nrp; rb += RB) {
                 double2 U[RB];
-                double Mq[RB], Kq[RB];
 #pragma unroll
                 for (int q = 0; q < RB; ++q) {
                     U[q] = make_double2(0.0, 0.0);
-                    Mq[q] = 0.0;
-                    Kq[q] = 0.0;
                     if (rb + q < nrp) {
                         const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
                         double2 uu = cpow_int(Ep, mm);
-                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
+                        if (THETA && kk) uu = cmul(uu, cpow_int(Et, kk));
                         U[q] = uu;
-                        Mq[q] = (double)mm;
-                        Kq[q] = (double)kk;
                     }
                 }
                 double2 v = V0;
@@ -136,12 +130,16 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
                             Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
                             Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
                             const double2 P = cmul(U[q], Wx);
+                            const double mq = (double)s_rm[r0 + rb + q];
                             T.x += P.x;
                             T.y += P.y;
-                            Tm.x = fma(Mq[q], P.x, Tm.x);
-                            Tm.y = fma(Mq[q], P.y, Tm.y);
-                            Tk.x = fma(Kq[q], P.x, Tk.x);
-                            Tk.y = fma(Kq[q], P.y, Tk.y);
+                            Tm.x = fma(mq, P.x, Tm.x);
+                            Tm.y = fma(mq, P.y, Tm.y);
+                            if (THETA) {
+                                const double kq = (double)s_rk[r0 + rb + q];
+                                Tk.x = fma(kq, P.x, Tk.x);
+                                Tk.y = fma(kq, P.y, Tk.y);
+                            }
                         }
                     }
                     const double dn = (double)(nlo + c);
@@ -151,7 +149,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
                     Dp.y += vTm.y;
                     Dr.x = fma(dn, vT.x, Dr.x);
                     Dr.y = fma(dn, vT.y, Dr.y);
-                    if (a.use_theta) {
+                    if (THETA) {
                         const double2 vTk = cmul(v, Tk);
                         Dt.x += vTk.x;
                         Dt.y += vTk.y;
@@ -164,37 +162,30 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_phase(AdjPhaseArgs a)
             const double ep = G.x * Dp.y - G.y * Dp.x;
             const double er = G.x * Dr.y - G.y * Dr.x;
             const double et = G.x * Dt.y - G.y * Dt.x;
-            // basis b_q(s): 1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3, s^4 s1^3
-            double b[8];
-            b[0] = 1.0;
-            b[1] = s;
-            b[2] = s * s1;
-            b[3] = b[2] * s;
-            b[4] = b[3] * s1;
-            b[5] = b[4] * s;
-            b[6] = b[5] * s1;
-            b[7] = b[6] * s;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                acc[q] = fma(ep, b[q], acc[q]);
-                acc[8 + q] = fma(et, b[q], acc[8 + q]);
-                acc[16 + q] = fma(er, b[q], acc[16 + q]);
-            }
+            // partial over this pass's rows; passes add in a fixed order
+            s_e[0][i - lo] += ep;
+            s_e[1][i - lo] += et;
+            s_e[2][i - lo] += er;
         }
     }
-    // block reduction in a fixed order
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < 24; ++q) {
-        double v = acc[q];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) s_red[warp][q] = v;
-    }
     __syncthreads();
-    if (threadIdx.x < 24) {
+    // project on the basis b_q(s) = 1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3,
+    // s^4 s1^3: warp w produces outputs w, w+8, w+16 (24 = 3 fields x 8 terms)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int o = warp; o < 24; o += nwarp) {
+        const int f = o >> 3, q = o & 7;
         double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_red[w][threadIdx.x];
-        a.partial[(long long)u * 24 + threadIdx.x] = v;
+        for (int j = lane; j < hi - lo; j += 32) {
+            const double t = rmul(a.dt, (double)(lo + j));
+            const double s = __ddiv_rn(rsub(t, pt0), pw);
+            const double s1 = rsub(1.0, s);
+            double b = 1.0;
+            // b_q: alternate factors s, s1 starting with s
+            for (int k = 0; k < q; ++k) b *= (k & 1) ? s1 : s;
+            v = fma(s_e[f][j], b, v);
+        }
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) a.partial[(long long)u * 24 + o] = v;
     }
 }
 
@@ -666,9 +657,15 @@ int launch_adj_phase(const double2 *grad, const double2 *W, const double *pc, in
     const int rpp = (int)std::min<long long>(R, kSmemBudget / row_bytes);
     if (rpp < 1) return fail(FEW_ERR_SIZE, "adjoint: NN=%d too large for one row in shared memory", NN);
     a.rows_per_pass = rpp;
-    FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      kSmemBudget));
-    k_adj_phase<kRowBlock><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
+    if (use_theta) {
+        FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSmemBudget));
+        k_adj_phase<kRowBlock, true><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
+    } else {
+        FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSmemBudget));
+        k_adj_phase<kRowBlock, false><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
+    }
     FEW_LAUNCH_CHECK("k_adj_phase");
     return FEW_OK;
 }
@@ -704,13 +701,21 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     a.nkeys_pass = R * NN;
     a.dt = dt;
     const int colg = (NN + kGCols - 1) / kGCols;
-    if (R <= 4 * kGRowBlocks) {
-        dim3 grid(nseg, (R + 4 * kGRowBlocks - 1) / (4 * kGRowBlocks), colg);
-        k_adj_G<4><<<grid, kAdjThreads, 0, st>>>(a);
-    } else {
-        dim3 grid(nseg, (R + 8 * kGRowBlocks - 1) / (8 * kGRowBlocks), colg);
-        k_adj_G<8><<<grid, kAdjThreads, 0, st>>>(a);
+    // rows per CTA = 4 row blocks x RB; take the RB with the least padding
+    int best = 4, best_pad = 1 << 30;
+    for (int rb : {4, 6, 8}) {
+        const int rg = kGRowBlocks * rb;
+        const int pad = (R + rg - 1) / rg * rg - R;
+        if (pad < best_pad || (pad == best_pad && rb > best)) {
+            best = rb;
+            best_pad = pad;
+        }
     }
+    const int rg = kGRowBlocks * best;
+    dim3 grid(nseg, (R + rg - 1) / rg, colg);
+    if (best == 4) k_adj_G<4><<<grid, kAdjThreads, 0, st>>>(a);
+    else if (best == 6) k_adj_G<6><<<grid, kAdjThreads, 0, st>>>(a);
+    else k_adj_G<8><<<grid, kAdjThreads, 0, st>>>(a);
     FEW_LAUNCH_CHECK("k_adj_G");
     return FEW_OK;
 }

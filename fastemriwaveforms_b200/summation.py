@@ -363,6 +363,8 @@ class InterpolatedModeSum(SummationBase):
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.precision = precision
+        if not 1 <= int(chunk) <= 1024:
+            raise ValueError("chunk must be within 1..1024 output samples")
         self.chunk = int(chunk)
         self._fold_cache: OrderedDict = OrderedDict()
         self.record_stages = False  # set True to time the kernels of each call with CUDA events

@@ -249,7 +249,8 @@ FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs,
  * Phasors are recomputed from the phase polynomials, not stored.  All other
  * arguments are the forward's. */
 
-/* dL/d(phase coefficients), per work unit: partial [device] (nunits, 24) =
+/* dL/d(phase coefficients), per work unit (units of at most 1024 samples, as
+ * few_segment_plan makes them with chunk <= 1024): partial [device] (nunits, 24) =
  * sum over the unit's samples of dL/dPhi_f(t_i) b_q(s_i), f = phi, theta, r,
  * b_q the 8-term basis (1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3, s^4 s1^3). */
 FEW_API int few_adjoint_phase(const void *grad, const void *W, const double *phase_coeffs, int N,
