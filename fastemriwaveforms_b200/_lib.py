@@ -55,6 +55,8 @@ SIGNATURES = {
     "few_fold_mixed": [_vp, _vp, _c_int, _c_int, _c_int, _vp, _vp],
     "few_sum_mixed": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
                       _vp, _vp],
+    "few_sum_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp],
+    "few_sum_mixed_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _vp, _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
 }

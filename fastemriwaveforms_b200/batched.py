@@ -1,0 +1,236 @@
+"""Many waveforms of uneven length, knot count and mode count in one
+persistent launch, optionally captured in a CUDA graph.
+
+The reference sums one waveform at a time, one kernel launch per knot segment
+(src/few/cutils/interpolate.cu:745-781).  Here every waveform of a batch gets
+its spline build and fold (small launches), and then a single persistent sum
+kernel (``few_sum_batched`` / ``few_sum_mixed_batched``) strides over the work
+units of all waveforms, longest units first, so the SMs stay busy while short
+and long waveforms finish together.  The unit length and the CTAs per SM come
+from the autotuner (``fastemriwaveforms_b200.autotune``).  ``capture()``
+records the whole forward (and, with ``backward=True``, the adjoint of every
+waveform for fixed upstream-gradient buffers) in one CUDA graph; ``replay()``
+re-runs it after new amplitudes / phase coefficients are written into the
+static input buffers (``update``).
+
+Gradients of a batched forward are the FP64 adjoint of each waveform, as for
+``InterpolatedModeSum``.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib, autotune
+from .summation import InterpolatedModeSum, _device, _ptr, _stream
+from .synthetic import output_length
+
+# Layout of few_wave_desc (include/few_b200.h): 8 pointers, 6 ints, 1 double.
+DESC_DTYPE = np.dtype([("wf", "u8"), ("W", "u8"), ("Bpk", "u8"), ("pc", "u8"), ("seg_info", "u8"),
+                       ("t_knots", "u8"), ("row_m", "u8"), ("row_k", "u8"), ("N", "i4"), ("R", "i4"),
+                       ("nlo", "i4"), ("NN", "i4"), ("use_theta", "i4"), ("reserved", "i4"), ("dt", "f8")])
+assert DESC_DTYPE.itemsize == 96
+
+
+def _args_of(w):
+    """(call args, T, dt) of a waveform given as ModeSumInputs or a dict."""
+    if hasattr(w, "call_args"):
+        return w.call_args(), float(w.T), float(w.dt)
+    keys = ("t", "teuk_modes", "ylms", "phase_interp_t", "phase_interp_coeffs", "l_arr", "m_arr", "k_arr", "n_arr")
+    return tuple(w[k] for k in keys), float(w.get("T", 1.0)), float(w.get("dt", 10.0))
+
+
+class BatchedInterpolatedModeSum:
+    """Batched interpolated mode sum.
+
+    args:
+        precision: "mixed" (tensor cores), "exact" or "faithful" (FP64).
+        autotune: choose the unit length and CTAs per SM by timing (cached).
+        chunk, ctas_per_sm: fixed tile shape (overrides the autotuner).
+    """
+
+    def __init__(self, precision: str = "mixed", device=None, autotune: bool = True, chunk: int | None = None,
+                 ctas_per_sm: int | None = None):
+        if precision not in ("mixed", "exact", "faithful"):
+            raise ValueError("precision must be 'mixed', 'exact' or 'faithful'")
+        self.precision = precision
+        self.device = _device(device)
+        self.autotune = autotune
+        self.chunk = chunk
+        self.ctas_per_sm = ctas_per_sm
+        self.graph = None
+        self.tuning = None
+
+    # ------------------------------------------------------------------ set-up
+    def setup(self, waveforms, requires_grad: bool = False):
+        """Plans every waveform and allocates its buffers; returns self."""
+        dev = self.device
+        self.preps, self.mods, self.lengths = [], [], []
+        for w in waveforms:
+            args, T, dt = _args_of(w)
+            t = args[0]
+            t0 = float(t[0].item() if hasattr(t[0], "item") else t[0])
+            t1 = float(t[-1].item() if hasattr(t[-1], "item") else t[-1])
+            num_pts, num_pts_pad = output_length(np.array([t0, t1]), T, dt)
+            mod = InterpolatedModeSum(precision="exact", device=dev)
+            mod.num_pts = num_pts
+            prep = mod._prepare(*args, dt=dt, integrate_backwards=False)
+            if requires_grad:
+                prep.seg.backward_tables()
+            self.mods.append(mod)
+            self.preps.append(prep)
+            self.lengths.append(num_pts + num_pts_pad)
+        self.offsets = np.concatenate([[0], np.cumsum(self.lengths)]).astype(np.int64)
+        self.out = torch.zeros(int(self.offsets[-1]), dtype=torch.complex128, device=dev)
+        self.outputs = [self.out[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.preps))]
+        self.max_R = max(p.fold.R for p in self.preps)
+        max_NN = max(p.fold.NN for p in self.preps)
+        if self.precision == "mixed" and self.max_R > 128:
+            raise ValueError("precision='mixed' supports at most 128 (m, k) rows")
+        self.smem_bytes = int(min(200 * 1024, max(p.fold.R * p.fold.NN * 64 for p in self.preps)))
+        descs = np.zeros(len(self.preps), DESC_DTYPE)
+        for i, p in enumerate(self.preps):
+            p.coeffs = torch.empty((4, p.N, 2 * p.K), dtype=torch.float64, device=dev)
+            p.W = torch.empty((max(p.seg.nseg, 1), p.fold.R, p.fold.NN, 4), dtype=torch.complex128, device=dev)
+            p.Bpk = None
+            if self.precision == "mixed":
+                nbytes = int(_lib.load().few_mixed_operand_bytes(max(p.seg.nseg, 1), p.fold.R, p.fold.NN))
+                p.Bpk = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            d = descs[i]
+            d["wf"] = self.outputs[i].data_ptr()
+            d["W"] = p.W.data_ptr()
+            d["Bpk"] = p.Bpk.data_ptr() if p.Bpk is not None else 0
+            d["pc"] = p.pc.data_ptr()
+            d["seg_info"] = p.seg.d_seg_info.data_ptr()
+            d["t_knots"] = p.t_dev.data_ptr()
+            d["row_m"] = p.fold.d_row_m.data_ptr()
+            d["row_k"] = p.fold.d_row_k.data_ptr()
+            d["N"], d["R"], d["nlo"], d["NN"] = p.N, p.fold.R, p.fold.nlo, p.fold.NN
+            d["use_theta"] = p.fold.use_theta
+            d["dt"] = p.dt
+        self.descs = torch.from_numpy(descs.view(np.uint8).copy()).to(dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.mode_samples = sum(p.K * p.out_len for p in self.preps)
+        seg_lens = [np.diff(p.seg.seg_start).mean() for p in self.preps if p.seg.nseg > 0]
+        self._key = autotune.key_of(dev, self.precision, self.max_R, max_NN, float(np.mean(seg_lens)),
+                                    len(self.preps))
+        self.sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        chunk, per_sm = self.chunk, self.ctas_per_sm
+        if chunk is None or per_sm is None:
+            cached = autotune.lookup(self._key) if self.autotune else None
+            if cached is None and self.autotune:
+                self._prepare_operands()
+                cached = autotune.tune(self._key, self._runner)
+            if cached is None:
+                cached = {"chunk": 1024, "ctas_per_sm": 2 if self.precision != "mixed" else 2}
+            self.tuning = cached
+            chunk = chunk or cached["chunk"]
+            per_sm = per_sm or cached["ctas_per_sm"]
+        self.chunk, self.ctas_per_sm = int(chunk), int(per_sm)
+        self.units = self._units(self.chunk)
+        return self
+
+    def _units(self, chunk: int) -> torch.Tensor:
+        """Work units {waveform, segment, first, end} of every waveform, longest
+        (in key-samples) first so the persistent CTAs finish together."""
+        rows = []
+        for w, p in enumerate(self.preps):
+            st = p.seg.seg_start
+            for j in range(p.seg.nseg):
+                a, b = int(st[j]), int(st[j + 1])
+                for u in range(a, b, chunk):
+                    rows.append((w, j, u, min(u + chunk, b), (min(u + chunk, b) - u) * p.fold.R * p.fold.NN))
+        arr = np.array(rows, dtype=np.int64).reshape(-1, 5)
+        order = np.argsort(-arr[:, 4], kind="stable")
+        units = np.ascontiguousarray(arr[order, :4].astype(np.int32))
+        return torch.from_numpy(units.reshape(-1)).to(self.device)
+
+    # ------------------------------------------------------------ the kernels
+    def _prepare_operands(self):
+        """Spline builds and folds of every waveform (per-waveform launches)."""
+        for p in self.preps:
+            st = p.st
+            _lib.call("few_spline_build_factored", _ptr(p.fac), _ptr(p.teuk), 2 * p.K, 2, p.K, 1, 2 * p.K, p.N,
+                      _ptr(p.coeffs), _lib.FEW_LAYOUT_KNOT_MAJOR, st)
+            _lib.call("few_fold_coeffs", _ptr(p.coeffs), _ptr(p.ylm), _ptr(p.fold.d_key_ptr), _ptr(p.fold.d_key_list),
+                      p.K, p.N, p.seg.nseg, p.fold.R, p.fold.NN, _ptr(p.W), st)
+            if p.Bpk is not None:
+                _lib.call("few_fold_mixed", _ptr(p.W), _ptr(p.t_dev), p.seg.nseg, p.fold.R, p.fold.NN, _ptr(p.Bpk),
+                          st)
+
+    def _sum(self, units: torch.Tensor, ctas: int):
+        st = _stream(self.device)
+        nunits = units.numel() // 4
+        if self.precision == "mixed":
+            _lib.call("few_sum_mixed_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.max_R,
+                      ctas, _ptr(self.err), st)
+        else:
+            mode = _lib.FEW_SUM_FAITHFUL if self.precision == "faithful" else _lib.FEW_SUM_EXACT
+            _lib.call("few_sum_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.smem_bytes, mode,
+                      ctas, st)
+
+    def _runner(self, chunk: int, per_sm: int):
+        units = self._units(chunk)
+
+        def run():
+            self.out.zero_()
+            self._sum(units, per_sm * self.sms)
+
+        return run
+
+    def forward(self):
+        """All waveforms; returns the list of output tensors (views of one buffer)."""
+        self.out.zero_()
+        self._prepare_operands()
+        self._sum(self.units, self.ctas_per_sm * self.sms)
+        return self.outputs
+
+    def backward(self, grads):
+        """FP64 adjoint of every waveform for upstream gradients grads[i]
+        (torch's convention for a complex output); returns a list of
+        (dL/d teuk_modes, dL/d phase_interp_coeffs)."""
+        return [InterpolatedModeSum._backward(p, g) for p, g in zip(self.preps, grads)]
+
+    def mixed_error(self) -> bool:
+        return bool(int(self.err.item()) != 0)
+
+    # ------------------------------------------------------------ CUDA graphs
+    def update(self, i: int, teuk_modes=None, phase_interp_coeffs=None):
+        """Write new inputs of waveform i into the static buffers the graph reads."""
+        p = self.preps[i]
+        if teuk_modes is not None:
+            p.teuk.copy_(torch.as_tensor(teuk_modes, dtype=torch.complex128))
+        if phase_interp_coeffs is not None:
+            pc = torch.as_tensor(phase_interp_coeffs, dtype=torch.float64).to(self.device)
+            p.pc.copy_(pc.permute(2, 0, 1))
+
+    def capture(self, backward: bool = False, grads=None):
+        """Records forward (+ backward for the static gradient buffers `grads`,
+        zeros if None) in one CUDA graph."""
+        if backward:
+            self.grad_in = [torch.zeros_like(o) if grads is None else torch.as_tensor(g).to(self.device).clone()
+                            for o, g in zip(self.outputs, grads or [None] * len(self.outputs))]
+        # warm up outside the capture (sets kernel attributes, fills caches)
+        self.forward()
+        if backward:
+            self.backward(self.grad_in)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(self.graph, stream=s):
+                for p in self.preps:
+                    p.st = s.cuda_stream
+                self.forward()
+                self.grad_out = self.backward(self.grad_in) if backward else None
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        for p in self.preps:
+            p.st = _stream(self.device)
+        return self
+
+    def replay(self):
+        if self.graph is None:
+            raise RuntimeError("capture() first")
+        self.graph.replay()
+        return self.outputs

@@ -2,7 +2,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "few_common.cuh"
@@ -24,6 +27,22 @@ int fail(int code, const char *fmt, ...)
 }
 
 void clear_error() { g_last_error[0] = '\0'; }
+
+cudaError_t ensure_smem_attr(const void *kernel, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> done;  // (kernel, device) -> bytes set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kernel, dev);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
+}
 
 }  // namespace few
 

@@ -35,6 +35,10 @@ void clear_error();
                                cudaGetErrorString(few_err_));                                \
     } while (0)
 
+// Raises a kernel's dynamic shared-memory limit once per device (not during a
+// stream capture after the first call).
+cudaError_t ensure_smem_attr(const void *kernel, int bytes);
+
 // Host-side fold plan and segment plan (plan.cpp), also used by the
 // reference-shaped entry point.
 int fold_plan(const int *m, const int *k, const int *n, int K, int max_rows, int max_keys, int *row_m,

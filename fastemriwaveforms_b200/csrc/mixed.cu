@@ -225,37 +225,30 @@ struct MixedArgs {
     double dt;
 };
 
-__global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
+__device__ __forceinline__ void mixed_dims_dev(int R, int NN, int &NNp, int &NB, int &nchunks)
 {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    NNp = (NN + 31) / 32 * 32;
+    NB = max(16, (2 * R + 15) / 16 * 16);
+    nchunks = NNp / 8;
+}
+
+// One work unit (samples [lo, hi) of segment seg) on the tensor cores.  The
+// caller owns the TMEM accumulator (tmem), the mbarrier and its phase.
+// Returns false (for every thread) if a tensor-core wait timed out.
+__device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, uint32_t tmem,
+                           uint64_t *bar, uint32_t &phase, int *s_rm, int *s_rk, double *s_pc)
+{
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int NB = a.NB;
     unsigned char *sA_hi = smem_raw;                   // 128 x 64 bf16 = 16 KB
     unsigned char *sA_lo = sA_hi + kMT * kKC * 2;      // 16 KB
     unsigned char *sB_hi = sA_lo + kMT * kKC * 2;      // NB x 64 bf16
     unsigned char *sB_lo = sB_hi + NB * kKC * 2;
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_pc[24];
-
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int u = blockIdx.x;
-    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
     const int R = a.R, NN = a.NN, NNp = a.NNp, nlo = a.nlo;
     const long long nps = (long long)(a.N - 1) * 3;
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"((uint32_t)a.tmem_cols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (tid == 0) {
-        mbar_init(&s_bar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
     for (int r = tid; r < R; r += blockDim.x) {
         s_rm[r] = a.row_m[r];
         s_rk[r] = a.row_k[r];
@@ -267,12 +260,10 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = s_tmem;
     const uint32_t idesc = idesc_bf16(kMT, NB);
     const uint32_t aH = smem_u32(sA_hi), aL = smem_u32(sA_lo), bH = smem_u32(sB_hi), bL = smem_u32(sB_lo);
     const int halves = NNp / 32;
     const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * a.nchunks * 2 * NB * kKC;
-    uint32_t phase = 0;
     bool failed = false;
 
     for (int base = lo; base < hi && !failed; base += kMT) {
@@ -338,14 +329,11 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
                         mma_bf16(tmem, da_h, db_l, idesc, 1u);
                         mma_bf16(tmem, da_l, db_h, idesc, 1u);
                     }
-                    mma_commit(&s_bar);
+                    mma_commit(bar);
                 }
-                const bool ok = mbar_wait_bounded(&s_bar, phase);
+                const bool ok = mbar_wait_bounded(bar, phase);
                 phase ^= 1u;
-                if (__syncthreads_or(!ok)) {
-                    failed = true;
-                    if (tid == 0) atomicExch(a.err, 1);
-                }
+                if (__syncthreads_or(!ok)) failed = true;
             }
         }
         if (failed) break;
@@ -389,17 +377,97 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
         __syncthreads();
         tc_fence_after();
     }
-    if (failed) {
-        // let any MMA still in flight finish before TMEM is released
-        if (tid == 0) mbar_wait_bounded(&s_bar, phase);
+    return !failed;
+}
+
+__device__ __forceinline__ uint32_t mixed_setup(uint32_t *s_tmem, uint64_t *bar, int tmem_cols)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                     "r"((uint32_t)tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) {
+    tc_fence_after();
+    return *s_tmem;
+}
+
+// After a timeout: let any MMA still in flight finish, then free TMEM.
+__device__ __forceinline__ void mixed_teardown(bool failed, uint64_t *bar, uint32_t phase, uint32_t tmem,
+                                               int tmem_cols, int *err)
+{
+    if (failed && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait_bounded(bar, phase);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)a.tmem_cols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)tmem_cols)
                      : "memory");
     }
+}
+
+__global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    const uint32_t tmem = mixed_setup(&s_tmem, &s_bar, a.tmem_cols);
+    uint32_t phase = 0;
+    const int u = blockIdx.x;
+    const bool ok = mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, tmem, &s_bar,
+                               phase, s_rm, s_rk, s_pc);
+    mixed_teardown(!ok, &s_bar, phase, tmem, a.tmem_cols, a.err);
+}
+
+// Persistent form over many waveforms: TMEM and the mbarrier are set up once
+// per CTA; units {waveform, segment, first, end} are taken in stride.
+__global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_desc *__restrict__ descs,
+                                                              const int *__restrict__ units4, int nunits,
+                                                              int tmem_cols, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    const uint32_t tmem = mixed_setup(&s_tmem, &s_bar, tmem_cols);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        const few_wave_desc d = descs[units4[4 * u]];
+        MixedArgs a;
+        a.wf = (double2 *)d.wf;
+        a.Bpk = (const __nv_bfloat16 *)d.Bpk;
+        a.pc = d.phase_coeffs;
+        a.seg_info = d.seg_info;
+        a.t_knots = d.t_knots;
+        a.units = nullptr;
+        a.row_m = d.row_m;
+        a.row_k = d.row_k;
+        a.err = err;
+        a.N = d.N;
+        a.R = d.R;
+        a.nlo = d.nlo;
+        a.NN = d.NN;
+        a.use_theta = d.use_theta;
+        a.dt = d.dt;
+        a.tmem_cols = tmem_cols;
+        mixed_dims_dev(d.R, d.NN, a.NNp, a.NB, a.nchunks);
+        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, tmem, &s_bar, phase,
+                        s_rm, s_rk, s_pc);
+    }
+    mixed_teardown(!ok, &s_bar, phase, tmem, tmem_cols, err);
 }
 
 }  // namespace
@@ -461,13 +529,44 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
     a.use_theta = use_theta;
     a.dt = dt;
     const size_t smem = (size_t)2 * kMT * kKC * 2 + (size_t)2 * a.NB * kKC * 2;
-    FEW_CUDA_TRY(cudaFuncSetAttribute(k_sum_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed, (int)smem));
     k_sum_mixed<<<nunits, kMT, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_sum_mixed");
     return FEW_OK;
 }
 
+int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int nunits, int max_R, int ctas, int *err,
+                             cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    int NNp, NB, nch, cols;
+    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols);
+    if (rc) return rc;
+    if (ctas <= 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        ctas = 2 * sms;
+    }
+    ctas = std::min(ctas, nunits);
+    const size_t smem = (size_t)2 * kMT * kKC * 2 + (size_t)2 * NB * kKC * 2;
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
+    k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err);
+    FEW_LAUNCH_CHECK("k_sum_mixed_batched");
+    return FEW_OK;
+}
+
 }  // namespace few
+
+extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
+                                     int ctas, int *err, void *stream)
+{
+    few::clear_error();
+    if (!descs || !units4 || !err) return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: null pointer");
+    if (nwave < 1 || nunits < 0 || max_R < 1 || max_R > 128)
+        return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 128)");
+    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, err, (cudaStream_t)stream);
+}
 
 extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream)
 {

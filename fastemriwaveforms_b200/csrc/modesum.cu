@@ -96,16 +96,13 @@ struct SumArgs {
     double dt;
 };
 
+// One work unit (samples [lo, hi) of segment seg) of the folded sum; the
+// block's shared memory holds the segment's W rows.  Ends with a barrier so the
+// caller may reuse shared memory for the next unit.
 template <int RB, bool FAITHFUL>
-__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
+__device__ __forceinline__ void sum_unit(const SumArgs &a, int seg, int lo, int hi, double2 *sW, int *s_rm, int *s_rk,
+                                         double *s_pc)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *sW = reinterpret_cast<double2 *>(smem_raw);
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_pc[24];
-
-    const int u = blockIdx.x;
-    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const int R = a.R, NN = a.NN, nlo = a.nlo;
     const long long nps = (long long)(a.N - 1) * 3;
@@ -128,7 +125,6 @@ __global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
             for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
         }
         __syncthreads();
-
         for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             // Sample time and phases exactly as interpolate.cu:626-644.
             const double t = rmul(a.dt, (double)i);
@@ -215,20 +211,88 @@ __global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
             a.wf[i] = o;
         }
     }
+    __syncthreads();
+}
+
+template <int RB, bool FAITHFUL>
+__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    const int u = blockIdx.x;
+    sum_unit<RB, FAITHFUL>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2],
+                           reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
+}
+
+// Persistent form: CTAs stride over the work units of many waveforms; unit u
+// is {waveform, segment, first sample, end sample}.  The shared-memory budget
+// is fixed at launch; rows per pass follow each waveform's NN.
+template <int RB, bool FAITHFUL>
+__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded_batched(const few_wave_desc *__restrict__ descs,
+                                                                       const int *__restrict__ units4, int nunits,
+                                                                       int smem_bytes)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int w = units4[4 * u];
+        const few_wave_desc d = descs[w];
+        SumArgs a;
+        a.wf = (double2 *)d.wf;
+        a.W = (const double2 *)d.W;
+        a.pc = d.phase_coeffs;
+        a.seg_info = d.seg_info;
+        a.units = nullptr;
+        a.row_m = d.row_m;
+        a.row_k = d.row_k;
+        a.N = d.N;
+        a.R = d.R;
+        a.nlo = d.nlo;
+        a.NN = d.NN;
+        a.use_theta = d.use_theta;
+        a.dt = d.dt;
+        a.rows_per_pass = max(1, min(d.R, smem_bytes / (d.NN * 4 * (int)sizeof(double2))));
+        sum_unit<RB, FAITHFUL>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3],
+                               reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
+    }
 }
 
 template <int RB, bool F>
 int launch_sum_t(const SumArgs &a, int nunits, size_t smem, cudaStream_t st)
 {
-    // Per-device attribute; cheap, so set on every launch (one process may drive several devices).
-    FEW_CUDA_TRY(cudaFuncSetAttribute(k_sum_folded<RB, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      kSmemBudget));
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded<RB, F>, kSmemBudget));
     k_sum_folded<RB, F><<<nunits, kSumThreads, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_sum_folded");
     return FEW_OK;
 }
 
 }  // namespace
+
+int launch_sum_folded_batched(const few_wave_desc *descs, const int *units4, int nunits, int smem_bytes, int mode,
+                              int ctas, cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    if (smem_bytes < 64 || smem_bytes > kSmemBudget)
+        return fail(FEW_ERR_SIZE, "few_sum_batched: shared memory %d out of range", smem_bytes);
+    if (ctas <= 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        ctas = 2 * sms;
+    }
+    ctas = std::min(ctas, nunits);
+    if (mode == FEW_SUM_FAITHFUL) {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<kRowBlock, true>, kSmemBudget));
+        k_sum_folded_batched<kRowBlock, true><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
+    } else {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<kRowBlock, false>, kSmemBudget));
+        k_sum_folded_batched<kRowBlock, false><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
+    }
+    FEW_LAUNCH_CHECK("k_sum_folded_batched");
+    return FEW_OK;
+}
 
 int launch_fold(const double *coeffs, const double2 *ylms, const int *key_ptr, const int *key_list, int K, int N,
                 int nseg, int R, int NN, double2 *W, cudaStream_t st)
@@ -282,6 +346,16 @@ extern "C" int few_fold_coeffs(const double *coeffs, const void *ylms, const int
         return few::fail(FEW_ERR_SIZE, "few_fold_coeffs: bad sizes");
     return few::launch_fold(coeffs, (const double2 *)ylms, key_ptr, key_list, K, N, nseg, R, NN, (double2 *)W,
                             (cudaStream_t)stream);
+}
+
+extern "C" int few_sum_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int smem_bytes,
+                               int mode, int ctas, void *stream)
+{
+    few::clear_error();
+    if (!descs || !units4) return few::fail(FEW_ERR_ARG, "few_sum_batched: null pointer");
+    if (nwave < 1 || nunits < 0) return few::fail(FEW_ERR_SIZE, "few_sum_batched: bad sizes");
+    if (mode != FEW_SUM_FAITHFUL && mode != FEW_SUM_EXACT) return few::fail(FEW_ERR_ARG, "few_sum_batched: bad mode");
+    return few::launch_sum_folded_batched(descs, units4, nunits, smem_bytes, mode, ctas, (cudaStream_t)stream);
 }
 
 extern "C" int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, int N, const double *seg_info,

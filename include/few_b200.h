@@ -44,6 +44,21 @@ extern "C" {
 #define FEW_LAYOUT_KNOT_MAJOR 0   /* (4, length, ninterps): CubicSplineInterpolant.interp_array */
 #define FEW_LAYOUT_INTERP_MAJOR 1 /* (4, ninterps, length): interpolate_arrays' in-place layout */
 
+/* One waveform of a batched (persistent) launch: device pointers to its
+ * arrays, as the single-waveform entry points take them. */
+typedef struct few_wave_desc {
+    void *wf;                   /* (out_len,) complex, accumulated                     */
+    const void *W;              /* folded coefficients (few_fold_coeffs)               */
+    const void *Bpk;            /* tensor-core operand (few_fold_mixed), NULL if FP64  */
+    const double *phase_coeffs; /* (8, N-1, 3)                                         */
+    const double *seg_info;     /* (3*(N-1),) from few_segment_plan                    */
+    const double *t_knots;      /* (N,) amplitude knots                                */
+    const int *row_m;           /* (R,) fold rows                                      */
+    const int *row_k;           /* (R,)                                                */
+    int N, R, nlo, NN, use_theta, reserved;
+    double dt;
+} few_wave_desc;
+
 /* Message of the last failed call on the calling thread ("" if none). */
 FEW_API const char *few_last_error(void);
 
@@ -216,6 +231,16 @@ FEW_API int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, 
                    const int *units, int nunits, const int *row_m, const int *row_k, int R, int nlo,
                    int NN, double dt, int mode, int use_theta, void *stream);
 
+/* Persistent form of few_sum_folded over many waveforms (no counterpart in
+ * the reference, which launches one kernel per knot segment of one waveform):
+ * descs [device] (nwave,); units4 [device] (4*nunits,) = {waveform, segment,
+ * first sample, end sample}, segments' samples as few_segment_plan makes
+ * them (units of one waveform must not overlap).  smem_bytes: dynamic shared
+ * memory per CTA (<= 200 KiB; the largest R*NN*64 of the batch, capped);
+ * ctas: persistent CTAs (0: two per SM).  mode FEW_SUM_FAITHFUL or FEW_SUM_EXACT. */
+FEW_API int few_sum_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int smem_bytes,
+                            int mode, int ctas, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Mixed-precision sum on tcgen05 tensor cores (no counterpart in the        */
 /* reference, which computes in FP64 only)                                  */
@@ -240,6 +265,14 @@ FEW_API int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R
 FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
                           const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
                           int R, int nlo, int NN, double dt, int use_theta, int *err, void *stream);
+
+/* Persistent form of few_sum_mixed over many waveforms: descs [device]
+ * (nwave,) with Bpk set (few_fold_mixed per waveform); units4 [device]
+ * (4*nunits,) = {waveform, segment, first sample, end sample}; max_R: the
+ * largest R in the batch (<= 128, sizes shared memory and TMEM); ctas:
+ * persistent CTAs (0: two per SM); err [device] int as in few_sum_mixed. */
+FEW_API int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
+                                  int ctas, int *err, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Adjoint (no counterpart in the reference: it has no gradients)           */
