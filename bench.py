@@ -48,6 +48,9 @@ def parse():
                     help="output samples of the bounded single-core reference run (cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=32,
+                    help="waveforms of the uneven batch (drawn from the 256-waveform distribution)")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
     ap.add_argument("--profile-form", choices=["forward", "fwd_bwd"], default="forward",
@@ -334,6 +337,79 @@ def time_fwd_bwd(precision, inp, dev, steps, warmup):
     return a.elapsed_time(b) / steps, teuk.grad.detach().clone(), pc.grad.detach().clone()
 
 
+def bench_batched(count: int, dev, steps: int):
+    """Uneven batch (T ~ logU[1e5, 3.15e6] samples, N ~ U[50, 2000], K ~ U[200, 3843]):
+    looping InterpolatedModeSum (plain FP64, one call per waveform) vs the
+    persistent batched launch in a CUDA graph (mixed form), forward and
+    forward+backward."""
+    import torch
+
+    from fastemriwaveforms_b200 import InterpolatedModeSum
+    from fastemriwaveforms_b200 import synthetic as S
+    from fastemriwaveforms_b200.batched import BatchedInterpolatedModeSum
+
+    cases = S.batch_cases(count=count, seed=5)
+    ms_total = sum(c.num_modes * c.out_len for c in cases)
+    # loop: one plain FP64 call per waveform, inputs in HBM
+    loop = InterpolatedModeSum(precision="faithful")
+    dev_args = []
+    for c in cases:
+        dev_args.append((c.t, torch.from_numpy(c.teuk_modes).to(dev), torch.from_numpy(c.ylms).to(dev), c.phase_t,
+                         torch.from_numpy(c.phase_coeffs).to(dev), c.l, c.m, c.k, c.n))
+    for a_, c in zip(dev_args[:2], cases[:2]):
+        loop(*a_, T=c.T, dt=c.dt)
+    torch.cuda.synchronize()
+    per = []
+    ea = torch.cuda.Event(enable_timing=True)
+    eb = torch.cuda.Event(enable_timing=True)
+    ea.record()
+    for a_, c in zip(dev_args, cases):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        loop(*a_, T=c.T, dt=c.dt)
+        e1.record()
+        per.append((e0, e1))
+    eb.record()
+    torch.cuda.synchronize()
+    loop_ms = ea.elapsed_time(eb)
+    per_ms = sorted(e0.elapsed_time(e1) for e0, e1 in per)
+    del dev_args
+    out = {"waveforms": count, "mode_samples": ms_total,
+           "loop_plain_fp64": {"ms_total": loop_ms, "value": ms_total / (loop_ms * 1e-3),
+                               "p50_ms": per_ms[len(per_ms) // 2], "p99_ms": per_ms[min(len(per_ms) - 1,
+                                                                                         int(0.99 * len(per_ms)))]}}
+    # batched mixed, forward graph and forward+backward graph
+    b = BatchedInterpolatedModeSum(precision="mixed").setup(cases, requires_grad=True)
+    outs = b.forward()
+    grads = [torch.conj(o).clone() for o in outs]
+    b.capture(backward=False)
+    b.replay()
+    torch.cuda.synchronize()
+    ea.record()
+    for _ in range(steps):
+        b.replay()
+    eb.record()
+    torch.cuda.synchronize()
+    fwd_ms = ea.elapsed_time(eb) / steps
+    b.capture(backward=True, grads=grads)
+    b.replay()
+    torch.cuda.synchronize()
+    ea.record()
+    for _ in range(steps):
+        b.replay()
+    eb.record()
+    torch.cuda.synchronize()
+    fb_ms = ea.elapsed_time(eb) / steps
+    out["batched_mixed_graph"] = {"fwd_ms": fwd_ms, "fwd_value": ms_total / (fwd_ms * 1e-3),
+                                  "fwd_ms_per_waveform": fwd_ms / count, "fwd_bwd_ms": fb_ms,
+                                  "fwd_bwd_value": ms_total / (fb_ms * 1e-3), "tuning": b.tuning,
+                                  "chunk": b.chunk, "ctas_per_sm": b.ctas_per_sm, "mixed_error": b.mixed_error()}
+    del b
+    torch.cuda.empty_cache()
+    return out
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -497,6 +573,8 @@ def main():
     for prec in ("exact", "mixed"):
         fb_adj[prec] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1)[0]}
 
+    batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
+
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
     flops_per_key_sample = 30 if args.precision == "faithful" else 20
@@ -525,7 +603,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "cpu_baseline": cpu, "clocks": clk,
+            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "cpu_baseline": cpu, "clocks": clk,
             "device": torch.cuda.get_device_name(dev)}
     print(json.dumps(line), flush=True)
     if world > 1:
