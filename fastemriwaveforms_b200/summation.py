@@ -340,11 +340,12 @@ class _ModeSumFunction(torch.autograd.Function):
         module._launch(prep, out)
         prep.teuk_in = prep.pc_in = None  # do not keep the autograd inputs alive through ctx
         ctx.prep = prep
+        ctx.module = module
         return out
 
     @staticmethod
     def backward(ctx, grad):
-        g_teuk, g_pc = InterpolatedModeSum._backward(ctx.prep, grad, ctx.needs_input_grad[0], ctx.needs_input_grad[1])
+        g_teuk, g_pc = ctx.module._backward_hook(ctx.prep, grad, ctx.needs_input_grad[0], ctx.needs_input_grad[1])
         return g_teuk, g_pc, None, None, None
 
 
@@ -500,6 +501,10 @@ class InterpolatedModeSum(SummationBase):
         self._last_plan = (fold, seg)
         p.W = W
         return out
+
+    def _backward_hook(self, p, grad, need_teuk, need_pc):
+        """The backward of one call (overridden by the sharded summation)."""
+        return InterpolatedModeSum._backward(p, grad, need_teuk, need_pc)
 
     @staticmethod
     def _backward(p, grad, need_teuk=True, need_pc=True):

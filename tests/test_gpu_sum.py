@@ -204,3 +204,34 @@ def test_sum_rejects_bad_inputs(cuda):
         InterpolatedModeSum(output_type="wd")
     with pytest.raises(ValueError):
         InterpolatedModeSum(precision="half")
+
+
+def test_sharded_ranks_sum_to_the_whole(cuda):
+    """Ranks of a split waveform (run one after another on one GPU, without
+    collectives): their slices add up to the whole waveform bitwise and their
+    partial gradients to the whole gradient."""
+    from fastemriwaveforms_b200.distributed import ShardedInterpolatedModeSum
+
+    inp = S.plain_small()
+    whole, _ = run(inp, precision="exact")
+    world = 3
+    parts = []
+    g_teuk, g_pc = 0, 0
+    rng = np.random.default_rng(0)
+    G = torch.tensor(rng.standard_normal(len(whole)) + 1j * rng.standard_normal(len(whole)), device=cuda)
+    for r in range(world):
+        ims = ShardedInterpolatedModeSum(rank=r, world=world, gather=False, reduce_grads=False, precision="exact")
+        parts.append(ims(*inp.call_args(), T=inp.T, dt=inp.dt).cpu().numpy())
+        teuk = torch.tensor(inp.teuk_modes, device=cuda, requires_grad=True)
+        pc = torch.tensor(inp.phase_coeffs, device=cuda, requires_grad=True)
+        ims(inp.t, teuk, inp.ylms, inp.phase_t, pc, inp.l, inp.m, inp.k, inp.n, T=inp.T, dt=inp.dt).backward(G)
+        g_teuk = g_teuk + teuk.grad.cpu().numpy()
+        g_pc = g_pc + pc.grad.cpu().numpy()
+    assert np.array_equal(sum(parts), whole)
+    teuk = torch.tensor(inp.teuk_modes, device=cuda, requires_grad=True)
+    pc = torch.tensor(inp.phase_coeffs, device=cuda, requires_grad=True)
+    InterpolatedModeSum(precision="exact")(inp.t, teuk, inp.ylms, inp.phase_t, pc, inp.l, inp.m, inp.k, inp.n,
+                                           T=inp.T, dt=inp.dt).backward(G)
+    ref_t, ref_p = teuk.grad.cpu().numpy(), pc.grad.cpu().numpy()
+    assert np.abs(g_teuk - ref_t).max() <= 1e-11 * np.abs(ref_t).max()
+    assert np.abs(g_pc - ref_p).max() <= 1e-11 * np.abs(ref_p).max()
