@@ -162,15 +162,17 @@ __device__ __forceinline__ float2 fcpow(float2 z, int p)
     return r;
 }
 
-// exp(-i phi) in FP64 with the argument reduced mod 2 pi first, rounded to FP32.
+// exp(-i phi): the argument is reduced mod 2 pi in FP64 (phi reaches ~1e7 rad,
+// where FP32 would keep no fraction of a turn), then sine and cosine are taken
+// in FP32 on the reduced value in [-pi, pi].
 __device__ __forceinline__ float2 anchor(double phi)
 {
     const double two_pi = 6.283185307179586476925286766559;
-    const double k = rint(phi / two_pi);
-    const double red = fma(-k, two_pi, phi);
-    double s, c;
-    sincos(red, &s, &c);
-    return make_float2((float)c, (float)-s);
+    const double k = rint(phi * 0.15915494309189533576888376337251);
+    const float red = (float)fma(-k, two_pi, phi);
+    float s, c;
+    sincosf(red, &s, &c);
+    return make_float2(c, -s);
 }
 
 // ---------------------------------------------------------------------------
@@ -232,18 +234,53 @@ __device__ __forceinline__ void mixed_dims_dev(int R, int NN, int &NNp, int &NB,
     nchunks = NNp / 8;
 }
 
-// One work unit (samples [lo, hi) of segment seg) on the tensor cores.  The
-// caller owns the TMEM accumulator (tmem), the mbarrier and its phase.
-// Returns false (for every thread) if a tensor-core wait timed out.
-__device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, uint32_t tmem,
-                           uint64_t *bar, uint32_t &phase, int *s_rm, int *s_rk, double *s_pc)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Tensor-core state a CTA carries across units: TMEM accumulator, one
+// mbarrier per A/B buffer, their phases and whether a commit is outstanding
+// (scalars, so that nothing is indexed at run time and all stays in registers).
+struct MixedPipe {
+    uint32_t tmem;
+    uint64_t *bar;  // [2]
+    uint32_t ph0, ph1;
+    int pend0, pend1;
+};
+
+// Bounded wait for buffer b's outstanding MMAs.
+__device__ __forceinline__ bool pipe_drain(MixedPipe &p, int b)
+{
+    if (b == 0) {
+        if (!p.pend0) return true;
+        const bool ok = mbar_wait_bounded(&p.bar[0], p.ph0);
+        p.ph0 ^= 1u;
+        p.pend0 = 0;
+        return ok;
+    }
+    if (!p.pend1) return true;
+    const bool ok = mbar_wait_bounded(&p.bar[1], p.ph1);
+    p.ph1 ^= 1u;
+    p.pend1 = 0;
+    return ok;
+}
+
+// One work unit (samples [lo, hi) of segment seg) on the tensor cores.  Two
+// A/B buffers: while the tensor cores run chunk k's MMAs from one buffer, the
+// threads generate chunk k+1 into the other and its B tile arrives by
+// cp.async.  Returns false (for every thread) if a tensor-core wait timed out.
+__device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, MixedPipe &pp,
+                           int *s_rm, int *s_rk, double *s_pc)
 {
     const int tid = threadIdx.x, warp = tid >> 5;
     const int NB = a.NB;
-    unsigned char *sA_hi = smem_raw;                   // 128 x 64 bf16 = 16 KB
-    unsigned char *sA_lo = sA_hi + kMT * kKC * 2;      // 16 KB
-    unsigned char *sB_hi = sA_lo + kMT * kKC * 2;      // NB x 64 bf16
-    unsigned char *sB_lo = sB_hi + NB * kKC * 2;
+    const int bbytes = 2 * NB * kKC * 2;  // one B buffer: hi then lo
+    // A buffers (hi 16 KB then lo 16 KB each) at 0 and 32 KB, B buffers after them
+    unsigned char *const sA0 = smem_raw;
+    unsigned char *const sB0 = smem_raw + 4 * kMT * kKC * 2;
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
     const int R = a.R, NN = a.NN, NNp = a.NNp, nlo = a.nlo;
@@ -261,8 +298,8 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
     __syncthreads();
     tc_fence_after();
     const uint32_t idesc = idesc_bf16(kMT, NB);
-    const uint32_t aH = smem_u32(sA_hi), aL = smem_u32(sA_lo), bH = smem_u32(sB_hi), bL = smem_u32(sB_lo);
     const int halves = NNp / 32;
+    const int nch = 4 * halves;
     const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * a.nchunks * 2 * NB * kKC;
     bool failed = false;
 
@@ -281,66 +318,79 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
         const float2 Ep = anchor(Pp);
         const float2 Er = anchor(Pr);
         const float2 Et = a.use_theta ? anchor(Pt) : make_float2(1.f, 0.f);
-        const float taup[4] = {1.f, tau, tau * tau, tau * tau * tau};
+        const float tau2 = tau * tau, tau3 = tau2 * tau;
+        float2 v[32];
 
-        for (int hh = 0; hh < halves && !failed; ++hh) {
-            const int n0 = nlo + 32 * hh;
-            float2 v[32];
-            v[0] = anchor((double)n0 * Pr);
-#pragma unroll
-            for (int q = 1; q < 32; ++q) v[q] = fcmul(v[q - 1], Er);
-#pragma unroll
-            for (int q = 0; q < 32; ++q)
-                if (!valid || 32 * hh + q >= NN) v[q] = make_float2(0.f, 0.f);
-            for (int c = 0; c < 4 && !failed; ++c) {
-                const int ch = c * halves + hh;
-                const float sc = taup[c];
-                // A chunk, this thread's row: complex q -> real k = 2q (re), 2q+1 (im)
-#pragma unroll
-                for (int g = 0; g < 8; ++g) {  // 8 groups of 4 complex = 8 bf16 = 16 bytes
-                    uint32_t h4[4], l4[4];
-#pragma unroll
-                    for (int e2 = 0; e2 < 4; ++e2) {
-                        const float2 z = v[4 * g + e2];
-                        split2(sc * z.x, sc * z.y, h4[e2], l4[e2]);
-                    }
-                    const uint32_t off = tile_off(tid, 8 * g, kMT / 8);
-                    *reinterpret_cast<uint4 *>(sA_hi + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
-                    *reinterpret_cast<uint4 *>(sA_lo + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
-                }
-                // B chunk (hi then lo, contiguous) from global
-                {
-                    const uint4 *src = reinterpret_cast<const uint4 *>(Bseg + (long long)ch * 2 * NB * kKC);
-                    uint4 *dst = reinterpret_cast<uint4 *>(sB_hi);
-                    const int n16 = 2 * NB * kKC * 2 / 16;
-                    for (int q = tid; q < n16; q += blockDim.x) dst[q] = src[q];
-                }
-                fence_async_smem();
-                __syncthreads();
-                if (tid == 0) {
-                    tc_fence_after();
-#pragma unroll
-                    for (int st = 0; st < kKC / 16; ++st) {
-                        const uint64_t da_h = smem_desc(aH + st * (kMT / 8) * 256, 128, 256);
-                        const uint64_t da_l = smem_desc(aL + st * (kMT / 8) * 256, 128, 256);
-                        const uint64_t db_h = smem_desc(bH + st * (NB / 8) * 256, 128, 256);
-                        const uint64_t db_l = smem_desc(bL + st * (NB / 8) * 256, 128, 256);
-                        mma_bf16(tmem, da_h, db_h, idesc, (ch | st) != 0);
-                        mma_bf16(tmem, da_h, db_l, idesc, 1u);
-                        mma_bf16(tmem, da_l, db_h, idesc, 1u);
-                    }
-                    mma_commit(bar);
-                }
-                const bool ok = mbar_wait_bounded(bar, phase);
-                phase ^= 1u;
-                if (__syncthreads_or(!ok)) failed = true;
+        for (int k = 0; k < nch && !failed; ++k) {
+            const int b = k & 1;
+            const int hh = k >> 2, c = k & 3;
+            const int ch = c * halves + hh;  // the B packing's chunk index
+            // buffer b is free once the MMAs of chunk k-2 are done
+            if (__syncthreads_or(!pipe_drain(pp, b))) {
+                failed = true;
+                break;
             }
+            unsigned char *const sBb = sB0 + b * bbytes;
+            {
+                const unsigned char *src = reinterpret_cast<const unsigned char *>(Bseg + (long long)ch * 2 * NB * kKC);
+                for (int q = tid; q < bbytes / 16; q += blockDim.x) cp_async16(sBb + 16 * q, src + 16 * q);
+                cp_async_commit();
+            }
+            if (c == 0) {
+                v[0] = anchor((double)(nlo + 32 * hh) * Pr);
+#pragma unroll
+                for (int q = 1; q < 32; ++q) v[q] = fcmul(v[q - 1], Er);
+#pragma unroll
+                for (int q = 0; q < 32; ++q)
+                    if (!valid || 32 * hh + q >= NN) v[q] = make_float2(0.f, 0.f);
+            }
+            const float sc = c == 0 ? 1.f : (c == 1 ? tau : (c == 2 ? tau2 : tau3));
+            unsigned char *const aH = sA0 + b * (2 * kMT * kKC * 2), *const aL = aH + kMT * kKC * 2;
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {  // 8 groups of 4 complex = 8 bf16 = 16 bytes
+                uint32_t h4[4], l4[4];
+#pragma unroll
+                for (int e2 = 0; e2 < 4; ++e2) {
+                    const float2 z = v[4 * g + e2];
+                    split2(sc * z.x, sc * z.y, h4[e2], l4[e2]);
+                }
+                const uint32_t off = tile_off(tid, 8 * g, kMT / 8);
+                *reinterpret_cast<uint4 *>(aH + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
+                *reinterpret_cast<uint4 *>(aL + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
+            }
+            cp_async_wait_all();
+            fence_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t a_h = smem_u32(aH), a_l = smem_u32(aL);
+                const uint32_t b_h = smem_u32(sBb), b_l = b_h + NB * kKC * 2;
+#pragma unroll
+                for (int st = 0; st < kKC / 16; ++st) {
+                    const uint64_t da_h = smem_desc(a_h + st * (kMT / 8) * 256, 128, 256);
+                    const uint64_t da_l = smem_desc(a_l + st * (kMT / 8) * 256, 128, 256);
+                    const uint64_t db_h = smem_desc(b_h + st * (NB / 8) * 256, 128, 256);
+                    const uint64_t db_l = smem_desc(b_l + st * (NB / 8) * 256, 128, 256);
+                    mma_bf16(pp.tmem, da_h, db_h, idesc, (k | st) != 0);
+                    mma_bf16(pp.tmem, da_h, db_l, idesc, 1u);
+                    mma_bf16(pp.tmem, da_l, db_h, idesc, 1u);
+                }
+                mma_commit(&pp.bar[b]);
+            }
+            if (b == 0) pp.pend0 = 1;
+            else pp.pend1 = 1;
         }
         if (failed) break;
+        // all MMAs of the tile done before the accumulator is read
+        const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
+        if (__syncthreads_or(!(ok0 && ok1))) {
+            failed = true;
+            break;
+        }
         // epilogue: this thread's accumulator row (TMEM lane = tid), 8 rows (m', k')
         // per 16-column load; u_r by one multiplication when m' steps by one
         tc_fence_after();
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
         float hr = 0.f, hi_ = 0.f;
         float2 uu = make_float2(1.f, 0.f);
         int pm = 0x7fffffff, pk = 0x7fffffff;
@@ -377,10 +427,11 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
         __syncthreads();
         tc_fence_after();
     }
+    cp_async_wait_all();
     return !failed;
 }
 
-__device__ __forceinline__ uint32_t mixed_setup(uint32_t *s_tmem, uint64_t *bar, int tmem_cols)
+__device__ __forceinline__ void mixed_setup(uint32_t *s_tmem, uint64_t *bars, int tmem_cols, MixedPipe &pp)
 {
     if ((threadIdx.x >> 5) == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
@@ -389,28 +440,31 @@ __device__ __forceinline__ uint32_t mixed_setup(uint32_t *s_tmem, uint64_t *bar,
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    return *s_tmem;
+    pp.tmem = *s_tmem;
+    pp.bar = bars;
+    pp.ph0 = pp.ph1 = 0;
+    pp.pend0 = pp.pend1 = 0;
 }
 
 // After a timeout: let any MMA still in flight finish, then free TMEM.
-__device__ __forceinline__ void mixed_teardown(bool failed, uint64_t *bar, uint32_t phase, uint32_t tmem,
-                                               int tmem_cols, int *err)
+__device__ __forceinline__ void mixed_teardown(bool failed, MixedPipe &pp, int tmem_cols, int *err)
 {
-    if (failed && threadIdx.x == 0) {
-        atomicExch(err, 1);
-        mbar_wait_bounded(bar, phase);
-    }
+    if (failed && threadIdx.x == 0) atomicExch(err, 1);
+    pipe_drain(pp, 0);
+    pipe_drain(pp, 1);
     tc_fence_before();
     __syncthreads();
     if ((threadIdx.x >> 5) == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)tmem_cols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(pp.tmem),
+                     "r"((uint32_t)tmem_cols)
                      : "memory");
     }
 }
@@ -418,31 +472,31 @@ __device__ __forceinline__ void mixed_teardown(bool failed, uint64_t *bar, uint3
 __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
     __shared__ double s_pc[24];
-    const uint32_t tmem = mixed_setup(&s_tmem, &s_bar, a.tmem_cols);
-    uint32_t phase = 0;
+    MixedPipe pp;
+    mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
     const int u = blockIdx.x;
-    const bool ok = mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, tmem, &s_bar,
-                               phase, s_rm, s_rk, s_pc);
-    mixed_teardown(!ok, &s_bar, phase, tmem, a.tmem_cols, a.err);
+    const bool ok =
+        mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
+    mixed_teardown(!ok, pp, a.tmem_cols, a.err);
 }
 
-// Persistent form over many waveforms: TMEM and the mbarrier are set up once
+// Persistent form over many waveforms: TMEM and the mbarriers are set up once
 // per CTA; units {waveform, segment, first, end} are taken in stride.
 __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_desc *__restrict__ descs,
                                                               const int *__restrict__ units4, int nunits,
                                                               int tmem_cols, int *err)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
     __shared__ double s_pc[24];
-    const uint32_t tmem = mixed_setup(&s_tmem, &s_bar, tmem_cols);
-    uint32_t phase = 0;
+    MixedPipe pp;
+    mixed_setup(&s_tmem, s_bar, tmem_cols, pp);
     bool ok = true;
     for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
         const few_wave_desc d = descs[units4[4 * u]];
@@ -464,10 +518,9 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.dt = d.dt;
         a.tmem_cols = tmem_cols;
         mixed_dims_dev(d.R, d.NN, a.NNp, a.NB, a.nchunks);
-        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, tmem, &s_bar, phase,
-                        s_rm, s_rk, s_pc);
+        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
     }
-    mixed_teardown(!ok, &s_bar, phase, tmem, tmem_cols, err);
+    mixed_teardown(!ok, pp, tmem_cols, err);
 }
 
 }  // namespace
@@ -528,7 +581,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const size_t smem = (size_t)2 * kMT * kKC * 2 + (size_t)2 * a.NB * kKC * 2;
+    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * a.NB * kKC * 2;
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed, (int)smem));
     k_sum_mixed<<<nunits, kMT, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_sum_mixed");
@@ -549,7 +602,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
         ctas = 2 * sms;
     }
     ctas = std::min(ctas, nunits);
-    const size_t smem = (size_t)2 * kMT * kKC * 2 + (size_t)2 * NB * kKC * 2;
+    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * NB * kKC * 2;
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
     k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");

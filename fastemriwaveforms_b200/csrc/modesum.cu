@@ -30,6 +30,8 @@
 // stages that segment's W block in shared memory (broadcast reads), and each
 // thread writes its own samples: no atomics, deterministic, coalesced stores.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "few_common.cuh"
 #include "few_internal.h"
@@ -97,9 +99,11 @@ struct SumArgs {
 };
 
 // One work unit (samples [lo, hi) of segment seg) of the folded sum; the
-// block's shared memory holds the segment's W rows.  Ends with a barrier so the
-// caller may reuse shared memory for the next unit.
-template <int RB, bool FAITHFUL>
+// block's shared memory holds the segment's W rows.  Each thread carries SPT
+// samples (i, i + blockDim, ...) through the key loop together, so every
+// shared-memory read of W feeds SPT samples and the samples' dependency chains
+// interleave.  Ends with a barrier so the caller may reuse shared memory.
+template <int RB, bool FAITHFUL, int SPT>
 __device__ __forceinline__ void sum_unit(const SumArgs &a, int seg, int lo, int hi, double2 *sW, int *s_rm, int *s_rk,
                                          double *s_pc)
 {
@@ -125,111 +129,143 @@ __device__ __forceinline__ void sum_unit(const SumArgs &a, int seg, int lo, int 
             for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
         }
         __syncthreads();
-        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            // Sample time and phases exactly as interpolate.cu:626-644.
-            const double t = rmul(a.dt, (double)i);
-            const double x = rsub(t, t0);
-            const double s = __ddiv_rn(rsub(t, pt0), pw);
-            const double s1 = rsub(1.0, s);
-            const double Pp = phase_poly(s_pc, s, s1);
-            const double Pr = phase_poly(s_pc + 16, s, s1);
-            const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
-            double sn, cs;
-            sincos(Pp, &sn, &cs);
-            const double2 Ep = make_double2(cs, -sn);
-            sincos(Pr, &sn, &cs);
-            const double2 Er = make_double2(cs, -sn);
-            double2 Et = make_double2(1.0, 0.0);
-            if (a.use_theta) {
-                sincos(Pt, &sn, &cs);
-                Et = make_double2(cs, -sn);
+        for (int ib = lo + threadIdx.x; ib < hi; ib += SPT * blockDim.x) {
+            double x[SPT], Pp[SPT], Pr[SPT], Pt[SPT];
+            double2 Ep[SPT], Er[SPT], Et[SPT], V0[SPT], h[SPT];
+#pragma unroll
+            for (int sm = 0; sm < SPT; ++sm) {
+                // a sample past the end repeats the first one; its result is dropped
+                const int i = (ib + sm * (int)blockDim.x < hi) ? ib + sm * (int)blockDim.x : ib;
+                // Sample time and phases exactly as interpolate.cu:626-644.
+                const double t = rmul(a.dt, (double)i);
+                x[sm] = rsub(t, t0);
+                const double s = __ddiv_rn(rsub(t, pt0), pw);
+                const double s1 = rsub(1.0, s);
+                Pp[sm] = phase_poly(s_pc, s, s1);
+                Pr[sm] = phase_poly(s_pc + 16, s, s1);
+                Pt[sm] = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
+                double sn, cs;
+                sincos(Pp[sm], &sn, &cs);
+                Ep[sm] = make_double2(cs, -sn);
+                sincos(Pr[sm], &sn, &cs);
+                Er[sm] = make_double2(cs, -sn);
+                Et[sm] = make_double2(1.0, 0.0);
+                if (a.use_theta) {
+                    sincos(Pt[sm], &sn, &cs);
+                    Et[sm] = make_double2(cs, -sn);
+                }
+                V0[sm] = cpow_int(Er[sm], nlo);
+                h[sm] = make_double2(0.0, 0.0);
             }
-            const double2 V0 = cpow_int(Er, nlo);
-            double2 h = make_double2(0.0, 0.0);
 
             for (int rb = 0; rb < nrp; rb += RB) {
-                double2 U[RB];
-                double S12[RB];
+                double2 U[SPT][RB];
+                double S12[SPT][RB];
 #pragma unroll
                 for (int q = 0; q < RB; ++q) {
-                    U[q] = make_double2(0.0, 0.0);
-                    S12[q] = 0.0;
+#pragma unroll
+                    for (int sm = 0; sm < SPT; ++sm) {
+                        U[sm][q] = make_double2(0.0, 0.0);
+                        S12[sm][q] = 0.0;
+                    }
                     if (rb + q < nrp) {
                         const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
-                        double2 uu = cpow_int(Ep, mm);
-                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
-                        if (FAITHFUL) {
-                            const double dm = (double)mm, dk = (double)kk;
-                            const double p1 = rmul(dm, Pp);
-                            const double e1 = fma(dm, Pp, -p1);
-                            const double p2 = rmul(dk, Pt);
-                            const double e2 = fma(dk, Pt, -p2);
-                            const double s12 = radd(p1, p2);
-                            const double e12 = two_sum_err(p1, p2, s12);
-                            uu = crot_small(uu, (e1 + e2) + e12);
-                            S12[q] = s12;
+#pragma unroll
+                        for (int sm = 0; sm < SPT; ++sm) {
+                            double2 uu = cpow_int(Ep[sm], mm);
+                            if (kk) uu = cmul(uu, cpow_int(Et[sm], kk));
+                            if (FAITHFUL) {
+                                const double dm = (double)mm, dk = (double)kk;
+                                const double p1 = rmul(dm, Pp[sm]);
+                                const double e1 = fma(dm, Pp[sm], -p1);
+                                const double p2 = rmul(dk, Pt[sm]);
+                                const double e2 = fma(dk, Pt[sm], -p2);
+                                const double s12 = radd(p1, p2);
+                                const double e12 = two_sum_err(p1, p2, s12);
+                                uu = crot_small(uu, (e1 + e2) + e12);
+                                S12[sm][q] = s12;
+                            }
+                            U[sm][q] = uu;
                         }
-                        U[q] = uu;
                     }
                 }
-                double2 v = V0;
+                double2 v[SPT];
+#pragma unroll
+                for (int sm = 0; sm < SPT; ++sm) v[sm] = V0[sm];
                 const double2 *wrow = sW + (long long)rb * NN * 4;
                 for (int c = 0; c < NN; ++c) {
-                    double2 vv = v;
-                    double p3 = 0.0;
-                    if (FAITHFUL) {
-                        const double dn = (double)(nlo + c);
-                        p3 = rmul(dn, Pr);
-                        vv = crot_small(v, fma(dn, Pr, -p3));
+                    double2 vv[SPT], T[SPT];
+                    double p3[SPT];
+#pragma unroll
+                    for (int sm = 0; sm < SPT; ++sm) {
+                        vv[sm] = v[sm];
+                        p3[sm] = 0.0;
+                        if (FAITHFUL) {
+                            const double dn = (double)(nlo + c);
+                            p3[sm] = rmul(dn, Pr[sm]);
+                            vv[sm] = crot_small(v[sm], fma(dn, Pr[sm], -p3[sm]));
+                        }
+                        T[sm] = make_double2(0.0, 0.0);
                     }
-                    double2 T = make_double2(0.0, 0.0);
                     const double2 *wc = wrow + c * 4;
 #pragma unroll
                     for (int q = 0; q < RB; ++q) {
                         if (rb + q < nrp) {
                             const double2 *w = wc + (long long)q * NN * 4;
                             const double2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
-                            double2 Wx;
-                            Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
-                            Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
-                            if (FAITHFUL) {
-                                const double sp = radd(S12[q], p3);
-                                Wx = crot_small(Wx, two_sum_err(S12[q], p3, sp));
+#pragma unroll
+                            for (int sm = 0; sm < SPT; ++sm) {
+                                double2 Wx;
+                                Wx.x = fma(fma(fma(w3.x, x[sm], w2.x), x[sm], w1.x), x[sm], w0.x);
+                                Wx.y = fma(fma(fma(w3.y, x[sm], w2.y), x[sm], w1.y), x[sm], w0.y);
+                                if (FAITHFUL) {
+                                    const double sp = radd(S12[sm][q], p3[sm]);
+                                    Wx = crot_small(Wx, two_sum_err(S12[sm][q], p3[sm], sp));
+                                }
+                                T[sm].x = fma(U[sm][q].x, Wx.x, fma(-U[sm][q].y, Wx.y, T[sm].x));
+                                T[sm].y = fma(U[sm][q].x, Wx.y, fma(U[sm][q].y, Wx.x, T[sm].y));
                             }
-                            T.x = fma(U[q].x, Wx.x, fma(-U[q].y, Wx.y, T.x));
-                            T.y = fma(U[q].x, Wx.y, fma(U[q].y, Wx.x, T.y));
                         }
                     }
-                    h.x = fma(vv.x, T.x, fma(-vv.y, T.y, h.x));
-                    h.y = fma(vv.x, T.y, fma(vv.y, T.x, h.y));
-                    v = cmul(v, Er);
+#pragma unroll
+                    for (int sm = 0; sm < SPT; ++sm) {
+                        h[sm].x = fma(vv[sm].x, T[sm].x, fma(-vv[sm].y, T[sm].y, h[sm].x));
+                        h[sm].y = fma(vv[sm].x, T[sm].y, fma(vv[sm].y, T[sm].x, h[sm].y));
+                        v[sm] = cmul(v[sm], Er[sm]);
+                    }
                 }
             }
-            double2 o = a.wf[i];
-            o.x += h.x;
-            o.y += h.y;
-            a.wf[i] = o;
+#pragma unroll
+            for (int sm = 0; sm < SPT; ++sm) {
+                const int i = ib + sm * (int)blockDim.x;
+                if (i < hi) {
+                    double2 o = a.wf[i];
+                    o.x += h[sm].x;
+                    o.y += h[sm].y;
+                    a.wf[i] = o;
+                }
+            }
         }
     }
     __syncthreads();
 }
 
-template <int RB, bool FAITHFUL>
-__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded(SumArgs a)
+template <int RB, bool FAITHFUL, int SPT>
+__global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_sum_folded(SumArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
     __shared__ double s_pc[24];
     const int u = blockIdx.x;
-    sum_unit<RB, FAITHFUL>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2],
-                           reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
+    sum_unit<RB, FAITHFUL, SPT>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2],
+                                reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
 }
 
 // Persistent form: CTAs stride over the work units of many waveforms; unit u
 // is {waveform, segment, first sample, end sample}.  The shared-memory budget
 // is fixed at launch; rows per pass follow each waveform's NN.
-template <int RB, bool FAITHFUL>
-__global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded_batched(const few_wave_desc *__restrict__ descs,
+template <int RB, bool FAITHFUL, int SPT>
+__global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_sum_folded_batched(const few_wave_desc *__restrict__ descs,
                                                                        const int *__restrict__ units4, int nunits,
                                                                        int smem_bytes)
 {
@@ -254,17 +290,50 @@ __global__ void __launch_bounds__(kSumThreads, 2) k_sum_folded_batched(const few
         a.use_theta = d.use_theta;
         a.dt = d.dt;
         a.rows_per_pass = max(1, min(d.R, smem_bytes / (d.NN * 4 * (int)sizeof(double2))));
-        sum_unit<RB, FAITHFUL>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3],
-                               reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
+        sum_unit<RB, FAITHFUL, SPT>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3],
+                                    reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
     }
 }
 
-template <int RB, bool F>
+template <int RB, bool F, int SPT>
 int launch_sum_t(const SumArgs &a, int nunits, size_t smem, cudaStream_t st)
 {
-    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded<RB, F>, kSmemBudget));
-    k_sum_folded<RB, F><<<nunits, kSumThreads, smem, st>>>(a);
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded<RB, F, SPT>, kSmemBudget));
+    k_sum_folded<RB, F, SPT><<<nunits, kSumThreads, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_sum_folded");
+    return FEW_OK;
+}
+
+// Shape of the FP64 sum: rows held in registers (RB) x samples per thread (SPT).
+struct SumShape {
+    int rb, spt;
+};
+
+// Measured on B200 at the one-year 3843-mode waveform: faithful 8 rows x 2
+// samples per thread (8.65 ms vs 9.17 ms for 8x1), exact 4 rows x 1 sample
+// (6.32 ms vs 7.15 ms).  FEW_B200_SUM_SHAPE="RBxSPT" overrides both.
+SumShape sum_shape(int mode)
+{
+    static const SumShape forced = [] {
+        SumShape sh{0, 0};
+        const char *v = getenv("FEW_B200_SUM_SHAPE");
+        if (v) {
+            int rb = 0, spt = 0;
+            if (sscanf(v, "%dx%d", &rb, &spt) == 2 && (rb == 4 || rb == 8) && (spt == 1 || spt == 2)) sh = {rb, spt};
+        }
+        return sh;
+    }();
+    if (forced.rb) return forced;
+    return mode == FEW_SUM_FAITHFUL ? SumShape{8, 2} : SumShape{4, 1};
+}
+
+template <int RB, bool F, int SPT>
+int launch_batched_t(const few_wave_desc *descs, const int *units4, int nunits, int smem_bytes, int ctas,
+                     cudaStream_t st)
+{
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<RB, F, SPT>, kSmemBudget));
+    k_sum_folded_batched<RB, F, SPT><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
+    FEW_LAUNCH_CHECK("k_sum_folded_batched");
     return FEW_OK;
 }
 
@@ -283,15 +352,20 @@ int launch_sum_folded_batched(const few_wave_desc *descs, const int *units4, int
         ctas = 2 * sms;
     }
     ctas = std::min(ctas, nunits);
-    if (mode == FEW_SUM_FAITHFUL) {
-        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<kRowBlock, true>, kSmemBudget));
-        k_sum_folded_batched<kRowBlock, true><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
-    } else {
-        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<kRowBlock, false>, kSmemBudget));
-        k_sum_folded_batched<kRowBlock, false><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
-    }
-    FEW_LAUNCH_CHECK("k_sum_folded_batched");
-    return FEW_OK;
+    // the same shape as the single-waveform kernel, so both give the same bits
+    const SumShape sh = sum_shape(mode);
+    const bool F = mode == FEW_SUM_FAITHFUL;
+    if (sh.rb == 4 && sh.spt == 2)
+        return F ? launch_batched_t<4, true, 2>(descs, units4, nunits, smem_bytes, ctas, st)
+                 : launch_batched_t<4, false, 2>(descs, units4, nunits, smem_bytes, ctas, st);
+    if (sh.rb == 8 && sh.spt == 2)
+        return F ? launch_batched_t<8, true, 2>(descs, units4, nunits, smem_bytes, ctas, st)
+                 : launch_batched_t<8, false, 2>(descs, units4, nunits, smem_bytes, ctas, st);
+    if (sh.rb == 4)
+        return F ? launch_batched_t<4, true, 1>(descs, units4, nunits, smem_bytes, ctas, st)
+                 : launch_batched_t<4, false, 1>(descs, units4, nunits, smem_bytes, ctas, st);
+    return F ? launch_batched_t<8, true, 1>(descs, units4, nunits, smem_bytes, ctas, st)
+             : launch_batched_t<8, false, 1>(descs, units4, nunits, smem_bytes, ctas, st);
 }
 
 int launch_fold(const double *coeffs, const double2 *ylms, const int *key_ptr, const int *key_list, int K, int N,
@@ -331,8 +405,18 @@ int launch_sum_folded(double2 *wf, const double2 *W, const double *pc, int N, co
     if (rpp < 1) return fail(FEW_ERR_SIZE, "few_sum_folded: NN=%d too large for one row in shared memory", NN);
     a.rows_per_pass = rpp;
     const size_t smem = (size_t)rpp * row_bytes;
-    if (mode == FEW_SUM_FAITHFUL) return launch_sum_t<kRowBlock, true>(a, nunits, smem, st);
-    return launch_sum_t<kRowBlock, false>(a, nunits, smem, st);
+    const SumShape sh = sum_shape(mode);
+    if (sh.rb == 4 && sh.spt == 2)
+        return mode == FEW_SUM_FAITHFUL ? launch_sum_t<4, true, 2>(a, nunits, smem, st)
+                                        : launch_sum_t<4, false, 2>(a, nunits, smem, st);
+    if (sh.rb == 8 && sh.spt == 2)
+        return mode == FEW_SUM_FAITHFUL ? launch_sum_t<8, true, 2>(a, nunits, smem, st)
+                                        : launch_sum_t<8, false, 2>(a, nunits, smem, st);
+    if (sh.rb == 4)
+        return mode == FEW_SUM_FAITHFUL ? launch_sum_t<4, true, 1>(a, nunits, smem, st)
+                                        : launch_sum_t<4, false, 1>(a, nunits, smem, st);
+    return mode == FEW_SUM_FAITHFUL ? launch_sum_t<8, true, 1>(a, nunits, smem, st)
+                                    : launch_sum_t<8, false, 1>(a, nunits, smem, st);
 }
 
 }  // namespace few
