@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib, autotune
-from .summation import InterpolatedModeSum, _device, _ptr, _stream
+from .summation import InterpolatedModeSum, _device, _ptr, _stream, _upload
 from .synthetic import output_length
 
 # Layout of few_wave_desc (include/few_b200.h): 8 pointers, 6 ints, 1 double.
@@ -108,7 +108,7 @@ class BatchedInterpolatedModeSum:
             d["N"], d["R"], d["nlo"], d["NN"] = p.N, p.fold.R, p.fold.nlo, p.fold.NN
             d["use_theta"] = p.fold.use_theta
             d["dt"] = p.dt
-        self.descs = torch.from_numpy(descs.view(np.uint8).copy()).to(dev)
+        self.descs = _upload(descs.view(np.uint8), dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.mode_samples = sum(p.K * p.out_len for p in self.preps)
         seg_lens = [np.diff(p.seg.seg_start).mean() for p in self.preps if p.seg.nseg > 0]
@@ -143,7 +143,7 @@ class BatchedInterpolatedModeSum:
         arr = np.array(rows, dtype=np.int64).reshape(-1, 5)
         order = np.argsort(-arr[:, 4], kind="stable")
         units = np.ascontiguousarray(arr[order, :4].astype(np.int32))
-        return torch.from_numpy(units.reshape(-1)).to(self.device)
+        return _upload(units.reshape(-1), self.device)
 
     # ------------------------------------------------------------ the kernels
     def _prepare_operands(self):

@@ -20,7 +20,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .summation import InterpolatedModeSum
+from .summation import InterpolatedModeSum, _upload
 
 
 def shard_range(out_len: int, rank: int, world: int) -> tuple[int, int]:
@@ -103,7 +103,7 @@ class ShardedInterpolatedModeSum(InterpolatedModeSum):
         local = restrict_units(seg.units_host, lo, hi)
         seg.units_host = local
         seg.nunits = len(local) // 3
-        seg.d_units = torch.from_numpy(local.copy() if seg.nunits else np.zeros(3, np.int32)).to(p.dev)
+        seg.d_units = _upload(local if seg.nunits else np.zeros(3, np.int32), p.dev)
         seg.seg_start = clip_seg_start(seg.seg_start, lo, hi)
         if hasattr(seg, "_bwd"):
             del seg._bwd

@@ -58,7 +58,18 @@ def _to_device(x, dtype, device) -> torch.Tensor:
         a = a.astype(np.float64, copy=False)
     elif dtype == torch.int32:
         a = a.astype(np.int32, copy=False)
-    return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    return _upload(a, device)
+
+
+def _upload(a: np.ndarray, device) -> torch.Tensor:
+    """Host array -> device through pinned staging, without blocking the host:
+    a copy from pageable memory would wait for the kernels already queued on
+    the stream, leaving the GPU idle while the next call is planned.  torch's
+    pinned-block cache keeps the staging buffer alive until the copy is done."""
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if torch.device(device).type != "cuda":
+        return t.to(device)
+    return t.pin_memory().to(device, non_blocking=True)
 
 
 def _to_host(x, dtype) -> np.ndarray:
@@ -281,7 +292,7 @@ class _FoldPlan:
                     self.key_plus[code >> 1] = q
         host = np.concatenate([self.row_m, self.row_k, self.key_ptr, self.key_list, self.key_plus,
                                self.key_minus]).astype(np.int32)
-        self.table = torch.from_numpy(host).to(device)
+        self.table = _upload(host, device)
         o = 0
         self.d_row_m = self.table[o:o + self.R]; o += self.R
         self.d_row_k = self.table[o:o + self.R]; o += self.R
@@ -307,9 +318,8 @@ class _SegmentPlan:
         self.seg_start = seg_start[: self.nseg + 1]
         self.units_host = units[: 3 * self.nunits]
         self.seg_info_host = seg_info[: 3 * max(self.nseg, 1)]
-        self.d_seg_info = torch.from_numpy(self.seg_info_host.copy()).pin_memory().to(device, non_blocking=True)
-        self.d_units = torch.from_numpy(self.units_host.copy() if self.nunits else np.zeros(3, np.int32)).pin_memory() \
-            .to(device, non_blocking=True)
+        self.d_seg_info = _upload(self.seg_info_host, device)
+        self.d_units = _upload(self.units_host if self.nunits else np.zeros(3, np.int32), device)
         self._device = device
 
     def backward_tables(self):
@@ -319,7 +329,7 @@ class _SegmentPlan:
             useg = self.units_host.reshape(-1, 3)[:, 0] if self.nunits else np.zeros(0, np.int32)
             seg_units[1:] = np.cumsum(np.bincount(useg, minlength=self.nseg)[: self.nseg])
             host = np.concatenate([self.seg_start.astype(np.int32), seg_units])
-            t = torch.from_numpy(host).to(self._device)
+            t = _upload(host, self._device)
             self._bwd = (t[: self.nseg + 1], t[self.nseg + 1:])
         return self._bwd
 
@@ -448,12 +458,12 @@ class InterpolatedModeSum(SummationBase):
             if isinstance(phase_interp_coeffs, torch.Tensor) else _to_device(phase_interp_coeffs, torch.float64, dev)
         p.dev, p.st, p.N, p.K, p.dt = dev, _stream(dev), N, K, float(dt)
         p.teuk, p.teuk_in, p.pc_in = teuk, (teuk_in if keep else None), (pc_in if keep else None)
-        p.t_dev = torch.from_numpy(h_t).to(dev)
+        p.t_dev = _upload(h_t, dev)
         p.fac = spline_factor_table(h_t, dev)
         # ylms[K:] *= (-1)^l (interpolatedmodesum.py:357-358)
         sign = np.where(l_h % 2 == 0, 1.0, -1.0)
         ylm = _to_device(ylms, torch.complex128, dev).clone()
-        ylm[K:] *= torch.from_numpy(sign).to(dev)
+        ylm[K:] *= _upload(sign, dev)
         p.ylm = ylm
         # (N-1, 3, 8) -> (8, N-1, 3) (interpolatedmodesum.py:352-354)
         p.pc = pc_in.detach().permute(2, 0, 1).contiguous()
