@@ -297,7 +297,7 @@ def time_forward(ims, call_args, inp, steps, warmup):
     return a.elapsed_time(b) / steps, stage
 
 
-def time_fwd_bwd(precision, inp, dev, steps, warmup):
+def time_fwd_bwd(precision, inp, dev, steps, warmup, backward=None):
     """Forward + backward through torch.autograd (dL/d amplitude knots and
     dL/d phase coefficients), upstream gradient conj(h_ref + w) with w white,
     sigma = 0.1 rms(h_ref).  Device time per step (ms)."""
@@ -305,7 +305,7 @@ def time_fwd_bwd(precision, inp, dev, steps, warmup):
 
     from fastemriwaveforms_b200 import InterpolatedModeSum
 
-    ims = InterpolatedModeSum(precision=precision)
+    ims = InterpolatedModeSum(precision=precision, backward=backward)
     teuk = torch.from_numpy(inp.teuk_modes).to(dev).requires_grad_(True)
     pc = torch.from_numpy(inp.phase_coeffs).to(dev).requires_grad_(True)
     ylms = torch.from_numpy(inp.ylms).to(dev)
@@ -555,13 +555,16 @@ def main():
                                  "algorithmic": f"2 x {8 * nnp} x {nb} x 3 split products per sample"}
         forms[prec] = entry
     fb = {}
-    for prec in ("exact", "mixed"):
-        ms_fb, gt, gp = time_fwd_bwd(prec, inp, dev, max(2, args.steps // 2), 1)
-        fb[prec] = {"ms_per_step": ms_fb}
-        if prec == "exact":
+    # exact: FP64 forward and adjoint; mixed: tensor-core forward and adjoint;
+    # mixed_fp64_adjoint: tensor-core forward, FP64 adjoint
+    for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
+                            ("mixed_fp64_adjoint", "mixed", "fp64")):
+        ms_fb, gt, gp = time_fwd_bwd(prec, inp, dev, max(2, args.steps // 2), 1, backward=bwd)
+        fb[name] = {"ms_per_step": ms_fb}
+        if name == "exact":
             g_ref = (gt, gp)
         else:
-            fb[prec]["grad_rel_l2_vs_exact"] = {
+            fb[name]["grad_rel_l2_vs_exact"] = {
                 "amplitude_knots": float(torch.linalg.norm(gt - g_ref[0]) / torch.linalg.norm(g_ref[0])),
                 "phase_coeffs": float(torch.linalg.norm(gp - g_ref[1]) / torch.linalg.norm(g_ref[1]))}
     del g_ref
@@ -570,8 +573,9 @@ def main():
 
     adj = S.adjoint_case(seed=4 + rank)
     fb_adj = {"workload": f"K={adj.num_modes}, N={adj.num_knots}, T={adj.out_len}"}
-    for prec in ("exact", "mixed"):
-        fb_adj[prec] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1)[0]}
+    for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
+                            ("mixed_fp64_adjoint", "mixed", "fp64")):
+        fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1, backward=bwd)[0]}
 
     batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
 

@@ -57,10 +57,17 @@ SIGNATURES = {
                       _vp, _vp],
     "few_sum_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp],
     "few_sum_mixed_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_adjoint_G_mixed": [_vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
+                            _vp, _vp, _vp],
+    "few_mixed_adjoint_operand_bytes": [_c_int, _c_int, _c_int],
+    "few_fold_mixed_adjoint": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_adjoint_phase_mixed": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl,
+                                _c_int, _vp, _vp, _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
 }
-_RESTYPE = {"few_last_error": ctypes.c_char_p, "few_mixed_operand_bytes": ctypes.c_longlong}
+_RESTYPE = {"few_last_error": ctypes.c_char_p, "few_mixed_operand_bytes": ctypes.c_longlong,
+            "few_mixed_adjoint_operand_bytes": ctypes.c_longlong}
 
 _lock = threading.Lock()
 _lib = None

@@ -29,6 +29,7 @@
 
 #include "few_common.cuh"
 #include "few_internal.h"
+#include "few_tc.cuh"
 
 namespace few {
 
@@ -36,150 +37,13 @@ namespace {
 
 constexpr int kMT = 128;   // samples per tile (MMA M)
 constexpr int kKC = 64;    // real K per chunk
-constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s of global time per wait
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Bounded wait; false if the phase did not complete within kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    while (global_ns() - t0 < kWaitLimitNs)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version for sm_100; base offset 0; no swizzle
-    return d;
-}
-
-// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                         uint32_t accumulate)
-{
-    uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// Byte offset of element (row, k) of a K-major, no-swizzle tile whose K-steps
-// of 16 hold `groups` 8-row groups: K-step stride groups*256, 8-row group
-// stride (SBO) 256, K-half stride (LBO) 128, row 16, element 2.
-__host__ __device__ __forceinline__ uint32_t tile_off(int row, int k, int groups)
-{
-    return (uint32_t)((k >> 4) * groups * 256 + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
-
-// x = hi + lo with hi, lo bf16, packed two complex numbers (re, im, re, im) at a time.
-__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
-{
-    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    float2 hf = __bfloat1622float2(h);
-    __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
-    hi = *reinterpret_cast<uint32_t *>(&h);
-    lo = *reinterpret_cast<uint32_t *>(&l);
-}
-
-__device__ __forceinline__ float2 fcmul(float2 a, float2 b)
-{
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 fcpow(float2 z, int p)
-{
-    if (p < 0) {
-        z.y = -z.y;
-        p = -p;
-    }
-    float2 r = make_float2(1.f, 0.f);
-    while (p) {
-        if (p & 1) r = fcmul(r, z);
-        p >>= 1;
-        if (p) z = fcmul(z, z);
-    }
-    return r;
-}
-
-// exp(-i phi): the argument is reduced mod 2 pi in FP64 (phi reaches ~1e7 rad,
-// where FP32 would keep no fraction of a turn), then sine and cosine are taken
-// in FP32 on the reduced value in [-pi, pi].
-__device__ __forceinline__ float2 anchor(double phi)
-{
-    const double two_pi = 6.283185307179586476925286766559;
-    const double k = rint(phi * 0.15915494309189533576888376337251);
-    const float red = (float)fma(-k, two_pi, phi);
-    float s, c;
-    sincosf(red, &s, &c);
-    return make_float2(c, -s);
-}
-
 // ---------------------------------------------------------------------------
 // B operand: per segment and K chunk, hi and lo bf16 tiles in the smem layout.
 // ---------------------------------------------------------------------------
+// cpr = columns per row: 2 for the sum (Re Y_r, Im Y_r), 4 for the phase
+// adjoint (Re Y_r, Im Y_r, Re Z_r, Im Z_r) with Z_r built from n' W.
 __global__ void k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots, int nseg, int R,
-                             int NN, int NNp, int NB, int nchunks, __nv_bfloat16 *__restrict__ Bpk)
+                             int NN, int NNp, int NB, int nchunks, int cpr, int nlo, __nv_bfloat16 *__restrict__ Bpk)
 {
     const long long per_chunk = (long long)NB * kKC;
     const long long total = (long long)nseg * nchunks * per_chunk;
@@ -194,13 +58,14 @@ __global__ void k_fold_mixed(const double2 *__restrict__ W, const double *__rest
     const int part = kk & 1;  // 0: multiplies Re X, 1: Im X
     const int c = kappa / NNp, nidx = kappa - c * NNp;
     double val = 0.0;
-    if (j < 2 * R && nidx < NN) {
-        const int r = j >> 1;
-        const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r
+    const int r = j / cpr;
+    if (r < R && nidx < NN) {
+        const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r (Z_r: +2)
+        const double scale = ((j % cpr) >> 1) ? (double)(nlo + nidx) : 1.0;
         const double h = t_knots[s + 1] - t_knots[s];
         const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
         const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
-        const double wr = w.x * hc, wi = w.y * hc;
+        const double wr = w.x * hc * scale, wi = w.y * hc * scale;
         if (part == 0) val = im_col ? wi : wr;     // Re Y += Re X Re W ; Im Y += Re X Im W
         else val = im_col ? wr : -wi;              // Re Y -= Im X Im W ; Im Y += Im X Re W
     }
@@ -223,6 +88,8 @@ struct MixedArgs {
     const int *row_m;
     const int *row_k;
     int *err;
+    const double2 *grad;  // phase adjoint: torch upstream gradient G (g = conj(G))
+    double *partial;      // phase adjoint: (nunits, 24) unit partials
     int N, R, nlo, NN, NNp, NB, nchunks, use_theta, tmem_cols;
     double dt;
 };
@@ -234,49 +101,18 @@ __device__ __forceinline__ void mixed_dims_dev(int R, int NN, int &NNp, int &NB,
     nchunks = NNp / 8;
 }
 
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Tensor-core state a CTA carries across units: TMEM accumulator, one
-// mbarrier per A/B buffer, their phases and whether a commit is outstanding
-// (scalars, so that nothing is indexed at run time and all stays in registers).
-struct MixedPipe {
-    uint32_t tmem;
-    uint64_t *bar;  // [2]
-    uint32_t ph0, ph1;
-    int pend0, pend1;
-};
-
-// Bounded wait for buffer b's outstanding MMAs.
-__device__ __forceinline__ bool pipe_drain(MixedPipe &p, int b)
-{
-    if (b == 0) {
-        if (!p.pend0) return true;
-        const bool ok = mbar_wait_bounded(&p.bar[0], p.ph0);
-        p.ph0 ^= 1u;
-        p.pend0 = 0;
-        return ok;
-    }
-    if (!p.pend1) return true;
-    const bool ok = mbar_wait_bounded(&p.bar[1], p.ph1);
-    p.ph1 ^= 1u;
-    p.pend1 = 0;
-    return ok;
-}
-
 // One work unit (samples [lo, hi) of segment seg) on the tensor cores.  Two
 // A/B buffers: while the tensor cores run chunk k's MMAs from one buffer, the
 // threads generate chunk k+1 into the other and its B tile arrives by
 // cp.async.  Returns false (for every thread) if a tensor-core wait timed out.
+template <bool ADJ>
 __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, MixedPipe &pp,
-                           int *s_rm, int *s_rk, double *s_pc)
+                           int *s_rm, int *s_rk, double *s_pc, int unit = 0, float *s_e = nullptr,
+                           double *s_s = nullptr)
 {
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NB = a.NB;
+    double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // phase adjoint: this lane's share of 6 outputs
     const int bbytes = 2 * NB * kKC * 2;  // one B buffer: hi then lo
     // A buffers (hi 16 KB then lo 16 KB each) at 0 and 32 KB, B buffers after them
     unsigned char *const sA0 = smem_raw;
@@ -387,86 +223,127 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
             failed = true;
             break;
         }
-        // epilogue: this thread's accumulator row (TMEM lane = tid), 8 rows (m', k')
-        // per 16-column load; u_r by one multiplication when m' steps by one
         tc_fence_after();
         const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
-        float hr = 0.f, hi_ = 0.f;
         float2 uu = make_float2(1.f, 0.f);
         int pm = 0x7fffffff, pk = 0x7fffffff;
-        for (int c0 = 0; c0 < NB; c0 += 16) {
-            float D[16];
-            tmem_ld16(trow + c0, D);
-            tmem_wait_ld();
+        if constexpr (!ADJ) {
+            // epilogue: this thread's accumulator row (TMEM lane = tid), 8 rows
+            // (m', k') per 16-column load; u_r by one multiplication when m' steps by one
+            float hr = 0.f, hi_ = 0.f;
+            for (int c0 = 0; c0 < NB; c0 += 16) {
+                float D[16];
+                tmem_ld16(trow + c0, D);
+                tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int r = (c0 >> 1) + q;
-                if (r < R) {
-                    const int mm = s_rm[r], kk = s_rk[r];
-                    if (kk == pk && mm == pm + 1) {
-                        uu = fcmul(uu, Ep);
-                    } else {
-                        uu = fcpow(Ep, mm);
-                        if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                for (int q = 0; q < 8; ++q) {
+                    const int r = (c0 >> 1) + q;
+                    if (r < R) {
+                        const int mm = s_rm[r], kk = s_rk[r];
+                        if (kk == pk && mm == pm + 1) {
+                            uu = fcmul(uu, Ep);
+                        } else {
+                            uu = fcpow(Ep, mm);
+                            if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                        }
+                        pm = mm;
+                        pk = kk;
+                        const float yr = D[2 * q], yi = D[2 * q + 1];
+                        hr = fmaf(uu.x, yr, fmaf(-uu.y, yi, hr));
+                        hi_ = fmaf(uu.x, yi, fmaf(uu.y, yr, hi_));
                     }
-                    pm = mm;
-                    pk = kk;
-                    const float yr = D[2 * q], yi = D[2 * q + 1];
-                    hr = fmaf(uu.x, yr, fmaf(-uu.y, yi, hr));
-                    hi_ = fmaf(uu.x, yi, fmaf(uu.y, yr, hi_));
                 }
             }
-        }
-        if (valid) {
-            double2 o = a.wf[i];
-            o.x += (double)hr;
-            o.y += (double)hi_;
-            a.wf[i] = o;
+            if (valid) {
+                double2 o = a.wf[i];
+                o.x += (double)hr;
+                o.y += (double)hi_;
+                a.wf[i] = o;
+            }
+        } else {
+            // phase adjoint: 4 rows per 16-column load, (Y_r, Z_r) per row;
+            // dh/dPhi_phi = -i sum m' u Y, dh/dPhi_theta = -i sum k' u Y,
+            // dh/dPhi_r = -i sum u Z, and e_f = Re(g dh/dPhi_f) = Im(g S_f)
+            float2 Sp = make_float2(0.f, 0.f), St = Sp, Sr = Sp;
+            for (int c0 = 0; c0 < NB; c0 += 16) {
+                float D[16];
+                tmem_ld16(trow + c0, D);
+                tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int r = (c0 >> 2) + q;
+                    if (r < R) {
+                        const int mm = s_rm[r], kk = s_rk[r];
+                        if (kk == pk && mm == pm + 1) {
+                            uu = fcmul(uu, Ep);
+                        } else {
+                            uu = fcpow(Ep, mm);
+                            if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                        }
+                        pm = mm;
+                        pk = kk;
+                        const float2 P = fcmul(uu, make_float2(D[4 * q], D[4 * q + 1]));
+                        const float2 Q = fcmul(uu, make_float2(D[4 * q + 2], D[4 * q + 3]));
+                        const float fm = (float)mm, fk = (float)kk;
+                        Sp.x = fmaf(fm, P.x, Sp.x);
+                        Sp.y = fmaf(fm, P.y, Sp.y);
+                        St.x = fmaf(fk, P.x, St.x);
+                        St.y = fmaf(fk, P.y, St.y);
+                        Sr.x += Q.x;
+                        Sr.y += Q.y;
+                    }
+                }
+            }
+            float ep = 0.f, et = 0.f, er = 0.f;
+            if (valid) {
+                const double2 Gt = a.grad[i];
+                const float gx = (float)Gt.x, gy = (float)Gt.y;
+                ep = gx * Sp.y - gy * Sp.x;
+                et = gx * St.y - gy * St.x;
+                er = gx * Sr.y - gy * Sr.x;
+            }
+            s_e[tid] = ep;
+            s_e[kMT + tid] = et;
+            s_e[2 * kMT + tid] = er;
+            s_s[tid] = s;
+            __syncthreads();
+            // project on b_q(s) = 1, s, s s1, s^2 s1, ... (factors s, s1 alternating):
+            // warp w accumulates outputs o = w + 4k (field o / 8, term o % 8)
+#pragma unroll
+            for (int m = 0; m < kMT / 32; ++m) {
+                const int jj = lane + 32 * m;
+                const double sj = s_s[jj], s1j = 1.0 - sj;
+                double bq[8];
+                bq[0] = 1.0;
+#pragma unroll
+                for (int q = 1; q < 8; ++q) bq[q] = bq[q - 1] * ((q & 1) ? sj : s1j);
+#pragma unroll
+                for (int kq = 0; kq < 6; ++kq) {
+                    const int o = warp + 4 * kq;
+                    const int f = o >> 3, q = o & 7;
+                    double bsel = bq[0];
+#pragma unroll
+                    for (int qq = 1; qq < 8; ++qq) bsel = (q == qq) ? bq[qq] : bsel;
+                    proj[kq] = fma(bsel, (double)s_e[f * kMT + jj], proj[kq]);
+                }
+            }
         }
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
     }
+    if constexpr (ADJ) {
+        if (!failed) {
+#pragma unroll
+            for (int kq = 0; kq < 6; ++kq) {
+                double v = proj[kq];
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+                if (lane == 0) a.partial[(long long)unit * 24 + warp + 4 * kq] = v;
+            }
+        }
+    }
     cp_async_wait_all();
     return !failed;
-}
-
-__device__ __forceinline__ void mixed_setup(uint32_t *s_tmem, uint64_t *bars, int tmem_cols, MixedPipe &pp)
-{
-    if ((threadIdx.x >> 5) == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
-                     "r"((uint32_t)tmem_cols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    pp.tmem = *s_tmem;
-    pp.bar = bars;
-    pp.ph0 = pp.ph1 = 0;
-    pp.pend0 = pp.pend1 = 0;
-}
-
-// After a timeout: let any MMA still in flight finish, then free TMEM.
-__device__ __forceinline__ void mixed_teardown(bool failed, MixedPipe &pp, int tmem_cols, int *err)
-{
-    if (failed && threadIdx.x == 0) atomicExch(err, 1);
-    pipe_drain(pp, 0);
-    pipe_drain(pp, 1);
-    tc_fence_before();
-    __syncthreads();
-    if ((threadIdx.x >> 5) == 0) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(pp.tmem),
-                     "r"((uint32_t)tmem_cols)
-                     : "memory");
-    }
 }
 
 __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
@@ -480,7 +357,7 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
     mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
     const int u = blockIdx.x;
     const bool ok =
-        mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
+        mixed_unit<false>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
     mixed_teardown(!ok, pp, a.tmem_cols, a.err);
 }
 
@@ -507,6 +384,8 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.seg_info = d.seg_info;
         a.t_knots = d.t_knots;
         a.units = nullptr;
+        a.grad = nullptr;
+        a.partial = nullptr;
         a.row_m = d.row_m;
         a.row_k = d.row_k;
         a.err = err;
@@ -518,18 +397,41 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.dt = d.dt;
         a.tmem_cols = tmem_cols;
         mixed_dims_dev(d.R, d.NN, a.NNp, a.NB, a.nchunks);
-        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
+        ok = mixed_unit<false>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
     }
     mixed_teardown(!ok, pp, tmem_cols, err);
 }
 
+// Phase adjoint on the tensor cores: the forward contraction with B holding
+// (Y_r, Z_r) column pairs (Z from n' W), an epilogue that forms dL/dPhi at each
+// sample and projects it on the phase basis; one CTA per work unit writes the
+// unit's 24 partials (field-major: phi, theta, r x 8 terms).
+__global__ void __launch_bounds__(kMT, 1) k_adj_phase_mixed(MixedArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ double s_pc[24];
+    __shared__ float s_e[3 * kMT];
+    __shared__ double s_s[kMT];
+    MixedPipe pp;
+    mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
+    const int u = blockIdx.x;
+    const bool ok = mixed_unit<true>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm,
+                                     s_rk, s_pc, u, s_e, s_s);
+    mixed_teardown(!ok, pp, a.tmem_cols, a.err);
+}
+
 }  // namespace
 
-int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
+// cpr = B columns per (m', k') row: 2 for the sum, 4 for the phase adjoint.
+int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols, int cpr)
 {
-    if (2 * R > 256) return fail(FEW_ERR_SIZE, "mixed sum: %d rows exceed the 128 the tensor-core tile holds", R);
+    if (cpr * R > 256)
+        return fail(FEW_ERR_SIZE, "mixed form: %d rows x %d columns exceed the 256 one MMA holds", R, cpr);
     *NNp = (NN + 31) / 32 * 32;
-    *NB = std::max(16, (2 * R + 15) / 16 * 16);
+    *NB = std::max(16, (cpr * R + 15) / 16 * 16);
     *nchunks = 4 * (*NNp) / 32;
     int cols = 32;
     while (cols < *NB) cols <<= 1;
@@ -537,24 +439,57 @@ int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
     return FEW_OK;
 }
 
-size_t mixed_bpk_bytes(int nseg, int R, int NN)
+size_t mixed_bpk_bytes(int nseg, int R, int NN, int cpr)
 {
     int NNp, NB, nch, cols;
-    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols)) return 0;
+    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols, cpr)) return 0;
     return (size_t)nseg * nch * 2 * NB * kKC * sizeof(__nv_bfloat16);
 }
 
-int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, cudaStream_t st)
+int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, int nlo, int cpr, void *Bpk,
+                      cudaStream_t st)
 {
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols);
+    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols, cpr);
     if (rc) return rc;
     const long long total = (long long)nseg * nch * NB * kKC;
     if (total == 0) return FEW_OK;
     const int threads = 256;
     k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NNp, NB, nch,
-                                                                                 (__nv_bfloat16 *)Bpk);
+                                                                                 cpr, nlo, (__nv_bfloat16 *)Bpk);
     FEW_LAUNCH_CHECK("k_fold_mixed");
+    return FEW_OK;
+}
+
+int launch_adj_phase_mixed(const double2 *grad, const void *Bpk, const double *pc, int N, const double *seg_info,
+                           const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
+                           int R, int nlo, int NN, double dt, int use_theta, double *partial, int *err, cudaStream_t st)
+{
+    if (nunits == 0) return FEW_OK;
+    MixedArgs a;
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, 4);
+    if (rc) return rc;
+    a.wf = nullptr;
+    a.Bpk = (const __nv_bfloat16 *)Bpk;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.t_knots = t_knots;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.err = err;
+    a.grad = grad;
+    a.partial = partial;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * a.NB * kKC * 2;
+    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_phase_mixed, (int)smem));
+    k_adj_phase_mixed<<<nunits, kMT, smem, st>>>(a);
+    FEW_LAUNCH_CHECK("k_adj_phase_mixed");
     return FEW_OK;
 }
 
@@ -564,9 +499,11 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
 {
     if (nunits == 0) return FEW_OK;
     MixedArgs a;
-    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols);
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, 2);
     if (rc) return rc;
     a.wf = wf;
+    a.grad = nullptr;
+    a.partial = nullptr;
     a.Bpk = (const __nv_bfloat16 *)Bpk;
     a.pc = pc;
     a.seg_info = seg_info;
@@ -593,7 +530,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols);
+    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols, 2);
     if (rc) return rc;
     if (ctas <= 0) {
         int dev = 0, sms = 148;
@@ -626,12 +563,12 @@ extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, in
     few::clear_error();
     if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed: null pointer");
     if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed: bad sizes");
-    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, Bpk, (cudaStream_t)stream);
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, 0, 2, Bpk, (cudaStream_t)stream);
 }
 
 extern "C" long long few_mixed_operand_bytes(int nseg, int R, int NN)
 {
-    return (long long)few::mixed_bpk_bytes(nseg, R, NN);
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN, 2);
 }
 
 extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
@@ -644,4 +581,32 @@ extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coef
     if (N < 2 || nunits < 0 || R < 1 || R > 128 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_sum_mixed: bad sizes");
     return few::launch_sum_mixed((double2 *)wf, Bpk, phase_coeffs, N, seg_info, t_knots, units, nunits, row_m, row_k,
                                  R, nlo, NN, dt, use_theta, err, (cudaStream_t)stream);
+}
+
+extern "C" long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN)
+{
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN, 4);
+}
+
+extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
+                                      void *stream)
+{
+    few::clear_error();
+    if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed_adjoint: null pointer");
+    if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: bad sizes");
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, nlo, 4, Bpk, (cudaStream_t)stream);
+}
+
+extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,
+                                       const double *seg_info, const double *t_knots, const int *units, int nunits,
+                                       const int *row_m, const int *row_k, int R, int nlo, int NN, double dt,
+                                       int use_theta, double *partial, int *err, void *stream)
+{
+    few::clear_error();
+    if (!grad || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !partial || !err)
+        return few::fail(FEW_ERR_ARG, "few_adjoint_phase_mixed: null pointer");
+    if (N < 2 || nunits < 0 || R < 1 || R > 64 || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_mixed: bad sizes (R <= 64)");
+    return few::launch_adj_phase_mixed((const double2 *)grad, Bpk, phase_coeffs, N, seg_info, t_knots, units, nunits,
+                                       row_m, row_k, R, nlo, NN, dt, use_theta, partial, err, (cudaStream_t)stream);
 }

@@ -16,8 +16,13 @@ path.  Extra keyword ``precision`` of ``InterpolatedModeSum``:
   combined phase (more accurate than the reference, ~2x less FP64 work);
 * ``"mixed"`` -- FP64 phases and anchors, FP32 phasor recurrence, the
   per-segment contraction on the tcgen05 tensor cores in split BF16 with FP32
-  accumulation (waveform mismatch ~1e-10 against FP64).  Gradients of a mixed
-  forward are computed by the FP64 adjoint.
+  accumulation (waveform mismatch ~1e-10 against FP64).
+
+Keyword ``backward`` chooses the adjoint used when gradients are requested:
+``"fp64"`` (the default for the FP64 forms) or ``"mixed"`` (the default for
+``precision="mixed"``): the amplitude gradient's per-segment contraction over
+samples and the phase gradient's per-sample sums on the tensor cores, with the
+precision plan of the mixed forward.
 """
 from __future__ import annotations
 
@@ -364,16 +369,24 @@ class InterpolatedModeSum(SummationBase):
     (reference: ``interpolatedmodesum.py:260-375``).
 
     args:
-        precision: "faithful" (default) or "exact"; see the module docstring.
+        precision: "faithful" (default), "exact" or "mixed"; see the module docstring.
+        backward: "fp64" or "mixed" adjoint (default: "mixed" for
+            precision="mixed", else "fp64").
         chunk: output samples per work unit of the sum kernel.
         Others as ``SummationBase``.
     """
 
-    def __init__(self, force_backend=None, precision: str = "faithful", chunk: int = DEFAULT_CHUNK, **kwargs):
+    def __init__(self, force_backend=None, precision: str = "faithful", chunk: int = DEFAULT_CHUNK,
+                 backward: str | None = None, **kwargs):
         SummationBase.__init__(self, force_backend=force_backend, **kwargs)
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.precision = precision
+        if backward is None:
+            backward = "mixed" if precision == "mixed" else "fp64"
+        if backward not in ("fp64", "mixed"):
+            raise ValueError("backward must be 'fp64' or 'mixed'")
+        self.backward = backward
         if not 1 <= int(chunk) <= 1024:
             raise ValueError("chunk must be within 1..1024 output samples")
         self.chunk = int(chunk)
@@ -468,6 +481,11 @@ class InterpolatedModeSum(SummationBase):
         # (N-1, 3, 8) -> (8, N-1, 3) (interpolatedmodesum.py:352-354)
         p.pc = pc_in.detach().permute(2, 0, 1).contiguous()
         p.fold = self._fold_plan(m_h, k_h, n_h, dev)
+        p.bwd_mixed = self.backward == "mixed"
+        if p.bwd_mixed:
+            if self._mixed_err is None or self._mixed_err.device != dev:
+                self._mixed_err = torch.zeros(1, dtype=torch.int32, device=dev)
+            p.err = self._mixed_err
         p.seg = _SegmentPlan(h_t, phase_t, self.num_pts, dt, self.chunk, dev)
         p.out_len = int(self.num_pts)
         return p
@@ -522,12 +540,20 @@ class InterpolatedModeSum(SummationBase):
         fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
         grad = grad[: p.out_len].to(torch.complex128).contiguous()
         g_teuk = g_pc = None
+        mixed = getattr(p, "bwd_mixed", False)
+        if mixed and need_pc and fold.R > 64:
+            raise ValueError("backward='mixed' supports at most 64 (m, k) rows for phase gradients")
         if need_teuk:
             seg_start, _ = seg.backward_tables()
             G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
-            _lib.call("few_adjoint_G", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg_start), seg.nseg,
-                      _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta,
-                      _ptr(G), st)
+            if mixed:
+                _lib.call("few_adjoint_G_mixed", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(p.t_dev),
+                          _ptr(seg_start), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                          fold.NN, p.dt, fold.use_theta, _ptr(G), _ptr(p.err), st)
+            else:
+                _lib.call("few_adjoint_G", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg_start),
+                          seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN, p.dt,
+                          fold.use_theta, _ptr(G), st)
             gcoef = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
             _lib.call("few_unfold", _ptr(G), _ptr(p.ylm), _ptr(fold.d_key_plus), _ptr(fold.d_key_minus), K, N,
                       seg.nseg, fold.R * fold.NN, _ptr(gcoef), st)
@@ -537,9 +563,18 @@ class InterpolatedModeSum(SummationBase):
         if need_pc:
             _, seg_units = seg.backward_tables()
             partial = torch.empty((max(seg.nunits, 1), 24), dtype=torch.float64, device=dev)
-            _lib.call("few_adjoint_phase", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
-                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
-                      fold.NN, p.dt, fold.use_theta, _ptr(partial), st)
+            if mixed:
+                nbytes = int(_lib.load().few_mixed_adjoint_operand_bytes(max(seg.nseg, 1), fold.R, fold.NN))
+                Bpk = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+                _lib.call("few_fold_mixed_adjoint", _ptr(p.W), _ptr(p.t_dev), seg.nseg, fold.R, fold.nlo, fold.NN,
+                          _ptr(Bpk), st)
+                _lib.call("few_adjoint_phase_mixed", _ptr(grad), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                          _ptr(p.t_dev), _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k),
+                          fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta, _ptr(partial), _ptr(p.err), st)
+            else:
+                _lib.call("few_adjoint_phase", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                          _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                          fold.NN, p.dt, fold.use_theta, _ptr(partial), st)
             g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
             _lib.call("few_adjoint_phase_reduce", _ptr(partial), _ptr(seg_units), seg.nseg, _ptr(g_pc), st)
         return g_teuk, g_pc

@@ -303,6 +303,34 @@ FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, c
                           const int *seg_start, int nseg, const int *row_m, const int *row_k, int R, int nlo, int NN,
                           double dt, int use_theta, void *G, void *stream);
 
+/* Mixed-precision adjoint (tcgen05, split BF16, FP32 accumulation; no
+ * counterpart in the reference).  Same quantities as few_adjoint_G and
+ * few_adjoint_phase, computed with the precision plan of few_sum_mixed; err
+ * [device] int is set to 1 if a tensor-core wait timed out. */
+
+/* few_adjoint_G on the tensor cores: the contraction over each segment's
+ * samples with K = samples.  t_knots [device] (N,).  R <= 128. */
+FEW_API int few_adjoint_G_mixed(const void *grad, const double *phase_coeffs, int N, const double *seg_info,
+                                const double *t_knots, const int *seg_start, int nseg, const int *row_m,
+                                const int *row_k, int R, int nlo, int NN, double dt, int use_theta, void *G, int *err,
+                                void *stream);
+
+/* Bytes of the B operand of the mixed phase adjoint (0 if R > 64). */
+FEW_API long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN);
+
+/* Packs W into the phase adjoint's B operand: per (m', k') row the columns
+ * (Re Y, Im Y) of few_fold_mixed and (Re Z, Im Z) from n' W (n' = nlo + column). */
+FEW_API int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
+                                   void *stream);
+
+/* few_adjoint_phase on the tensor cores: the forward contraction against the
+ * packed (Y, Z) operand, dL/dPhi per sample in the epilogue, projected on the
+ * basis per work unit into partial [device] (nunits, 24).  R <= 64. */
+FEW_API int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,
+                                    const double *seg_info, const double *t_knots, const int *units, int nunits,
+                                    const int *row_m, const int *row_k, int R, int nlo, int NN, double dt,
+                                    int use_theta, double *partial, int *err, void *stream);
+
 /* Transpose of few_fold_coeffs: gcoef [device] (4, N, 2K) = dL/d(spline
  * coefficients) (zero at knots >= nseg).  key_plus, key_minus [device] (K,):
  * key index of each mode's + and - term (-1: none). */
