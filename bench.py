@@ -48,8 +48,8 @@ def parse():
                     help="output samples of the bounded single-core reference run (cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--batch-count", type=int, default=32,
-                    help="waveforms of the uneven batch (drawn from the 256-waveform distribution)")
+    ap.add_argument("--batch-count", type=int, default=256,
+                    help="waveforms of the uneven batch (T ~ logU[1e5, 3.15e6], N ~ U[50, 2000], K ~ U[200, 3843])")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
@@ -339,9 +339,10 @@ def time_fwd_bwd(precision, inp, dev, steps, warmup, backward=None):
 
 def bench_batched(count: int, dev, steps: int):
     """Uneven batch (T ~ logU[1e5, 3.15e6] samples, N ~ U[50, 2000], K ~ U[200, 3843]):
-    looping InterpolatedModeSum (plain FP64, one call per waveform) vs the
-    persistent batched launch in a CUDA graph (mixed form), forward and
-    forward+backward."""
+    looping InterpolatedModeSum (plain FP64, one call per waveform; forward, and
+    forward + backward through autograd) vs the persistent batched launch in a
+    CUDA graph (mixed form with the tensor-core adjoint), upstream gradient
+    conj(h) per waveform."""
     import torch
 
     from fastemriwaveforms_b200 import InterpolatedModeSum
@@ -350,39 +351,58 @@ def bench_batched(count: int, dev, steps: int):
 
     cases = S.batch_cases(count=count, seed=5)
     ms_total = sum(c.num_modes * c.out_len for c in cases)
-    # loop: one plain FP64 call per waveform, inputs in HBM
     loop = InterpolatedModeSum(precision="faithful")
+    loop_fb = InterpolatedModeSum(precision="exact", backward="fp64")
     dev_args = []
     for c in cases:
-        dev_args.append((c.t, torch.from_numpy(c.teuk_modes).to(dev), torch.from_numpy(c.ylms).to(dev), c.phase_t,
-                         torch.from_numpy(c.phase_coeffs).to(dev), c.l, c.m, c.k, c.n))
-    for a_, c in zip(dev_args[:2], cases[:2]):
+        dev_args.append([c.t, torch.from_numpy(c.teuk_modes).to(dev), torch.from_numpy(c.ylms).to(dev), c.phase_t,
+                         torch.from_numpy(c.phase_coeffs).to(dev), c.l, c.m, c.k, c.n])
+
+    def fwd(a_, c):
         loop(*a_, T=c.T, dt=c.dt)
-    torch.cuda.synchronize()
-    per = []
-    ea = torch.cuda.Event(enable_timing=True)
-    eb = torch.cuda.Event(enable_timing=True)
-    ea.record()
-    for a_, c in zip(dev_args, cases):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        loop(*a_, T=c.T, dt=c.dt)
-        e1.record()
-        per.append((e0, e1))
-    eb.record()
-    torch.cuda.synchronize()
-    loop_ms = ea.elapsed_time(eb)
-    per_ms = sorted(e0.elapsed_time(e1) for e0, e1 in per)
+
+    def fwd_bwd(a_, c):
+        a_[1].grad = None
+        a_[4].grad = None
+        h = loop_fb(*a_, T=c.T, dt=c.dt)
+        h.backward(torch.conj(h.detach()))
+
+    def timed(fn):
+        for a_, c in zip(dev_args[:2], cases[:2]):
+            fn(a_, c)
+        torch.cuda.synchronize()
+        per = []
+        ea = torch.cuda.Event(enable_timing=True)
+        eb = torch.cuda.Event(enable_timing=True)
+        ea.record()
+        for a_, c in zip(dev_args, cases):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(a_, c)
+            e1.record()
+            per.append((e0, e1))
+        eb.record()
+        torch.cuda.synchronize()
+        total = ea.elapsed_time(eb)
+        pw = sorted(e0.elapsed_time(e1) for e0, e1 in per)
+        return {"ms_total": total, "value": ms_total / (total * 1e-3), "p50_ms": pw[len(pw) // 2],
+                "p99_ms": pw[min(len(pw) - 1, int(0.99 * len(pw)))]}
+
+    out = {"waveforms": count, "mode_samples": ms_total, "loop_plain_fp64": timed(fwd)}
+    for a_ in dev_args:
+        a_[1].requires_grad_(True)
+        a_[4].requires_grad_(True)
+    out["loop_plain_fp64_fwd_bwd"] = timed(fwd_bwd)
     del dev_args
-    out = {"waveforms": count, "mode_samples": ms_total,
-           "loop_plain_fp64": {"ms_total": loop_ms, "value": ms_total / (loop_ms * 1e-3),
-                               "p50_ms": per_ms[len(per_ms) // 2], "p99_ms": per_ms[min(len(per_ms) - 1,
-                                                                                         int(0.99 * len(per_ms)))]}}
-    # batched mixed, forward graph and forward+backward graph
+    torch.cuda.empty_cache()
+
+    # batched mixed: forward graph, then forward + backward graph
     b = BatchedInterpolatedModeSum(precision="mixed").setup(cases, requires_grad=True)
     outs = b.forward()
     grads = [torch.conj(o).clone() for o in outs]
+    ea = torch.cuda.Event(enable_timing=True)
+    eb = torch.cuda.Event(enable_timing=True)
     b.capture(backward=False)
     b.replay()
     torch.cuda.synchronize()
@@ -401,11 +421,24 @@ def bench_batched(count: int, dev, steps: int):
     eb.record()
     torch.cuda.synchronize()
     fb_ms = ea.elapsed_time(eb) / steps
+    # gradients of two waveforms against the FP64 backward with the same upstream gradient
+    errs = []
+    for i in range(min(2, count)):
+        c = cases[i]
+        teuk = torch.from_numpy(c.teuk_modes).to(dev).requires_grad_(True)
+        pc = torch.from_numpy(c.phase_coeffs).to(dev).requires_grad_(True)
+        h = InterpolatedModeSum(precision="exact", backward="fp64")(c.t, teuk, torch.from_numpy(c.ylms).to(dev),
+                                                                    c.phase_t, pc, c.l, c.m, c.k, c.n, T=c.T, dt=c.dt)
+        h.backward(b.grad_in[i])
+        gt, gp = b.grad_out[i]
+        errs.append({"amplitude_knots": float(torch.linalg.norm(gt - teuk.grad) / torch.linalg.norm(teuk.grad)),
+                     "phase_coeffs": float(torch.linalg.norm(gp - pc.grad) / torch.linalg.norm(pc.grad))})
     out["batched_mixed_graph"] = {"fwd_ms": fwd_ms, "fwd_value": ms_total / (fwd_ms * 1e-3),
                                   "fwd_ms_per_waveform": fwd_ms / count, "fwd_bwd_ms": fb_ms,
-                                  "fwd_bwd_value": ms_total / (fb_ms * 1e-3), "tuning": b.tuning,
+                                  "fwd_bwd_value": ms_total / (fb_ms * 1e-3), "fwd_bwd_ms_per_waveform": fb_ms / count,
+                                  "grad_rel_l2_vs_fp64": errs, "tuning": b.tuning,
                                   "chunk": b.chunk, "ctas_per_sm": b.ctas_per_sm, "mixed_error": b.mixed_error()}
-    del b
+    del b, outs, grads
     torch.cuda.empty_cache()
     return out
 

@@ -13,8 +13,9 @@ waveform for fixed upstream-gradient buffers) in one CUDA graph; ``replay()``
 re-runs it after new amplitudes / phase coefficients are written into the
 static input buffers (``update``).
 
-Gradients of a batched forward are the FP64 adjoint of each waveform, as for
-``InterpolatedModeSum``.
+Gradients of a batched forward are each waveform's adjoint, as for
+``InterpolatedModeSum``: the tensor-core adjoint for ``precision="mixed"``
+(``backward="mixed"``, the default there), the FP64 one otherwise.
 """
 from __future__ import annotations
 
@@ -47,13 +48,19 @@ class BatchedInterpolatedModeSum:
         precision: "mixed" (tensor cores), "exact" or "faithful" (FP64).
         autotune: choose the unit length and CTAs per SM by timing (cached).
         chunk, ctas_per_sm: fixed tile shape (overrides the autotuner).
+        backward: "mixed" or "fp64" adjoint (default: "mixed" for precision="mixed").
     """
 
     def __init__(self, precision: str = "mixed", device=None, autotune: bool = True, chunk: int | None = None,
-                 ctas_per_sm: int | None = None):
+                 ctas_per_sm: int | None = None, backward: str | None = None):
         if precision not in ("mixed", "exact", "faithful"):
             raise ValueError("precision must be 'mixed', 'exact' or 'faithful'")
         self.precision = precision
+        if backward is None:
+            backward = "mixed" if precision == "mixed" else "fp64"
+        if backward not in ("mixed", "fp64"):
+            raise ValueError("backward must be 'mixed' or 'fp64'")
+        self.backward_precision = backward
         self.device = _device(device)
         self.autotune = autotune
         self.chunk = chunk
@@ -72,7 +79,7 @@ class BatchedInterpolatedModeSum:
             t0 = float(t[0].item() if hasattr(t[0], "item") else t[0])
             t1 = float(t[-1].item() if hasattr(t[-1], "item") else t[-1])
             num_pts, num_pts_pad = output_length(np.array([t0, t1]), T, dt)
-            mod = InterpolatedModeSum(precision="exact", device=dev)
+            mod = InterpolatedModeSum(precision="exact", device=dev, backward=self.backward_precision)
             mod.num_pts = num_pts
             prep = mod._prepare(*args, dt=dt, integrate_backwards=False)
             if requires_grad:
@@ -192,7 +199,8 @@ class BatchedInterpolatedModeSum:
         return [InterpolatedModeSum._backward(p, g) for p, g in zip(self.preps, grads)]
 
     def mixed_error(self) -> bool:
-        return bool(int(self.err.item()) != 0)
+        """True if a tensor-core wait of the batched sum or of a mixed adjoint timed out."""
+        return bool(int(self.err.item()) != 0) or any(m.mixed_error() for m in self.mods)
 
     # ------------------------------------------------------------ CUDA graphs
     def update(self, i: int, teuk_modes=None, phase_interp_coeffs=None):

@@ -42,40 +42,52 @@ constexpr int kKC = 64;    // real K per chunk
 // ---------------------------------------------------------------------------
 // cpr = columns per row: 2 for the sum (Re Y_r, Im Y_r), 4 for the phase
 // adjoint (Re Y_r, Im Y_r, Re Z_r, Im Z_r) with Z_r built from n' W.
-__global__ void k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots, int nseg, int R,
-                             int NN, int NNp, int NB, int nchunks, int cpr, int nlo, __nv_bfloat16 *__restrict__ Bpk)
+// One thread per 16-byte row of a core matrix: column j, K elements
+// 8 kg .. 8 kg + 7 of chunk ch = 4 consecutive (c, n') of the fold, each as
+// its part-0 and part-1 value; writes the hi and the lo chunk.
+__global__ void __launch_bounds__(256) k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots,
+                                                    int nseg, int R, int NN, int NNp, int NB, int nchunks, int cpr,
+                                                    int nlo, __nv_bfloat16 *__restrict__ Bpk)
 {
     const long long per_chunk = (long long)NB * kKC;
-    const long long total = (long long)nseg * nchunks * per_chunk;
+    const long long total = (long long)nseg * nchunks * 8 * NB;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;
-    const int s = (int)(idx / (nchunks * per_chunk));
-    const long long rem = idx - (long long)s * nchunks * per_chunk;
-    const int ch = (int)(rem / per_chunk);
-    const int e = (int)(rem - (long long)ch * per_chunk);
-    const int j = e / kKC, kk = e - j * kKC;
-    const int kappa = ch * (kKC / 2) + (kk >> 1);
-    const int part = kk & 1;  // 0: multiplies Re X, 1: Im X
-    const int c = kappa / NNp, nidx = kappa - c * NNp;
-    double val = 0.0;
+    const int j = (int)(idx % NB);
+    long long rest = idx / NB;
+    const int kg = (int)(rest & 7);
+    rest >>= 3;
+    const int ch = (int)(rest % nchunks);
+    const int s = (int)(rest / nchunks);
     const int r = j / cpr;
-    if (r < R && nidx < NN) {
-        const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r (Z_r: +2)
-        const double scale = ((j % cpr) >> 1) ? (double)(nlo + nidx) : 1.0;
-        const double h = t_knots[s + 1] - t_knots[s];
-        const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
-        const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
-        const double wr = w.x * hc * scale, wi = w.y * hc * scale;
-        if (part == 0) val = im_col ? wi : wr;     // Re Y += Re X Re W ; Im Y += Re X Im W
-        else val = im_col ? wr : -wi;              // Re Y -= Im X Im W ; Im Y += Im X Re W
+    const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r (Z_r: +2)
+    const bool zcol = ((j % cpr) >> 1) != 0;
+    const int kappa0 = ch * (kKC / 2) + 4 * kg;  // 4 consecutive (c, n') within one c block
+    const int c = kappa0 / NNp, nidx0 = kappa0 - c * NNp;
+    const double h = t_knots[s + 1] - t_knots[s];
+    const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
+    float f[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int nidx = nidx0 + q;
+        double v0 = 0.0, v1 = 0.0;
+        if (r < R && nidx < NN) {
+            const double scale = zcol ? (double)(nlo + nidx) : 1.0;
+            const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
+            const double wr = w.x * hc * scale, wi = w.y * hc * scale;
+            v0 = im_col ? wi : wr;   // part 0: Re Y += Re X Re W ; Im Y += Re X Im W
+            v1 = im_col ? wr : -wi;  // part 1: Re Y -= Im X Im W ; Im Y += Im X Re W
+        }
+        f[2 * q] = (float)v0;
+        f[2 * q + 1] = (float)v1;
     }
-    const float f = (float)val;
-    const __nv_bfloat16 hi = __float2bfloat16_rn(f);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
-    const uint32_t off = tile_off(j, kk, NB / 8) / 2;  // in elements
-    __nv_bfloat16 *base = Bpk + (((long long)s * nchunks + ch) * 2) * per_chunk;
-    base[off] = hi;
-    base[per_chunk + off] = lo;
+    uint32_t h4[4], l4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split2(f[2 * e], f[2 * e + 1], h4[e], l4[e]);
+    const uint32_t off = tile_off(j, 8 * kg, NB / 8);  // bytes; 16-byte aligned
+    unsigned char *base = reinterpret_cast<unsigned char *>(Bpk + (((long long)s * nchunks + ch) * 2) * per_chunk);
+    *reinterpret_cast<uint4 *>(base + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
+    *reinterpret_cast<uint4 *>(base + per_chunk * 2 + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
 }
 
 struct MixedArgs {
@@ -452,7 +464,7 @@ int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, 
     int NNp, NB, nch, cols;
     int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols, cpr);
     if (rc) return rc;
-    const long long total = (long long)nseg * nch * NB * kKC;
+    const long long total = (long long)nseg * nch * NB * 8;
     if (total == 0) return FEW_OK;
     const int threads = 256;
     k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NNp, NB, nch,

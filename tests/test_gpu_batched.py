@@ -70,12 +70,15 @@ def test_graph_capture_replay_and_update(cuda, tmp_path, monkeypatch):
     assert np.array_equal(replayed[0], first[0])
 
 
-def test_batched_backward_matches_single(cuda, tmp_path, monkeypatch):
+@pytest.mark.parametrize("precision", ["exact", "mixed"])
+def test_batched_backward_matches_single(cuda, tmp_path, monkeypatch, precision):
+    """The batched graph's adjoint (FP64, or the tensor-core one for the mixed
+    form) equals the single-waveform autograd backward bit for bit."""
     monkeypatch.setenv("FEW_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     batch = uneven_batch(count=3, seed=7)
     rng = np.random.default_rng(1)
     grads = [torch.tensor(rng.standard_normal(len(single(w, "exact"))) + 0j, device=cuda) for w in batch]
-    b = BatchedInterpolatedModeSum(precision="exact", chunk=1024, ctas_per_sm=2).setup(batch, requires_grad=True)
+    b = BatchedInterpolatedModeSum(precision=precision, chunk=1024, ctas_per_sm=2).setup(batch, requires_grad=True)
     b.forward()
     b.capture(backward=True, grads=grads)
     b.replay()
@@ -83,8 +86,9 @@ def test_batched_backward_matches_single(cuda, tmp_path, monkeypatch):
     for inp, g, (gt, gp) in zip(batch, grads, b.grad_out):
         teuk = torch.tensor(inp.teuk_modes, device=cuda, requires_grad=True)
         pc = torch.tensor(inp.phase_coeffs, device=cuda, requires_grad=True)
-        h = InterpolatedModeSum(precision="exact")(inp.t, teuk, inp.ylms, inp.phase_t, pc, inp.l, inp.m, inp.k,
-                                                   inp.n, T=inp.T, dt=inp.dt)
+        h = InterpolatedModeSum(precision=precision)(inp.t, teuk, inp.ylms, inp.phase_t, pc, inp.l, inp.m, inp.k,
+                                                     inp.n, T=inp.T, dt=inp.dt)
         h.backward(g)
+        assert not b.mixed_error()
         assert torch.equal(gt, teuk.grad)
         assert torch.equal(gp, pc.grad)
