@@ -49,10 +49,13 @@ class BatchedInterpolatedModeSum:
         autotune: choose the unit length and CTAs per SM by timing (cached).
         chunk, ctas_per_sm: fixed tile shape (overrides the autotuner).
         backward: "mixed" or "fp64" adjoint (default: "mixed" for precision="mixed").
+        streams: side streams over which the per-waveform spline builds, folds
+            and adjoints are spread (they are small launches; running several
+            waveforms' chains at once keeps the GPU busy).
     """
 
     def __init__(self, precision: str = "mixed", device=None, autotune: bool = True, chunk: int | None = None,
-                 ctas_per_sm: int | None = None, backward: str | None = None):
+                 ctas_per_sm: int | None = None, backward: str | None = None, streams: int = 8):
         if precision not in ("mixed", "exact", "faithful"):
             raise ValueError("precision must be 'mixed', 'exact' or 'faithful'")
         self.precision = precision
@@ -61,6 +64,10 @@ class BatchedInterpolatedModeSum:
         if backward not in ("mixed", "fp64"):
             raise ValueError("backward must be 'mixed' or 'fp64'")
         self.backward_precision = backward
+        if streams < 1:
+            raise ValueError("streams must be >= 1")
+        self.nstreams = int(streams)
+        self._side = None
         self.device = _device(device)
         self.autotune = autotune
         self.chunk = chunk
@@ -153,10 +160,29 @@ class BatchedInterpolatedModeSum:
         return _upload(units.reshape(-1), self.device)
 
     # ------------------------------------------------------------ the kernels
+    def _streams(self):
+        if self._side is None:
+            self._side = [torch.cuda.Stream(self.device) for _ in range(self.nstreams)]
+        return self._side
+
+    def _fork(self):
+        main = torch.cuda.current_stream(self.device)
+        side = self._streams()
+        for s in side:
+            s.wait_stream(main)
+        return main, side
+
+    @staticmethod
+    def _join(main, side):
+        for s in side:
+            main.wait_stream(s)
+
     def _prepare_operands(self):
-        """Spline builds and folds of every waveform (per-waveform launches)."""
-        for p in self.preps:
-            st = p.st
+        """Spline builds and folds of every waveform, spread over the side streams."""
+        main, side = self._fork()
+        for i, p in enumerate(self.preps):
+            st = side[i % len(side)].cuda_stream
+            p.st = st
             _lib.call("few_spline_build_factored", _ptr(p.fac), _ptr(p.teuk), 2 * p.K, 2, p.K, 1, 2 * p.K, p.N,
                       _ptr(p.coeffs), _lib.FEW_LAYOUT_KNOT_MAJOR, st)
             _lib.call("few_fold_coeffs", _ptr(p.coeffs), _ptr(p.ylm), _ptr(p.fold.d_key_ptr), _ptr(p.fold.d_key_list),
@@ -164,6 +190,7 @@ class BatchedInterpolatedModeSum:
             if p.Bpk is not None:
                 _lib.call("few_fold_mixed", _ptr(p.W), _ptr(p.t_dev), p.seg.nseg, p.fold.R, p.fold.NN, _ptr(p.Bpk),
                           st)
+        self._join(main, side)
 
     def _sum(self, units: torch.Tensor, ctas: int):
         st = _stream(self.device)
@@ -193,10 +220,23 @@ class BatchedInterpolatedModeSum:
         return self.outputs
 
     def backward(self, grads):
-        """FP64 adjoint of every waveform for upstream gradients grads[i]
-        (torch's convention for a complex output); returns a list of
-        (dL/d teuk_modes, dL/d phase_interp_coeffs)."""
-        return [InterpolatedModeSum._backward(p, g) for p, g in zip(self.preps, grads)]
+        """Adjoint of every waveform for upstream gradients grads[i] (torch's
+        convention for a complex output), the waveforms spread over the side
+        streams; returns a list of (dL/d teuk_modes, dL/d phase_interp_coeffs)."""
+        main, side = self._fork()
+        out = []
+        for i, (p, g) in enumerate(zip(self.preps, grads)):
+            s = side[i % len(side)]
+            with torch.cuda.stream(s):
+                p.st = s.cuda_stream
+                out.append(InterpolatedModeSum._backward(p, g))
+        self._join(main, side)
+        if not torch.cuda.is_current_stream_capturing():
+            for pair in out:  # made on side streams, used on the caller's stream
+                for t in pair:
+                    if t is not None:
+                        t.record_stream(main)
+        return out
 
     def mixed_error(self) -> bool:
         """True if a tensor-core wait of the batched sum or of a mixed adjoint timed out."""
@@ -228,13 +268,9 @@ class BatchedInterpolatedModeSum:
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
             with torch.cuda.graph(self.graph, stream=s):
-                for p in self.preps:
-                    p.st = s.cuda_stream
                 self.forward()
                 self.grad_out = self.backward(self.grad_in) if backward else None
         torch.cuda.current_stream(self.device).wait_stream(s)
-        for p in self.preps:
-            p.st = _stream(self.device)
         return self
 
     def replay(self):
