@@ -99,8 +99,8 @@ class BatchedInterpolatedModeSum:
         self.outputs = [self.out[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.preps))]
         self.max_R = max(p.fold.R for p in self.preps)
         max_NN = max(p.fold.NN for p in self.preps)
-        if self.precision == "mixed" and self.max_R > 128:
-            raise ValueError("precision='mixed' supports at most 128 (m, k) rows")
+        if self.precision == "mixed" and self.max_R > 64:
+            raise ValueError("precision='mixed' supports at most 64 (m, k) rows")
         self.smem_bytes = int(min(200 * 1024, max(p.fold.R * p.fold.NN * 64 for p in self.preps)))
         descs = np.zeros(len(self.preps), DESC_DTYPE)
         for i, p in enumerate(self.preps):

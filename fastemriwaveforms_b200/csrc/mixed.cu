@@ -1,30 +1,37 @@
 // Mixed-precision mode sum on the 5th-generation tensor cores (tcgen05).
 //
-// Per knot segment s the folded sum is a dense complex contraction
-//     Y[i, r] = sum_{c, n'} X[i, (c, n')] W'[(c, n'), r],   h_i = sum_r u_r(t_i) Y[i, r]
-// with X[i, (c, n')] = tau_i^c v_{n'}(t_i), tau = (t - t_s)/h_s in [0, 1),
-// W'[c] = W[c] h_s^c (the folded coefficients rescaled so every X entry has
-// modulus <= 1), v_{n'} = exp(-i n' Phi_r), u_r = exp(-i (m' Phi_phi + k' Phi_theta)).
+// Per knot segment s the folded sum is
+//     h_i = sum_r u_r(t_i) Y_r(t_i),   Y_r = sum_c tau_i^c Z_{c,r}(t_i),
+//     Z_{c,r}(t_i) = sum_{n'} v_{n'}(t_i) W'[c][n'][r]
+// with tau = (t - t_s)/h_s in [0, 1), W'[c] = W[c] h_s^c (the folded
+// coefficients rescaled so that every power of tau is <= 1),
+// v_{n'} = exp(-i n' Phi_r), u_r = exp(-i (m' Phi_phi + k' Phi_theta)).  The
+// contraction over n' runs on the tensor cores as a real GEMM
+//     [Re v | Im v interleaved] (128 samples x 2 NNp)  x  B (2 NNp x 8R)
+// whose 8 columns per (m', k') row hold (Re Z_{c,r}, Im Z_{c,r}) for c = 0..3;
+// the epilogue applies tau^c (Horner) and u_r in FP32.  The phase adjoint uses
+// the same contraction with A = (v, tau v) and the 8 columns per row holding
+// (Y, Z) for c_b in {0, 2} (tau^c = tau^c_a tau^c_b, c_a from A), Z built from
+// n' W: Y_r = D0 + tau^2 D2, Z_r (the n'-weighted sum) likewise.
 //
 // Precision plan:
 //   * FP64: the phase polynomials, the per-sample anchors exp(-i Phi) and the
-//     anchors of the n' recurrence (every 32 steps), each reduced mod 2 pi;
+//     anchors of the n' recurrence (every 16 steps), each reduced mod 2 pi;
 //   * FP32: the phasor recurrence between anchors, the row phasors u_r, the
-//     epilogue sum over rows;
-//   * tensor cores: the contraction as a real GEMM
-//       [Re X | Im X interleaved] (128 x 2*4*NNp)  x  B (2*4*NNp x NB)
-//     in split BF16 (x = hi + lo, three products hi*hi + hi*lo + lo*hi) with
-//     FP32 accumulation in TMEM.  B's columns are (Re Y_r, Im Y_r) pairs,
-//     column 2r and 2r+1, padded to NB.
+//     powers of tau and the epilogue sums;
+//   * tensor cores: split BF16 (x = hi + lo, three products hi*hi + hi*lo +
+//     lo*hi) with FP32 accumulation in TMEM.
 //
 // Layout: A and B tiles are K-major, no swizzle: 8x8 bf16 core matrices of
 // 128 contiguous bytes; stride 128 B between the two K halves of a K=16 step
 // (LBO) and 256 B between 8-row groups (SBO).  One CTA of 128 threads owns a
 // work unit (<= 1024 samples of one segment); each thread owns one sample row of
-// a 128-sample tile.  Per 64-wide K chunk: threads write the chunk of A, copy
-// the segment's precomputed B chunk, one thread issues 12 tcgen05.mma (4 K-steps
-// x 3 split products) and commits to an mbarrier; every wait is bounded and a
-// timeout sets an error word and ends the kernel after freeing TMEM.
+// a 128-sample tile.  K runs in chunks of 32 (16 n' x {Re, Im}); two stages:
+// while the tensor cores run chunk k's MMAs (2 K-steps x 3 split products per
+// group of <= 256 columns), the threads write chunk k+1 of A and its B chunk
+// arrives by cp.async; an mbarrier per stage (tcgen05.commit) gates reuse.
+// Every wait is bounded and a timeout sets an error word and ends the kernel
+// after freeing TMEM.
 #include <cuda_bf16.h>
 
 #include "few_common.cuh"
@@ -36,47 +43,57 @@ namespace few {
 namespace {
 
 constexpr int kMT = 128;   // samples per tile (MMA M)
-constexpr int kKC = 64;    // real K per chunk
+constexpr int kKC = 32;    // real K per chunk: 16 n' x {Re, Im}
+constexpr int kAStage = 2 * kMT * kKC * 2;  // A hi + lo planes of one stage (16 KB)
+
 // ---------------------------------------------------------------------------
 // B operand: per segment and K chunk, hi and lo bf16 tiles in the smem layout.
 // ---------------------------------------------------------------------------
-// cpr = columns per row: 2 for the sum (Re Y_r, Im Y_r), 4 for the phase
-// adjoint (Re Y_r, Im Y_r, Re Z_r, Im Z_r) with Z_r built from n' W.
-// One thread per 16-byte row of a core matrix: column j, K elements
-// 8 kg .. 8 kg + 7 of chunk ch = 4 consecutive (c, n') of the fold, each as
-// its part-0 and part-1 value; writes the hi and the lo chunk.
+// Columns: 8 per (m', k') row r, slot = j % 8.  Sum: slot = 2 c + re/im.
+// Phase adjoint: slot = 4 yz + 2 cbl + re/im with c = c_a + 2 cbl and yz = 1
+// for the n'-weighted columns.  K chunk ch covers 16 n' (sum: block ch;
+// adjoint: block ch / 2 with c_a = ch % 2), element kk = 2 (n' - 16 block) + part.
+// One thread per 16-byte row of a core matrix (column j, K elements 8 kg ..
+// 8 kg + 7 = 4 n' x 2 parts); writes the hi and the lo chunk.
 __global__ void __launch_bounds__(256) k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots,
-                                                    int nseg, int R, int NN, int NNp, int NB, int nchunks, int cpr,
-                                                    int nlo, __nv_bfloat16 *__restrict__ Bpk)
+                                                    int nseg, int R, int NN, int NB, int nchunks, int adj, int nlo,
+                                                    __nv_bfloat16 *__restrict__ Bpk)
 {
-    const long long per_chunk = (long long)NB * kKC;
-    const long long total = (long long)nseg * nchunks * 8 * NB;
+    const long long per_chunk = (long long)NB * kKC;  // elements of one plane of one chunk
+    const long long total = (long long)nseg * nchunks * (kKC / 8) * NB;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int j = (int)(idx % NB);
     long long rest = idx / NB;
-    const int kg = (int)(rest & 7);
-    rest >>= 3;
+    const int kg = (int)(rest % (kKC / 8));
+    rest /= (kKC / 8);
     const int ch = (int)(rest % nchunks);
     const int s = (int)(rest / nchunks);
-    const int r = j / cpr;
-    const bool im_col = j & 1;  // column 2r holds Re Y_r, column 2r+1 holds Im Y_r (Z_r: +2)
-    const bool zcol = ((j % cpr) >> 1) != 0;
-    const int kappa0 = ch * (kKC / 2) + 4 * kg;  // 4 consecutive (c, n') within one c block
-    const int c = kappa0 / NNp, nidx0 = kappa0 - c * NNp;
+    const int r = j >> 3, slot = j & 7;
+    const bool im_col = slot & 1;
+    int c, nblk;
+    bool zcol = false;
+    if (adj) {
+        nblk = ch >> 1;
+        c = (ch & 1) + 2 * ((slot >> 1) & 1);
+        zcol = (slot >> 2) != 0;
+    } else {
+        nblk = ch;
+        c = slot >> 1;
+    }
     const double h = t_knots[s + 1] - t_knots[s];
     const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
     float f[8];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int nidx = nidx0 + q;
+        const int nidx = 16 * nblk + 4 * kg + q;
         double v0 = 0.0, v1 = 0.0;
         if (r < R && nidx < NN) {
             const double scale = zcol ? (double)(nlo + nidx) : 1.0;
             const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
             const double wr = w.x * hc * scale, wi = w.y * hc * scale;
-            v0 = im_col ? wi : wr;   // part 0: Re Y += Re X Re W ; Im Y += Re X Im W
-            v1 = im_col ? wr : -wi;  // part 1: Re Y -= Im X Im W ; Im Y += Im X Re W
+            v0 = im_col ? wi : wr;   // part 0: Re Z += Re v Re W ; Im Z += Re v Im W
+            v1 = im_col ? wr : -wi;  // part 1: Re Z -= Im v Im W ; Im Z += Im v Re W
         }
         f[2 * q] = (float)v0;
         f[2 * q + 1] = (float)v1;
@@ -106,17 +123,15 @@ struct MixedArgs {
     double dt;
 };
 
-__device__ __forceinline__ void mixed_dims_dev(int R, int NN, int &NNp, int &NB, int &nchunks)
+__host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, bool adj, int &NNp, int &NB, int &nchunks)
 {
-    NNp = (NN + 31) / 32 * 32;
-    NB = max(16, (2 * R + 15) / 16 * 16);
-    nchunks = NNp / 8;
+    NNp = (NN + 15) / 16 * 16;
+    NB = (8 * R + 15) / 16 * 16;
+    nchunks = (adj ? 2 : 1) * NNp / 16;
 }
 
-// One work unit (samples [lo, hi) of segment seg) on the tensor cores.  Two
-// A/B buffers: while the tensor cores run chunk k's MMAs from one buffer, the
-// threads generate chunk k+1 into the other and its B tile arrives by
-// cp.async.  Returns false (for every thread) if a tensor-core wait timed out.
+// One work unit (samples [lo, hi) of segment seg) on the tensor cores.
+// Returns false (for every thread) if a tensor-core wait timed out.
 template <bool ADJ>
 __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, MixedPipe &pp,
                            int *s_rm, int *s_rk, double *s_pc, int unit = 0, float *s_e = nullptr,
@@ -125,13 +140,11 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NB = a.NB;
     double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // phase adjoint: this lane's share of 6 outputs
-    const int bbytes = 2 * NB * kKC * 2;  // one B buffer: hi then lo
-    // A buffers (hi 16 KB then lo 16 KB each) at 0 and 32 KB, B buffers after them
-    unsigned char *const sA0 = smem_raw;
-    unsigned char *const sB0 = smem_raw + 4 * kMT * kKC * 2;
+    const int bchunk = 2 * NB * kKC * 2;               // one B chunk: hi then lo planes
+    const int stage = kAStage + bchunk;
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
-    const int R = a.R, NN = a.NN, NNp = a.NNp, nlo = a.nlo;
+    const int R = a.R, NN = a.NN, nlo = a.nlo, nch = a.nchunks;
     const long long nps = (long long)(a.N - 1) * 3;
 
     for (int r = tid; r < R; r += blockDim.x) {
@@ -145,10 +158,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t idesc = idesc_bf16(kMT, NB);
-    const int halves = NNp / 32;
-    const int nch = 4 * halves;
-    const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * a.nchunks * 2 * NB * kKC;
+    const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * nch * 2 * NB * kKC;
     bool failed = false;
 
     for (int base = lo; base < hi && !failed; base += kMT) {
@@ -166,36 +176,36 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
         const float2 Ep = anchor(Pp);
         const float2 Er = anchor(Pr);
         const float2 Et = a.use_theta ? anchor(Pt) : make_float2(1.f, 0.f);
-        const float tau2 = tau * tau, tau3 = tau2 * tau;
-        float2 v[32];
+        float2 v[16];
 
         for (int k = 0; k < nch && !failed; ++k) {
             const int b = k & 1;
-            const int hh = k >> 2, c = k & 3;
-            const int ch = c * halves + hh;  // the B packing's chunk index
-            // buffer b is free once the MMAs of chunk k-2 are done
+            const int nblk = ADJ ? (k >> 1) : k;
+            const bool second = ADJ && (k & 1);  // c_a = 1: A = tau v
+            // stage b is free once the MMAs of chunk k-2 are done
             if (__syncthreads_or(!pipe_drain(pp, b))) {
                 failed = true;
                 break;
             }
-            unsigned char *const sBb = sB0 + b * bbytes;
+            unsigned char *const sAb = smem_raw + b * stage;
+            unsigned char *const sBb = sAb + kAStage;
             {
-                const unsigned char *src = reinterpret_cast<const unsigned char *>(Bseg + (long long)ch * 2 * NB * kKC);
-                for (int q = tid; q < bbytes / 16; q += blockDim.x) cp_async16(sBb + 16 * q, src + 16 * q);
+                const unsigned char *src = reinterpret_cast<const unsigned char *>(Bseg + (long long)k * 2 * NB * kKC);
+                for (int q = tid; q < bchunk / 16; q += blockDim.x) cp_async16(sBb + 16 * q, src + 16 * q);
                 cp_async_commit();
             }
-            if (c == 0) {
-                v[0] = anchor((double)(nlo + 32 * hh) * Pr);
+            if (!second) {
+                v[0] = anchor((double)(nlo + 16 * nblk) * Pr);
 #pragma unroll
-                for (int q = 1; q < 32; ++q) v[q] = fcmul(v[q - 1], Er);
+                for (int q = 1; q < 16; ++q) v[q] = fcmul(v[q - 1], Er);
 #pragma unroll
-                for (int q = 0; q < 32; ++q)
-                    if (!valid || 32 * hh + q >= NN) v[q] = make_float2(0.f, 0.f);
+                for (int q = 0; q < 16; ++q)
+                    if (!valid || 16 * nblk + q >= NN) v[q] = make_float2(0.f, 0.f);
             }
-            const float sc = c == 0 ? 1.f : (c == 1 ? tau : (c == 2 ? tau2 : tau3));
-            unsigned char *const aH = sA0 + b * (2 * kMT * kKC * 2), *const aL = aH + kMT * kKC * 2;
+            const float sc = second ? tau : 1.f;
+            unsigned char *const aH = sAb, *const aL = sAb + kMT * kKC * 2;
 #pragma unroll
-            for (int g = 0; g < 8; ++g) {  // 8 groups of 4 complex = 8 bf16 = 16 bytes
+            for (int g = 0; g < 4; ++g) {  // 4 groups of 4 complex = 8 bf16 = 16 bytes
                 uint32_t h4[4], l4[4];
 #pragma unroll
                 for (int e2 = 0; e2 < 4; ++e2) {
@@ -217,11 +227,17 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                 for (int st = 0; st < kKC / 16; ++st) {
                     const uint64_t da_h = smem_desc(a_h + st * (kMT / 8) * 256, 128, 256);
                     const uint64_t da_l = smem_desc(a_l + st * (kMT / 8) * 256, 128, 256);
-                    const uint64_t db_h = smem_desc(b_h + st * (NB / 8) * 256, 128, 256);
-                    const uint64_t db_l = smem_desc(b_l + st * (NB / 8) * 256, 128, 256);
-                    mma_bf16(pp.tmem, da_h, db_h, idesc, (k | st) != 0);
-                    mma_bf16(pp.tmem, da_h, db_l, idesc, 1u);
-                    mma_bf16(pp.tmem, da_l, db_h, idesc, 1u);
+                    for (int n0 = 0; n0 < NB; n0 += 256) {  // column groups of <= 256 (one MMA each)
+                        const int nq = min(256, NB - n0);
+                        const uint32_t idesc = idesc_bf16(kMT, nq);
+                        const uint32_t boff = st * (NB / 8) * 256 + (n0 / 8) * 256;
+                        const uint64_t db_h = smem_desc(b_h + boff, 128, 256);
+                        const uint64_t db_l = smem_desc(b_l + boff, 128, 256);
+                        const uint32_t d = pp.tmem + (uint32_t)n0;
+                        mma_bf16(d, da_h, db_h, idesc, (k | st) != 0);
+                        mma_bf16(d, da_h, db_l, idesc, 1u);
+                        mma_bf16(d, da_l, db_h, idesc, 1u);
+                    }
                 }
                 mma_commit(&pp.bar[b]);
             }
@@ -235,67 +251,46 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
             failed = true;
             break;
         }
+        // epilogue: this thread's accumulator row (TMEM lane = tid); two (m', k')
+        // rows of 8 columns per 16-column load; u_r by one multiplication when m'
+        // steps by one
         tc_fence_after();
         const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
         float2 uu = make_float2(1.f, 0.f);
         int pm = 0x7fffffff, pk = 0x7fffffff;
-        if constexpr (!ADJ) {
-            // epilogue: this thread's accumulator row (TMEM lane = tid), 8 rows
-            // (m', k') per 16-column load; u_r by one multiplication when m' steps by one
-            float hr = 0.f, hi_ = 0.f;
-            for (int c0 = 0; c0 < NB; c0 += 16) {
-                float D[16];
-                tmem_ld16(trow + c0, D);
-                tmem_wait_ld();
+        const float tau2 = tau * tau;
+        float2 Sp = make_float2(0.f, 0.f), St = Sp, Sr = Sp;  // sum: Sp = h; adjoint: the three sums
+        for (int c0 = 0; c0 < NB; c0 += 16) {
+            float D[16];
+            tmem_ld16(trow + c0, D);
+            tmem_wait_ld();
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int r = (c0 >> 1) + q;
-                    if (r < R) {
-                        const int mm = s_rm[r], kk = s_rk[r];
-                        if (kk == pk && mm == pm + 1) {
-                            uu = fcmul(uu, Ep);
-                        } else {
-                            uu = fcpow(Ep, mm);
-                            if (kk) uu = fcmul(uu, fcpow(Et, kk));
-                        }
-                        pm = mm;
-                        pk = kk;
-                        const float yr = D[2 * q], yi = D[2 * q + 1];
-                        hr = fmaf(uu.x, yr, fmaf(-uu.y, yi, hr));
-                        hi_ = fmaf(uu.x, yi, fmaf(uu.y, yr, hi_));
+            for (int q = 0; q < 2; ++q) {
+                const int r = (c0 >> 3) + q;
+                if (r < R) {
+                    const int mm = s_rm[r], kk = s_rk[r];
+                    if (kk == pk && mm == pm + 1) {
+                        uu = fcmul(uu, Ep);
+                    } else {
+                        uu = fcpow(Ep, mm);
+                        if (kk) uu = fcmul(uu, fcpow(Et, kk));
                     }
-                }
-            }
-            if (valid) {
-                double2 o = a.wf[i];
-                o.x += (double)hr;
-                o.y += (double)hi_;
-                a.wf[i] = o;
-            }
-        } else {
-            // phase adjoint: 4 rows per 16-column load, (Y_r, Z_r) per row;
-            // dh/dPhi_phi = -i sum m' u Y, dh/dPhi_theta = -i sum k' u Y,
-            // dh/dPhi_r = -i sum u Z, and e_f = Re(g dh/dPhi_f) = Im(g S_f)
-            float2 Sp = make_float2(0.f, 0.f), St = Sp, Sr = Sp;
-            for (int c0 = 0; c0 < NB; c0 += 16) {
-                float D[16];
-                tmem_ld16(trow + c0, D);
-                tmem_wait_ld();
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int r = (c0 >> 2) + q;
-                    if (r < R) {
-                        const int mm = s_rm[r], kk = s_rk[r];
-                        if (kk == pk && mm == pm + 1) {
-                            uu = fcmul(uu, Ep);
-                        } else {
-                            uu = fcpow(Ep, mm);
-                            if (kk) uu = fcmul(uu, fcpow(Et, kk));
-                        }
-                        pm = mm;
-                        pk = kk;
-                        const float2 P = fcmul(uu, make_float2(D[4 * q], D[4 * q + 1]));
-                        const float2 Q = fcmul(uu, make_float2(D[4 * q + 2], D[4 * q + 3]));
+                    pm = mm;
+                    pk = kk;
+                    const float *d8 = D + 8 * q;
+                    if constexpr (!ADJ) {
+                        // Y = sum_c tau^c Z_c (Horner)
+                        const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
+                        const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
+                        Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
+                        Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
+                    } else {
+                        // dh/dPhi_phi = -i sum m' u Y, dh/dPhi_theta = -i sum k' u Y,
+                        // dh/dPhi_r = -i sum u Z
+                        const float2 Y = make_float2(fmaf(d8[2], tau2, d8[0]), fmaf(d8[3], tau2, d8[1]));
+                        const float2 Z = make_float2(fmaf(d8[6], tau2, d8[4]), fmaf(d8[7], tau2, d8[5]));
+                        const float2 P = fcmul(uu, Y);
+                        const float2 Q = fcmul(uu, Z);
                         const float fm = (float)mm, fk = (float)kk;
                         Sp.x = fmaf(fm, P.x, Sp.x);
                         Sp.y = fmaf(fm, P.y, Sp.y);
@@ -306,6 +301,16 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                     }
                 }
             }
+        }
+        if constexpr (!ADJ) {
+            if (valid) {
+                double2 o = a.wf[i];
+                o.x += (double)Sp.x;
+                o.y += (double)Sp.y;
+                a.wf[i] = o;
+            }
+        } else {
+            // e_f = Re(g dh/dPhi_f) = Im(g S_f), g = conj(G)
             float ep = 0.f, et = 0.f, er = 0.f;
             if (valid) {
                 const double2 Gt = a.grad[i];
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.use_theta = d.use_theta;
         a.dt = d.dt;
         a.tmem_cols = tmem_cols;
-        mixed_dims_dev(d.R, d.NN, a.NNp, a.NB, a.nchunks);
+        mixed_dims_core(d.R, d.NN, false, a.NNp, a.NB, a.nchunks);
         ok = mixed_unit<false>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
     }
     mixed_teardown(!ok, pp, tmem_cols, err);
@@ -437,38 +442,37 @@ __global__ void __launch_bounds__(kMT, 1) k_adj_phase_mixed(MixedArgs a)
 
 }  // namespace
 
-// cpr = B columns per (m', k') row: 2 for the sum, 4 for the phase adjoint.
-int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols, int cpr)
+// Tensor-core shapes of an R x NN fold grid (adj: the phase adjoint's operand).
+int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols, bool adj)
 {
-    if (cpr * R > 256)
-        return fail(FEW_ERR_SIZE, "mixed form: %d rows x %d columns exceed the 256 one MMA holds", R, cpr);
-    *NNp = (NN + 31) / 32 * 32;
-    *NB = std::max(16, (cpr * R + 15) / 16 * 16);
-    *nchunks = 4 * (*NNp) / 32;
+    if (R > 64) return fail(FEW_ERR_SIZE, "mixed form: %d (m, k) rows exceed the 64 the accumulator holds", R);
+    mixed_dims_core(R, NN, adj, *NNp, *NB, *nchunks);
     int cols = 32;
     while (cols < *NB) cols <<= 1;
     *tmem_cols = cols;
     return FEW_OK;
 }
 
-size_t mixed_bpk_bytes(int nseg, int R, int NN, int cpr)
+size_t mixed_smem_bytes(int NB) { return (size_t)2 * (kAStage + 2 * NB * kKC * 2); }
+
+size_t mixed_bpk_bytes(int nseg, int R, int NN, bool adj)
 {
     int NNp, NB, nch, cols;
-    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols, cpr)) return 0;
+    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols, adj)) return 0;
     return (size_t)nseg * nch * 2 * NB * kKC * sizeof(__nv_bfloat16);
 }
 
-int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, int nlo, int cpr, void *Bpk,
+int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, int nlo, bool adj, void *Bpk,
                       cudaStream_t st)
 {
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols, cpr);
+    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols, adj);
     if (rc) return rc;
-    const long long total = (long long)nseg * nch * NB * 8;
+    const long long total = (long long)nseg * nch * (kKC / 8) * NB;
     if (total == 0) return FEW_OK;
     const int threads = 256;
-    k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NNp, NB, nch,
-                                                                                 cpr, nlo, (__nv_bfloat16 *)Bpk);
+    k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NB, nch,
+                                                                                 adj ? 1 : 0, nlo, (__nv_bfloat16 *)Bpk);
     FEW_LAUNCH_CHECK("k_fold_mixed");
     return FEW_OK;
 }
@@ -479,7 +483,7 @@ int launch_adj_phase_mixed(const double2 *grad, const void *Bpk, const double *p
 {
     if (nunits == 0) return FEW_OK;
     MixedArgs a;
-    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, 4);
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, true);
     if (rc) return rc;
     a.wf = nullptr;
     a.Bpk = (const __nv_bfloat16 *)Bpk;
@@ -498,7 +502,7 @@ int launch_adj_phase_mixed(const double2 *grad, const void *Bpk, const double *p
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * a.NB * kKC * 2;
+    const size_t smem = mixed_smem_bytes(a.NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_phase_mixed, (int)smem));
     k_adj_phase_mixed<<<nunits, kMT, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_adj_phase_mixed");
@@ -511,7 +515,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
 {
     if (nunits == 0) return FEW_OK;
     MixedArgs a;
-    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, 2);
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, false);
     if (rc) return rc;
     a.wf = wf;
     a.grad = nullptr;
@@ -530,7 +534,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * a.NB * kKC * 2;
+    const size_t smem = mixed_smem_bytes(a.NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed, (int)smem));
     k_sum_mixed<<<nunits, kMT, smem, st>>>(a);
     FEW_LAUNCH_CHECK("k_sum_mixed");
@@ -542,7 +546,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols, 2);
+    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols, false);
     if (rc) return rc;
     if (ctas <= 0) {
         int dev = 0, sms = 148;
@@ -551,7 +555,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
         ctas = 2 * sms;
     }
     ctas = std::min(ctas, nunits);
-    const size_t smem = (size_t)4 * kMT * kKC * 2 + (size_t)4 * NB * kKC * 2;
+    const size_t smem = mixed_smem_bytes(NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
     k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");
@@ -565,8 +569,8 @@ extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, cons
 {
     few::clear_error();
     if (!descs || !units4 || !err) return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: null pointer");
-    if (nwave < 1 || nunits < 0 || max_R < 1 || max_R > 128)
-        return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 128)");
+    if (nwave < 1 || nunits < 0 || max_R < 1 || max_R > 64)
+        return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 64)");
     return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, err, (cudaStream_t)stream);
 }
 
@@ -575,12 +579,12 @@ extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, in
     few::clear_error();
     if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed: null pointer");
     if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed: bad sizes");
-    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, 0, 2, Bpk, (cudaStream_t)stream);
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, 0, false, Bpk, (cudaStream_t)stream);
 }
 
 extern "C" long long few_mixed_operand_bytes(int nseg, int R, int NN)
 {
-    return (long long)few::mixed_bpk_bytes(nseg, R, NN, 2);
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN, false);
 }
 
 extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
@@ -590,14 +594,15 @@ extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coef
     few::clear_error();
     if (!wf || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !err)
         return few::fail(FEW_ERR_ARG, "few_sum_mixed: null pointer");
-    if (N < 2 || nunits < 0 || R < 1 || R > 128 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_sum_mixed: bad sizes");
+    if (N < 2 || nunits < 0 || R < 1 || R > 64 || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_sum_mixed: bad sizes (R <= 64)");
     return few::launch_sum_mixed((double2 *)wf, Bpk, phase_coeffs, N, seg_info, t_knots, units, nunits, row_m, row_k,
                                  R, nlo, NN, dt, use_theta, err, (cudaStream_t)stream);
 }
 
 extern "C" long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN)
 {
-    return (long long)few::mixed_bpk_bytes(nseg, R, NN, 4);
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN, true);
 }
 
 extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
@@ -606,7 +611,7 @@ extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int 
     few::clear_error();
     if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed_adjoint: null pointer");
     if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: bad sizes");
-    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, nlo, 4, Bpk, (cudaStream_t)stream);
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, nlo, true, Bpk, (cudaStream_t)stream);
 }
 
 extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,

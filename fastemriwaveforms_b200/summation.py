@@ -511,7 +511,7 @@ class InterpolatedModeSum(SummationBase):
         if self.precision == "mixed":
             nbytes = int(_lib.load().few_mixed_operand_bytes(max(seg.nseg, 1), fold.R, fold.NN))
             if nbytes <= 0:
-                raise ValueError("precision='mixed' supports at most 128 (m, k) rows")
+                raise ValueError("precision='mixed' supports at most 64 (m, k) rows")
             Bpk = torch.empty(nbytes, dtype=torch.uint8, device=p.dev)
             if self._mixed_err is None or self._mixed_err.device != p.dev:
                 self._mixed_err = torch.zeros(1, dtype=torch.int32, device=p.dev)

@@ -247,21 +247,23 @@ FEW_API int few_sum_batched(const few_wave_desc *descs, int nwave, const int *un
 /* ------------------------------------------------------------------------ */
 
 /* Bytes of the tensor-core B operand for nseg segments of an R x NN fold grid
- * (0 if R > 128). */
+ * (0 if R > 64). */
 FEW_API long long few_mixed_operand_bytes(int nseg, int R, int NN);
 
 /* Packs the folded coefficients W (few_fold_coeffs) into the split-BF16 B
  * operand Bpk [device] (few_mixed_operand_bytes bytes): per segment the
  * coefficients are rescaled by h_s^c (h_s = t_knots[s+1] - t_knots[s]) and laid
- * out in the tensor-core tile order.  t_knots [device] (N,). */
+ * out in the tensor-core tile order, 8 columns per (m', k') row (the powers of
+ * tau x re/im).  t_knots [device] (N,). */
 FEW_API int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream);
 
 /* Mixed-precision sum into wf [device] (out_len,) complex (accumulated):
  * FP64 phases, anchors and mod-2pi reduction; FP32 phasor recurrence
- * re-anchored every 32 n' steps; the per-segment contraction on tcgen05 in
- * split BF16 with FP32 accumulation.  Arguments as few_sum_folded plus
+ * re-anchored every 16 n' steps; the per-segment contraction over n' on
+ * tcgen05 in split BF16 with FP32 accumulation, the powers of tau and the row
+ * phasors in the FP32 epilogue.  Arguments as few_sum_folded plus
  * t_knots [device] (N,) and err [device] int (set to 1 if a tensor-core wait
- * timed out; the kernel then stops early).  R <= 128. */
+ * timed out; the kernel then stops early).  R <= 64. */
 FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
                           const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
                           int R, int nlo, int NN, double dt, int use_theta, int *err, void *stream);
@@ -269,7 +271,7 @@ FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs,
 /* Persistent form of few_sum_mixed over many waveforms: descs [device]
  * (nwave,) with Bpk set (few_fold_mixed per waveform); units4 [device]
  * (4*nunits,) = {waveform, segment, first sample, end sample}; max_R: the
- * largest R in the batch (<= 128, sizes shared memory and TMEM); ctas:
+ * largest R in the batch (<= 64, sizes shared memory and TMEM); ctas:
  * persistent CTAs (0: two per SM); err [device] int as in few_sum_mixed. */
 FEW_API int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
                                   int ctas, int *err, void *stream);
