@@ -577,15 +577,15 @@ def main():
                  "max_rel_vs_faithful": float(d.abs().max() / ref_wf.abs().max())}
         if prec == "mixed":
             f_ = other._last_plan[0]
-            nnp = (f_.NN + 31) // 32 * 32
-            nb = max(16, (2 * f_.R + 15) // 16 * 16)
-            tflop = 2.0 * (8 * nnp) * nb * 3 * T / 1e12
+            kdim = 2 * ((f_.NN + 15) // 16 * 16)  # K: (n', re/im)
+            nb = (8 * f_.R + 15) // 16 * 16       # N: 8 columns per (m', k') row
+            tflop = 2.0 * kdim * nb * 3 * T / 1e12
             entry["mixed_error"] = other.mixed_error()
             entry["roofline"] = {"bound": "tensor", "kernel": "k_sum_mixed (+ k_fold_mixed)",
                                  "achieved": tflop / (st_o["sum"] * 1e-3), "peak": pk["bf16_tflops"],
                                  "unit": "TFLOP/s", "frac": tflop / (st_o["sum"] * 1e-3) / pk["bf16_tflops"],
                                  "peak_source": f"{pk_kind} bf16_tflops (burst)",
-                                 "algorithmic": f"2 x {8 * nnp} x {nb} x 3 split products per sample"}
+                                 "algorithmic": f"MMA work issued: 2 x K {kdim} x N {nb} x 3 split products per sample"}
         forms[prec] = entry
     fb = {}
     # exact: FP64 forward and adjoint; mixed: tensor-core forward and adjoint;
