@@ -24,7 +24,7 @@ FEW_SUM_FAITHFUL = 0
 FEW_SUM_EXACT = 1
 FEW_LAYOUT_KNOT_MAJOR = 0
 FEW_LAYOUT_INTERP_MAJOR = 1
-FEW_FAC_WIDTH = 12
+FEW_FAC_WIDTH = 16
 
 _c_int, _c_ll, _c_dbl, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p
 

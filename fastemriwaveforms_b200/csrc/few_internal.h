@@ -72,7 +72,8 @@ int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *g
 int launch_spline_adjoint_factored(const double *fac, double *gc, double *gy, long long sk, long long sp, int split,
                                    long long off2, int ni, int N, int accumulate, cudaStream_t st);
 
-constexpr int kFacWidth = 12;       // doubles per row of the shared spline factorization
+constexpr int kFacWidth = 16;       // doubles per row of the shared spline factorization
+constexpr int kScanChunks = 8;      // knot chunks of the scan form of the spline sweeps (warps per CTA)
 constexpr int kMaxRows = 256;        // distinct (m', k') rows of a fold plan
 constexpr int kDefaultChunk = 1024;  // output samples per work unit of the sum
 

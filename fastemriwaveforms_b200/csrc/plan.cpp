@@ -123,12 +123,17 @@ int segment_plan(const double *h_t, const double *phase_t, int init_len, int out
 // Factorization of the not-a-knot system shared by every series on knots t
 // (the elimination k_spline_build performs per thread, done once), and of the
 // interior block of its transpose for the adjoint (k_spline_adjoint_factored).
-// fac (N+1, kFacWidth = 12), row i:
+// fac (N+1, kFacWidth = 16), row i:
 //   0 lo_i, 1 1/den_i, 2 c'_i, 3 alpha_i, 4 beta_i  (rows 1..N-2; forward sweep
 //     r'_i = (alpha_i delta_{i-1} + beta_i delta_i - lo_i r'_{i-1}) / den_i, the
 //     two boundary rows' right-hand sides folded into rows 1 and N-2)
 //   5 h_i, 6 1/h_i                                   (rows 0..N-2)
 //   7 lo~_i = h_{i-2}, 8 1/den~_i, 9 c~_i           (rows 1..N-2; transposed block)
+//   10, 11  products of the sweep factors -lo_j/den_j over [chunk start, i] and of
+//           -c'_j over [i, chunk end), 12, 13 the same for the transposed block
+//           (-lo~_j/den~_j and -c~_j): the interior rows 1..N-2 are cut into
+//           kScanChunks chunks of ceil((N-2)/kScanChunks) rows, and a chunk's
+//           sweeps, run with a zero carry-in, are corrected by carry x product.
 // Row N: gamma0, gamma1 (b0 = gamma0 delta_0 + gamma1 delta_1), d0 = x2 - x0, h1,
 // eps0, eps1 (bE = eps0 delta_{N-3} + eps1 delta_{N-2}), dE = x_{N-1} - x_{N-3},
 // hA = x_{N-2} - x_{N-3}.
@@ -183,6 +188,25 @@ int spline_factor(const double *x, int N, double *fac)
         fac[W * i + 8] = 1.0 / dent;
         fac[W * i + 9] = ct;
         ctprev = ct;
+    }
+    // chunk products for the scan form of both sweeps
+    const int M = N - 2, L = (M + kScanChunks - 1) / kScanChunks;
+    for (int a = 1; a <= N - 2; a += L) {
+        const int e = std::min(a + L, N - 1);  // rows [a, e)
+        double pf = 1.0, pft = 1.0;
+        for (int i = a; i < e; ++i) {
+            pf *= -fac[W * i + 0] * fac[W * i + 1];
+            pft *= -fac[W * i + 7] * fac[W * i + 8];
+            fac[W * i + 10] = pf;
+            fac[W * i + 12] = pft;
+        }
+        double pb = 1.0, pbt = 1.0;
+        for (int i = e - 1; i >= a; --i) {
+            pb *= -fac[W * i + 2];
+            pbt *= -fac[W * i + 9];
+            fac[W * i + 11] = pb;
+            fac[W * i + 13] = pbt;
+        }
     }
     double *b = fac + (size_t)W * N;
     b[0] = g0;

@@ -151,103 +151,177 @@ __global__ void __launch_bounds__(128) k_spline_build(SplineArgs a)
     o0[0] = y0;
 }
 
-// Shared-knot build from a host factorization (few_spline_factor): per step the
-// forward sweep is r'_i = (alpha_i delta_{i-1} + beta_i delta_i - lo_i r'_{i-1}) / den_i
-// and the backward sweep s_i = r'_i - c'_i s_{i+1}; no division per series and
-// only r' parked in the c3 output row.  Loads are issued kSweepBatch steps
-// ahead of the recurrence (they do not depend on it), so a thread keeps that
-// many in flight instead of waiting on one load per step.
+// Shared-knot build from a host factorization (few_spline_factor), in scan form.
+// The sweeps are linear recurrences whose factors depend on the knots only:
+//     r'_i = A_i r'_{i-1} + (alpha_i delta_{i-1} + beta_i delta_i) / den_i,  A_i = -lo_i / den_i
+//     s_i  = C_i s_{i+1} + r'_i,                                            C_i = -c'_i
+// so the interior rows are cut into kScanChunks chunks (one warp each; lane =
+// series, 32 series per CTA, every access coalesced across the series): each
+// warp runs its chunk's forward sweep from a zero carry, the chunk carries are
+// chained through shared memory (r'_end = rho_end + (prod A) r'_in), the
+// warp corrects its rows (r' = rho + prod_{chunk start..i} A x carry) and runs
+// the backward sweep from a zero carry the same way, and finally writes the
+// coefficients of its segments from the corrected slopes.  The products come
+// from the factor table; the sweep temporaries are parked in the c3 output
+// row, which the last pass overwrites.  Loads are issued kSweepBatch steps
+// ahead of the arithmetic that uses them.
 constexpr int kSweepBatch = 8;
 
-__global__ void __launch_bounds__(64) k_spline_build_factored(const double *__restrict__ fac,
-                                                            const double *__restrict__ y, long long sk, long long sp,
-                                                            int split, long long off2, int ni, int N,
-                                                            double *__restrict__ out, long long os_i, long long os_p)
+__global__ void __launch_bounds__(32 * kScanChunks) k_spline_build_factored(
+    const double *__restrict__ fac, const double *__restrict__ y, long long sk, long long sp, int split,
+    long long off2, int ni, int N, double *__restrict__ out, long long os_i, long long os_p)
 {
     constexpr int W = kFacWidth;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= ni) return;
+    constexpr int P = kScanChunks;
+    __shared__ double s_end[P][32];
+    __shared__ double s_carry[P + 1][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int p0 = blockIdx.x * 32 + lane;
+    const bool live = p0 < ni;
+    const int p = live ? p0 : ni - 1;  // idle lanes compute on a valid series and store nothing
     const double *yb = (p < split) ? y + (long long)p * sp : y + off2 + (long long)(p - split) * sp;
     const long long plane = (long long)N * ni;
     double *o0 = out + (long long)p * os_p;
     double *o1 = o0 + plane;
     double *o2 = o1 + plane;
     double *o3 = o2 + plane;
-    const double *bnd = fac + (long long)W * N;
-    const double g0 = __ldg(bnd + 0), g1 = __ldg(bnd + 1), d0 = __ldg(bnd + 2), h1 = __ldg(bnd + 3);
-    const double e0 = __ldg(bnd + 4), e1 = __ldg(bnd + 5), dE = __ldg(bnd + 6), hA = __ldg(bnd + 7);
+    const int L = (N - 2 + P - 1) / P;
+    const int a = 1 + w * L, e = min(a + L, N - 1);  // this warp's rows [a, e); empty if a >= e
 
-    const double y0 = yb[0], y1 = yb[sk], y2 = yb[2 * sk];
-    const double del0 = (y1 - y0) * __ldg(fac + 6);
-    const double del1 = (y2 - y1) * __ldg(fac + W + 6);
-    const double b0 = g0 * del0 + g1 * del1;
-    double ym = y1, dprev = del0, rprev = 0.0, bE = 0.0;
-    for (int i0 = 1; i0 <= N - 2; i0 += kSweepBatch) {
-        double yv[kSweepBatch], fl[kSweepBatch], fi[kSweepBatch], fa[kSweepBatch], fb[kSweepBatch], fh[kSweepBatch];
+    // pass 1: forward sweep from a zero carry
+    double rho = 0.0;
+    if (a < e) {
+        double ym = yb[(long long)a * sk];
+        double dprev = (ym - yb[(long long)(a - 1) * sk]) * __ldg(fac + W * (a - 1) + 6);
+        for (int i0 = a; i0 < e; i0 += kSweepBatch) {
+            double yv[kSweepBatch], fl[kSweepBatch], fi[kSweepBatch], fa[kSweepBatch], fb[kSweepBatch], fh[kSweepBatch];
 #pragma unroll
-        for (int q = 0; q < kSweepBatch; ++q) {
-            const int i = min(i0 + q, N - 2);
-            yv[q] = yb[(long long)(i + 1) * sk];
-            const double *f = fac + (long long)W * i;
-            fl[q] = __ldg(f + 0);
-            fi[q] = __ldg(f + 1);
-            fa[q] = __ldg(f + 3);
-            fb[q] = __ldg(f + 4);
-            fh[q] = __ldg(f + 6);
-        }
+            for (int q = 0; q < kSweepBatch; ++q) {
+                const int i = min(i0 + q, e - 1);
+                yv[q] = yb[(long long)(i + 1) * sk];
+                const double *f = fac + (long long)W * i;
+                fl[q] = __ldg(f + 0);
+                fi[q] = __ldg(f + 1);
+                fa[q] = __ldg(f + 3);
+                fb[q] = __ldg(f + 4);
+                fh[q] = __ldg(f + 6);
+            }
 #pragma unroll
-        for (int q = 0; q < kSweepBatch; ++q) {
-            const int i = i0 + q;
-            if (i <= N - 2) {
-                const double del = (yv[q] - ym) * fh[q];
-                const double rp = (fa[q] * dprev + fb[q] * del - fl[q] * rprev) * fi[q];
-                o3[(long long)i * os_i] = rp;
-                if (i == N - 2) bE = e0 * dprev + e1 * del;
-                rprev = rp;
-                dprev = del;
-                ym = yv[q];
+            for (int q = 0; q < kSweepBatch; ++q) {
+                const int i = i0 + q;
+                if (i < e) {
+                    const double del = (yv[q] - ym) * fh[q];
+                    rho = (fa[q] * dprev + fb[q] * del - fl[q] * rho) * fi[q];
+                    if (live) o3[(long long)i * os_i] = rho;
+                    dprev = del;
+                    ym = yv[q];
+                }
             }
         }
     }
+    s_end[w][lane] = rho;
+    __syncthreads();
+    if (w == 0) {  // chain the forward carries: r' entering chunk q
+        double c = 0.0;
+        for (int q = 0; q < P; ++q) {
+            s_carry[q][lane] = c;
+            const int aq = 1 + q * L, eq = min(aq + L, N - 1);
+            if (aq < eq) c = s_end[q][lane] + __ldg(fac + (long long)W * (eq - 1) + 10) * c;
+        }
+    }
+    __syncthreads();
+    const double cf = s_carry[w][lane];
 
-    // backward: s_{N-2} = r'_{N-2}, s_{N-1} from the last row, then segments N-2 .. 0
-    double s_ip1 = rprev;
-    const double s_last = (bE - dE * s_ip1) / hA;
-    double yr = yb[(long long)(N - 1) * sk];
-    {
+    // pass 2: r' = rho + prod(A) cf, then the backward sweep from a zero carry
+    double sig = 0.0;
+    if (a < e) {
+        for (int i0 = e - 1; i0 >= a; i0 -= kSweepBatch) {
+            double rv[kSweepBatch], fp[kSweepBatch], fc[kSweepBatch];
+#pragma unroll
+            for (int q = 0; q < kSweepBatch; ++q) {
+                const int i = max(i0 - q, a);
+                rv[q] = o3[(long long)i * os_i];
+                fp[q] = __ldg(fac + (long long)W * i + 10);
+                fc[q] = __ldg(fac + (long long)W * i + 2);
+            }
+#pragma unroll
+            for (int q = 0; q < kSweepBatch; ++q) {
+                const int i = i0 - q;
+                if (i >= a) {
+                    const double r = fma(fp[q], cf, rv[q]);
+                    sig = r - fc[q] * sig;
+                    if (live) o3[(long long)i * os_i] = sig;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    s_end[w][lane] = sig;
+    __syncthreads();
+    if (w == 0) {  // chain the backward carries: s at the row after chunk q; s_1 last
+        double c = 0.0;
+        for (int q = P - 1; q >= 0; --q) {
+            s_carry[q][lane] = c;
+            const int aq = 1 + q * L, eq = min(aq + L, N - 1);
+            if (aq < eq) c = s_end[q][lane] + __ldg(fac + (long long)W * aq + 11) * c;
+        }
+        s_carry[P][lane] = c;
+    }
+    __syncthreads();
+    if (a >= e || !live) return;
+    const double cb = s_carry[w][lane];
+
+    // pass 3: slopes s_i = sig_i + prod(C) cb and the coefficients of segments
+    // [a, e) (fill_coefficients, interpolate.cu:29-43); the last chunk also the
+    // extrapolated last knot (fill_final_derivs, interpolate.cu:241-280), the
+    // first chunk segment 0 from the first not-a-knot row
+    double s_ip1, yr;
+    int top = e - 1;
+    if (e == N - 1) {
+        const double *bnd = fac + (long long)W * N;
+        const double e0 = __ldg(bnd + 4), e1 = __ldg(bnd + 5), dE = __ldg(bnd + 6), hA = __ldg(bnd + 7);
         const long long i = N - 2;
-        const double yl = yb[i * sk];
+        const double ya = yb[(i - 1) * sk], yl = yb[i * sk], yc = yb[(i + 1) * sk];
+        const double sN2 = fma(__ldg(fac + W * i + 11), cb, o3[i * os_i]);
+        const double dA = (yl - ya) * __ldg(fac + W * (i - 1) + 6);
         const double ih = __ldg(fac + W * i + 6), xx = __ldg(fac + W * i + 5);
-        const double dl = (yr - yl) * ih;
-        const double tt = (s_ip1 + s_last - 2 * dl) * ih;
-        const double c1 = s_ip1, c2 = (dl - s_ip1) * ih - tt, c3 = tt * ih;
+        const double dl = (yc - yl) * ih;
+        const double bE = e0 * dA + e1 * dl;
+        const double s_last = (bE - dE * sN2) / hA;
+        const double tt = (sN2 + s_last - 2 * dl) * ih;
+        const double c1 = sN2, c2 = (dl - sN2) * ih - tt, c3 = tt * ih;
         const long long off = i * os_i, offe = (long long)(N - 1) * os_i;
         o0[off] = yl;
         o1[off] = c1;
         o2[off] = c2;
         o3[off] = c3;
-        o0[offe] = yr;
+        o0[offe] = yc;
         o1[offe] = c1 + 2 * c2 * xx + 3 * c3 * xx * xx;
         o2[offe] = (2. * c2 + 6. * c3 * xx) / 2.;
         o3[offe] = c3;
+        s_ip1 = sN2;
         yr = yl;
+        top = N - 3;
+    } else {
+        s_ip1 = cb;
+        yr = yb[(long long)e * sk];
     }
-    for (int i0 = N - 3; i0 >= 1; i0 -= kSweepBatch) {
-        double yv[kSweepBatch], rv[kSweepBatch], fc[kSweepBatch], fh[kSweepBatch];
+    for (int i0 = top; i0 >= a; i0 -= kSweepBatch) {
+        double yv[kSweepBatch], rv[kSweepBatch], fq[kSweepBatch], fh[kSweepBatch];
 #pragma unroll
         for (int q = 0; q < kSweepBatch; ++q) {
-            const int i = max(i0 - q, 1);
+            const int i = max(i0 - q, a);
             yv[q] = yb[(long long)i * sk];
             rv[q] = o3[(long long)i * os_i];
-            fc[q] = __ldg(fac + (long long)W * i + 2);
+            fq[q] = __ldg(fac + (long long)W * i + 11);
             fh[q] = __ldg(fac + (long long)W * i + 6);
         }
 #pragma unroll
         for (int q = 0; q < kSweepBatch; ++q) {
             const int i = i0 - q;
-            if (i >= 1) {
+            if (i >= a) {
                 const long long off = (long long)i * os_i;
-                const double s_i = rv[q] - fc[q] * s_ip1;
+                const double s_i = fma(fq[q], cb, rv[q]);
                 const double dl = (yr - yv[q]) * fh[q];
                 const double tt = (s_i + s_ip1 - 2 * dl) * fh[q];
                 o0[off] = yv[q];
@@ -259,9 +333,14 @@ __global__ void __launch_bounds__(64) k_spline_build_factored(const double *__re
             }
         }
     }
-    const double s0 = (b0 - d0 * s_ip1) / h1;
-    {
+    if (w == 0) {
+        // s_0 from the first row: b0 = gamma0 delta_0 + gamma1 delta_1
+        const double *bnd = fac + (long long)W * N;
+        const double g0 = __ldg(bnd + 0), g1 = __ldg(bnd + 1), d0 = __ldg(bnd + 2), h1 = __ldg(bnd + 3);
+        const double y0 = yb[0], y1 = yr, y2 = yb[2 * sk];
         const double ih0 = __ldg(fac + 6);
+        const double del0 = (y1 - y0) * ih0, del1 = (y2 - y1) * __ldg(fac + W + 6);
+        const double s0 = (g0 * del0 + g1 * del1 - d0 * s_ip1) / h1;
         const double tt = (s0 + s_ip1 - 2 * del0) * ih0;
         o0[0] = y0;
         o1[0] = s0;
@@ -359,8 +438,7 @@ extern "C" int few_spline_build_factored(const double *fac, const double *y, lon
     if (y_split < 0 || y_split > ninterps) return few::fail(FEW_ERR_ARG, "few_spline_build_factored: bad y_split");
     const long long os_i = layout == FEW_LAYOUT_KNOT_MAJOR ? ninterps : 1;
     const long long os_p = layout == FEW_LAYOUT_KNOT_MAJOR ? 1 : length;
-    const int threads = 64;
-    few::k_spline_build_factored<<<(ninterps + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(
+    few::k_spline_build_factored<<<(ninterps + 31) / 32, 32 * few::kScanChunks, 0, (cudaStream_t)stream>>>(
         fac, y, y_knot_stride, y_interp_stride, y_split, y_split_offset, ninterps, length, coeffs, os_i, os_p);
     FEW_LAUNCH_CHECK("k_spline_build_factored");
     return FEW_OK;

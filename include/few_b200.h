@@ -148,7 +148,7 @@ FEW_API int few_spline_build(const double *t, long long t_row_stride, const doub
                      int length, double *coeffs, int layout, void *stream);
 
 /* Width of a row of few_spline_factor's table. */
-#define FEW_FAC_WIDTH 12
+#define FEW_FAC_WIDTH 16
 
 /* Host factorization of the not-a-knot system (and of its transpose) for knots
  * t [host] (N,), shared by every series on those knots: fac [host]
