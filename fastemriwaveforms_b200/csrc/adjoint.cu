@@ -492,17 +492,39 @@ __global__ void __launch_bounds__(128) k_spline_adjoint(SplineAdjArgs a)
 }
 
 // k_spline_adjoint for knots shared by every series, from the host
-// factorization (few_spline_factor, columns 5-9 and the boundary row); loads
-// batched ahead of the two recurrences as in k_spline_build_factored.
+// factorization (few_spline_factor, columns 5-9 and 12-13 and the boundary
+// row); loads batched ahead of the recurrences as in k_spline_build_factored.
 constexpr int kAdjBatch = 8;
 
-__global__ void __launch_bounds__(64) k_spline_adjoint_factored(const double *__restrict__ fac, double *__restrict__ gc,
-                                                              double *__restrict__ gy, long long sk, long long sp,
-                                                              int split, long long off2, int ni, int N, int accumulate)
+// Transpose of the shared-knot build, in scan form (the sweeps of the
+// transposed interior block are linear recurrences with knot-only factors, as
+// in k_spline_build_factored): rows 1..N-2 are cut into kScanChunks chunks,
+// one warp each, lane = series (32 per CTA).
+//   pass 1  dL/d slopes (gs) and dL/d delta (direct part, parked in g3), and the
+//           forward sweep of A~^T from a zero carry (parked in g2); row 0 and
+//           the extrapolated last knot's gradient are folded in as in the
+//           sequential form; the neighbour row each chunk reads (the previous
+//           segment's contribution to gs) is loaded before any warp writes;
+//   carry   chained through shared memory with the chunk products (table
+//           columns 12 and 13);
+//   pass 2  corrected forward values and the back substitution from a zero
+//           carry (parked in g2);
+//   pass 3  w = corrected back substitution, dL/d delta and dL/dy for the
+//           chunk's knots; the two rows past the chunk end come from the next
+//           chunks' parked values and carries.
+__global__ void __launch_bounds__(32 * kScanChunks) k_spline_adjoint_factored(
+    const double *__restrict__ fac, double *__restrict__ gc, double *__restrict__ gy, long long sk, long long sp,
+    int split, long long off2, int ni, int N, int accumulate)
 {
     constexpr int W = kFacWidth;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= ni) return;
+    constexpr int P = kScanChunks;
+    __shared__ double s_end[P][32];
+    __shared__ double s_carry[P + 1][32];
+    __shared__ double s_w0[32], s_wE[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int p0 = blockIdx.x * 32 + lane;
+    const bool live = p0 < ni;
+    const int p = live ? p0 : ni - 1;  // idle lanes compute on a valid series and store nothing
     double *gyb = (p < split) ? gy + (long long)p * sp : gy + off2 + (long long)(p - split) * sp;
     const long long nil = ni, plane = (long long)N * ni;
     double *g0 = gc + p;
@@ -512,109 +534,195 @@ __global__ void __launch_bounds__(64) k_spline_adjoint_factored(const double *__
     const double *bnd = fac + (long long)W * N;
     const double gam0 = __ldg(bnd + 0), gam1 = __ldg(bnd + 1), d0 = __ldg(bnd + 2), h1 = __ldg(bnd + 3);
     const double e0 = __ldg(bnd + 4), e1 = __ldg(bnd + 5), dE = __ldg(bnd + 6), hA = __ldg(bnd + 7);
-    const long long oE = (long long)(N - 1) * nil;
-    const double gE1 = g1[oE], gE2 = g2[oE], gE3 = g3[oE];
+    const int L = (N - 2 + P - 1) / P;
+    const int a = 1 + w * L, e = min(a + L, N - 1);  // rows [a, e)
+    auto fa = [&](long long i, int col) { return __ldg(fac + (long long)W * i + col); };
 
-    // Pass F: dL/ds and the forward sweep of the transposed interior block
-    double carry = 0.0, w0 = 0.0, wE = 0.0, rprev = 0.0;
-    for (int i0 = 0; i0 <= N - 2; i0 += kAdjBatch) {
-        double v1[kAdjBatch], v2[kAdjBatch], v3[kAdjBatch], fh[kAdjBatch], fih[kAdjBatch], flt[kAdjBatch],
-            fidt[kAdjBatch];
-#pragma unroll
-        for (int q = 0; q < kAdjBatch; ++q) {
-            const int i = min(i0 + q, N - 2);
-            const long long o = (long long)i * nil;
-            v1[q] = g1[o];
-            v2[q] = g2[o];
-            v3[q] = g3[o];
-            const double *f = fac + (long long)W * i;
-            fh[q] = __ldg(f + 5);
-            fih[q] = __ldg(f + 6);
-            flt[q] = __ldg(f + 7);
-            fidt[q] = __ldg(f + 8);
+    // neighbour row a-1 (its gtt feeds gs_a); row 0 also gives w0 and its direct term
+    double carry = 0.0, w0 = 0.0, vd0 = 0.0;
+    if (a < e) {
+        const long long o = (long long)(a - 1) * nil;
+        const double a1 = g1[o], a2 = g2[o], a3 = g3[o];
+        const double ih = fa(a - 1, 6);
+        const double gtt = -a2 + a3 * ih;
+        carry = gtt * ih;
+        if (a == 1) {
+            w0 = (a1 - a2 * ih + gtt * ih) / h1;  // gs_0 has no previous segment
+            vd0 = a2 * ih - 2.0 * gtt * ih;
         }
+    }
+    __syncthreads();
+    if (w == 0) {
+        s_w0[lane] = w0;
+        if (live) g3[0] = vd0;
+    }
+
+    // pass 1
+    double rho = 0.0, wE = 0.0;
+    if (a < e) {
+        const long long oE = (long long)(N - 1) * nil;
+        for (int i0 = a; i0 < e; i0 += kAdjBatch) {
+            double v1[kAdjBatch], v2[kAdjBatch], v3[kAdjBatch], fh[kAdjBatch], fih[kAdjBatch], flt[kAdjBatch],
+                fidt[kAdjBatch];
 #pragma unroll
-        for (int q = 0; q < kAdjBatch; ++q) {
-            const int i = i0 + q;
-            if (i <= N - 2) {
+            for (int q = 0; q < kAdjBatch; ++q) {
+                const int i = min(i0 + q, e - 1);
                 const long long o = (long long)i * nil;
-                double a1 = v1[q], a2 = v2[q], a3 = v3[q];
-                const double h = fh[q], ih = fih[q];
-                if (i == N - 2) {
-                    a1 += gE1;
-                    a2 += 2 * h * gE1 + gE2;
-                    a3 += 3 * h * h * gE1 + 3 * h * gE2 + gE3;
-                }
-                const double gtt = -a2 + a3 * ih;
-                const double gs = carry + a1 - a2 * ih + gtt * ih;
-                carry = gtt * ih;
-                g3[o] = a2 * ih - 2.0 * gtt * ih;  // direct dL/d delta_i
-                if (i == 0) {
-                    w0 = gs / h1;
-                } else {
-                    double rhs = gs;
+                v1[q] = g1[o];
+                v2[q] = g2[o];
+                v3[q] = g3[o];
+                fh[q] = fa(i, 5);
+                fih[q] = fa(i, 6);
+                flt[q] = fa(i, 7);
+                fidt[q] = fa(i, 8);
+            }
+#pragma unroll
+            for (int q = 0; q < kAdjBatch; ++q) {
+                const int i = i0 + q;
+                if (i < e) {
+                    const long long o = (long long)i * nil;
+                    double a1 = v1[q], a2 = v2[q], a3 = v3[q];
+                    const double h = fh[q], ih = fih[q];
+                    if (i == N - 2) {  // the extrapolated last knot depends on segment N-2
+                        const double gE1 = g1[oE], gE2 = g2[oE], gE3 = g3[oE];
+                        a1 += gE1;
+                        a2 += 2 * h * gE1 + gE2;
+                        a3 += 3 * h * h * gE1 + 3 * h * gE2 + gE3;
+                    }
+                    const double gtt = -a2 + a3 * ih;
+                    double rhs = carry + a1 - a2 * ih + gtt * ih;
+                    carry = gtt * ih;
+                    if (live) g3[o] = a2 * ih - 2.0 * gtt * ih;  // direct dL/d delta_i
                     if (i == 1) rhs -= d0 * w0;
                     if (i == N - 2) {
                         wE = carry / hA;
                         rhs -= dE * wE;
                     }
-                    const double rp = (rhs - flt[q] * rprev) * fidt[q];
-                    g2[o] = rp;
-                    rprev = rp;
+                    rho = (rhs - flt[q] * rho) * fidt[q];
+                    if (live) g2[o] = rho;
                 }
             }
         }
     }
+    s_end[w][lane] = rho;
+    if (e == N - 1) s_wE[lane] = wE;
+    __syncthreads();
+    if (w == 0) {
+        double c = 0.0;
+        for (int q = 0; q < P; ++q) {
+            s_carry[q][lane] = c;
+            const int aq = 1 + q * L, eq = min(aq + L, N - 1);
+            if (aq < eq) c = s_end[q][lane] + fa(eq - 1, 12) * c;
+        }
+    }
+    __syncthreads();
+    const double cf = s_carry[w][lane];
 
-    // Pass B: back substitution, dL/d delta, dL/dy
-    const double w_last = rprev;
-    const double zE = wE - w_last;
+    // pass 2
+    double sig = 0.0;
+    if (a < e) {
+        for (int i0 = e - 1; i0 >= a; i0 -= kAdjBatch) {
+            double rv[kAdjBatch], fp[kAdjBatch], fct[kAdjBatch];
+#pragma unroll
+            for (int q = 0; q < kAdjBatch; ++q) {
+                const int i = max(i0 - q, a);
+                rv[q] = g2[(long long)i * nil];
+                fp[q] = fa(i, 12);
+                fct[q] = fa(i, 9);
+            }
+#pragma unroll
+            for (int q = 0; q < kAdjBatch; ++q) {
+                const int i = i0 - q;
+                if (i >= a) {
+                    const double r = fma(fp[q], cf, rv[q]);
+                    sig = r - fct[q] * sig;
+                    if (live) g2[(long long)i * nil] = sig;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    s_end[w][lane] = sig;
+    __syncthreads();
+    if (w == 0) {
+        double c = 0.0;
+        for (int q = P - 1; q >= 0; --q) {
+            s_carry[q][lane] = c;
+            const int aq = 1 + q * L, eq = min(aq + L, N - 1);
+            if (aq < eq) c = s_end[q][lane] + fa(aq, 13) * c;
+        }
+        s_carry[P][lane] = c;
+    }
+    __syncthreads();
+    if (a >= e || !live) return;
+
+    // pass 3
+    const double w0v = s_w0[lane];
+    const double w_last = g2[(long long)(N - 2) * nil];  // the last row's product factor is 0
+    const double zE = s_wE[lane] - w_last;
     const double rE_a = zE * e0, rE_b = zE * e1;
-    double w_ip1 = 0.0, gdel_ip1 = 0.0, pend = 0.0;
+    auto w_at = [&](int j) {  // w_j for any interior row j
+        const int cj = (j - 1) / L;
+        return fma(fa(j, 13), s_carry[cj][lane], g2[(long long)j * nil]);
+    };
+    auto gdel_at = [&](int j, double wj, double wj1) {  // dL/d delta_j given w_j, w_{j+1}
+        double gd = g3[(long long)j * nil] + 3.0 * fa(j - 1, 5) * wj;
+        if (j + 1 <= N - 2) gd += 3.0 * fa(j + 1, 5) * wj1;
+        if (j == N - 2) gd += rE_b;
+        if (j == N - 3) gd += rE_a;
+        if (j == 1) gd += (w0v - wj) * gam1;
+        return gd;
+    };
     auto put = [&](long long knot, double v) {
         double *dst = gyb + knot * sk;
         *dst = accumulate ? *dst + v : v;
     };
-    for (int i0 = N - 2; i0 >= 1; i0 -= kAdjBatch) {
-        double vr[kAdjBatch], vd[kAdjBatch], vn[kAdjBatch], fct[kAdjBatch], fhl[kAdjBatch], fhr[kAdjBatch],
-            fihr[kAdjBatch], fihn[kAdjBatch];
+    const double cb = s_carry[w][lane];
+    double w_ip1 = 0.0, gdel_ip1 = 0.0;
+    if (e <= N - 2) {
+        w_ip1 = cb;  // w at row e
+        const double w_e1 = (e + 1 <= N - 2) ? w_at(e + 1) : 0.0;
+        gdel_ip1 = gdel_at(e, w_ip1, w_e1);
+    }
+    for (int i0 = e - 1; i0 >= a; i0 -= kAdjBatch) {
+        double vs[kAdjBatch], vd[kAdjBatch], vn[kAdjBatch], fq[kAdjBatch], fhl[kAdjBatch], fhr[kAdjBatch],
+            fih[kAdjBatch];
 #pragma unroll
         for (int q = 0; q < kAdjBatch; ++q) {
-            const int i = max(i0 - q, 1);
+            const int i = max(i0 - q, a);
             const long long o = (long long)i * nil;
-            vr[q] = g2[o];
+            vs[q] = g2[o];
             vd[q] = g3[o];
             vn[q] = g0[o + nil];
-            fct[q] = __ldg(fac + (long long)W * i + 9);
-            fhl[q] = __ldg(fac + (long long)W * (i - 1) + 5);
-            fhr[q] = __ldg(fac + (long long)W * i + 5);
-            fihr[q] = __ldg(fac + (long long)W * i + 6);
-            fihn[q] = __ldg(fac + (long long)W * (i + 1) + 6);
+            fq[q] = fa(i, 13);
+            fhl[q] = fa(i - 1, 5);
+            fhr[q] = fa(i + 1, 5);
+            fih[q] = fa(i, 6);
         }
 #pragma unroll
         for (int q = 0; q < kAdjBatch; ++q) {
             const int i = i0 - q;
-            if (i >= 1) {
-                const double w_i = (i == N - 2) ? w_last : (vr[q] - fct[q] * w_ip1);
-                double gdel_i = vd[q] + 3.0 * fhl[q] * w_i + pend;
+            if (i >= a) {
+                const double w_i = fma(fq[q], cb, vs[q]);
+                double gdel_i = vd[q] + 3.0 * fhl[q] * w_i;
+                if (i + 1 <= N - 2) gdel_i += 3.0 * fhr[q] * w_ip1;
                 if (i == N - 2) gdel_i += rE_b;
                 if (i == N - 3) gdel_i += rE_a;
-                if (i == 1) gdel_i += (w0 - w_i) * gam1;
-                double gy_ip1 = vn[q] + gdel_i * fihr[q];
-                if (i + 1 <= N - 2) gy_ip1 -= gdel_ip1 * fihn[q];
+                if (i == 1) gdel_i += (w0v - w_i) * gam1;
+                double gy_ip1 = vn[q] + gdel_i * fih[q];
+                if (i + 1 <= N - 2) gy_ip1 -= gdel_ip1 * fa(i + 1, 6);
                 put(i + 1, gy_ip1);
-                pend = 3.0 * fhr[q] * w_i;
-                gdel_ip1 = gdel_i;
                 w_ip1 = w_i;
-                if (i == 1) {
-                    const double z0 = w0 - w_i;
-                    const double ih0 = __ldg(fac + 6);
-                    const double gdel0 = g3[0] + pend + z0 * gam0;
-                    put(1, g0[nil] + gdel0 * ih0 - gdel_i * fihr[q]);
-                    put(0, g0[0] - gdel0 * ih0);
-                }
+                gdel_ip1 = gdel_i;
             }
         }
+    }
+    if (w == 0) {
+        // knots 1 and 0 from row 0 (after the loop: w_ip1 = w_1, gdel_ip1 = gdel_1)
+        const double ih0 = fa(0, 6);
+        const double gdel0 = g3[0] + 3.0 * fa(1, 5) * w_ip1 + (w0v - w_ip1) * gam0;
+        put(1, g0[nil] + gdel0 * ih0 - gdel_ip1 * fa(1, 6));
+        put(0, g0[0] - gdel0 * ih0);
     }
 }
 
@@ -623,9 +731,8 @@ __global__ void __launch_bounds__(64) k_spline_adjoint_factored(const double *__
 int launch_spline_adjoint_factored(const double *fac, double *gc, double *gy, long long sk, long long sp, int split,
                                    long long off2, int ni, int N, int accumulate, cudaStream_t st)
 {
-    const int threads = 64;
-    k_spline_adjoint_factored<<<(ni + threads - 1) / threads, threads, 0, st>>>(fac, gc, gy, sk, sp, split, off2, ni,
-                                                                               N, accumulate);
+    k_spline_adjoint_factored<<<(ni + 31) / 32, 32 * kScanChunks, 0, st>>>(fac, gc, gy, sk, sp, split, off2, ni, N,
+                                                                          accumulate);
     FEW_LAUNCH_CHECK("k_spline_adjoint_factored");
     return FEW_OK;
 }
