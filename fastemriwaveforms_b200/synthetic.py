@@ -276,3 +276,28 @@ def small_case(K: int = 10, N: int = 20, out_len: int = 4000, seed: int = 7, dt:
     return ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
                          phase_coeffs=phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=T,
                          name="small", seed=seed)
+
+
+def many_rows_case(seed: int = 9, N: int = 30, out_len: int = 20000, mmax: int = 10, kmax: int = 1,
+                   nmax: int = 5, dt: float = 10.0) -> ModeSumInputs:
+    """Every (m, k) with m in 0..mmax and |k| <= kmax, n in -nmax..nmax (l = max(2, m)):
+    (2 mmax + 1) (2 kmax + 1) fold rows (63 by default, more than 32, so the
+    tensor-core forms use two MMA column groups); phases as ``small_case``."""
+    base = small_case(K=4, N=N, out_len=out_len, seed=seed, dt=dt, theta=True)
+    rng = np.random.default_rng(seed + 1)
+    modes = [(max(2, m), m, k, n) for m in range(mmax + 1) for k in range(-kmax, kmax + 1)
+             for n in range(-nmax, nmax + 1)]
+    l = np.array([q[0] for q in modes], np.int32)
+    m = np.array([q[1] for q in modes], np.int32)
+    k = np.array([q[2] for q in modes], np.int32)
+    n = np.array([q[3] for q in modes], np.int32)
+    K = len(modes)
+    t = base.t
+    frac = (t / t[-1])[:, None]
+    lo = rng.uniform(-1, 1, (2, K))
+    hi = rng.uniform(-1, 1, (2, K))
+    teuk = (lo[0] + (hi[0] - lo[0]) * frac) + 1j * (lo[1] + (hi[1] - lo[1]) * frac)
+    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    return ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
+                         phase_coeffs=base.phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=base.T,
+                         name="many_rows", seed=seed)

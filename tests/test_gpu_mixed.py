@@ -24,7 +24,7 @@ def run(inp, precision):
     return wf.cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["theta", "m0", "plain_small", "plain_full"])
+@pytest.mark.parametrize("case", ["theta", "m0", "plain_small", "plain_full", "many_rows"])
 def test_mixed_matches_fp64(cuda, case):
     if case == "theta":
         inp, _ = load_case("sum_small_theta.npz")
@@ -32,6 +32,8 @@ def test_mixed_matches_fp64(cuda, case):
         inp, _ = load_case("sum_small_m0.npz")
     elif case == "plain_small":
         inp = S.plain_small()
+    elif case == "many_rows":
+        inp = S.many_rows_case()  # 63 (m', k') rows: two MMA column groups
     else:
         inp = S.plain_full()
     ref = run(inp, "exact")
@@ -49,3 +51,11 @@ def test_mixed_deterministic(cuda):
     a = run(inp, "mixed")
     b = run(inp, "mixed")
     assert np.array_equal(a, b)
+
+
+def test_mixed_row_limit(cuda):
+    """More than 64 (m', k') rows: the mixed form refuses (the FP64 forms do not)."""
+    inp = S.many_rows_case(mmax=12)  # 75 rows
+    with pytest.raises(ValueError):
+        run(inp, "mixed")
+    assert np.isfinite(run(inp, "exact")).all()

@@ -50,6 +50,7 @@ CASES = {
     "plain_small": lambda: S.plain_small(seed=1),
     "plain_full": lambda: S.plain_full(seed=2),
     "small_theta": lambda: S.small_case(K=40, N=30, out_len=20000, seed=5, theta=True),
+    "many_rows": lambda: S.many_rows_case(),  # 63 rows: two MMA column groups in the phase adjoint
 }
 
 
