@@ -77,6 +77,45 @@ def _upload(a: np.ndarray, device) -> torch.Tensor:
     return t.pin_memory().to(device, non_blocking=True)
 
 
+_COPY_STREAMS: dict = {}
+
+
+def _copy_stream(device) -> torch.cuda.Stream:
+    d = torch.device(device)
+    key = d.index if d.index is not None else torch.cuda.current_device()
+    if key not in _COPY_STREAMS:
+        _COPY_STREAMS[key] = torch.cuda.Stream(torch.device("cuda", key))
+    return _COPY_STREAMS[key]
+
+
+def _input(x, dtype, device) -> torch.Tensor:
+    """A user input on the device.  Device tensors (and host tensors that
+    require grad) go through torch's ``.to``; host data is copied on a separate
+    copy stream, so the copy does not queue behind kernels already on the
+    caller's stream (the next call's inputs arrive while the previous call's
+    kernels run).  The caller's stream waits for the copy, and the call returns
+    only once the copy has read the caller's buffer, as a blocking copy would."""
+    if isinstance(x, torch.Tensor) and (x.is_cuda or x.requires_grad or torch.device(device).type != "cuda"):
+        return x.to(device=device, dtype=dtype).contiguous()
+    if isinstance(x, torch.Tensor):
+        src = x.detach().to(dtype).contiguous()
+    else:
+        a = np.asarray(x)
+        a = a.astype(np.complex128 if dtype.is_complex else np.float64, copy=False)
+        src = torch.from_numpy(np.ascontiguousarray(a))
+    pinned = src if src.is_pinned() else src.pin_memory()
+    cs = _copy_stream(device)
+    with torch.cuda.stream(cs):
+        dst = torch.empty(pinned.shape, dtype=pinned.dtype, device=device)
+        dst.copy_(pinned, non_blocking=True)
+    main = torch.cuda.current_stream(device)
+    main.wait_stream(cs)
+    dst.record_stream(main)
+    if pinned is src and (isinstance(x, torch.Tensor) and pinned.data_ptr() == x.data_ptr()):
+        cs.synchronize()  # the copy reads the caller's own pinned buffer
+    return dst
+
+
 def _to_host(x, dtype) -> np.ndarray:
     if isinstance(x, torch.Tensor):
         x = x.detach().cpu().numpy()
@@ -446,8 +485,7 @@ class InterpolatedModeSum(SummationBase):
             raise ValueError("t must increase strictly.")
         if len(phase_t) != N:
             raise ValueError("phase_interp_t must have the same length as t.")
-        teuk_in = teuk_modes.to(device=dev, dtype=torch.complex128) if isinstance(teuk_modes, torch.Tensor) \
-            else _to_device(teuk_modes, torch.complex128, dev)
+        teuk_in = _input(teuk_modes, torch.complex128, dev)
         teuk = teuk_in.detach().contiguous()
         if teuk.ndim != 2 or teuk.shape[0] != N:
             raise ValueError("teuk_modes must have shape (len(t), num_teuk_modes).")
@@ -467,15 +505,14 @@ class InterpolatedModeSum(SummationBase):
             offset = h_t[-1] - int(h_t[-1] / dt) * dt
             h_t = h_t - offset
             phase_t = phase_t - offset
-        pc_in = phase_interp_coeffs.to(device=dev, dtype=torch.float64) \
-            if isinstance(phase_interp_coeffs, torch.Tensor) else _to_device(phase_interp_coeffs, torch.float64, dev)
+        pc_in = _input(phase_interp_coeffs, torch.float64, dev)
         p.dev, p.st, p.N, p.K, p.dt = dev, _stream(dev), N, K, float(dt)
         p.teuk, p.teuk_in, p.pc_in = teuk, (teuk_in if keep else None), (pc_in if keep else None)
         p.t_dev = _upload(h_t, dev)
         p.fac = spline_factor_table(h_t, dev)
         # ylms[K:] *= (-1)^l (interpolatedmodesum.py:357-358)
         sign = np.where(l_h % 2 == 0, 1.0, -1.0)
-        ylm = _to_device(ylms, torch.complex128, dev).clone()
+        ylm = _input(ylms, torch.complex128, dev).clone()
         ylm[K:] *= _upload(sign, dev)
         p.ylm = ylm
         # (N-1, 3, 8) -> (8, N-1, 3) (interpolatedmodesum.py:352-354)
