@@ -628,8 +628,13 @@ def main():
     sum_flops = float(keys) * T * flops_per_key_sample
     achieved = sum_flops / (stage["sum"] * 1e-3) / 1e12
     spline_bytes = 40.0 * inp.num_knots * 2 * K
+    # DRAM bytes of one launch at this workload from an ncu capture (dram__bytes_read.sum +
+    # dram__bytes_write.sum), summarised in profiles/; null for workloads not captured
+    captured = args.workload == "plain_full" and args.precision == "faithful"
+    traffic = {"bytes_per_launch": 161.1e6, "source": "profiles/k_sum_folded_plain_full_faithful.md",
+               "algorithmic_bytes": float(keys) * 64.0 * seg.nseg + 2.0 * 16.0 * T} if captured else None
     roofline = {"bound": "fp64", "kernel": "k_sum_folded", "achieved": achieved, "peak": fp64_tflops,
-                "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": traffic,
                 "peak_source": "measured in this run: few_probe_fp64_fma (FP64 FMA pipe)",
                 "algorithmic": f"{flops_per_key_sample} flop x {keys} keys x {T} samples per launch",
                 "launch_ms": stage["sum"]}
@@ -637,6 +642,8 @@ def main():
                    "peak": pk["hbm_gbs"], "unit": "GB/s",
                    "frac": spline_bytes / (stage["spline"] * 1e-3) / 1e9 / pk["hbm_gbs"],
                    "peak_source": f"{pk_kind} hbm_gbs", "algorithmic": "40 B per (knot, series)",
+                   "traffic": ({"bytes_per_launch": 466.7e6, "source": "profiles/k_spline_build_factored_plain_full.md"}
+                               if args.workload == "plain_full" else None),
                    "launch_ms": stage["spline"]}
 
     if rank != 0:
