@@ -443,6 +443,64 @@ def bench_batched(count: int, dev, steps: int):
     return out
 
 
+def bench_amplitude(dev, steps: int, pk, pk_kind, cpu: bool):
+    """Amplitude grids (AmpInterp2D): 3843 modes x (real, imaginary) bicubic
+    grids of 40 x 40 knots evaluated at 1000 trajectory points into the mode
+    sum's (points, modes) layout; device time of few_amp_interp2d with inputs in
+    HBM, HBM roofline on the algorithmic bytes (every coefficient read once,
+    the output written once), and the reference's CPU interp2D on a sample."""
+    import time
+
+    import torch
+
+    from fastemriwaveforms_b200 import _lib
+    from fastemriwaveforms_b200 import synthetic as S
+    from fastemriwaveforms_b200.summation import _ptr, _stream
+
+    K, N, nw = 3843, 1000, 40
+    tw, tu, coeff = S.amplitude_grids(K, nw=nw, nu=nw)
+    w, u = S.amplitude_points(N)
+    d = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
+         for k, v in (("tw", tw), ("tu", tu), ("c", coeff), ("w", w), ("u", u))}
+    out = torch.empty((N, K), dtype=torch.complex128, device=dev)
+    nc = coeff.shape[2]
+
+    def run():
+        _lib.call("few_amp_interp2d", _ptr(out), _ptr(d["tw"]), nw, _ptr(d["tu"]), nw, _ptr(d["c"]), 3, 3,
+                  _ptr(d["w"]), _ptr(d["u"]), N, None, K, nc, _stream(dev))
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(max(steps, 5)):
+        run()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / max(steps, 5)
+    nbytes = coeff.nbytes + out.numel() * 16
+    entry = {"workload": f"{K} modes x 2 grids of {nw} x {nw} knots (bicubic), {N} points", "ms": ms,
+             "value": K * N / (ms * 1e-3), "unit": "mode-points/s",
+             "roofline": {"bound": "hbm", "kernel": "k_amp_interp2d", "achieved": nbytes / (ms * 1e-3) / 1e9,
+                          "peak": pk["hbm_gbs"], "unit": "GB/s",
+                          "frac": nbytes / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], "peak_source": f"{pk_kind} hbm_gbs",
+                          "algorithmic": "coefficients read once + output written once"}}
+    if cpu:
+        from oracle import oracle as O
+
+        if O.have_ref():
+            Ks = K  # every mode at every point (about a second on one core)
+            cs = np.ascontiguousarray(coeff[:Ks].reshape(2 * Ks, -1))
+            t0 = time.perf_counter()
+            O.interp2d(tw, tu, cs, 3, 3, w, u, impl="ref")
+            dt = time.perf_counter() - t0
+            entry["cpu_baseline"] = {"value": Ks * N / dt, "unit": "mode-points/s", "cores": 1, "kind": "reference",
+                                     "sample": f"{Ks} modes x {N} points ({dt:.2f} s)"}
+    return entry
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -621,6 +679,7 @@ def main():
         fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1, backward=bwd)[0]}
 
     batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
+    amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
 
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
@@ -657,7 +716,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "cpu_baseline": cpu, "clocks": clk,
+            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "cpu_baseline": cpu, "clocks": clk,
             "device": torch.cuda.get_device_name(dev)}
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -4,7 +4,8 @@ Drop-in for ``few.summation.interpolatedmodesum.InterpolatedModeSum`` and its
 ``CubicSplineInterpolant``: Python host code over hand-written sm_100a CUDA
 kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
 """
+from .amplitude import AmpInterp2D
 from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBase
 from .utility import get_mismatch, get_overlap
 
-__all__ = ["CubicSplineInterpolant", "InterpolatedModeSum", "SummationBase", "get_mismatch", "get_overlap"]
+__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "InterpolatedModeSum", "SummationBase", "get_mismatch", "get_overlap"]

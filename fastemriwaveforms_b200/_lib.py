@@ -63,6 +63,9 @@ SIGNATURES = {
     "few_fold_mixed_adjoint": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
     "few_adjoint_phase_mixed": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl,
                                 _c_int, _vp, _vp, _vp],
+    "few_interp2d": [_vp, _vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _vp],
+    "few_amp_interp2d": [_vp, _vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_int,
+                         _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
 }

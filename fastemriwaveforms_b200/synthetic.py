@@ -301,3 +301,24 @@ def many_rows_case(seed: int = 9, N: int = 30, out_len: int = 20000, mmax: int =
     return ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
                          phase_coeffs=base.phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=base.T,
                          name="many_rows", seed=seed)
+
+
+def amplitude_grids(num_modes: int, nw: int = 40, nu: int = 40, seed: int = 11, degree: int = 3):
+    """Seeded B-spline amplitude grids in the shape the reference's data files
+    hold: clamped knots on w in [0, 1] and u in [0, 1] (end knots repeated
+    degree + 1 times, interior knots uniform), coefficients (num_modes, 2,
+    (nw - degree - 1)(nu - degree - 1)) decaying with the mode index."""
+    rng = np.random.default_rng(seed)
+    k1 = degree + 1
+    tw = np.concatenate([np.zeros(k1), np.linspace(0, 1, nw - 2 * k1 + 2)[1:-1], np.ones(k1)])
+    tu = np.concatenate([np.zeros(k1), np.linspace(0, 1, nu - 2 * k1 + 2)[1:-1], np.ones(k1)])
+    nc = (nw - k1) * (nu - k1)
+    scale = 1.0 / (1.0 + np.arange(num_modes))[:, None, None]
+    coeff = rng.standard_normal((num_modes, 2, nc)) * scale
+    return tw, tu, coeff
+
+
+def amplitude_points(N: int, seed: int = 12):
+    """A smooth trajectory in (w, u) through the grid's domain, N points."""
+    s = np.linspace(0.0, 1.0, N)
+    return 0.05 + 0.9 * s ** 1.5, 0.5 + 0.4 * np.sin(2.0 * np.pi * s) * (1.0 - s)

@@ -354,6 +354,30 @@ FEW_API int few_spline_adjoint_factored(const double *fac, double *gcoeffs, doub
                                         int ninterps, int length, int accumulate, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Amplitudes: tensor-product B-spline grids (the producer of teuk_modes)    */
+/* ------------------------------------------------------------------------ */
+
+/* Drop-in for interp2D_wrap (src/few/cutils/AmpInterp2D.hh:6-8, kernel
+ * AmpInterp2D.cu:86-208): z [device] (num_indiv_c, mx) = each coefficient grid
+ * c [device] (num_indiv_c, len_indiv_c) evaluated at the points (x[i], y[i])
+ * [device] (mx,) as a B-spline of degrees kx, ky (1..5) with knots tx [device]
+ * (nx,), ty [device] (ny,); len_indiv_c = (nx-kx-1)(ny-ky-1); points outside
+ * the knots are clamped as FITPACK does.  mx must equal my.  The values equal
+ * the reference's CPU path bit for bit. */
+FEW_API int few_interp2d(double *z, const double *tx, int nx, const double *ty, int ny, const double *c, int kx,
+                         int ky, const double *x, int mx, const double *y, int my, int num_indiv_c, int len_indiv_c,
+                         void *stream);
+
+/* The amplitudes directly in the mode sum's layout (what AmpInterp2D.__call__,
+ * src/few/amplitude/ampinterp2d.py:127-189, assembles on the host): out
+ * [device] (m, nmodes) complex128, out[i][j] = grid 2 mode_j + i grid 2 mode_j + 1
+ * at (x[i], y[i]), with c [device] (num_teuk_modes, 2, len_indiv_c) and
+ * mode_j = mode_idx[j] [device] (nmodes,), or j when mode_idx is null. */
+FEW_API int few_amp_interp2d(void *out, const double *tx, int nx, const double *ty, int ny, const double *c, int kx,
+                             int ky, const double *x, const double *y, int m, const int *mode_idx, int nmodes,
+                             int len_indiv_c, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */
 

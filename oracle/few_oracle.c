@@ -330,3 +330,64 @@ int oracle_get_waveform(double *wf, const double *interp_array, const double *ph
     free(start);
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Amplitude grids: tensor-product B-spline evaluation                       */
+/* ------------------------------------------------------------------------- */
+
+/* The k+1 non-zero B-splines of degree k at x, for t[l-1] <= x < t[l]: the
+ * de Boor-Cox recurrence as FITPACK's fpbspl states it (Dierckx), the form
+ * AmpInterp2D.cu:20-44 restates; each operation rounded separately. */
+static void oracle_bspl(const double *t, int k, double x, int l, double *h)
+{
+    double hh[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    h[0] = 1.0;
+    for (int j = 1; j <= k; ++j) {
+        for (int i = 0; i < k; ++i) hh[i] = h[i];
+        h[0] = 0.0;
+        for (int i = 0; i < j; ++i) {
+            const int li = l + i, lj = li - j;
+            const double f = hh[i] / (t[li] - t[lj]);
+            h[i] = h[i] + f * (t[li] - x);
+            h[i + 1] = f * (x - t[lj]);
+        }
+    }
+}
+
+/* Interval of x (clamped to [t[k], t[n-k-1]]): the first l >= k+1 with
+ * x < t[l], at most n-k-1 (FITPACK fpbisp's search, AmpInterp2D.cu:68-79);
+ * fills the basis and returns l - (k+1). */
+static int oracle_basis(const double *t, int n, int k, double x, double *h)
+{
+    const int k1 = k + 1, nk1 = n - k1;
+    double arg = x;
+    if (arg < t[k1 - 1]) arg = t[k1 - 1];
+    if (arg > t[nk1]) arg = t[nk1];
+    int l = k1;
+    while (!(arg < t[l] || l == nk1)) ++l;
+    oracle_bspl(t, k, arg, l, h);
+    return l - k1;
+}
+
+/* interp2D (AmpInterp2D.cu:86-176), CPU branch: z[g * m + i] = grid g at
+ * (x[i], y[i]), summed over the (kx+1)(ky+1) coefficients in FITPACK's order. */
+void oracle_interp2d(double *z, const double *tx, int nx, const double *ty, int ny, const double *c, int kx, int ky,
+                     const double *x, const double *y, int m, int ngrid, int len_indiv_c)
+{
+    const int nky1 = ny - ky - 1;
+    for (int i = 0; i < m; ++i) {
+        double wx[6], wy[6];
+        const int lx = oracle_basis(tx, nx, kx, x[i], wx);
+        const int ly = oracle_basis(ty, ny, ky, y[i], wy);
+        for (int g = 0; g < ngrid; ++g) {
+            const double *cg = c + (size_t)g * len_indiv_c;
+            double sp = 0.0;
+            int l1 = lx * nky1 + ly;
+            for (int a = 0; a <= kx; ++a) {
+                for (int b = 0; b <= ky; ++b) sp += cg[l1 + b] * wx[a] * wy[b];
+                l1 += nky1;
+            }
+            z[(size_t)g * m + i] = sp;
+        }
+    }
+}

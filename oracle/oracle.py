@@ -61,6 +61,9 @@ def _lib(impl: str):
                                             ctypes.c_int, ctypes.c_int]
         lib.oracle_find_start_inds.restype = ctypes.c_int
         lib.oracle_find_start_inds.argtypes = [_ip, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        lib.oracle_interp2d.argtypes = [_dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                        _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_interp2d.restype = None
     elif impl == "ref":
         if not os.path.isfile(LIB_REF):
             raise FileNotFoundError("reference CPU build missing: make -C oracle ref")
@@ -68,6 +71,9 @@ def _lib(impl: str):
         lib.few_ref_interpolate_arrays.restype = None
         lib.few_ref_interpolate_arrays.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]
         lib.few_ref_get_waveform.restype = None
+        lib.few_ref_interp2d.argtypes = [_dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                         _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.few_ref_interp2d.restype = None
         lib.few_ref_get_waveform.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _ip, _ip, _ip, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
                                              _dp, ctypes.c_int]
@@ -259,3 +265,22 @@ def run_window(prob, impl: str = "ref") -> np.ndarray:
         if st != 0:
             raise ValueError(f"oracle mode sum failed with status {st}")
     return wf
+
+
+def interp2d(tx, ty, c, kx: int, ky: int, x, y, impl: str = "oracle") -> np.ndarray:
+    """``interp2D`` (``src/few/cutils/AmpInterp2D.cu:86-208``): every grid of c
+    (ngrid, len_indiv_c) evaluated at the points (x, y) -> (ngrid, m)."""
+    tx = np.ascontiguousarray(tx, dtype=np.float64)
+    ty = np.ascontiguousarray(ty, dtype=np.float64)
+    c = np.ascontiguousarray(c, dtype=np.float64).reshape(-1, (len(tx) - kx - 1) * (len(ty) - ky - 1))
+    x = np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+    y = np.ascontiguousarray(np.atleast_1d(y), dtype=np.float64)
+    m, ngrid, nc = len(x), c.shape[0], c.shape[1]
+    z = np.zeros((ngrid, m), dtype=np.float64)
+    if impl == "ref":
+        _lib("ref").few_ref_interp2d(_p(z), _p(tx), len(tx), _p(ty), len(ty), _p(c), kx, ky, _p(x), m, _p(y), m,
+                                     ngrid, nc)
+    else:
+        _lib("oracle").oracle_interp2d(_p(z), _p(tx), len(tx), _p(ty), len(ty), _p(c), kx, ky, _p(x), _p(y), m,
+                                       ngrid, nc)
+    return z

@@ -2,6 +2,7 @@
 // (src/few/cutils/interpolate.hh:27-31), so the oracle tests can call it
 // through ctypes.  Built only by oracle/Makefile into oracle/_ref; test
 // infrastructure, never part of the product path.
+#include "AmpInterp2D.hh"
 #include "interpolate.hh"
 
 extern "C" {
@@ -10,6 +11,12 @@ void few_ref_interpolate_arrays(double *t_arr, double *interp_array, int ninterp
                                 double *B, double *upper_diag, double *diag, double *lower_diag)
 {
     interpolate_arrays(t_arr, interp_array, ninterps, length, B, upper_diag, diag, lower_diag);
+}
+
+void few_ref_interp2d(double *z, const double *tx, int nx, const double *ty, int ny, double *c, int kx, int ky,
+                      const double *x, int mx, const double *y, int my, int num_indiv_c, int len_indiv_c)
+{
+    interp2D_wrap(z, tx, nx, ty, ny, c, kx, ky, x, mx, y, my, num_indiv_c, len_indiv_c);
 }
 
 void few_ref_get_waveform(void *d_waveform, double *interp_array, double *phase_interp_t,

@@ -8,7 +8,8 @@ scipy.interpolate.CubicSpline (tests/test_mode_summation.py:23-52) and the sum
 against a direct numpy sum (tests/test_mode_summation.py:64-151), which the
 tests here restate as well.
 
-    python tests/golden/make_golden.py      (needs the reference sources)
+    python tests/golden/make_golden.py                    (needs the reference sources)
+    python tests/golden/make_golden.py --only amplitude   (the amplitude case alone)
 """
 from __future__ import annotations
 
@@ -42,8 +43,27 @@ def save_case(name, inp, wf, extra=None):
     np.savez_compressed(os.path.join(HERE, name), **d)
 
 
-def main():
+def amplitude_case():
+    """The reference's interp2D (AmpInterp2D.cu) on seeded clamped B-spline grids:
+    bicubic, and degrees (1, 5); points inside, on knots and outside the domain."""
+    rng = np.random.default_rng(77)
+    out = {}
+    for tag, kx, ky, nx, ny in (("k33", 3, 3, 14, 17), ("k15", 1, 5, 9, 16)):
+        tx = np.concatenate([np.zeros(kx + 1), np.sort(rng.uniform(0, 1, nx - 2 * kx - 2)), np.ones(kx + 1)])
+        ty = np.concatenate([-np.ones(ky + 1), np.sort(rng.uniform(-1, 2, ny - 2 * ky - 2)), 2 * np.ones(ky + 1)])
+        c = rng.standard_normal((6, (nx - kx - 1) * (ny - ky - 1)))
+        x = np.concatenate([rng.uniform(-0.2, 1.2, 40), tx[kx:kx + 5], [0.0, 1.0]])
+        y = np.concatenate([rng.uniform(-1.3, 2.3, 40), ty[ky:ky + 5], [-1.0, 2.0]])
+        out.update({f"{tag}_tx": tx, f"{tag}_ty": ty, f"{tag}_c": c, f"{tag}_x": x, f"{tag}_y": y,
+                    f"{tag}_z": O.interp2d(tx, ty, c, kx, ky, x, y, impl="ref")})
+    np.savez_compressed(os.path.join(HERE, "amp_interp2d.npz"), **out)
+
+
+def main(only=None):
     O.build(ref=True)
+    if only == "amplitude":
+        amplitude_case()
+        return
     rng = np.random.default_rng(2024)
 
     # 1. the reference spline test's inputs: cos/sin on 1000 uniform knots
@@ -86,8 +106,9 @@ def main():
     np.savez_compressed(os.path.join(HERE, "plain_small_ref.npz"), idx=idx, values=wf[idx],
                         norm=np.linalg.norm(wf), sum=wf.sum(), out_len=len(wf),
                         digest=inputs_digest(inp), seed=inp.seed)
+    amplitude_case()
     print("golden vectors written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[2] if len(sys.argv) > 2 and sys.argv[1] == "--only" else None)

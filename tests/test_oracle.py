@@ -85,3 +85,20 @@ def test_restatement_equals_reference_build(oracle):
     t = np.sort(np.random.default_rng(3).uniform(0, 10, 64))
     y = np.random.default_rng(4).standard_normal((7, 64))
     assert np.array_equal(oracle.interpolate_arrays(t, y), oracle.interpolate_arrays(t, y, impl="ref"))
+
+
+def test_interp2d_oracle_matches_reference_golden_and_scipy(oracle):
+    """The restated FITPACK evaluation (interp2D, AmpInterp2D.cu) equals the
+    reference's own output bit for bit, and scipy's bisplev (the same FITPACK
+    routine) on clamped points."""
+    from scipy.interpolate import bisplev
+
+    d = np.load(os.path.join(GOLDEN, "amp_interp2d.npz"))
+    for tag, kx, ky in (("k33", 3, 3), ("k15", 1, 5)):
+        tx, ty, c, x, y = (d[f"{tag}_{q}"] for q in ("tx", "ty", "c", "x", "y"))
+        z = oracle.interp2d(tx, ty, c, kx, ky, x, y)
+        assert np.array_equal(z, d[f"{tag}_z"]), tag
+        xs = np.clip(x, tx[kx], tx[len(tx) - kx - 1])
+        ys = np.clip(y, ty[ky], ty[len(ty) - ky - 1])
+        zs = np.array([[bisplev(a, b, (tx, ty, cg, kx, ky)) for a, b in zip(xs, ys)] for cg in c])
+        assert np.abs(z - zs).max() <= 1e-14 * np.abs(zs).max(), tag
