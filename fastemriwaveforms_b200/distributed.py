@@ -110,7 +110,9 @@ class ShardedInterpolatedModeSum(InterpolatedModeSum):
         p.shard = (lo, hi)
         return p
 
-    def _launch(self, p, out):
+    def _launch(self, p, out, host_out=None):
+        if host_out is not None:
+            raise ValueError("host_out is not supported when the waveform is split across ranks.")
         super()._launch(p, out)
         if self.gather and self.world > 1:
             out.copy_(gather_waveform(out, p.out_len, self.rank, self.world, self.group))

@@ -88,6 +88,17 @@ def _copy_stream(device) -> torch.cuda.Stream:
     return _COPY_STREAMS[key]
 
 
+_D2H_STREAMS: dict = {}
+
+
+def _download_stream(device) -> torch.cuda.Stream:
+    d = torch.device(device)
+    key = d.index if d.index is not None else torch.cuda.current_device()
+    if key not in _D2H_STREAMS:
+        _D2H_STREAMS[key] = torch.cuda.Stream(torch.device("cuda", key))
+    return _D2H_STREAMS[key]
+
+
 def _input(x, dtype, device) -> torch.Tensor:
     """A user input on the device.  Device tensors (and host tensors that
     require grad) go through torch's ``.to``; host data is copied on a separate
@@ -452,7 +463,7 @@ class InterpolatedModeSum(SummationBase):
         return plan
 
     def sum(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, *args,
-            dt: float = 10.0, integrate_backwards: bool = False, **kwargs):
+            dt: float = 10.0, integrate_backwards: bool = False, host_out=None, **kwargs):
         """Interpolated summation into ``self.waveform`` (``interpolatedmodesum.py:283-375``).
 
         If ``teuk_modes`` or ``phase_interp_coeffs`` is a torch tensor that
@@ -460,13 +471,21 @@ class InterpolatedModeSum(SummationBase):
         ``torch.autograd.Function`` whose backward runs the adjoint kernels."""
         needs_grad = torch.is_grad_enabled() and any(
             isinstance(x, torch.Tensor) and x.requires_grad for x in (teuk_modes, phase_interp_coeffs))
+        if host_out is not None:
+            if needs_grad:
+                raise ValueError("host_out is for calls without gradients.")
+            if not (isinstance(host_out, torch.Tensor) and host_out.device.type == "cpu" and host_out.is_pinned()
+                    and host_out.dtype == torch.complex128 and host_out.is_contiguous()
+                    and host_out.numel() >= self.waveform.numel()):
+                raise ValueError("host_out must be a pinned, contiguous complex128 CPU tensor at least as long as "
+                                 "the waveform.")
         prep = self._prepare(t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr,
                              dt, integrate_backwards, keep=needs_grad)
         if needs_grad:
             total = self.waveform.shape[0]
             self.waveform = _ModeSumFunction.apply(prep.teuk_in, prep.pc_in, self, prep, total)
         else:
-            self._launch(prep, self.waveform)
+            self._launch(prep, self.waveform, host_out)
         return self.waveform
 
     def _prepare(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, dt,
@@ -527,8 +546,11 @@ class InterpolatedModeSum(SummationBase):
         p.out_len = int(self.num_pts)
         return p
 
-    def _launch(self, p, out):
-        """Spline build, fold and sum into `out` (three launches on the current stream)."""
+    def _launch(self, p, out, host_out=None):
+        """Spline build, fold and sum into `out` (three launches on the current stream).
+        With `host_out` the sum runs in parts of consecutive work units (consecutive
+        output samples) and each finished slice is copied to `host_out` on a
+        download stream while the next part computes."""
         fold, seg, N, K, st = p.fold, p.seg, p.N, p.K, p.st
         coeffs = torch.empty((4, N, 2 * K), dtype=torch.float64, device=p.dev)
         W = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=p.dev)
@@ -553,19 +575,53 @@ class InterpolatedModeSum(SummationBase):
             if self._mixed_err is None or self._mixed_err.device != p.dev:
                 self._mixed_err = torch.zeros(1, dtype=torch.int32, device=p.dev)
             _lib.call("few_fold_mixed", _ptr(W), _ptr(p.t_dev), seg.nseg, fold.R, fold.NN, _ptr(Bpk), st)
-            _lib.call("few_sum_mixed", _ptr(out), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(p.t_dev),
-                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
-                      fold.NN, p.dt, fold.use_theta, _ptr(self._mixed_err), st)
+
+            def run(u0, u1):
+                _lib.call("few_sum_mixed", _ptr(out), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                          _ptr(p.t_dev), _ptr(seg.d_units) + 12 * u0, u1 - u0, _ptr(fold.d_row_m),
+                          _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta,
+                          _ptr(self._mixed_err), st)
         else:
-            _lib.call("few_sum_folded", _ptr(out), _ptr(W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
-                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
-                      fold.NN, p.dt, _PRECISIONS[self.precision], fold.use_theta, st)
+            def run(u0, u1):
+                _lib.call("few_sum_folded", _ptr(out), _ptr(W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                          _ptr(seg.d_units) + 12 * u0, u1 - u0, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R,
+                          fold.nlo, fold.NN, p.dt, _PRECISIONS[self.precision], fold.use_theta, st)
+        if host_out is None or seg.nunits == 0:
+            run(0, seg.nunits)
+            if host_out is not None:
+                host_out[: out.numel()].copy_(out)
+        else:
+            self._sum_streamed(run, seg, out, host_out, p.dev)
         if ev:
             ev[3].record()
             self._stage_events = ev
         self._last_plan = (fold, seg)
         p.W = W
         return out
+
+    @staticmethod
+    def _sum_streamed(run, seg, out, host_out, dev, parts: int = 4):
+        """The sum in `parts` launches over consecutive units; after each, the
+        samples it finished go to host_out on the download stream."""
+        main = torch.cuda.current_stream(dev)
+        ds = _download_stream(dev)
+        units = seg.units_host.reshape(-1, 3)
+        n = seg.nunits
+        bounds = sorted({min(n, (n * q + parts - 1) // parts) for q in range(parts + 1)})
+        done = 0
+        for u0, u1 in zip(bounds[:-1], bounds[1:]):
+            if u1 <= u0:
+                continue
+            run(u0, u1)
+            end = out.numel() if u1 == n else int(units[u1, 1])
+            ev = torch.cuda.Event()
+            ev.record(main)
+            ds.wait_event(ev)
+            with torch.cuda.stream(ds):
+                host_out[done:end].copy_(out[done:end], non_blocking=True)
+            done = end
+        out.record_stream(ds)
+        main.wait_stream(ds)
 
     def _backward_hook(self, p, grad, need_teuk, need_pc):
         """The backward of one call (overridden by the sharded summation)."""

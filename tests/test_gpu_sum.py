@@ -235,3 +235,24 @@ def test_sharded_ranks_sum_to_the_whole(cuda):
     ref_t, ref_p = teuk.grad.cpu().numpy(), pc.grad.cpu().numpy()
     assert np.abs(g_teuk - ref_t).max() <= 1e-11 * np.abs(ref_t).max()
     assert np.abs(g_pc - ref_p).max() <= 1e-11 * np.abs(ref_p).max()
+
+
+@pytest.mark.parametrize("precision", ["faithful", "mixed"])
+def test_host_out_streams_the_same_waveform(cuda, precision):
+    """host_out: the sum in parts with each finished slice copied to pinned host
+    memory while the next part runs; bitwise the device waveform, two calls in a
+    row, and refused where it does not apply."""
+    inp = S.plain_small()
+    ims = InterpolatedModeSum(precision=precision, chunk=256)  # many units: four real parts
+    ref = ims(*inp.call_args(), T=inp.T, dt=inp.dt).cpu().numpy()
+    host = torch.zeros(len(ref) + 5, dtype=torch.complex128).pin_memory()
+    for _ in range(2):
+        host.zero_()
+        wf = ims(*inp.call_args(), T=inp.T, dt=inp.dt, host_out=host)
+        torch.cuda.synchronize()
+        assert np.array_equal(host[: len(ref)].numpy(), ref)
+        assert np.array_equal(wf.cpu().numpy(), ref)
+    with pytest.raises(ValueError):
+        ims(*inp.call_args(), T=inp.T, dt=inp.dt, host_out=torch.zeros(len(ref), dtype=torch.complex128))
+    with pytest.raises(ValueError):
+        ims(*inp.call_args(), T=inp.T, dt=inp.dt, host_out=host[:10])
