@@ -229,7 +229,7 @@ class BatchedInterpolatedModeSum:
             s = side[i % len(side)]
             with torch.cuda.stream(s):
                 p.st = s.cuda_stream
-                out.append(InterpolatedModeSum._backward(p, g))
+                out.append(InterpolatedModeSum._backward(p, g, concurrent=False))
         self._join(main, side)
         if not torch.cuda.is_current_stream_capturing():
             for pair in out:  # made on side streams, used on the caller's stream

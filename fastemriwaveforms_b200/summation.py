@@ -99,6 +99,18 @@ def _download_stream(device) -> torch.cuda.Stream:
     return _D2H_STREAMS[key]
 
 
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device) -> torch.cuda.Stream:
+    """A second compute stream per device (the phase branch of a backward)."""
+    d = torch.device(device)
+    key = d.index if d.index is not None else torch.cuda.current_device()
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(torch.device("cuda", key))
+    return _SIDE_STREAMS[key]
+
+
 def _input(x, dtype, device) -> torch.Tensor:
     """A user input on the device.  Device tensors (and host tensors that
     require grad) go through torch's ``.to``; host data is copied on a separate
@@ -628,10 +640,19 @@ class InterpolatedModeSum(SummationBase):
         return InterpolatedModeSum._backward(p, grad, need_teuk, need_pc)
 
     @staticmethod
-    def _backward(p, grad, need_teuk=True, need_pc=True):
-        """Adjoint kernels: (dL/d teuk_modes (N, K) complex, dL/d phase_interp_coeffs (N-1, 3, 8))."""
+    def _backward(p, grad, need_teuk=True, need_pc=True, concurrent=True):
+        """Adjoint kernels: (dL/d teuk_modes (N, K) complex, dL/d phase_interp_coeffs (N-1, 3, 8)).
+        With both gradients wanted and ``concurrent``, the phase branch runs on a
+        second stream beside the amplitude branch (the two kernels leave room for
+        each other on an SM)."""
         fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
         grad = grad[: p.out_len].to(torch.complex128).contiguous()
+        both = need_teuk and need_pc and concurrent
+        main = torch.cuda.current_stream(dev)
+        side = None
+        if both:
+            side = _side_stream(dev)
+            side.wait_stream(main)
         g_teuk = g_pc = None
         mixed = getattr(p, "bwd_mixed", False)
         if mixed and need_pc and fold.R > 64:
@@ -654,23 +675,35 @@ class InterpolatedModeSum(SummationBase):
             _lib.call("few_spline_adjoint_factored", _ptr(p.fac), _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N,
                       0, st)
         if need_pc:
-            _, seg_units = seg.backward_tables()
-            partial = torch.empty((max(seg.nunits, 1), 24), dtype=torch.float64, device=dev)
-            if mixed:
-                nbytes = int(_lib.load().few_mixed_adjoint_operand_bytes(max(seg.nseg, 1), fold.R, fold.NN))
-                Bpk = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-                _lib.call("few_fold_mixed_adjoint", _ptr(p.W), _ptr(p.t_dev), seg.nseg, fold.R, fold.nlo, fold.NN,
-                          _ptr(Bpk), st)
-                _lib.call("few_adjoint_phase_mixed", _ptr(grad), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info),
-                          _ptr(p.t_dev), _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k),
-                          fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta, _ptr(partial), _ptr(p.err), st)
-            else:
-                _lib.call("few_adjoint_phase", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
-                          _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
-                          fold.NN, p.dt, fold.use_theta, _ptr(partial), st)
-            g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
-            _lib.call("few_adjoint_phase_reduce", _ptr(partial), _ptr(seg_units), seg.nseg, _ptr(g_pc), st)
+            with torch.cuda.stream(side) if both else torch.cuda.stream(main):
+                g_pc = InterpolatedModeSum._phase_backward(p, grad, mixed, side.cuda_stream if both else st)
+            if both:
+                main.wait_stream(side)
+                if not torch.cuda.is_current_stream_capturing():
+                    g_pc.record_stream(main)
         return g_teuk, g_pc
+
+    @staticmethod
+    def _phase_backward(p, grad, mixed, st):
+        """dL/d phase_interp_coeffs on stream st (tensors allocated on the current stream)."""
+        fold, seg, N, dev = p.fold, p.seg, p.N, p.dev
+        _, seg_units = seg.backward_tables()
+        partial = torch.empty((max(seg.nunits, 1), 24), dtype=torch.float64, device=dev)
+        if mixed:
+            nbytes = int(_lib.load().few_mixed_adjoint_operand_bytes(max(seg.nseg, 1), fold.R, fold.NN))
+            Bpk = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            _lib.call("few_fold_mixed_adjoint", _ptr(p.W), _ptr(p.t_dev), seg.nseg, fold.R, fold.nlo, fold.NN,
+                      _ptr(Bpk), st)
+            _lib.call("few_adjoint_phase_mixed", _ptr(grad), _ptr(Bpk), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                      _ptr(p.t_dev), _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k),
+                      fold.R, fold.nlo, fold.NN, p.dt, fold.use_theta, _ptr(partial), _ptr(p.err), st)
+        else:
+            _lib.call("few_adjoint_phase", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info),
+                      _ptr(seg.d_units), seg.nunits, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                      fold.NN, p.dt, fold.use_theta, _ptr(partial), st)
+        g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
+        _lib.call("few_adjoint_phase_reduce", _ptr(partial), _ptr(seg_units), seg.nseg, _ptr(g_pc), st)
+        return g_pc
 
     def stage_times(self) -> dict:
         """Kernel times (ms) of the last call with ``record_stages`` set:
