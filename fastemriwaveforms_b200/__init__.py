@@ -1,11 +1,15 @@
 """B200-native interpolated mode summation for FastEMRIWaveforms.
 
 Drop-in for ``few.summation.interpolatedmodesum.InterpolatedModeSum`` and its
-``CubicSplineInterpolant``: Python host code over hand-written sm_100a CUDA
+``CubicSplineInterpolant`` (and, around it, ``FDInterpolatedModeSum``,
+``get_fundamental_frequencies`` and ``AmpInterp2D``): Python host code over hand-written sm_100a CUDA
 kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
 """
 from .amplitude import AmpInterp2D
+from .fdinterp import FDInterpolatedModeSum
+from .geodesic import get_fundamental_frequencies
 from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBase
 from .utility import get_mismatch, get_overlap
 
-__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "InterpolatedModeSum", "SummationBase", "get_mismatch", "get_overlap"]
+__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "InterpolatedModeSum", "SummationBase",
+           "get_fundamental_frequencies", "get_mismatch", "get_overlap"]

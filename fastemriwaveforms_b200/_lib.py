@@ -68,6 +68,19 @@ SIGNATURES = {
                          _vp],
     "few_get_waveform_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_dbl, _vp,
                                  _c_int, _vp],
+    "few_fundamental_frequencies": [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_int, _vp, _vp, _vp, _vp, _vp],
+    "few_fd_turn_bytes": [],
+    "few_fd_plan_extrema": [_vp, _c_int, _c_dbl, _c_dbl, _c_dbl, _vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp,
+                            _vp],
+    "few_fd_plan_bins": [_vp, _vp, _vp, _vp, _c_int, _c_int, _vp, _vp, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
+                         _vp, _vp, _vp, _vp, _vp],
+    "few_fd_scan": [_vp, _c_ll, _vp, _vp],
+    "few_fd_frequency_grid": [_vp, _c_int, _c_dbl, _vp],
+    "few_fd_sum": [_vp, _c_int, _vp, _c_int, _c_int, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll,
+                   _c_ll, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp],
+    "few_fd_finalize": [_vp, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_get_waveform_fd": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_dbl, _vp, _c_int, _c_int, _vp, _vp, _vp,
+                            _c_int, _vp, _c_int, _c_int, _c_int, _vp],
 }
 _RESTYPE = {"few_last_error": ctypes.c_char_p, "few_mixed_operand_bytes": ctypes.c_longlong,
             "few_mixed_adjoint_operand_bytes": ctypes.c_longlong}

@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -21,7 +22,8 @@ LIBDIR = os.path.join(PKG, "lib")
 LIBNAME = "libfew_b200.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
-SOURCES = ["api.cu", "plan.cpp", "spline.cu", "modesum.cu", "probe.cu", "noalloc.cu", "adjoint.cu", "mixed.cu", "mixed_adjoint.cu", "amplitude.cu"]
+SOURCES = ["api.cu", "plan.cpp", "spline.cu", "modesum.cu", "probe.cu", "noalloc.cu", "adjoint.cu", "mixed.cu",
+           "mixed_adjoint.cu", "amplitude.cu", "geodesic.cu", "fdsum.cu"]
 HEADERS = ["few_common.cuh", "few_internal.h", "few_tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -48,27 +50,42 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    """Compile every CUDA source for sm_100a into one shared library."""
+    """Compile every CUDA source for sm_100a (one object per source, in
+    parallel) and link them into one shared library."""
     if not force and up_to_date():
         return LIBPATH
     os.makedirs(LIBDIR, exist_ok=True)
     nvcc = nvcc_path()
-    tmp = LIBPATH + f".tmp{os.getpid()}"
-    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
-           f"-I{INCLUDE}", f"-I{CSRC}", "-o", tmp]
+    objdir = os.path.join(LIBDIR, "_build", f"obj{os.getpid()}")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
     if ptxas_verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    cmd += ["-lcudart"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    res = subprocess.run(cmd, capture_output=True, text=True)
+        common += ["-Xptxas", "-v"]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    log = ""
+    for src, (obj, res) in zip(SOURCES, results):
+        log += res.stdout + res.stderr
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src} ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+    tmp = LIBPATH + f".tmp{os.getpid()}"
+    link = [nvcc, *ARCH, "-shared", "-o", tmp, *(obj for obj, _ in results), "-lcudart"]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+        raise RuntimeError(f"nvcc link failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
     if verbose or ptxas_verbose:
-        sys.stderr.write(res.stdout + res.stderr)
+        sys.stderr.write(log + res.stdout + res.stderr)
     os.replace(tmp, LIBPATH)
+    shutil.rmtree(objdir, ignore_errors=True)
     return LIBPATH
 
 

@@ -16,6 +16,9 @@ Workloads (sizes are part of the benchmark definition):
 * ``adjoint``      -- K=1000 (prefix of the full list), N=500 knots,
   1,000,000 samples.
 * ``batch``        -- many waveforms with uneven T, N and K.
+* ``fd_case``      -- inputs of the frequency-domain sum: the above plus a
+  trajectory (M, a, p(t), e(t), x) whose Kerr geodesic frequencies set each
+  mode's frequency track; ``fd_full`` is the one-year, 3843-mode size.
 
 Phases are closed-form integrals of a chirping frequency
 f(t) = 1e-3 (1 - t/t_c)^(-3/8) Hz:
@@ -322,3 +325,80 @@ def amplitude_points(N: int, seed: int = 12):
     """A smooth trajectory in (w, u) through the grid's domain, N points."""
     s = np.linspace(0.0, 1.0, N)
     return 0.05 + 0.9 * s ** 1.5, 0.5 + 0.4 * np.sin(2.0 * np.pi * s) * (1.0 - s)
+
+
+@dataclass
+class FDTrajectory:
+    """The orbit arguments of ``FDInterpolatedModeSum.sum`` (fdinterp.py:138-160)."""
+
+    M: float          # primary mass, solar masses
+    a: float          # dimensionless spin
+    p: np.ndarray     # (N,) semi-latus rectum at the knots
+    e: np.ndarray     # (N,) eccentricity at the knots
+    xI: np.ndarray    # (N,) cos of the inclination at the knots
+
+
+def fd_mode_list(lmax: int, kmax: int, nmax: int, count: int | None = None):
+    """(l, m, k, n) for l = 2..lmax, m = 0..l, k = -kmax..kmax, n = -nmax..nmax."""
+    modes = [(l, m, k, n) for l in range(2, lmax + 1) for m in range(0, l + 1)
+             for k in range(-kmax, kmax + 1) for n in range(-nmax, nmax + 1)]
+    if count is not None:
+        modes = modes[:count]
+    arr = np.asarray(modes, dtype=np.int32).reshape(-1, 4)
+    return (np.ascontiguousarray(arr[:, i]) for i in range(4))
+
+
+def phase_knots_from_frequencies(t, t_dense, f_dense):
+    """Phases 2 pi int_{t0}^{t} f dt at the knots t from frequencies f_dense
+    (3, D) sampled on t_dense (through the antiderivative of a cubic spline)."""
+    from scipy.interpolate import CubicSpline
+
+    cs = CubicSpline(t_dense, np.asarray(f_dense), axis=1)
+    anti = cs.antiderivative()
+    return 2.0 * np.pi * (anti(np.asarray(t)) - anti(np.asarray(t)[0])[:, None])
+
+
+def fd_case(K: int = 77, N: int = 50, span: float = 2e6, seed: int = 21, a: float = 0.0, x: float = 1.0,
+            M: float = 1e6, lmax: int = 3, kmax: int = 0, nmax: int = 5, dt: float = 10.0,
+            p_range=(12.0, 7.4), e_range=(0.4, 0.2), frequencies=None, name: str = "fd"):
+    """Inputs of the frequency-domain sum: (ModeSumInputs, FDTrajectory).
+
+    p falls from p_range[0] to p_range[1] as 1 - (1 - u)^0.8 (u = t/span) and
+    e linearly; x is constant.  Amplitudes and harmonics are drawn as in
+    ``make_inputs``.  ``frequencies`` (optional) maps times (D,) to the three
+    frequencies (3, D) in Hz; given it, the phases are their integrals (a
+    self-consistent waveform), otherwise the closed-form chirp of
+    ``phase_values`` (any smooth phases exercise the sum)."""
+    rng = np.random.default_rng(seed)
+    t = knot_times(rng, N, span, 0.099 * span / (N - 1))
+    u = t / span
+    p = p_range[0] + (p_range[1] - p_range[0]) * (1.0 - (1.0 - u) ** 0.8)
+    e = e_range[0] + (e_range[1] - e_range[0]) * u
+    xI = np.full(N, float(x))
+    l, m, k, n = fd_mode_list(lmax, kmax, nmax, K)
+    K = len(l)
+    amp = (rng.standard_normal(K) + 1j * rng.standard_normal(K)) / np.sqrt(2.0)
+    amp *= np.exp(-np.abs(n) / 4.0) / (l.astype(np.float64) ** 2)
+    omega = rng.uniform(0.0, 1e-6, K)
+    teuk = amp[None, :] * (1.0 + 0.5 * u[:, None]) * np.exp(1j * omega[None, :] * t[:, None])
+    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    if frequencies is None:
+        phi, phr = phase_values(t, 1.2 * span, span)
+        phase_knots = np.stack([phi, 0.6 * phi, phr])
+    else:
+        td = np.linspace(t[0], t[-1], 20 * N)
+        phase_knots = phase_knots_from_frequencies(t, td, frequencies(td))
+    phase_coeffs = phase_basis_from_knots(t, phase_knots)
+    T = (span + dt) / YRSID_SI
+    inp = ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),
+                        phase_coeffs=phase_coeffs, l=l, m=m, k=k, n=n, dt=dt, T=T,
+                        phase_knots=phase_knots, name=name, seed=seed)
+    return inp, FDTrajectory(M=M, a=a, p=p, e=e, xI=xI)
+
+
+def fd_full(seed: int = 23, frequencies=None):
+    """One year at dt = 10 s: K = 3843 modes (l = 2..10, m = 0..l, n = -30..30),
+    N = 1000 knots on [0, 3.15e7] s, M = 1e6, a = 0.5, prograde equatorial,
+    p 12 -> 7.4, e 0.4 -> 0.2."""
+    return fd_case(K=3843, N=1000, span=3.15e7, seed=seed, a=0.5, x=1.0, lmax=10, kmax=0, nmax=30,
+                   frequencies=frequencies, name="fd_full")

@@ -378,6 +378,92 @@ FEW_API int few_amp_interp2d(void *out, const double *tx, int nx, const double *
                              int len_indiv_c, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Frequency-domain sum (FDInterpolatedModeSum, fdinterp.py:92-542)         */
+/* ------------------------------------------------------------------------ */
+
+/* Kerr geodesic fundamental frequencies (get_fundamental_frequencies,
+ * src/few/utils/geodesic.py:470-535, and its kernels geodesic.py:157-451):
+ * for i < n, (a[i*a_stride], p[i], e[i], x[i]) [device] -> o_phi, o_theta,
+ * o_r [device] (n,), each divided by denom (1 for the dimensionless
+ * frequencies, 2 pi M MTSUN_SI for Hz); abs_phi != 0 stores |o_phi| (the
+ * frequency-domain sum's convention).  a_stride is 0 (one spin) or 1.
+ * status [device] int (may be NULL) gets bit 1 OR-ed in when an elliptic
+ * modulus falls outside [0, 1] (the reference raises ValueError there). */
+FEW_API int few_fundamental_frequencies(const double *a, int a_stride, const double *p, const double *e,
+                                        const double *x, int n, double denom, int abs_phi, double *o_phi,
+                                        double *o_theta, double *o_r, int *status, void *stream);
+
+/* Size in bytes of one per-mode turnover record of few_fd_plan_extrema. */
+FEW_API int few_fd_turn_bytes(void);
+
+/* Turnover search of fdinterp.py:262-376 for every mode: fdense [device]
+ * (3, D) = the frequency splines at the dense grid t_j = j*tn_step + tn_start
+ * (j < D-1), t_{D-1} = tn_stop (numpy.linspace); t [device] (N,) knots;
+ * fcoef [device] (4, N, 3) the frequency splines' coefficients (knot-major);
+ * m, k, n [device] (K,).  turns [device] (K, 2) records (few_fd_turn_bytes
+ * each): for the maximum and the minimum of each mode's frequency, whether it
+ * is an interior turnover, its segment and the frequency at the root of the
+ * cubic's derivative.  flags [device] int, zeroed by the caller: bit 1 some
+ * root was kept, bit 2 a segment kept both roots, bit 4 a discriminant below
+ * -1e10 (the reference stops at a breakpoint() for 2 and 4), bit 8 a NaN. */
+FEW_API int few_fd_plan_extrema(const double *fdense, int D, double tn_start, double tn_step, double tn_stop,
+                                const double *t, int N, const double *fcoef, const int *m, const int *k, const int *n,
+                                int K, void *turns, int *flags, void *stream);
+
+/* Bin ranges of every (mode, segment) (fdinterp.py:271-430): fknots [device]
+ * (3, N) the frequencies at the knots; turns/flags from few_fd_plan_extrema;
+ * f0 = frequency[0], df = frequency[1] - frequency[0]; has_farr selects the
+ * user-grid rule for positive frequencies with fpos1 = frequency[zero_index+1].
+ * Outputs [device] (K*(N-1),), entry mode*(N-1)+seg: start32/end32 the
+ * reference's int32 seg_start_inds/seg_end_inds; lo and count the bins its
+ * kernel visits, [lo, lo+count) within [0, L). */
+FEW_API int few_fd_plan_bins(const double *fknots, const int *m, const int *k, const int *n, int K, int N,
+                             const void *turns, const int *flags, double f0, double df, int has_farr, double fpos1,
+                             int zero_index, int L, int *start32, int *end32, int *lo, long long *count,
+                             void *stream);
+
+/* prefix [device] (E+1,) = exclusive prefix sums of count [device] (E,). */
+FEW_API int few_fd_scan(const long long *count, long long E, long long *prefix, void *stream);
+
+/* f [device] (L,) = the default two-sided grid (j - L/2) / Ldt, Ldt = L*dt
+ * (fdinterp.py:398-403). */
+FEW_API int few_fd_frequency_grid(double *f, int L, double Ldt, void *stream);
+
+/* The stationary-phase sum (make_generic_kerr_waveform_fd,
+ * interpolate.cu:1141-1520) over the planned bins: wf [device] (L,) complex,
+ * accumulated; freq [device] (L,).  Amplitude spline coefficient q of series p
+ * (0..2K-1: real parts then imaginary parts) at knot j is
+ * amp[q*aq + p*ap + j*aj]; the frequency splines' (series 0..2 = f_phi,
+ * f_theta, f_r) fco[q*fq + p*fp + j*fj]; phase coefficient c (0..7) of field
+ * (Phi_phi, Phi_theta, Phi_r) on segment s is pc[c*pcc + field*pcf + s*pcs].
+ * ylms [device] (2K) complex, the -m half already times (-1)^l.  lo, prefix
+ * [device] from few_fd_plan_bins / few_fd_scan.  blocks <= 0 picks the
+ * default grid.  Accumulation is by FP64 atomics: sums are reproducible to
+ * rounding, not bit for bit. */
+FEW_API int few_fd_sum(void *wf, int L, const double *freq, int zero_index, int include_minus_m, const double *amp,
+                       long long aq, long long ap, long long aj, const double *fco, long long fq, long long fp,
+                       long long fj, const double *pc, long long pcc, long long pcf, long long pcs,
+                       const double *phase_t, const double *t, int N, const int *m, const int *k, const int *n, int K,
+                       const void *ylms, const int *lo, const long long *prefix, int blocks, void *stream);
+
+/* (h+, hx) from the two-sided sum (fdinterp.py:518-536): out [device]
+ * (2, count) complex, rows h+ and hx at bins first .. first+count-1. */
+FEW_API int few_fd_finalize(const void *wf, int L, int first, int count, void *out, void *stream);
+
+/* Drop-in for get_waveform_generic_fd (src/few/cutils/interpolate.hh:33-38):
+ * the reference's argument list and layouts (interp_array (4, 2K+3, N),
+ * phase_interp_coeffs (8, 3, N-1), seg_start/end_inds (K, N-1)), all
+ * [device], plus the stream.  separate_modes != 0 is refused (FEW_ERR_ARG):
+ * the reference kernel writes mode_i * data_length + i into a buffer of
+ * data_length elements. */
+FEW_API int few_get_waveform_fd(void *waveform, const double *interp_array, const double *phase_interp_t,
+                                const double *phase_interp_coeffs, const int *m, const int *k, const int *n,
+                                int num_teuk_modes, double delta_t, const double *old_time_arr, int init_length,
+                                int data_length, const double *frequencies, const int *seg_start_inds,
+                                const int *seg_end_inds, int num_segments, const void *Ylm_all, int zero_index,
+                                int include_minus_m, int separate_modes, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */
 

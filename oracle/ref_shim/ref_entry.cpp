@@ -1,5 +1,5 @@
 // C-linkage entry points into the reference's own CPU implementation
-// (src/few/cutils/interpolate.hh:27-31), so the oracle tests can call it
+// (src/few/cutils/interpolate.hh:27-38, AmpInterp2D.hh:6-8), so the oracle tests can call it
 // through ctypes.  Built only by oracle/Makefile into oracle/_ref; test
 // infrastructure, never part of the product path.
 #include "AmpInterp2D.hh"
@@ -17,6 +17,18 @@ void few_ref_interp2d(double *z, const double *tx, int nx, const double *ty, int
                       const double *x, int mx, const double *y, int my, int num_indiv_c, int len_indiv_c)
 {
     interp2D_wrap(z, tx, nx, ty, ny, c, kx, ky, x, mx, y, my, num_indiv_c, len_indiv_c);
+}
+
+void few_ref_get_waveform_fd(void *waveform, double *interp_array, double *phase_interp_t,
+                             double *phase_interp_coeffs, int *m, int *k, int *n, int num_teuk_modes,
+                             double delta_t, double *old_time_arr, int init_length, int data_length,
+                             double *frequencies, int *seg_start_inds, int *seg_end_inds, int num_segments,
+                             void *ylms, int zero_index, int include_minus_m, int separate_modes)
+{
+    get_waveform_generic_fd((cmplx *)waveform, interp_array, phase_interp_t, phase_interp_coeffs, m, k, n,
+                            num_teuk_modes, delta_t, old_time_arr, init_length, data_length, frequencies,
+                            seg_start_inds, seg_end_inds, num_segments, (cmplx *)ylms, zero_index,
+                            include_minus_m != 0, separate_modes != 0);
 }
 
 void few_ref_get_waveform(void *d_waveform, double *interp_array, double *phase_interp_t,

@@ -146,3 +146,17 @@ def test_mismatch_known_answer():
     assert abs(get_overlap(x0, x0) - 1.0) < 1e-12
     assert abs(get_overlap(x0, x2) - 0.499981442642142) < 1e-7
     assert abs(get_mismatch(x0, x0)) < 1e-12
+
+
+def test_fd_dense_grid_is_numpy_linspace():
+    """The turnover search rebuilds numpy.linspace's points on the device from
+    (start, step, stop): y_j = j*step + start, the last point = stop."""
+    from fastemriwaveforms_b200.fdinterp import DENSE_POINTS, _linspace_params
+
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        t = np.sort(rng.uniform(0, rng.uniform(1e4, 1e8), 40))
+        t0, step, t1 = _linspace_params(t.min(), t.max(), DENSE_POINTS)
+        mine = np.arange(DENSE_POINTS) * step + t0
+        mine[-1] = t1
+        assert np.array_equal(mine, np.linspace(t.min(), t.max(), DENSE_POINTS))
