@@ -254,7 +254,8 @@ struct Turn {
     int pad;
 };
 
-// flags bits (few_fd_plan_extrema / few_fd_plan_bins)
+// flags[0] bits (few_fd_plan_extrema / few_fd_plan_bins); flags[1] counts the
+// interior turnovers over all modes and both lists.
 constexpr int kFlagAnyKeep = 1;    // some turnover root lies inside its segment
 constexpr int kFlagBothKeep = 2;   // a segment holds both roots (the reference stops there)
 constexpr int kFlagDiscBad = 4;    // a discriminant below -1e10 (the reference stops there)
@@ -310,6 +311,7 @@ __global__ void k_fd_extrema(const double *__restrict__ fdense, int D, double tn
         double tof = t_dense(which == 0 ? mx.i : mn.i, D, tn_start, tn_step, tn_stop);
         if (tof > 0.0 && tof < tlast) {
             o.valid = 1;
+            atomicAdd(flags + 1, 1);
             int seg = search_left(t, N, tof) - 1;          // may be -1 (Python wraps it)
             int sc = seg < 0 ? seg + N : seg;              // coefficient column
             double t0 = t[sc], t1 = t[seg + 1 < N ? seg + 1 : seg + 1 - N];
@@ -366,7 +368,10 @@ __global__ void k_fd_bins(const double *__restrict__ fk, const int *__restrict__
                           int has_farr, double fpos1, int zero_index, int L, int *__restrict__ start32,
                           int *__restrict__ end32, int *__restrict__ lo_out, long long *__restrict__ count) {
     long long E = (long long)K * (N - 1);
-    bool apply = (*flags & kFlagAnyKeep) != 0;
+    // fdinterp.py:367-376 joins the (n, 2) segment bounds with the (1, n) row of
+    // turnover frequencies; for n != 1 that raises the ValueError its handler
+    // swallows, so the widening happens only for a single interior turnover.
+    bool apply = (flags[0] & kFlagAnyKeep) != 0 && flags[1] == 1;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
          e += (long long)gridDim.x * blockDim.x) {
         int mode = (int)(e / (N - 1)), seg = (int)(e % (N - 1));

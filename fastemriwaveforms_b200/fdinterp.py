@@ -102,7 +102,7 @@ class FDInterpolatedModeSum(SummationBase):
         fk = _to_device(frequencies, torch.float64, dev)
         if tuple(fk.shape) != (3, N):
             raise ValueError("frequencies must have shape (3, len(t)).")
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        status = torch.zeros(2, dtype=torch.int32, device=dev)  # planning flags, turnover count
 
         # 2. splines: amplitudes (4, N, 2K) knot-major, frequencies (4, N, 3)
         amp = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
@@ -177,7 +177,7 @@ class FDInterpolatedModeSum(SummationBase):
         # the one synchronisation: the reference's errors
         if _geodesic_status is not None and int(_geodesic_status.item()) & 1:
             raise ValueError("Elliptic integral K(k) valid only for k in [0, 1].")
-        flags = int(status.item())
+        flags = int(status[0].item())
         if flags & 2:
             raise ValueError("a turnover segment holds both roots of the frequency derivative "
                              "(the reference stops at a breakpoint(), fdinterp.py:353-354)")

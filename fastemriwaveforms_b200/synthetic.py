@@ -365,15 +365,20 @@ def fd_case(K: int = 77, N: int = 50, span: float = 2e6, seed: int = 21, a: floa
 
     p falls from p_range[0] to p_range[1] as 1 - (1 - u)^0.8 (u = t/span) and
     e linearly; x is constant.  Amplitudes and harmonics are drawn as in
-    ``make_inputs``.  ``frequencies`` (optional) maps times (D,) to the three
-    frequencies (3, D) in Hz; given it, the phases are their integrals (a
-    self-consistent waveform), otherwise the closed-form chirp of
-    ``phase_values`` (any smooth phases exercise the sum)."""
+    ``make_inputs``.  ``frequencies`` (optional) is a callable
+    (M, a, p, e, x) -> (3, D) array of (|f_phi|, f_theta, f_r) in Hz along
+    the trajectory; given it, the phases are their integrals (a self-consistent
+    waveform, whose stationary phase is flat at the roots), otherwise the
+    closed-form chirp of ``phase_values`` (any smooth phases exercise the sum)."""
     rng = np.random.default_rng(seed)
     t = knot_times(rng, N, span, 0.099 * span / (N - 1))
+    def orbit(tt):
+        u = np.asarray(tt) / span
+        return (p_range[0] + (p_range[1] - p_range[0]) * (1.0 - (1.0 - u) ** 0.8),
+                e_range[0] + (e_range[1] - e_range[0]) * u)
+
     u = t / span
-    p = p_range[0] + (p_range[1] - p_range[0]) * (1.0 - (1.0 - u) ** 0.8)
-    e = e_range[0] + (e_range[1] - e_range[0]) * u
+    p, e = orbit(t)
     xI = np.full(N, float(x))
     l, m, k, n = fd_mode_list(lmax, kmax, nmax, K)
     K = len(l)
@@ -387,7 +392,9 @@ def fd_case(K: int = 77, N: int = 50, span: float = 2e6, seed: int = 21, a: floa
         phase_knots = np.stack([phi, 0.6 * phi, phr])
     else:
         td = np.linspace(t[0], t[-1], 20 * N)
-        phase_knots = phase_knots_from_frequencies(t, td, frequencies(td))
+        pd, ed = orbit(td)
+        fdense = np.asarray(frequencies(M, a, pd, ed, np.full(len(td), float(x))), dtype=np.float64)
+        phase_knots = phase_knots_from_frequencies(t, td, fdense)
     phase_coeffs = phase_basis_from_knots(t, phase_knots)
     T = (span + dt) / YRSID_SI
     inp = ModeSumInputs(t=t, teuk_modes=np.ascontiguousarray(teuk), ylms=ylms, phase_t=t.copy(),

@@ -403,9 +403,11 @@ FEW_API int few_fd_turn_bytes(void);
  * m, k, n [device] (K,).  turns [device] (K, 2) records (few_fd_turn_bytes
  * each): for the maximum and the minimum of each mode's frequency, whether it
  * is an interior turnover, its segment and the frequency at the root of the
- * cubic's derivative.  flags [device] int, zeroed by the caller: bit 1 some
- * root was kept, bit 2 a segment kept both roots, bit 4 a discriminant below
- * -1e10 (the reference stops at a breakpoint() for 2 and 4), bit 8 a NaN. */
+ * cubic's derivative.  flags [device] int[2], zeroed by the caller: flags[0]
+ * bit 1 some root was kept, bit 2 a segment kept both roots, bit 4 a
+ * discriminant below -1e10 (the reference stops at a breakpoint() for 2 and
+ * 4), bit 8 a NaN; flags[1] the number of interior turnovers (the reference
+ * widens a segment only when there is exactly one, fdinterp.py:367-376). */
 FEW_API int few_fd_plan_extrema(const double *fdense, int D, double tn_start, double tn_step, double tn_stop,
                                 const double *t, int N, const double *fcoef, const int *m, const int *k, const int *n,
                                 int K, void *turns, int *flags, void *stream);

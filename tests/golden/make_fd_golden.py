@@ -186,19 +186,34 @@ def geodesic_case(geo):
     return len(rows)
 
 
+def reference_frequencies(geo):
+    """(M, a, p, e, x) -> (3, D) Hz by the reference's own geodesic code and
+    conversion (fdinterp.py:224-236): the phases of the golden inputs are the
+    integrals of these, so each mode's phase is stationary at its roots."""
+
+    def freqs(M, a, p, e, x):
+        Ophi, Oth, Or = geo.get_fundamental_frequencies(a, p, e, x)
+        den = 2 * np.pi * M * MTSUN_SI
+        return np.stack([np.abs(Ophi / den), Oth / den, Or / den])
+
+    return freqs
+
+
 def main():
     O.build(ref=True)
     geo, ims, fdi = load_reference()
     print("geodesic rows:", geodesic_case(geo))
+    freqs = reference_frequencies(geo)
 
     # 1. Schwarzschild, eccentric, default frequency grid, +/- m
-    inp, tr = S.fd_case(K=77, N=50, span=1e6, seed=21, a=0.0, x=1.0, lmax=3, nmax=5)
+    inp, tr = S.fd_case(K=77, N=50, span=1e6, seed=21, a=0.0, x=1.0, lmax=3, nmax=5, frequencies=freqs)
     wf, freq, cap, lens = run_reference_fd(fdi, ims, inp, tr, inp.T, inp.dt)
     save_fd("fd_schwarzschild.npz", inp, tr, wf, freq, cap, lens)
     print("fd_schwarzschild", wf.shape, float(np.abs(wf).max()))
 
     # 2. Kerr prograde equatorial, user frequency grid (positive-side index rule)
-    inp, tr = S.fd_case(K=66, N=40, span=8e5, seed=22, a=0.6, x=1.0, lmax=3, nmax=4, p_range=(11.0, 6.6))
+    inp, tr = S.fd_case(K=66, N=40, span=8e5, seed=22, a=0.6, x=1.0, lmax=3, nmax=4, p_range=(11.0, 6.6),
+                        frequencies=freqs)
     L = 2 * 40001 + 1
     f_arr = np.hstack((np.arange(-(L // 2), 0), np.arange(0, (L - 1) // 2 + 1))) * (1.0 / (L * 11.0))
     wf, freq, cap, lens = run_reference_fd(fdi, ims, inp, tr, inp.T, inp.dt, f_arr=f_arr)
@@ -207,7 +222,7 @@ def main():
 
     # 3. generic inclined orbit (k != 0 modes), +m only, positive frequencies only
     inp, tr = S.fd_case(K=90, N=36, span=6e5, seed=24, a=0.7, x=0.8, lmax=2, kmax=1, nmax=4,
-                        p_range=(12.0, 8.0), e_range=(0.3, 0.15))
+                        p_range=(12.0, 8.0), e_range=(0.3, 0.15), frequencies=freqs)
     wf, freq, cap, lens = run_reference_fd(fdi, ims, inp, tr, inp.T, inp.dt, include_minus_m=False,
                                            mask_positive=True)
     save_fd("fd_generic_pos.npz", inp, tr, wf, freq, cap, lens, include_minus_m=0, mask_positive=1)

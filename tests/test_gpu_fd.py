@@ -12,8 +12,9 @@ the stationary-phase sum.  Checked here:
   (M, a, p, e, x): relative L2 within the FD tolerances below.  The kernel
   uses CUDA's transcendental functions where the reference uses glibc's;
   Cardano's root formula amplifies those last-place differences in the root
-  time, but the stationary phase is flat at the root, so the waveform moves
-  only at second order;
+  time, but on a self-consistent trajectory (the golden phases are integrals
+  of the reference's frequencies) the phase is stationary at the root, so the
+  waveform moves only at second order;
 * the C ABI drop-in few_get_waveform_fd on the reference's own kernel inputs.
 """
 import os
@@ -28,8 +29,11 @@ from fastemriwaveforms_b200.summation import _ptr
 
 pytestmark = pytest.mark.gpu
 
-REL_GEODESIC = 1e-12   # fundamental frequencies vs the reference (max relative)
-REL_FD = 1e-9          # FD waveform vs the reference, relative L2
+REL_GEODESIC = 1e-11   # fundamental frequencies vs the reference (max relative; near-circular orbits
+                       # lose a few digits to cancellation in both implementations)
+REL_FD = 1e-11         # FD waveform vs the reference given its knot frequencies, relative L2
+REL_FD_E2E = 1e-9      # end to end from (M, a, p, e, x): the geodesic frequencies differ from the
+                       # reference's in the last places, which moves the spline roots
 
 CASES = {
     "fd_schwarzschild": dict(),
@@ -77,7 +81,9 @@ def test_geodesic_frequencies_match_reference(cuda):
     arr = get_fundamental_frequencies(d["a"], d["p"], d["e"], d["x"])
     for q, key in enumerate(("OmegaPhi", "OmegaTheta", "OmegaR")):
         np.testing.assert_allclose(arr[q].cpu().numpy(), d[key], rtol=REL_GEODESIC, atol=0)
-    print(f"\ngeodesic frequencies: {len(errs)} orbits, max relative error {max(errs):.3e}")
+    worst = int(np.argmax(errs))
+    print(f"\ngeodesic frequencies: {len(errs)} orbits, max relative error {max(errs):.3e} at "
+          f"(a, p, e, x) = {tuple(float(d[q][worst]) for q in 'apex')}; median {np.median(errs):.1e}")
     assert max(errs) <= REL_GEODESIC
 
 
@@ -115,7 +121,7 @@ def test_fd_end_to_end_matches_reference(cuda, name):
     starts = fd.seg_start_inds.cpu().numpy().reshape(-1)
     diff = int(np.count_nonzero(starts != d["start_inds"]))
     print(f"\n{name}: FD waveform end to end rel L2 {e:.3e} ({diff} bin starts differ from the reference's)")
-    assert e <= REL_FD
+    assert e <= REL_FD_E2E
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -165,3 +171,32 @@ def test_fd_repeatable_and_errors(cuda):
         bad = list(args)
         bad[11] = np.full(len(d["t"]), 6.0)
         fd(*bad, T=float(d["T"]), dt=float(d["dt"]))
+
+
+def test_fd_matches_fft_of_time_domain(cuda):
+    """The reference's own check (tests/test_fd.py:92-150): on a self-consistent
+    trajectory (phases = integrals of the geodesic frequencies), the FD h+ at
+    positive frequencies overlaps the FFT of the real part of the time-domain
+    waveform to better than 1e-2."""
+    from fastemriwaveforms_b200 import InterpolatedModeSum
+    from fastemriwaveforms_b200 import synthetic as S
+    from fastemriwaveforms_b200.geodesic import MTSUN_SI
+
+    def gpu_freqs(M, a, p, e, x):
+        O = get_fundamental_frequencies(a, p, e, x)
+        den = 2 * np.pi * M * MTSUN_SI
+        return np.stack([np.abs(O[0].cpu().numpy() / den), O[1].cpu().numpy() / den, O[2].cpu().numpy() / den])
+
+    inp, tr = S.fd_case(K=77, N=120, span=4e6, seed=31, a=0.0, x=1.0, lmax=3, nmax=5, p_range=(12.0, 9.0),
+                        e_range=(0.3, 0.2), frequencies=gpu_freqs)
+    td = InterpolatedModeSum(pad_output=True, odd_len=True)
+    h = td(*inp.call_args(), T=inp.T, dt=inp.dt)
+    fd = FDInterpolatedModeSum(pad_output=True)
+    hf = fd(*inp.call_args(), tr.M, tr.a, tr.p, tr.e, tr.xI, T=inp.T, dt=inp.dt)
+    assert hf.shape[1] == h.numel()
+    mask = fd.frequency >= 0.0
+    a = torch.fft.fftshift(torch.fft.fft(h.real))[mask]
+    b = hf[0, mask]
+    ov = (torch.vdot(a, b) / torch.sqrt(torch.vdot(a, a) * torch.vdot(b, b))).real.item()
+    print(f"\nFD vs FFT(TD): 1 - overlap = {1 - ov:.3e}")
+    assert 1 - ov < 1e-2
