@@ -1,6 +1,7 @@
 /*
  * few_oracle.c -- CPU restatement of the FastEMRIWaveforms time-domain
- * interpolated mode sum.
+ * interpolated mode sum, the amplitude grid evaluation and the
+ * frequency-domain (stationary-phase) sum.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is checked
  * against.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
@@ -20,6 +21,7 @@
  *   src/few/cutils/interpolate.cu:444-689  make_waveform (CPU branch)
  *   src/few/cutils/interpolate.cu:694-723  find_start_inds
  *   src/few/cutils/interpolate.cu:726-797  get_waveform
+ *   src/few/cutils/interpolate.cu:1041-1520 SPAFunc, cube_roots, make_generic_kerr_waveform_fd
  *
  * Build with -ffp-contract=off: every a*b+c in the reference source is two
  * rounded operations here, in the order the source writes them.
@@ -388,6 +390,186 @@ void oracle_interp2d(double *z, const double *tx, int nx, const double *ty, int 
                 l1 += nky1;
             }
             z[(size_t)g * m + i] = sp;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Frequency-domain sum (stationary phase)                                   */
+/* ------------------------------------------------------------------------- */
+/* Restates make_generic_kerr_waveform_fd (src/few/cutils/interpolate.cu:
+ * 1141-1520) with its helpers cube_roots (:1113-1133) and SPAFunc
+ * (:1041-1097), and the complex arithmetic of cuda_complex.hpp (C99 Annex G
+ * forms: products without contraction, the quotient with a power-of-two
+ * scaled divisor, principal branches through atan2/hypot).  Inputs in the
+ * reference kernel's layouts: interp (4, 2K+3, N), pc (8, 3, N-1), start/end
+ * (K, N-1), ylms (2K) interleaved with the -m half already times (-1)^l;
+ * wf (L) interleaved, accumulated, visited in the reference's order
+ * (mode, segment, bin, root).  The SPA series coefficients are generated
+ * from their recurrences (the same numbers the reference writes out). */
+
+typedef struct { double re, im; } ocx;
+
+static ocx ocx_mk(double r, double i) { ocx z; z.re = r; z.im = i; return z; }
+static ocx ocx_add(ocx a, ocx b) { return ocx_mk(a.re + b.re, a.im + b.im); }
+static ocx ocx_scale(ocx a, double s) { return ocx_mk(a.re * s, a.im * s); }
+static ocx ocx_divr(ocx a, double s) { return ocx_mk(a.re / s, a.im / s); }
+static ocx ocx_mul(ocx a, ocx b)
+{
+    double ac = a.re * b.re, bd = a.im * b.im, ad = a.re * b.im, bc = a.im * b.re;
+    return ocx_mk(ac - bd, ad + bc);
+}
+static ocx ocx_div(ocx z, ocx w)
+{
+    double a = z.re, b = z.im, c = w.re, d = w.im, lg = logb(fmax(fabs(c), fabs(d)));
+    int sc = 0;
+    if (isfinite(lg)) { sc = (int)lg; c = scalbn(c, -sc); d = scalbn(d, -sc); }
+    double den = c * c + d * d;
+    return ocx_mk(scalbn((a * c + b * d) / den, -sc), scalbn((b * c - a * d) / den, -sc));
+}
+static ocx ocx_polar(double rho, double th)
+{
+    if (isnan(rho) || signbit(rho)) return ocx_mk(NAN, NAN);
+    double x = rho * cos(th), y = rho * sin(th);
+    if (isnan(x)) x = 0.0;
+    if (isnan(y)) y = 0.0;
+    return ocx_mk(x, y);
+}
+static ocx ocx_exp(ocx z) { double e = exp(z.re); return ocx_mk(e * cos(z.im), e * sin(z.im)); }
+static ocx ocx_log(ocx z) { return ocx_mk(log(hypot(z.re, z.im)), atan2(z.im, z.re)); }
+static ocx ocx_sqrt(ocx z)
+{
+    if (isinf(z.im)) return ocx_mk(INFINITY, z.im);
+    return ocx_polar(sqrt(hypot(z.re, z.im)), atan2(z.im, z.re) / 2.0);
+}
+static ocx ocx_powr(ocx z, double p) { return ocx_exp(ocx_mul(ocx_mk(p, 0.0), ocx_log(z))); }
+
+static double spa_s1[14], spa_s2[14], spa_ar[9], spa_ai[9];
+static int spa_ready = 0;
+
+static void spa_init(void)
+{
+    double c1 = 0.5, c2 = 1.0, a = 1.0;
+    for (int j = 0; j < 14; ++j) {
+        spa_s1[j] = c1;
+        spa_s2[j] = c2;
+        c1 = c1 * (-0.25) / ((j + 1) * (j + 4.0 / 3.0));
+        c2 = c2 * (-0.25) / ((j + 1) * (j + 2.0 / 3.0));
+    }
+    for (int j = 0; j < 9; ++j) {
+        int q = (j + 1) & 3;
+        spa_ar[j] = (q == 0) ? a : (q == 2 ? -a : 0.0);
+        spa_ai[j] = (q == 1) ? a : (q == 3 ? -a : 0.0);
+        a = a * (4.0 / 9.0 - (2.0 * j + 1.0) * (2.0 * j + 1.0)) / (8.0 * (j + 1));
+    }
+    spa_ready = 1;
+}
+
+static ocx oracle_spa(double x)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    if (fabs(x) <= 7.0) {
+        ocx e23 = ocx_exp(ocx_divr(ocx_scale(ocx_mk(0.0, 1.0), -2.0 * pi), 3.0));
+        ocx e13 = ocx_exp(ocx_divr(ocx_scale(ocx_mk(0.0, 1.0), -pi), 3.0));
+        ocx p6 = ocx_powr(ocx_mk(x, 0.0), 1.0 / 6.0);
+        ocx q = e23;
+        for (int i = 0; i < 5; ++i) q = ocx_mul(q, p6);
+        ocx pref1 = ocx_divr(ocx_scale(q, -4.062353818279201250), 1.259921049894873165);
+        ocx pref2 = ocx_divr(ocx_scale(ocx_mul(e13, p6), 2.678938534707747633), 1.587401051968199475);
+        double x2 = x * x, s1 = spa_s1[13], s2 = spa_s2[13];
+        for (int j = 12; j >= 0; --j) { s1 = spa_s1[j] + x2 * s1; s2 = spa_s2[j] + x2 * s2; }
+        ocx ph = ocx_exp(ocx_scale(ocx_mk(-0.0, -1.0), x));
+        return ocx_mul(ph, ocx_add(ocx_scale(pref1, s1), ocx_scale(pref2, s2)));
+    }
+    ocx y = ocx_mk(1.0 / x, 0.0);
+    ocx pref = ocx_scale(ocx_exp(ocx_scale(ocx_scale(ocx_mk(-0.0, -1.0), 0.75), pi)), sqrt(0.5 * pi));
+    ocx ser = ocx_mk(spa_ar[8], spa_ai[8]);
+    for (int j = 7; j >= 0; --j) ser = ocx_add(ocx_mk(spa_ar[j], spa_ai[j]), ocx_mul(y, ser));
+    return ocx_mul(pref, ser);
+}
+
+static void oracle_cube_roots(double a, double b, double c, double d, ocx xi, double r[3])
+{
+    double b2 = b * b, b3 = b2 * b, a2 = a * a;
+    double D0 = b2 - 3 * a * c;
+    double D1 = 2 * b3 - 9 * a * b * c + 27 * a2 * d;
+    ocx S = ocx_sqrt(ocx_mk(D1 * D1 - 4 * (D0 * D0 * D0), 0.0));
+    ocx C = ocx_powr(ocx_divr(ocx_mk(S.re + D1, S.im), 2.0), 1.0 / 3.0);
+    double s = -(1.0 / (3 * a));
+    ocx D0c = ocx_mk(D0, 0.0), xC = ocx_mul(xi, C), xxC = ocx_mul(ocx_mul(xi, xi), C);
+    r[0] = ocx_scale(ocx_add(ocx_mk(b + C.re, C.im), ocx_div(D0c, C)), s).re;
+    r[1] = ocx_scale(ocx_add(ocx_mk(b + xC.re, xC.im), ocx_div(D0c, xC)), s).re;
+    r[2] = ocx_scale(ocx_add(ocx_mk(b + xxC.re, xxC.im), ocx_div(D0c, xxC)), s).re;
+}
+
+void oracle_fd_sum(double *wf, const double *interp, const double *phase_t, const double *pc, const int *m_arr,
+                   const int *k_arr, const int *n_arr, int K, const double *t, int N, int L, const double *freq,
+                   const int *start, const int *end, const double *ylms, int zero_index, int include_minus_m)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    if (!spa_ready) spa_init();
+    const long nb = (long)(2 * K + 3) * N, nps = (long)(N - 1) * 3;
+    ocx S3 = ocx_sqrt(ocx_mk(-3.0, 0.0));
+    ocx xi = ocx_divr(ocx_mk(S3.re + -1.0, S3.im), 2.0);
+    for (int mode = 0; mode < K; ++mode) {
+        const int m = m_arr[mode], k = k_arr[mode], n = n_arr[mode];
+        ocx yp = ocx_mk(ylms[2 * mode], ylms[2 * mode + 1]);
+        ocx ym = ocx_mk(ylms[2 * (K + mode)], ylms[2 * (K + mode) + 1]);
+        for (int seg = 0; seg < N - 1; ++seg) {
+            const double ts = t[seg], te = t[seg + 1];
+            const double *re = interp + (long)mode * N + seg, *im = interp + (long)(K + mode) * N + seg;
+            const double *fp = interp + (long)(2 * K) * N + seg, *ft = fp + N, *fr = fp + 2 * N;
+            double fy = m * fp[0] + k * ft[0] + n * fr[0];
+            double fc1 = m * fp[nb] + k * ft[nb] + n * fr[nb];
+            double fc2 = m * fp[2 * nb] + k * ft[2 * nb] + n * fr[2 * nb];
+            double fc3 = m * fp[3 * nb] + k * ft[3 * nb] + n * fr[3 * nb];
+            double h = phase_t[seg + 1] - phase_t[seg], h2 = h * h, h3 = h * h2;
+            int s0 = start[mode * (N - 1) + seg], s1e = end[mode * (N - 1) + seg];
+            for (int i = s0 < 0 ? 0 : s0; i <= s1e && i <= L - 1; ++i) {
+                double f = freq[i], roots[3];
+                oracle_cube_roots(fc3, fc2, fc1, fy - f, xi, roots);
+                for (int r = 0; r < 3; ++r) {
+                    double x = roots[r], tt = ts + x;
+                    if (!(tt < te && tt >= ts)) continue;
+                    double x2 = x * x, x3 = x * x2;
+                    double Rre = re[0] + re[nb] * x + re[2 * nb] * x2 + re[3 * nb] * x3;
+                    double Rim = im[0] + im[nb] * x + im[2 * nb] * x2 + im[3 * nb] * x3;
+                    double s = (tt - phase_t[seg]) / h, sm = 1.0 - s;
+                    double q2 = s * s, q3 = s * q2, q4 = s * q3, q5 = s * q4;
+                    double phase = 0.0, fdot = 0.0, fddot = 0.0;
+                    for (int q = 0; q < 3; ++q) {
+                        const int mult = q == 0 ? m : (q == 1 ? k : n);
+                        const double *c = pc + (long)q * (N - 1) + seg;
+                        double c0 = c[0], c1 = c[nps], c2 = c[2 * nps], c3 = c[3 * nps], c4 = c[4 * nps],
+                               c5 = c[5 * nps], c6 = c[6 * nps], c7 = c[7 * nps];
+                        double P = c0 + s * (c1 + sm * (c2 + s * (c3 + sm * (c4 + s * (c5 + sm * (c6 + s * c7))))));
+                        double d2 = (-2. * c2 + c3 * (2. - 6. * s) + c4 * (2. - 12. * s + 12. * q2) +
+                                     c5 * (6. * s - 24. * q2 + 20. * q3) + c6 * (6. * s - 36. * q2 + 60. * q3 - 30. * q4) +
+                                     c7 * (12. * q2 - 60. * q3 + 90. * q4 - 42. * q5)) / (2. * pi * h2);
+                        double d3 = (-6. * c3 + c4 * (-12. + 24. * s) + c5 * (6. - 48. * s + 60. * q2) +
+                                     c6 * (6. - 72. * s + 180. * q2 - 120. * q3) +
+                                     c7 * (24. * s - 180. * q2 + 360. * q3 - 210. * q4)) / (2. * pi * h3);
+                        if (q == 0) { phase = mult * P; fdot = mult * d2; fddot = mult * d3; }
+                        else { phase += mult * P; fdot += mult * d2; fddot += mult * d3; }
+                    }
+                    double arg = 2. * pi * fdot * fdot * fdot / (3. * fddot * fddot);
+                    double pre = -1.0 * fdot / fabs(fddot) * 2. / sqrt(3.);
+                    ocx amp2 = ocx_div(ocx_scale(oracle_spa(arg), pre), ocx_sqrt(ocx_mk(arg, 0.0)));
+                    double ph = 2. * pi * f * tt - phase;
+                    ocx tex = ocx_mul(ocx_mul(ocx_mk(Rre, Rim), amp2), ocx_exp(ocx_mk(0.0 * ph, ph)));
+                    ocx rt = ocx_mul(yp, tex);
+                    wf[2 * i] += rt.re;
+                    wf[2 * i + 1] += rt.im;
+                    if (m != 0 && include_minus_m) {
+                        int imn = 2 * zero_index - i;
+                        if (imn >= 0 && imn < L) {
+                            ocx lt = ocx_mul(ym, ocx_mk(tex.re, -tex.im));
+                            wf[2 * imn] += lt.re;
+                            wf[2 * imn + 1] += lt.im;
+                        }
+                    }
+                }
+            }
         }
     }
 }

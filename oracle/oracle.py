@@ -1,6 +1,7 @@
 """ctypes front end for the oracle (test infrastructure only).
 
-Two CPU implementations of the reference's time-domain interpolated mode sum:
+Two CPU implementations of the reference's time-domain interpolated mode sum
+(and of its amplitude grid evaluation and frequency-domain sum):
 
 * ``impl="oracle"`` -- ``few_oracle.c``, the C restatement in this folder;
 * ``impl="ref"``    -- the reference's own CPU path
@@ -284,3 +285,137 @@ def interp2d(tx, ty, c, kx: int, ky: int, x, y, impl: str = "oracle") -> np.ndar
         _lib("oracle").oracle_interp2d(_p(z), _p(tx), len(tx), _p(ty), len(ty), _p(c), kx, ky, _p(x), _p(y), m,
                                        ngrid, nc)
     return z
+
+
+# ---------------------------------------------------------------------------
+# Frequency-domain sum (FDInterpolatedModeSum.sum, src/few/summation/fdinterp.py)
+# ---------------------------------------------------------------------------
+
+FD_DENSE_POINTS = 5000  # fdinterp.py:266
+
+
+def fd_frequency_grid(L: int, dt: float) -> np.ndarray:
+    """The default two-sided grid (fdinterp.py:398-403)."""
+    return np.hstack((np.arange(-(L // 2), 0), np.arange(0, (L - 1) // 2 + 1))) / (L * dt)
+
+
+def fd_plan(t, fknots, fcoef, m, k, n, frequency, has_farr: bool):
+    """Bin ranges of every (mode, segment): restates fdinterp.py:262-430.
+
+    fknots (3, N): |f_phi|, f_theta, f_r at the knots; fcoef (4, N, 3): their
+    spline coefficients.  Returns (start, end) int32 (K, N-1) as the reference
+    hands them to its kernel.  Mirrored details: numpy.argmax/argmin on the
+    5000-point dense grid, the Python index -1 for a turnover found at the
+    first knot, and the widening of a turnover segment only when there is
+    exactly one interior turnover (the join of the (n, 2) bounds with the
+    (1, n) turnover row raises the ValueError the reference swallows)."""
+    t = np.asarray(t, dtype=np.float64)
+    m, k, n = (np.asarray(v, dtype=np.int64) for v in (m, k, n))
+    N = len(t)
+    tn = np.linspace(t.min(), t.max(), FD_DENSE_POINTS)
+    dense = spline_eval(t, fcoef, tn)                                   # (3, D)
+    knot = m[:, None] * fknots[0][None] + k[:, None] * fknots[1][None] + n[:, None] * fknots[2][None]
+    bounds = np.sort(np.stack([knot[:, :-1], knot[:, 1:]], axis=-1), axis=-1)   # (K, N-1, 2)
+    per_mode = m[:, None] * dense[0][None] + k[:, None] * dense[1][None] + n[:, None] * dense[2][None]
+    turns = []
+    for extreme in (per_mode.argmax(axis=-1), per_mode.argmin(axis=-1)):
+        t_ext = tn[extreme]
+        modes = np.where((t_ext > 0.0) & (t_ext < t[-1]))[0]
+        segs = np.searchsorted(t, t_ext[modes]) - 1
+        turns.extend(zip(modes.tolist(), segs.tolist()))
+    if turns:
+        modes = np.array([q[0] for q in turns])
+        segs = np.array([q[1] for q in turns])
+        cf = [m[modes] * fcoef[c][segs, 0] + k[modes] * fcoef[c][segs, 1] + n[modes] * fcoef[c][segs, 2]
+              for c in range(4)]
+        d, c, b, a = cf
+        disc = (2 * b) ** 2 - 4 * (3 * a) * c
+        if np.any(disc < -1e10):
+            raise ValueError("turnover discriminant below -1e10")
+        disc[disc < 0.0] = 0.0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r1 = (-(2 * b) + np.sqrt(disc)) / (2 * (3 * a))
+            r2 = (-(2 * b) - np.sqrt(disc)) / (2 * (3 * a))
+        tr1, tr2 = t[segs] + r1, t[segs] + r2
+        keep1 = (t[segs] < tr1) & (t[segs + 1] > tr1)
+        keep2 = (t[segs] < tr2) & (t[segs + 1] > tr2)
+        if np.any(keep1 & keep2):
+            raise ValueError("a turnover segment holds both roots")
+        if np.any(keep1 | keep2) and len(turns) == 1:
+            x = tr1 * keep1 + tr2 * keep2 - t[segs]
+            f_ext = a * x ** 3 + b * x ** 2 + c * x + d
+            three = np.sort(np.concatenate([bounds[modes, segs], f_ext[:, None]], axis=-1), axis=-1)
+            bounds[modes, segs] = three[:, [0, 2]]
+    f0 = frequency[0]
+    df = frequency[1] - frequency[0]
+    idx = np.abs((bounds - f0) / df).astype(int)
+    if has_farr:
+        z = int(np.where(frequency == 0.0)[0][0])
+        pos = bounds > 0.0
+        idx[pos] = (np.abs((bounds - frequency[z + 1]) / df).astype(int) + z + 1)[pos]
+    return (idx[..., 0] + 1).astype(np.int32), idx[..., 1].astype(np.int32)
+
+
+def fd_kernel(interp, phase_t, pc_kernel, m, k, n, t, frequency, start, end, ylms_signed, zero_index: int,
+              include_minus_m: bool, impl: str = "oracle") -> np.ndarray:
+    """The stationary-phase kernel on the reference's kernel inputs: few_oracle.c's
+    restatement (impl="oracle") or the reference's get_waveform_generic_fd
+    (impl="ref").  Returns the two-sided sum (L,) complex."""
+    K, N, L = len(m), len(t), len(frequency)
+    wf = np.zeros(L, dtype=np.complex128)
+    a = dict(interp=np.ascontiguousarray(interp, dtype=np.float64).reshape(-1),
+             pt=np.ascontiguousarray(phase_t, dtype=np.float64), pc=np.ascontiguousarray(pc_kernel).reshape(-1),
+             m=np.ascontiguousarray(m, dtype=np.int32), k=np.ascontiguousarray(k, dtype=np.int32),
+             n=np.ascontiguousarray(n, dtype=np.int32), t=np.ascontiguousarray(t, dtype=np.float64),
+             f=np.ascontiguousarray(frequency, dtype=np.float64),
+             s=np.ascontiguousarray(start, dtype=np.int32).reshape(-1),
+             e=np.ascontiguousarray(end, dtype=np.int32).reshape(-1),
+             y=np.ascontiguousarray(ylms_signed, dtype=np.complex128))
+    lib = _lib(impl)
+    if impl == "oracle":
+        fn = lib.oracle_fd_sum
+        fn.restype = None
+        fn(wf.ctypes.data_as(_dp), _p(a["interp"]), _p(a["pt"]), _p(a["pc"]), _p(a["m"], _ip), _p(a["k"], _ip),
+           _p(a["n"], _ip), ctypes.c_int(K), _p(a["t"]), ctypes.c_int(N), ctypes.c_int(L), _p(a["f"]),
+           _p(a["s"], _ip), _p(a["e"], _ip), a["y"].ctypes.data_as(_dp), ctypes.c_int(zero_index),
+           ctypes.c_int(int(include_minus_m)))
+    else:
+        fn = lib.few_ref_get_waveform_fd
+        fn.restype = None
+        fn(wf.ctypes.data_as(ctypes.c_void_p), _p(a["interp"]), _p(a["pt"]), _p(a["pc"]), _p(a["m"], _ip),
+           _p(a["k"], _ip), _p(a["n"], _ip), ctypes.c_int(K), ctypes.c_double(0.0), _p(a["t"]), ctypes.c_int(N),
+           ctypes.c_int(L), _p(a["f"]), _p(a["s"], _ip), _p(a["e"], _ip), ctypes.c_int(N - 1),
+           a["y"].ctypes.data_as(ctypes.c_void_p), ctypes.c_int(zero_index), ctypes.c_int(int(include_minus_m)),
+           ctypes.c_int(0))
+    return wf
+
+
+def fd_finalize(w: np.ndarray, frequency: np.ndarray, mask_positive: bool) -> np.ndarray:
+    """(h+, hx) from the two-sided sum (fdinterp.py:518-536)."""
+    s = -np.flip(w)
+    p = np.real(s + np.flip(s)) / 2.0 + 1j * np.imag(s - np.flip(s)) / 2.0
+    c = -np.imag(s + np.flip(s)) / 2.0 + 1j * np.real(s - np.flip(s)) / 2.0
+    if mask_positive:
+        keep = frequency >= 0.0
+        return np.vstack((p[keep], c[keep]))
+    return np.vstack((p, c))
+
+
+def fd_sum(inp, fknots, L: int | None = None, f_arr=None, include_minus_m: bool = True,
+           mask_positive: bool = False, impl: str = "oracle"):
+    """The whole FD sum on the CPU from the trajectory's knot frequencies
+    (3, N) in Hz: splines (the reference's interpolate_arrays layout), bin
+    plan, kernel, (h+, hx).  Returns (waveform, frequency, start, end)."""
+    K = inp.teuk_modes.shape[1]
+    y_all = np.concatenate([inp.teuk_modes.T.real, inp.teuk_modes.T.imag, np.asarray(fknots)], axis=0)
+    interp = interpolate_arrays(inp.t, y_all, impl="oracle" if impl == "oracle" else "ref")   # (4, 2K+3, N)
+    fcoef = np.ascontiguousarray(np.transpose(interp[:, 2 * K:], (0, 2, 1)))                 # (4, N, 3)
+    frequency = np.asarray(f_arr, dtype=np.float64) if f_arr is not None else fd_frequency_grid(L, inp.dt)
+    start, end = fd_plan(inp.t, np.asarray(fknots), fcoef, inp.m, inp.k, inp.n, frequency, f_arr is not None)
+    pc_kernel = np.transpose(np.asarray(inp.phase_coeffs, dtype=np.float64), (2, 1, 0))      # (8, 3, N-1)
+    ylms = np.array(inp.ylms, dtype=np.complex128, copy=True)
+    ylms[K:] *= (-1) ** np.asarray(inp.l)
+    zero_index = int(np.where(frequency == 0.0)[0][0])
+    w = fd_kernel(interp, inp.phase_t, pc_kernel, inp.m, inp.k, inp.n, inp.t, frequency, start, end, ylms,
+                  zero_index, include_minus_m, impl=impl)
+    return fd_finalize(w, frequency, mask_positive), frequency, start, end
