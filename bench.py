@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=256,
                     help="waveforms of the uneven batch (T ~ logU[1e5, 3.15e6], N ~ U[50, 2000], K ~ U[200, 3843])")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-fd", action="store_true", help="skip the frequency-domain sum measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
     ap.add_argument("--profile-form", choices=["forward", "fwd_bwd"], default="forward",
@@ -501,6 +502,95 @@ def bench_amplitude(dev, steps: int, pk, pk_kind, cpu: bool):
     return entry
 
 
+def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
+    """Frequency-domain sum (FDInterpolatedModeSum): one year at dt = 10 s,
+    3843 modes (l = 2..10, m = 0..l, n = -30..30), 1000 knots, M = 1e6,
+    a = 0.5 prograde equatorial, p 12 -> 7.4, e 0.4 -> 0.2, phases integrated
+    from the geodesic frequencies.  Device time of the whole call (geodesic
+    frequencies, splines, plan, sum, (h+, hx)) with inputs in HBM, the sum
+    kernel alone, the end-to-end call from host arrays with the (2, L) result
+    copied back, and the reference's CPU kernel on a sample of the modes."""
+    import time
+
+    import torch
+
+    from fastemriwaveforms_b200 import FDInterpolatedModeSum, get_fundamental_frequencies
+    from fastemriwaveforms_b200 import synthetic as S
+    from fastemriwaveforms_b200.geodesic import MTSUN_SI
+
+    def gpu_freqs(M, a, p, e, x):
+        o = get_fundamental_frequencies(a, p, e, x)
+        den = 2 * np.pi * M * MTSUN_SI
+        return np.stack([np.abs(o[0].cpu().numpy() / den), o[1].cpu().numpy() / den, o[2].cpu().numpy() / den])
+
+    inp, tr = S.fd_full(frequencies=gpu_freqs)
+    host_args = inp.call_args() + (tr.M, tr.a, tr.p, tr.e, tr.xI)
+    dev_args = tuple(torch.tensor(np.ascontiguousarray(v), device=dev) if isinstance(v, np.ndarray) else v
+                     for v in host_args)
+    fd = FDInterpolatedModeSum(pad_output=True)
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    for _ in range(2):
+        fd(*dev_args, T=inp.T, dt=inp.dt)
+    torch.cuda.synchronize()
+    n = max(steps, 3)
+    call_ms, sum_ms = [], []
+    for _ in range(n):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        fd.sum_events = ev
+        a.record()
+        out = fd(*dev_args, T=inp.T, dt=inp.dt)
+        b.record()
+        torch.cuda.synchronize()
+        call_ms.append(a.elapsed_time(b))
+        sum_ms.append(ev[0].elapsed_time(ev[1]))
+    fd.sum_events = None
+    bins = int(fd.total_bins.item())
+    L = out.shape[1]
+    # end to end: host inputs in, (2, L) waveform out to host
+    e2e_ms = []
+    for _ in range(n):
+        a = time.perf_counter()
+        h = fd(*host_args, T=inp.T, dt=inp.dt).cpu()
+        e2e_ms.append((time.perf_counter() - a) * 1e3)
+    h2d = sum(v.nbytes for v in host_args if isinstance(v, np.ndarray))
+    ms, kms, ems = float(np.median(call_ms)), float(np.median(sum_ms)), float(np.median(e2e_ms))
+    entry = {"workload": "one year at dt=10 s, K=3843 (l=2..10, m=0..l, n=-30..30), N=1000 knots, "
+                         f"M=1e6, a=0.5 prograde equatorial; L={L} frequency bins, {bins} (mode, bin) evaluations",
+             "ms": ms, "sum_kernel_ms": kms, "value": bins / (kms * 1e-3), "unit": "mode-bins/s (sum kernel)",
+             "call_value": bins / (ms * 1e-3),
+             "e2e": {"ms": ems, "value": bins / (ems * 1e-3), "unit": "mode-bins/s", "h2d_bytes_per_step": int(h2d),
+                     "d2h_bytes_per_step": int(h.numel() * 16)},
+             "fp64_peak_tflops": fp64_tflops}
+    if cpu:
+        from oracle import oracle as O
+
+        if O.have_ref():
+            # the reference's get_waveform_generic_fd (single core) on the first Ks modes, with this
+            # run's own bin plan and the reference's spline of those modes' amplitudes + frequencies
+            Ks = 40
+            fk = gpu_freqs(tr.M, tr.a, tr.p, tr.e, tr.xI)
+            y = np.concatenate([inp.teuk_modes[:, :Ks].T.real, inp.teuk_modes[:, :Ks].T.imag, fk], axis=0)
+            interp = O.interpolate_arrays(inp.t, y, impl="ref")
+            s32 = fd.seg_start_inds[:Ks].cpu().numpy()
+            e32 = fd.seg_end_inds[:Ks].cpu().numpy()
+            freq = fd.frequency.cpu().numpy()
+            lo = np.clip(s32.astype(np.int64), 0, None)
+            hi = np.clip(e32.astype(np.int64), None, len(freq) - 1)
+            sample_bins = int(np.clip(hi - lo + 1, 0, None).sum())
+            pc = np.transpose(inp.phase_coeffs, (2, 1, 0))
+            yl = np.concatenate([inp.ylms[:Ks], inp.ylms[3843:3843 + Ks] * (-1.0) ** inp.l[:Ks]])
+            t0 = time.perf_counter()
+            O.fd_kernel(interp, inp.phase_t, pc, inp.m[:Ks], inp.k[:Ks], inp.n[:Ks], inp.t, freq, s32, e32, yl,
+                        L // 2, True, impl="ref")
+            dt = time.perf_counter() - t0
+            entry["cpu_baseline"] = {"value": sample_bins / dt, "unit": "mode-bins/s", "cores": 1,
+                                     "kind": "reference",
+                                     "sample": f"the reference's FD kernel on the first {Ks} modes: {sample_bins} "
+                                               f"(mode, bin) evaluations in {dt:.1f} s"}
+    return entry
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -679,6 +769,8 @@ def main():
 
     batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
     amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
+    fdsum = None if args.no_fd else bench_fd(dev, args.steps, fp64_tflops,
+                                             cpu=(rank == 0 and not args.no_cpu_baseline))
 
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
@@ -715,7 +807,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "cpu_baseline": cpu, "clocks": clk,
+            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "fd": fdsum, "cpu_baseline": cpu, "clocks": clk,
             "device": torch.cuda.get_device_name(dev)}
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -77,7 +77,7 @@ SIGNATURES = {
     "few_fd_scan": [_vp, _c_ll, _vp, _vp],
     "few_fd_frequency_grid": [_vp, _c_int, _c_dbl, _vp],
     "few_fd_sum": [_vp, _c_int, _vp, _c_int, _c_int, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll,
-                   _c_ll, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp],
+                   _c_ll, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _vp],
     "few_fd_finalize": [_vp, _c_int, _c_int, _c_int, _vp, _vp],
     "few_get_waveform_fd": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_dbl, _vp, _c_int, _c_int, _vp, _vp, _vp,
                             _c_int, _vp, _c_int, _c_int, _c_int, _vp],

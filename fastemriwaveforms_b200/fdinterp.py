@@ -47,6 +47,12 @@ class FDInterpolatedModeSum(SummationBase):
         kw = {k: v for k, v in kwargs.items() if k in ("pad_output", "odd_len")}
         SummationBase.__init__(self, output_type="fd", device=device, **kw)
         self.frequency = None
+        # optional (start, end) torch.cuda.Events recorded around the sum kernel
+        self.sum_events = None
+        # launch shape of the sum kernel (few_fd_sum): grid CTAs (0: 16 per SM) and
+        # the register budget (resident CTAs per SM, 0: the default)
+        self.sum_blocks = 0
+        self.sum_ctas_per_sm = 0
 
     def sum(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, M, a, p, e,
             xI, *args, include_minus_m=True, separate_modes=False, dt=10.0, f_arr=None, mask_positive=False,
@@ -166,9 +172,14 @@ class FDInterpolatedModeSum(SummationBase):
 
         # 5. the sum and (h+, hx)
         wf = torch.zeros(L, dtype=torch.complex128, device=dev)
+        if self.sum_events is not None:
+            self.sum_events[0].record()
         _lib.call("few_fd_sum", _ptr(wf), L, _ptr(self.frequency), zero_index, int(bool(include_minus_m)), _ptr(amp),
                   N * 2 * K, 1, 2 * K, _ptr(fco), 3 * N, 1, 3, _ptr(pc), 1, 8, 24, _ptr(pt), _ptr(t_d), N, _ptr(m_d),
-                  _ptr(k_d), _ptr(n_d), K, _ptr(y_d), _ptr(lo), _ptr(prefix), 0, st)
+                  _ptr(k_d), _ptr(n_d), K, _ptr(y_d), _ptr(lo), _ptr(prefix), self.sum_blocks, self.sum_ctas_per_sm, st)
+        if self.sum_events is not None:
+            self.sum_events[1].record()
+        self.total_bins = prefix[E]  # device scalar: bins the sum visited
         first, cnt = (first_pos, npos) if mask_positive else (0, L)
         out = torch.empty((2, cnt), dtype=torch.complex128, device=dev)
         _lib.call("few_fd_finalize", _ptr(wf), L, first, cnt, _ptr(out), st)

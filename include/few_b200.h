@@ -439,14 +439,16 @@ FEW_API int few_fd_frequency_grid(double *f, int L, double Ldt, void *stream);
  * f_theta, f_r) fco[q*fq + p*fp + j*fj]; phase coefficient c (0..7) of field
  * (Phi_phi, Phi_theta, Phi_r) on segment s is pc[c*pcc + field*pcf + s*pcs].
  * ylms [device] (2K) complex, the -m half already times (-1)^l.  lo, prefix
- * [device] from few_fd_plan_bins / few_fd_scan.  blocks <= 0 picks the
- * default grid.  Accumulation is by FP64 atomics: sums are reproducible to
- * rounding, not bit for bit. */
+ * [device] from few_fd_plan_bins / few_fd_scan.  blocks: CTAs of 256 threads
+ * (<= 0: 32 per SM); ctas_per_sm: the register budget the kernel is built for
+ * (1, 2 or 3 resident CTAs per SM; <= 0: 2).  Accumulation is by FP64
+ * atomics: sums are reproducible to rounding, not bit for bit. */
 FEW_API int few_fd_sum(void *wf, int L, const double *freq, int zero_index, int include_minus_m, const double *amp,
                        long long aq, long long ap, long long aj, const double *fco, long long fq, long long fp,
                        long long fj, const double *pc, long long pcc, long long pcf, long long pcs,
                        const double *phase_t, const double *t, int N, const int *m, const int *k, const int *n, int K,
-                       const void *ylms, const int *lo, const long long *prefix, int blocks, void *stream);
+                       const void *ylms, const int *lo, const long long *prefix, int blocks, int ctas_per_sm,
+                       void *stream);
 
 /* (h+, hx) from the two-sided sum (fdinterp.py:518-536): out [device]
  * (2, count) complex, rows h+ and hx at bins first .. first+count-1. */
