@@ -74,7 +74,7 @@ SIGNATURES = {
                             _vp],
     "few_fd_plan_bins": [_vp, _vp, _vp, _vp, _c_int, _c_int, _vp, _vp, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
                          _vp, _vp, _vp, _vp, _vp],
-    "few_fd_scan": [_vp, _c_ll, _vp, _vp],
+    "few_fd_scan": [_vp, _c_ll, _vp, _vp, _vp],
     "few_fd_frequency_grid": [_vp, _c_int, _c_dbl, _vp],
     "few_fd_sum": [_vp, _c_int, _vp, _c_int, _c_int, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll,
                    _c_ll, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _vp],

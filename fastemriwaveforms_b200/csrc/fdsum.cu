@@ -601,31 +601,78 @@ __global__ void k_fd_range(const int *__restrict__ start32, const int *__restric
     }
 }
 
-// Exclusive prefix of count (E,) into prefix (E + 1,), one block of 1024
-// threads: each thread sums a contiguous run, the run totals are scanned in
-// shared memory, then each thread writes its run's prefixes.
-__global__ void __launch_bounds__(1024) k_fd_scan(const long long *__restrict__ count, long long E,
-                                                  long long *__restrict__ prefix) {
-    __shared__ long long s_tot[1024];
-    const int tid = threadIdx.x, T = blockDim.x;
-    const long long per = (E + T - 1) / T;
-    const long long b0 = per * tid < E ? per * tid : E, b1 = per * (tid + 1) < E ? per * (tid + 1) : E;
-    long long sum = 0;
-    for (long long e = b0; e < b1; ++e) sum += count[e];
-    s_tot[tid] = sum;
+// Exclusive prefix of count (E,) into prefix (E + 1,) in three launches over
+// G contiguous chunks: the chunk totals, their scan (one CTA), then each
+// chunk's own scan offset by its chunk's prefix, in tiles of 256 x 4 counts.
+constexpr int kScanThreads = 256, kScanPer = 4, kScanMaxChunks = 1024;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long *s_warp, long long *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    long long x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
     __syncthreads();
-    for (int off = 1; off < T; off <<= 1) {  // inclusive Hillis-Steele scan of the run totals
-        long long v = tid >= off ? s_tot[tid - off] : 0;
-        __syncthreads();
-        s_tot[tid] += v;
-        __syncthreads();
+    if (w == 0) {
+        long long t = lane < nw ? s_warp[lane] : 0;
+        for (int off = 1; off < 32; off <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, t, off);
+            if (lane >= off) t += y;
+        }
+        if (lane < nw) s_warp[lane] = t;  // inclusive warp totals
     }
-    long long run = tid > 0 ? s_tot[tid - 1] : 0;
-    for (long long e = b0; e < b1; ++e) {
-        prefix[e] = run;
-        run += count[e];
+    __syncthreads();
+    long long before = (w > 0 ? s_warp[w - 1] : 0) + x - v;
+    *total = s_warp[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_fd_scan_totals(const long long *__restrict__ count, long long E,
+                                                                 long long chunk, long long *__restrict__ totals) {
+    __shared__ long long s_warp[32];
+    const long long c0 = blockIdx.x * chunk, c1 = c0 + chunk < E ? c0 + chunk : E;
+    long long sum = 0;
+    for (long long e = c0 + threadIdx.x; e < c1; e += blockDim.x) sum += count[e];
+    long long tot;
+    block_exclusive_scan(sum, s_warp, &tot);
+    if (threadIdx.x == 0) totals[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanMaxChunks) k_fd_scan_chunks(long long *__restrict__ totals, int G,
+                                                                  long long *__restrict__ prefix, long long E) {
+    __shared__ long long s_warp[32];
+    long long v = threadIdx.x < G ? totals[threadIdx.x] : 0, tot;
+    long long before = block_exclusive_scan(v, s_warp, &tot);
+    if (threadIdx.x < G) totals[threadIdx.x] = before;
+    if (threadIdx.x == 0) prefix[E] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_fd_scan_write(const long long *__restrict__ count, long long E,
+                                                                long long chunk, const long long *__restrict__ offs,
+                                                                long long *__restrict__ prefix) {
+    __shared__ long long s_warp[32];
+    const long long c0 = blockIdx.x * chunk, c1 = c0 + chunk < E ? c0 + chunk : E;
+    long long run = offs[blockIdx.x];
+    for (long long base = c0; base < c1; base += (long long)kScanThreads * kScanPer) {
+        const long long e0 = base + (long long)threadIdx.x * kScanPer;
+        long long v[kScanPer], sum = 0;
+#pragma unroll
+        for (int j = 0; j < kScanPer; ++j) {
+            v[j] = e0 + j < c1 ? count[e0 + j] : 0;
+            sum += v[j];
+        }
+        long long tot;
+        long long p = run + block_exclusive_scan(sum, s_warp, &tot);
+#pragma unroll
+        for (int j = 0; j < kScanPer; ++j) {
+            if (e0 + j < c1) prefix[e0 + j] = p;
+            p += v[j];
+        }
+        run += tot;
     }
-    if (tid == T - 1) prefix[E] = s_tot[T - 1];
 }
 
 }  // namespace fd
@@ -743,14 +790,31 @@ extern "C" FEW_API int few_fd_frequency_grid(double *f, int L, double Ldt, void 
     return FEW_OK;
 }
 
-extern "C" FEW_API int few_fd_scan(const long long *count, long long E, long long *prefix, void *stream) {
-    few::clear_error();
-    if (E < 0) return few::fail(FEW_ERR_SIZE, "few_fd_scan: E=%lld", E);
-    if (!count || !prefix) return few::fail(FEW_ERR_ARG, "few_fd_scan: null pointer");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    few::fd::k_fd_scan<<<1, 1024, 0, st>>>(count, E, prefix);
+namespace few {
+namespace fd {
+
+// prefix (E + 1) of count (E); scratch holds kScanMaxChunks long longs.
+static int launch_scan(const long long *count, long long E, long long *prefix, long long *scratch, cudaStream_t st) {
+    long long G = (E + 4095) / 4096;  // at least 4096 counts a chunk
+    if (G < 1) G = 1;
+    if (G > kScanMaxChunks) G = kScanMaxChunks;
+    const long long chunk = (E + G - 1) / G > 0 ? (E + G - 1) / G : 1;
+    k_fd_scan_totals<<<(int)G, kScanThreads, 0, st>>>(count, E, chunk, scratch);
+    k_fd_scan_chunks<<<1, kScanMaxChunks, 0, st>>>(scratch, (int)G, prefix, E);
+    k_fd_scan_write<<<(int)G, kScanThreads, 0, st>>>(count, E, chunk, scratch, prefix);
     FEW_LAUNCH_CHECK("k_fd_scan");
     return FEW_OK;
+}
+
+}  // namespace fd
+}  // namespace few
+
+extern "C" FEW_API int few_fd_scan(const long long *count, long long E, long long *prefix, long long *scratch,
+                                   void *stream) {
+    few::clear_error();
+    if (E < 0) return few::fail(FEW_ERR_SIZE, "few_fd_scan: E=%lld", E);
+    if (!count || !prefix || !scratch) return few::fail(FEW_ERR_ARG, "few_fd_scan: null pointer");
+    return few::fd::launch_scan(count, E, prefix, scratch, static_cast<cudaStream_t>(stream));
 }
 
 // Drop-in for get_waveform_generic_fd (interpolate.hh:33-38, interpolate.cu:1525-1563)
@@ -781,22 +845,20 @@ extern "C" FEW_API int few_get_waveform_fd(void *waveform, const double *interp_
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long E = (long long)K * (N - 1);
     void *buf = nullptr;
-    size_t bytes = (size_t)E * sizeof(int) + (size_t)(2 * E + 1) * sizeof(long long) + 64;
+    size_t bytes = (size_t)E * sizeof(int) + (size_t)(2 * E + 1 + few::fd::kScanMaxChunks) * sizeof(long long) + 64;
     FEW_CUDA_TRY(cudaMallocAsync(&buf, bytes, st));
     long long *count = static_cast<long long *>(buf);
     long long *prefix = count + E;
-    int *lo = reinterpret_cast<int *>(prefix + E + 1);
+    long long *scratch = prefix + E + 1;
+    int *lo = reinterpret_cast<int *>(scratch + few::fd::kScanMaxChunks);
     int blocks = (int)((E + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     few::fd::k_fd_range<<<blocks, 256, 0, st>>>(seg_start_inds, seg_end_inds, E, L, lo, count);
     cudaError_t e1 = cudaGetLastError();
-    if (e1 == cudaSuccess) {
-        few::fd::k_fd_scan<<<1, 1024, 0, st>>>(count, E, prefix);
-        e1 = cudaGetLastError();
-    }
     int status = FEW_OK;
     if (e1 != cudaSuccess) {
         status = few::fail(FEW_ERR_CUDA, "few_get_waveform_fd: launch failed: %s", cudaGetErrorString(e1));
+    } else if ((status = few::fd::launch_scan(count, E, prefix, scratch, st)) != FEW_OK) {
     } else {
         const long long ns = 2LL * K + 3;
         status = few_fd_sum(waveform, L, frequencies, zero_index, include_minus_m, interp_array, ns * N, N, 1,

@@ -166,8 +166,8 @@ class FDInterpolatedModeSum(SummationBase):
         count = torch.empty(E, dtype=torch.int64, device=dev)
         _lib.call("few_fd_plan_bins", _ptr(fk), _ptr(m_d), _ptr(k_d), _ptr(n_d), K, N, _ptr(turns), _ptr(status),
                   f0, df, has_farr, fpos1, zero_index, L, _ptr(start32), _ptr(end32), _ptr(lo), _ptr(count), st)
-        prefix = torch.empty(E + 1, dtype=torch.int64, device=dev)
-        _lib.call("few_fd_scan", _ptr(count), E, _ptr(prefix), st)
+        prefix = torch.empty(E + 1 + 1024, dtype=torch.int64, device=dev)  # prefix, then the scan's scratch
+        _lib.call("few_fd_scan", _ptr(count), E, _ptr(prefix), _ptr(prefix[E + 1:]), st)
         self.seg_start_inds, self.seg_end_inds = start32.view(K, N - 1), end32.view(K, N - 1)
 
         # 5. the sum and (h+, hx)

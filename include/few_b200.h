@@ -424,8 +424,9 @@ FEW_API int few_fd_plan_bins(const double *fknots, const int *m, const int *k, c
                              int zero_index, int L, int *start32, int *end32, int *lo, long long *count,
                              void *stream);
 
-/* prefix [device] (E+1,) = exclusive prefix sums of count [device] (E,). */
-FEW_API int few_fd_scan(const long long *count, long long E, long long *prefix, void *stream);
+/* prefix [device] (E+1,) = exclusive prefix sums of count [device] (E,);
+ * scratch [device] 1024 long longs. */
+FEW_API int few_fd_scan(const long long *count, long long E, long long *prefix, long long *scratch, void *stream);
 
 /* f [device] (L,) = the default two-sided grid (j - L/2) / Ldt, Ldt = L*dt
  * (fdinterp.py:398-403). */
