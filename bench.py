@@ -54,8 +54,11 @@ def parse():
     ap.add_argument("--no-fd", action="store_true", help="skip the frequency-domain sum measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
-    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd"], default="forward",
-                    help="with --profile: forward calls, or forward+backward through autograd")
+    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd"], default="forward",
+                    help="with --profile: forward calls, forward+backward through autograd, or the "
+                         "frequency-domain sum")
+    ap.add_argument("--fd-modes", type=int, default=3843,
+                    help="with --profile-form fd: the first modes of the one-year FD trajectory")
     return ap.parse_args()
 
 
@@ -630,6 +633,22 @@ def main():
     call_args = (inp.t, teuk_d, ylms_d, inp.phase_t, pc_d, inp.l, inp.m, inp.k, inp.n)
 
     if args.profile:
+        if args.profile_form == "fd":
+            # the frequency-domain sum on the one-year trajectory, first --fd-modes modes
+            from fastemriwaveforms_b200 import FDInterpolatedModeSum
+            from fastemriwaveforms_b200 import synthetic as S
+
+            fin, ftr = S.fd_full()
+            Kf = min(args.fd_modes, fin.num_modes)
+            sel = np.r_[0:Kf, fin.num_modes:fin.num_modes + Kf]
+            fargs = (fin.t, np.ascontiguousarray(fin.teuk_modes[:, :Kf]), fin.ylms[sel], fin.phase_t,
+                     fin.phase_coeffs, fin.l[:Kf], fin.m[:Kf], fin.k[:Kf], fin.n[:Kf], ftr.M, ftr.a, ftr.p, ftr.e,
+                     ftr.xI)
+            fd = FDInterpolatedModeSum(pad_output=True)
+            for _ in range(args.warmup + args.steps):
+                fd(*fargs, T=fin.T, dt=fin.dt)
+            torch.cuda.synchronize()
+            return 0
         if args.profile_form == "fwd_bwd":
             time_fwd_bwd(args.precision, inp, dev, args.steps, args.warmup)
         else:
