@@ -8,8 +8,10 @@ kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
 from .amplitude import AmpInterp2D
 from .fdinterp import FDInterpolatedModeSum
 from .geodesic import get_fundamental_frequencies
+from .modeselector import ModeSelector
 from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBase
 from .utility import get_mismatch, get_overlap
+from .ylm import GetYlms
 
-__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "InterpolatedModeSum", "SummationBase",
-           "get_fundamental_frequencies", "get_mismatch", "get_overlap"]
+__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "GetYlms", "InterpolatedModeSum",
+           "ModeSelector", "SummationBase", "get_fundamental_frequencies", "get_mismatch", "get_overlap"]

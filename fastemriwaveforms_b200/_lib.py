@@ -79,6 +79,9 @@ SIGNATURES = {
     "few_fd_sum": [_vp, _c_int, _vp, _c_int, _c_int, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll, _c_ll, _c_ll, _vp, _c_ll,
                    _c_ll, _c_ll, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _vp],
     "few_fd_finalize": [_vp, _c_int, _c_int, _c_int, _vp, _vp],
+    "few_ylm": [_vp, _vp, _c_int, _c_int, _c_dbl, _c_dbl, _vp, _vp, _vp],
+    "few_mode_snr2": [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp],
+    "few_mode_keep": [_vp, _c_int, _c_dbl, _vp, _vp],
     "few_get_waveform_fd": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_dbl, _vp, _c_int, _c_int, _vp, _vp, _vp,
                             _c_int, _vp, _c_int, _c_int, _c_int, _vp],
 }

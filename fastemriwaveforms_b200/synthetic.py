@@ -409,3 +409,46 @@ def fd_full(seed: int = 23, frequencies=None):
     p 12 -> 7.4, e 0.4 -> 0.2."""
     return fd_case(K=3843, N=1000, span=3.15e7, seed=seed, a=0.5, x=1.0, lmax=10, kmax=0, nmax=30,
                    frequencies=frequencies, name="fd_full")
+
+
+class FixedAmplitudes:
+    """A stand-in amplitude generator for ``ModeSelector``: seeded amplitudes
+    (N, K) on the mode list of the reference's amplitude modules
+    (``src/few/utils/baseclasses.py:205-330``: l = 2..lmax, m = 0..l,
+    k = -kmax..kmax, n = -nmax..nmax, ordered m = 0 first), with the mode
+    bookkeeping attributes ModeSelector reads (``l_arr_no_mask`` ...,
+    ``unique_l``, ``unique_m``, ``inverse_lm``, ``index_map_arr`` with Python's
+    wrap-around for negative m, k, n).  The amplitude magnitudes fall off with
+    l and |n| so that a power threshold keeps a strict subset."""
+
+    def __init__(self, lmax: int = 4, kmax: int = 0, nmax: int = 6, N: int = 60, seed: int = 41):
+        md = [(l, m, k, n) for l in range(2, lmax + 1) for m in range(0, l + 1)
+              for k in range(-kmax, kmax + 1) for n in range(-nmax, nmax + 1)]
+        md = np.asarray(md, dtype=np.int32)
+        order = np.concatenate([np.where(md[:, 1] == 0)[0], np.where(md[:, 1] != 0)[0]])
+        md = md[order]
+        self.l_arr_no_mask, self.m_arr_no_mask, self.k_arr_no_mask, self.n_arr_no_mask = (
+            np.ascontiguousarray(md[:, i]) for i in range(4))
+        nz = self.m_arr_no_mask != 0
+        self.l_arr = np.concatenate([self.l_arr_no_mask, self.l_arr_no_mask[nz]])
+        self.m_arr = np.concatenate([self.m_arr_no_mask, -self.m_arr_no_mask[nz]])
+        self.k_arr = np.concatenate([self.k_arr_no_mask, self.k_arr_no_mask[nz]])
+        self.n_arr = np.concatenate([self.n_arr_no_mask, self.n_arr_no_mask[nz]])
+        temp, self.inverse_lm = np.unique(np.asarray([self.l_arr, self.m_arr]).T, axis=0, return_inverse=True)
+        self.inverse_lm = self.inverse_lm.reshape(-1)
+        self.unique_l, self.unique_m = np.asarray(temp).T
+        self.index_map_arr = np.full((lmax + 1, 2 * lmax + 1, 2 * kmax + 1, 2 * nmax + 1), -1, dtype=np.int32)
+        for i, (l, m, k, n) in enumerate(zip(self.l_arr, self.m_arr, self.k_arr, self.n_arr)):
+            self.index_map_arr[l, m, k, n] = i
+        rng = np.random.default_rng(seed)
+        K = len(md)
+        mag = np.exp(-np.abs(self.n_arr_no_mask) / 1.5) / self.l_arr_no_mask.astype(np.float64) ** 3
+        amp = (rng.standard_normal(K) + 1j * rng.standard_normal(K)) * mag
+        s = np.linspace(0.0, 1.0, N)
+        self.teuk = np.ascontiguousarray(amp[None, :] * (1.0 + 0.6 * s[:, None])
+                                         * np.exp(1j * rng.uniform(0, 2, K)[None, :] * s[:, None]))
+
+    def __call__(self, a, p, e, xI, specific_modes=None):
+        if specific_modes is None:
+            return self.teuk
+        return self.teuk[:, np.asarray(specific_modes)]

@@ -469,6 +469,32 @@ FEW_API int few_get_waveform_fd(void *waveform, const double *interp_array, cons
                                 int include_minus_m, int separate_modes, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Harmonics and mode selection (the producers of ylms and the mode list)   */
+/* ------------------------------------------------------------------------ */
+
+/* -2 spin-weighted spherical harmonics (GetYlms, src/few/utils/ylm.py:278-365):
+ * out [device] (n,) complex = Y_{l[i], m[i]}(theta, phi) for l, m [device]
+ * (n,) int; with include_minus_m != 0, out holds 2n values, the second half
+ * Y_{l[i], -m[i]}.  Requires 2 <= l <= 64, |m| <= l; other entries give NaN and
+ * OR 1 into status [device] int (may be NULL). */
+FEW_API int few_ylm(const int *l, const int *m, int n, int include_minus_m, double theta, double phi, void *out,
+                    int *status, void *stream);
+
+/* Per-mode power estimate of ModeSelector's threshold form
+ * (src/few/utils/modeselector.py:393-423): teuk [device] (N, K) complex,
+ * ylms [device] complex, minus_index [device] (K,) int: the ylms index of mode
+ * j's -m harmonic or -1 (m = 0), psd [device] (N, K) or NULL, t [device]
+ * (N,).  snr2 [device] (K,) = sum_{n<N-1} (|A Y|^2 + |conj(A) Y^-|^2) / psd
+ * * (t[n+1] - t[n]), summed in knot order. */
+FEW_API int few_mode_snr2(const void *teuk, int N, int K, const void *ylms, const int *minus_index,
+                          const double *psd, const double *t, double *snr2, void *stream);
+
+/* The keep rule (modeselector.py:428-434) on estimates sorted descending:
+ * keep [device] (K,) int, keep[0] = 1, keep[i] = cumsum[i-1] < total
+ * (1 - threshold)^2, with the cumulative sum taken in order. */
+FEW_API int few_mode_keep(const double *sorted_desc, int K, double threshold, int *keep, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */
 

@@ -1,5 +1,6 @@
-"""Generates the frequency-domain golden vectors (tests/golden/fd_*.npz and
-geodesic_frequencies.npz) from the reference itself.
+"""Generates the frequency-domain golden vectors (tests/golden/fd_*.npz,
+geodesic_frequencies.npz) and the spin-weighted harmonics (ylm.npz) from the
+reference itself.
 
 The reference's Python modules for this path are imported from its sources
 with stand-ins for the packages this image lacks: ``numba`` (njit and
@@ -10,6 +11,9 @@ defines them).  The rest runs unmodified:
 
 * ``get_fundamental_frequencies`` (src/few/utils/geodesic.py:470-535) with
   the elliptic integrals of src/few/utils/elliptic.py;
+* the -2 spin-weighted harmonics of ``GetYlms`` (src/few/utils/ylm.py:17-276)
+  and the selections of ``ModeSelector`` (src/few/utils/modeselector.py:252-490)
+  on a fixed-amplitude generator;
 * ``FDInterpolatedModeSum.sum`` (src/few/summation/fdinterp.py:138-542) with
   the reference's ``CubicSplineInterpolant`` (interpolatedmodesum.py:12-257),
   whose native ``interpolate_arrays`` and ``get_waveform_generic_fd`` are the
@@ -199,10 +203,53 @@ def reference_frequencies(geo):
     return freqs
 
 
+def ylm_case():
+    """The reference's GetYlms kernel (src/few/utils/ylm.py:17-276) for every
+    (l, m), l = 2..10, at viewing angles including the poles."""
+    ylm = _load("few.utils.ylm", os.path.join(REF, "utils/ylm.py"))
+    ls = np.array([l for l in range(2, 11) for m in range(-l, l + 1)], dtype=np.int32)
+    ms = np.array([m for l in range(2, 11) for m in range(-l, l + 1)], dtype=np.int32)
+    angles = np.array([(0.0, 0.0), (np.pi / 3, np.pi / 4), (1.1, -2.3), (np.pi / 2, 0.7), (2.9, 5.5),
+                       (np.pi, 1.0), (1e-3, 0.2)])
+    out = np.zeros((len(angles), len(ls)), dtype=np.complex128)
+    for i, (th, ph) in enumerate(angles):
+        out[i] = ylm._ylm_kernel(np.zeros(len(ls), dtype=np.complex128), ls, ms, th, ph)
+    np.savez_compressed(os.path.join(HERE, "ylm.npz"), l=ls, m=ms, angles=angles, ylm=out)
+    return out.shape
+
+
+def modeselector_case():
+    """The reference's ModeSelector (src/few/utils/modeselector.py:14-490) on a
+    fixed-amplitude generator: the threshold form at two thresholds, the 'all'
+    form and a list of modes (its amplitude generator and trajectory imports
+    stubbed; GetYlms is the reference's)."""
+    _module("few.trajectory")
+    _module("few.trajectory.inspiral", EMRIInspiral=object)
+    _load("few.utils.ylm", os.path.join(REF, "utils/ylm.py"))
+    ms_mod = _load("few.utils.modeselector", os.path.join(REF, "utils/modeselector.py"))
+    gen = S.FixedAmplitudes()
+    t = np.sort(np.random.default_rng(5).uniform(0, 1e6, gen.teuk.shape[0]))
+    sel = ms_mod.ModeSelector(gen)
+    out = {"t": t}
+    for tag, thr in (("thr5", 1e-5), ("thr2", 1e-2)):
+        r = sel(t, 0.5, None, None, None, 1.1, 0.7, mode_selection_threshold=thr, return_sort_inds=True)
+        for name, v in zip(("teuk", "ylms", "l", "m", "k", "n", "inv"), r):
+            out[f"{tag}_{name}"] = np.asarray(v)
+    r = sel(t, 0.5, None, None, None, 0.4, 2.0, mode_selection="all")
+    out["all_ylms"] = np.asarray(r[1])
+    modes = [(2, 2, 0, 0), (3, 1, 0, -2), (4, 0, 0, 3)]
+    r = sel(t, 0.5, None, None, None, 0.4, 2.0, mode_selection=modes)
+    out["list_teuk"], out["list_ylms"] = np.asarray(r[0]), np.asarray(r[1])
+    np.savez_compressed(os.path.join(HERE, "modeselector.npz"), **out)
+    return {k: v.shape for k, v in out.items() if k.endswith("_l")}
+
+
 def main():
     O.build(ref=True)
     geo, ims, fdi = load_reference()
     print("geodesic rows:", geodesic_case(geo))
+    print("ylm:", ylm_case())
+    print("modeselector:", modeselector_case())
     freqs = reference_frequencies(geo)
 
     # 1. Schwarzschild, eccentric, default frequency grid, +/- m
