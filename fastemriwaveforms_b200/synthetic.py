@@ -451,4 +451,6 @@ class FixedAmplitudes:
     def __call__(self, a, p, e, xI, specific_modes=None):
         if specific_modes is None:
             return self.teuk
+        if hasattr(specific_modes, "cpu"):  # a torch tensor (the GPU ModeSelector passes device indices)
+            specific_modes = specific_modes.cpu().numpy()
         return self.teuk[:, np.asarray(specific_modes)]
