@@ -5,6 +5,7 @@ Drop-in for ``few.summation.interpolatedmodesum.InterpolatedModeSum`` and its
 ``get_fundamental_frequencies`` and ``AmpInterp2D``): Python host code over hand-written sm_100a CUDA
 kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
 """
+from .aakwave import AAKSummation
 from .amplitude import AmpInterp2D
 from .fdinterp import FDInterpolatedModeSum
 from .geodesic import get_fundamental_frequencies
@@ -13,5 +14,5 @@ from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBas
 from .utility import get_mismatch, get_overlap
 from .ylm import GetYlms
 
-__all__ = ["AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "GetYlms", "InterpolatedModeSum",
+__all__ = ["AAKSummation", "AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "GetYlms", "InterpolatedModeSum",
            "ModeSelector", "SummationBase", "get_fundamental_frequencies", "get_mismatch", "get_overlap"]

@@ -454,3 +454,52 @@ class FixedAmplitudes:
         if hasattr(specific_modes, "cpu"):  # a torch tensor (the GPU ModeSelector passes device indices)
             specific_modes = specific_modes.cpu().numpy()
         return self.teuk[:, np.asarray(specific_modes)]
+
+
+@dataclass
+class AAKInputs:
+    """Arguments of ``AAKSummation.__call__`` (aakwave.py:35-60) for one waveform."""
+
+    t: np.ndarray              # (N,) knot times (tvec and interp_t)
+    interp_coeffs: np.ndarray  # (N-1, 6, 8): (p, e, Y, Phi_phi, Phi_theta, Phi_r) in the 8-term basis
+    m1: float
+    a: float
+    dist: float
+    m2: float
+    qS: float
+    phiS: float
+    qK: float
+    phiK: float
+    nmodes: int
+    dt: float
+    T: float
+
+    def call_args(self):
+        return (self.t, self.m1, self.a, self.dist, self.m2, self.qS, self.phiS, self.qK, self.phiK, self.nmodes,
+                self.t, self.interp_coeffs)
+
+
+def aak_case(N: int = 60, span: float = 1e6, seed: int = 51, e_range=(0.6, 0.35), Y: float = 0.7,
+             nmodes: int | None = None, dt: float = 10.0, a: float = 0.6, f0: float = 1.5e-3) -> AAKInputs:
+    """A seeded AAK trajectory: p 12 -> 8, e and Y smooth, phases from the
+    closed-form chirp (Phi_theta and Phi_r slightly slower than Phi_phi, so the
+    precession angles grow), all as not-a-knot cubics in the 8-term basis.
+    nmodes defaults to the reference's rule int(30 e0) (src/few/waveform/base.py:596)."""
+    rng = np.random.default_rng(seed)
+    t = knot_times(rng, N, span, 0.099 * span / (N - 1))
+    u = t / span
+    p = 12.0 - 4.0 * u ** 1.2
+    e = e_range[0] + (e_range[1] - e_range[0]) * u
+    Yv = Y + 0.02 * np.sin(3 * u)
+    w = 1.0 - t / (1.3 * span)
+    phi = 2.0 * np.pi * f0 * 1.3 * span * 1.6 * (1.0 - w ** 0.625)
+    knots = np.stack([p, e, Yv, phi, 0.995 * phi, 0.97 * phi])
+    coeffs = np.zeros((N - 1, 6, 8))
+    h = np.diff(t)
+    for q in range(6):
+        y0, c1, c2, c3 = not_a_knot_coeffs(t, knots[q])
+        coeffs[:, q, :] = cubic_to_basis(y0, c1, c2, c3, h)
+    if nmodes is None:
+        nmodes = int(30 * e_range[0])
+    return AAKInputs(t=t, interp_coeffs=coeffs, m1=1e6, a=a, dist=1.0, m2=10.0, qS=0.8, phiS=1.9, qK=2.1,
+                     phiK=0.4, nmodes=nmodes, dt=dt, T=(span + dt) / YRSID_SI)

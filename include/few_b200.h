@@ -495,6 +495,23 @@ FEW_API int few_mode_snr2(const void *teuk, int N, int K, const void *ylms, cons
 FEW_API int few_mode_keep(const double *sorted_desc, int K, double threshold, int *keep, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* AAK summation (AAKSummation, src/few/summation/aakwave.py:12-196)         */
+/* ------------------------------------------------------------------------ */
+
+/* Drop-in for get_waveform of src/few/cutils/gpuAAK.hh:6-10 (kernel
+ * gpuAAK.cu:181-482): waveform [device] (out_len,) complex, hI - i hII on the
+ * samples the trajectory covers (segment j owns [ceil(t_j/dt), ceil(t_j+1/dt))
+ * up to T = (out_len-1) dt, as gpuAAK.cu:495-519); interp_array [device]
+ * (8, init_len-1, 6) = dense-output coefficients of (p, e, Y, Phi_phi,
+ * Phi_theta, Phi_r); h_t [host] (init_len,).  Plus the stream; returns after
+ * the kernel has finished (the reference synchronises too).  A trajectory
+ * that ends before T leaves the later samples untouched (the reference reads
+ * past its arrays there). */
+FEW_API int few_aak_waveform(void *waveform, const double *interp_array, double M_phys, double S_phys, double mu,
+                             double qS, double phiS, double qK, double phiK, double dist, int nmodes, int mich,
+                             int init_len, int out_len, double delta_t, const double *h_t, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */
 

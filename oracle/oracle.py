@@ -419,3 +419,156 @@ def fd_sum(inp, fknots, L: int | None = None, f_arr=None, include_minus_m: bool 
     w = fd_kernel(interp, inp.phase_t, pc_kernel, inp.m, inp.k, inp.n, inp.t, frequency, start, end, ylms,
                   zero_index, include_minus_m, impl=impl)
     return fd_finalize(w, frequency, mask_positive), frequency, start, end
+
+
+# ---------------------------------------------------------------------------
+# AAK summation (AAKSummation.sum, src/few/summation/aakwave.py; kernel gpuAAK.cu)
+# ---------------------------------------------------------------------------
+
+_GPCINSEC = 1.02927125054339e+17     # global.h:26
+_AUSEC = 499.00478383615643          # global.h:27
+_MTSUN = 4.9254909491978065e-06      # global.h:24
+_YRSID = 31558149.763545595          # global.h:23
+
+
+def aak_segments(h_t, out_len: int, dt: float):
+    """First sample of each trajectory segment (gpuAAK.cu:495-519): ceil(t_j/dt)
+    while t_j < T = (out_len-1) dt, then out_len at the first knot past T."""
+    T = (out_len - 1) * dt
+    first = [0]
+    for tt in h_t[1:]:
+        if tt < T:
+            first.append(int(np.ceil(tt / dt)))
+        else:
+            first.append(out_len)
+            break
+    return np.array(first, dtype=np.int64)
+
+
+def aak_waveform(interp_t, interp_coeffs, M, S, mu, qS, phiS, qK, phiK, dist, nmodes: int, mich: bool,
+                 out_len: int, dt: float, impl: str = "numpy") -> np.ndarray:
+    """The AAK waveform (out_len,) complex: restated in numpy with scipy's
+    Bessel functions (impl="numpy", restates gpuAAK.cu:181-482), or the
+    reference's own CPU kernel (impl="ref", whose Bessel functions are the
+    Numerical Recipes approximations).  interp_coeffs (N-1, 6, 8) as
+    AAKSummation.sum receives them (after its |Y| == 1 substitution)."""
+    interp_t = np.ascontiguousarray(interp_t, dtype=np.float64)
+    N = len(interp_t)
+    kernel_layout = np.ascontiguousarray(np.transpose(np.asarray(interp_coeffs, dtype=np.float64), (2, 0, 1)))
+    wf = np.zeros(out_len, dtype=np.complex128)
+    if impl == "ref":
+        fn = _lib("ref").few_ref_aak_waveform
+        fn.restype = None
+        fn(wf.ctypes.data_as(ctypes.c_void_p), _p(kernel_layout.reshape(-1)), ctypes.c_double(M), ctypes.c_double(S),
+           ctypes.c_double(mu), ctypes.c_double(qS), ctypes.c_double(phiS), ctypes.c_double(qK), ctypes.c_double(phiK),
+           ctypes.c_double(dist), ctypes.c_int(nmodes), ctypes.c_int(int(mich)), ctypes.c_int(N),
+           ctypes.c_int(out_len), ctypes.c_double(dt), _p(interp_t))
+        return wf
+    from scipy.special import jv
+
+    first = aak_segments(interp_t, out_len, dt)
+    nseg = len(first) - 1
+    idx = np.arange(first[0], first[-1])
+    seg = np.searchsorted(first, idx, side="right") - 1
+    seg = np.clip(seg, 0, nseg - 1)
+    c = np.asarray(interp_coeffs, dtype=np.float64)[seg]          # (ns, 6, 8)
+    t = dt * idx
+    h = interp_t[seg + 1] - interp_t[seg]
+    s = (t - interp_t[seg]) / h
+    s1 = 1.0 - s
+
+    def nested(q):
+        cc = c[:, q]
+        return cc[:, 0] + s * (cc[:, 1] + s1 * (cc[:, 2] + s * (cc[:, 3] + s1 * (cc[:, 4] + s * (cc[:, 5] + s1 * (
+            cc[:, 6] + s * cc[:, 7]))))))
+
+    def deriv(q):
+        cc = c[:, q]
+        s2, s3, s4, s5, s6 = s * s, s ** 3, s ** 4, s ** 5, s ** 6
+        return (cc[:, 1] + cc[:, 2] * (1. - 2. * s) + cc[:, 3] * (2. * s - 3. * s2)
+                + cc[:, 4] * (2. * s - 6. * s2 + 4. * s3) + cc[:, 5] * (3. * s2 - 8. * s3 + 5. * s4)
+                + cc[:, 6] * (3. * s2 - 12. * s3 + 15 * s4 - 6. * s5)
+                + cc[:, 7] * (4. * s3 - 15. * s4 + 18. * s5 - 7. * s6)) / h
+
+    fill = 1e-6
+    qS = min(max(qS, fill), np.pi - fill)
+    qK = min(max(qK, fill), np.pi - fill)
+    cosqS, sinqS, cosqK, sinqK = np.cos(qS), np.sin(qS), np.cos(qK), np.sin(qK)
+    cosphiK, sinphiK = np.cos(phiK), np.sin(phiK)
+    halfsqrt3 = np.sqrt(3.) / 2.
+    zeta = mu * _MTSUN / dist / _GPCINSEC
+    e, Y = nested(1), nested(2)
+    Pphi, Pth, Pr = nested(3), nested(4), nested(5)
+    Ophi, Oth, Or = deriv(3), deriv(4), deriv(5)
+    Phi, gim, alp = Pr, Pth - Pr, Pphi - Pth
+    nu, gimdot = Or / (2. * np.pi), Oth - Or
+    lam = np.arccos(Y)
+    coslam, sinlam, cosalp, sinalp = np.cos(lam), np.sin(lam), np.cos(alp), np.sin(alp)
+    cosqL = cosqK * coslam + sinqK * sinlam * cosalp
+    sinqL = np.sqrt(1. - cosqL * cosqL)
+    up = sinqK * sinphiK * coslam - cosphiK * sinlam * sinalp - cosqK * sinphiK * sinlam * cosalp
+    down = sinqK * cosphiK * coslam + sinphiK * sinlam * sinalp - cosqK * cosphiK * sinlam * cosalp
+    phiL = np.arctan2(up, down)
+    Ldotn = cosqL * cosqS + sinqL * sinqS * np.cos(phiL - phiS)
+    Ldotn2 = Ldotn * Ldotn
+    Sdotn = cosqK * cosqS + sinqK * sinqS * np.cos(phiK - phiS)
+    bup = -Sdotn + coslam * Ldotn
+    bdown = sinqS * np.sin(phiK - phiS) * sinlam * cosalp + (cosqK * Sdotn - cosqS) / sinqK * sinlam * sinalp
+    beta = np.where((S == 0.0) | (lam < 1e-10) | (lam > np.pi - 1e-10), 0.0, np.arctan2(bup, bdown))
+    gam = 2. * (gim + beta)
+    cos2gam, sin2gam = np.cos(gam), np.sin(gam)
+    if mich:
+        orb = 2. * np.pi * t / _YRSID
+        cosorb, sinorb = np.cos(orb - phiS), np.sin(orb - phiS)
+        cosq = .5 * cosqS - halfsqrt3 * sinqS * cosorb
+        phiw = orb + np.arctan2(halfsqrt3 * cosqS + .5 * sinqS * cosorb, sinqS * sinorb)
+        psiup = .5 * cosqK - halfsqrt3 * sinqK * np.cos(orb - phiK) - cosq * (cosqK * cosqS + sinqK * sinqS * np.cos(phiK - phiS))
+        psidown = (.5 * sinqK * sinqS * np.sin(phiK - phiS)
+                   - halfsqrt3 * np.cos(orb) * (cosqK * sinqS * np.sin(phiS) - cosqS * sinqK * np.sin(phiK))
+                   - halfsqrt3 * np.sin(orb) * (cosqS * sinqK * np.cos(phiK) - cosqK * sinqS * np.cos(phiS)))
+        psi = np.arctan2(psiup, psidown)
+        cosq1 = .5 * (1. + cosq * cosq)
+        c2phi, s2phi, c2psi, s2psi = np.cos(2. * phiw), np.sin(2. * phiw), np.cos(2. * psi), np.sin(2. * psi)
+        FpI = cosq1 * c2phi * c2psi - cosq * s2phi * s2psi
+        FcI = cosq1 * c2phi * s2psi + cosq * s2phi * c2psi
+        FpII = cosq1 * s2phi * c2psi + cosq * c2phi * s2psi
+        FcII = cosq1 * s2phi * s2psi - cosq * c2phi * c2psi
+    else:
+        FpI, FcI, FpII, FcII = 1.0, 0.0, 0.0, 1.0
+    Amp = (np.abs(Ophi) * M * _MTSUN) ** (2. / 3.) * zeta
+    # polarisation rotation (gpuAAK.cu:141-177)
+    nv = np.array([np.sin(qS) * np.cos(phiS), np.sin(qS) * np.sin(phiS), np.cos(qS)])
+    Sv = np.array([np.sin(qK) * np.cos(phiK), np.sin(qK) * np.sin(phiK), np.cos(qK)])
+    ci, si = np.cos(lam), np.sin(lam)
+    Lv = np.stack([ci * np.sin(qK) * np.cos(phiK) + si * (sinalp * np.sin(phiK) - cosalp * np.cos(qK) * np.cos(phiK)),
+                   ci * np.sin(qK) * np.sin(phiK) - si * (sinalp * np.cos(phiK) + cosalp * np.cos(qK) * np.sin(phiK)),
+                   ci * np.cos(qK) + si * cosalp * np.sin(qK)], axis=1)
+    nxL = np.cross(np.broadcast_to(nv, Lv.shape), Lv)
+    nxS = np.cross(nv, Sv)
+    norm = np.linalg.norm(nxL, axis=1) * np.linalg.norm(nxS)
+    norm = np.where(norm < 1e-6, 1e-6, norm)
+    cosrot = (nxL @ nxS) / norm
+    sinrot = (Lv @ nxS - nxL @ Sv) / norm
+    rot0, rot1 = 2. * cosrot * cosrot - 1., cosrot * sinrot
+    rot2, rot3 = -rot1, rot0
+    hI = np.zeros_like(t)
+    hII = np.zeros_like(t)
+    for n in range(1, nmodes + 1):
+        if mich:
+            fn = n * nu + gimdot / np.pi
+            nPhi = n * Phi + 2. * np.pi * fn * _AUSEC * sinqS * cosorb
+        else:
+            nPhi = n * Phi
+        x = n * e
+        J0, J1, J2, J3, J4 = (jv(n - 2 + q, x) for q in range(5))
+        a = -n * Amp * (J0 - 2. * e * J1 + 2. / n * J2 + 2. * e * J3 - J4) * np.cos(nPhi)
+        b = -n * Amp * np.sqrt(1 - e * e) * (J0 - 2. * J2 + J4) * np.sin(nPhi)
+        cc = 2. * Amp * J2 * np.cos(nPhi)
+        Ap0 = -(1. + Ldotn2) * (a * cos2gam - b * sin2gam) + cc * (1 - Ldotn2)
+        Ac0 = 2. * Ldotn * (b * cos2gam + a * sin2gam)
+        Ap, Ac = Ap0 * rot0 + Ac0 * rot1, Ap0 * rot2 + Ac0 * rot3
+        scale = halfsqrt3 if mich else 1.0
+        hI += scale * (FpI * Ap + FcI * Ac)
+        hII += scale * (FpII * Ap + FcII * Ac)
+    wf[idx] = hI - 1j * hII
+    return wf

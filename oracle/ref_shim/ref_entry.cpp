@@ -1,11 +1,25 @@
 // C-linkage entry points into the reference's own CPU implementation
-// (src/few/cutils/interpolate.hh:27-38, AmpInterp2D.hh:6-8), so the oracle tests can call it
+// (src/few/cutils/interpolate.hh:27-38, AmpInterp2D.hh:6-8, gpuAAK.hh:6-10), so the oracle tests can call it
 // through ctypes.  Built only by oracle/Makefile into oracle/_ref; test
 // infrastructure, never part of the product path.
 #include "AmpInterp2D.hh"
 #include "interpolate.hh"
 
+// gpuAAK.cu's get_waveform (gpuAAK.hh:6-10), compiled under the name aak_get_waveform
+void aak_get_waveform(cmplx *waveform, double *interp_array, double M_phys, double S_phys, double mu, double qS,
+                      double phiS, double qK, double phiK, double dist, int nmodes, bool mich, int init_len,
+                      int out_len, double delta_t, double *h_t);
+
 extern "C" {
+
+void few_ref_aak_waveform(void *waveform, double *interp_array, double M_phys, double S_phys, double mu, double qS,
+                          double phiS, double qK, double phiK, double dist, int nmodes, int mich, int init_len,
+                          int out_len, double delta_t, double *h_t)
+{
+    aak_get_waveform((cmplx *)waveform, interp_array, M_phys, S_phys, mu, qS, phiS, qK, phiK, dist, nmodes,
+                     mich != 0, init_len, out_len, delta_t, h_t);
+}
+
 
 void few_ref_interpolate_arrays(double *t_arr, double *interp_array, int ninterps, int length,
                                 double *B, double *upper_diag, double *diag, double *lower_diag)

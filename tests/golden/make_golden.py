@@ -10,6 +10,7 @@ tests here restate as well.
 
     python tests/golden/make_golden.py                    (needs the reference sources)
     python tests/golden/make_golden.py --only amplitude   (the amplitude case alone)
+    python tests/golden/make_golden.py --only aak         (the AAK case alone)
 """
 from __future__ import annotations
 
@@ -59,10 +60,26 @@ def amplitude_case():
     np.savez_compressed(os.path.join(HERE, "amp_interp2d.npz"), **out)
 
 
+def aak_case():
+    """The reference's AAK kernel (gpuAAK.cu, CPU path) on a seeded trajectory
+    (synthetic.aak_case), plain and with the long-wavelength response."""
+    inp = S.aak_case(N=40, span=3e5)
+    L = int(inp.t[-1] / inp.dt) + 1
+    out = dict(t=inp.t, interp_coeffs=inp.interp_coeffs, L=L)
+    for mich in (0, 1):
+        out[f"wf_mich{mich}"] = O.aak_waveform(inp.t, inp.interp_coeffs, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS,
+                                               inp.qK, inp.phiK, inp.dist, inp.nmodes, bool(mich), L, inp.dt,
+                                               impl="ref")
+    np.savez_compressed(os.path.join(HERE, "aak_ref.npz"), **out)
+
+
 def main(only=None):
     O.build(ref=True)
     if only == "amplitude":
         amplitude_case()
+        return
+    if only == "aak":
+        aak_case()
         return
     rng = np.random.default_rng(2024)
 
@@ -107,6 +124,7 @@ def main(only=None):
                         norm=np.linalg.norm(wf), sum=wf.sum(), out_len=len(wf),
                         digest=inputs_digest(inp), seed=inp.seed)
     amplitude_case()
+    aak_case()
     print("golden vectors written to", HERE)
 
 

@@ -137,3 +137,24 @@ def test_fd_oracle_matches_reference_golden(oracle, name):
     if oracle.have_ref():  # the reference's kernel behind the restated plan reproduces the golden exactly
         wf_ref, *_ = oracle.fd_sum(inp, d["fknots"], impl="ref", **kw)
         assert np.array_equal(wf_ref, d["waveform"])
+
+
+def test_aak_oracle_matches_reference_golden(oracle):
+    """The AAK restatement (numpy, scipy's Bessel functions) against the
+    reference's own AAK kernel (golden vectors from its CPU path): the
+    difference is the reference's Numerical Recipes Bessel approximations
+    (~1e-7 of the waveform); the reference build reproduces its golden file."""
+    d = np.load(os.path.join(GOLDEN, "aak_ref.npz"))
+    inp = S.aak_case(N=40, span=3e5)
+    assert np.array_equal(inp.interp_coeffs, d["interp_coeffs"])
+    L = int(d["L"])
+    for mich in (0, 1):
+        ref = d[f"wf_mich{mich}"]
+        got = oracle.aak_waveform(inp.t, inp.interp_coeffs, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, inp.qK,
+                                  inp.phiK, inp.dist, inp.nmodes, bool(mich), L, inp.dt)
+        e = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert e <= 3e-7, e
+        if oracle.have_ref():
+            again = oracle.aak_waveform(inp.t, inp.interp_coeffs, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, inp.qK,
+                                        inp.phiK, inp.dist, inp.nmodes, bool(mich), L, inp.dt, impl="ref")
+            assert np.array_equal(again, ref)
