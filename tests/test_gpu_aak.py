@@ -58,11 +58,11 @@ def test_aak_equatorial_poles_and_short_trajectory(cuda, oracle):
     got = run(inp, False)
     c = inp.interp_coeffs.copy()
     c[:, 4] = c[:, 3]
-    want = oracle.aak_waveform(inp.t, c, inp.m1, inp.a, inp.m2, 1e-6 if inp.qS < 1e-6 else inp.qS, inp.phiS, 1e-6,
-                               inp.phiK, inp.dist, inp.nmodes, False, len(got), inp.dt)
+    want = oracle.aak_waveform(inp.t, c, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, 0.0, inp.phiK, inp.dist,
+                               inp.nmodes, False, len(got), inp.dt)  # the oracle applies the same pole shift
     assert rel(got, want) <= REL_ORACLE
     assert inp.interp_coeffs[0, 4, 1] != inp.interp_coeffs[0, 3, 1]  # the caller's array is untouched
     # observation longer than the trajectory (pad_output): samples past the last knot are zero
     long = run(S.aak_case(N=30, span=2e5, seed=54), False, T=3e5 / S.YRSID_SI, pad=True)
-    last = int(np.ceil(2e5 / 10.0))
+    last = int(2e5 / 10.0) + 1  # num_pts: the samples up to the last knot
     assert len(long) > last and np.all(long[last:] == 0) and np.all(long[:last] != 0)
