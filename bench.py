@@ -52,6 +52,7 @@ def parse():
                     help="waveforms of the uneven batch (T ~ logU[1e5, 3.15e6], N ~ U[50, 2000], K ~ U[200, 3843])")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="skip the frequency-domain sum measurement")
+    ap.add_argument("--no-aak", action="store_true", help="skip the AAK summation measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
     ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd"], default="forward",
@@ -594,6 +595,53 @@ def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
     return entry
 
 
+def bench_aak(dev, steps: int, cpu: bool):
+    """AAK summation (AAKSummation): one year at dt = 10 s (3,150,001 samples),
+    a 1000-knot trajectory with e 0.6 -> 0.35, 18 harmonics (the reference's
+    int(30 e0)); device time of the call with the coefficients in HBM, and the
+    reference's CPU AAK kernel on the first 20,000 samples."""
+    import time
+
+    import torch
+
+    from fastemriwaveforms_b200 import AAKSummation
+    from fastemriwaveforms_b200 import synthetic as S
+
+    inp = S.aak_case(N=1000, span=3.15e7, seed=55)
+    args = list(inp.call_args())
+    args[11] = torch.tensor(inp.interp_coeffs, device=dev)
+    aak = AAKSummation()
+    for _ in range(2):
+        out = aak(*args, T=inp.T, dt=inp.dt)
+    torch.cuda.synchronize()
+    n = max(steps, 3)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(n):
+        out = aak(*args, T=inp.T, dt=inp.dt)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / n
+    L = out.numel()
+    entry = {"workload": f"one year at dt=10 s: {L} samples, N={len(inp.t)} knots, {inp.nmodes} harmonics, "
+                         "plain polarisations (mich=False)",
+             "ms": ms, "value": L / (ms * 1e-3), "unit": "samples/s",
+             "harmonic_value": L * inp.nmodes / (ms * 1e-3)}
+    if cpu:
+        from oracle import oracle as O
+
+        if O.have_ref():
+            Ls = 20000
+            t0 = time.perf_counter()
+            O.aak_waveform(inp.t, inp.interp_coeffs, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, inp.qK, inp.phiK,
+                           inp.dist, inp.nmodes, False, Ls, inp.dt, impl="ref")
+            dt = time.perf_counter() - t0
+            entry["cpu_baseline"] = {"value": Ls / dt, "unit": "samples/s", "cores": 1, "kind": "reference",
+                                     "sample": f"the reference's AAK kernel on the first {Ls} samples ({dt:.2f} s)"}
+    return entry
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -790,6 +838,7 @@ def main():
     amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
     fdsum = None if args.no_fd else bench_fd(dev, args.steps, fp64_tflops,
                                              cpu=(rank == 0 and not args.no_cpu_baseline))
+    aakw = None if args.no_aak else bench_aak(dev, args.steps, cpu=(rank == 0 and not args.no_cpu_baseline))
 
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
@@ -826,7 +875,7 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
             "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "fd": fdsum, "cpu_baseline": cpu, "clocks": clk,
+            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "fd": fdsum, "aak": aakw, "cpu_baseline": cpu, "clocks": clk,
             "device": torch.cuda.get_device_name(dev)}
     print(json.dumps(line), flush=True)
     if world > 1:
