@@ -67,8 +67,10 @@ __device__ void bessel_band(int n, double x, double J[5]) {
     double Jm1 = 0.0;  // b_1, for J_{-1} = -J_1
     double got[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int k = M; k >= 1; --k) {
-        // b holds b_k, bp holds b_{k+1}
-        if (k <= n + 2 && k >= n - 2) got[k - (n - 2)] = b;
+        // b holds b_k, bp holds b_{k+1}; constant indices keep got[] in registers
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            if (k == n - 2 + q) got[q] = b;
         if ((k & 1) == 0) sum += b;
         double bm = k * tox * b - bp;  // b_{k-1}
         bp = b;
@@ -83,11 +85,76 @@ __device__ void bessel_band(int n, double x, double J[5]) {
     }
     // b = b_0, bp = b_1
     Jm1 = bp;
-    if (n - 2 <= 0) got[0 - (n - 2)] = b;  // k = 0 lies in the band when n <= 2
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+        if (n - 2 + q == 0) got[q] = b;  // k = 0 lies in the band when n <= 2
     const double norm = b + 2.0 * sum;
 #pragma unroll
     for (int q = 0; q < 5; ++q) J[q] = got[q] / norm;
     if (n == 1) J[0] = -Jm1 / norm;  // J_{-1} = -J_1
+}
+
+// bessel_band for two harmonics at once (n and n + 1 at x1 = n e and x2 =
+// (n + 1) e): one recurrence loop from a common start index (the larger one,
+// which only adds accuracy to the other), two independent chains for the
+// scheduler to interleave.  The loop runs in three phases so that only the six
+// steps inside the bands capture values (with constant indices, so the bands
+// stay in registers).
+__device__ __forceinline__ void miller_step(int k, double t1, double t2, double &b1, double &bp1, double &s1,
+                                            double &b2, double &bp2, double &s2, double g1[5], double g2[5]) {
+    const double even = (k & 1) ? 0.0 : 1.0;
+    s1 += even * b1;
+    s2 += even * b2;
+    const double kf = (double)k;
+    const double m1 = kf * t1 * b1 - bp1, m2 = kf * t2 * b2 - bp2;
+    bp1 = b1; b1 = m1;
+    bp2 = b2; b2 = m2;
+    if (fabs(b1) > 1e250) {
+        b1 *= 1e-250; bp1 *= 1e-250; s1 *= 1e-250;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) g1[q] *= 1e-250;
+    }
+    if (fabs(b2) > 1e250) {
+        b2 *= 1e-250; bp2 *= 1e-250; s2 *= 1e-250;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) g2[q] *= 1e-250;
+    }
+}
+
+__device__ void bessel_band2(int n, double x1, double x2, double J1[5], double J2[5]) {
+    if (x1 == 0.0 || x2 == 0.0) {
+        bessel_band(n, x1, J1);
+        bessel_band(n + 1, x2, J2);
+        return;
+    }
+    const int top = n + 3 > (int)x2 ? n + 3 : (int)x2;
+    int M = top + 24 + (int)sqrt(60.0 * top);
+    M += M & 1;
+    const double t1 = 2.0 / x1, t2 = 2.0 / x2;
+    double bp1 = 0.0, b1 = 1.0, s1 = 0.0, bp2 = 0.0, b2 = 1.0, s2 = 0.0;
+    double g1[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, g2[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = M; k > n + 3; --k) miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+    // k = n+3 .. n-2: band 1 holds k = n-2+q (q = 0..4), band 2 holds k = n-1+q
+#pragma unroll
+    for (int q = 5; q >= 0; --q) {
+        const int k = n - 2 + q;
+        if (k >= 1) {
+            if (q <= 4) g1[q] = b1;
+            if (q >= 1) g2[q - 1] = b2;
+            miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+        }
+    }
+    for (int k = n - 3; k >= 1; --k) miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+    // k = 0 (b = b_0, bp = b_1) lies in band 1 when n <= 2 and in band 2 when n == 1
+    if (n == 1) { g1[1] = b1; g2[0] = b2; }
+    if (n == 2) g1[0] = b1;
+    const double nm1 = b1 + 2.0 * s1, nm2 = b2 + 2.0 * s2;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        J1[q] = g1[q] / nm1;
+        J2[q] = g2[q] / nm2;
+    }
+    if (n == 1) J1[0] = -bp1 / nm1;  // J_{-1} = -J_1
 }
 
 struct AakArgs {
@@ -232,6 +299,7 @@ __global__ void __launch_bounds__(128) k_aak(AakArgs A) {
     const double sqrt1me2 = sqrt(1 - e * e);
 
     double hI = 0.0, hII = 0.0;
+    double Ja[5], Jb[5];  // Bessel bands of the odd harmonic n and of n + 1
     for (int n = 1; n <= A.nmodes; ++n) {
         double nPhi;
         if (A.mich) {
@@ -241,8 +309,12 @@ __global__ void __launch_bounds__(128) k_aak(AakArgs A) {
         } else {
             nPhi = n * Phi;
         }
+        // Bessel values two harmonics at a time (odd n computes n and n + 1)
+        const bool odd = (n & 1) != 0;
+        if (odd) bessel_band2(n, n * e, (n + 1) * e, Ja, Jb);  // the last n + 1 may go unused
         double J[5];
-        bessel_band(n, n * e, J);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) J[q] = odd ? Ja[q] : Jb[q];
         double sn, cn;
         sincos_big(nPhi, &sn, &cn);
         const double a = -n * Amp * (J[0] - 2. * e * J[1] + 2. / n * J[2] + 2. * e * J[3] - J[4]) * cn;
