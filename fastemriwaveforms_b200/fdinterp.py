@@ -56,7 +56,7 @@ class FDInterpolatedModeSum(SummationBase):
 
     def sum(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr, n_arr, M, a, p, e,
             xI, *args, include_minus_m=True, separate_modes=False, dt=10.0, f_arr=None, mask_positive=False,
-            integrate_backwards=False, **kwargs):
+            integrate_backwards=False, host_out=None, **kwargs):
         dev = self.device
         N = len(t)
         p_d, e_d, x_d = (_to_device(np.atleast_1d(_to_host(v, np.float64)), torch.float64, dev) for v in (p, e, xI))
@@ -71,16 +71,19 @@ class FDInterpolatedModeSum(SummationBase):
                                      abs_phi=True, status=status)
         self.sum_with_frequencies(t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr,
                                   n_arr, fk, include_minus_m=include_minus_m, separate_modes=separate_modes, dt=dt,
-                                  f_arr=f_arr, mask_positive=mask_positive, _geodesic_status=status)
+                                  f_arr=f_arr, mask_positive=mask_positive, host_out=host_out,
+                                  _geodesic_status=status)
 
     def sum_with_frequencies(self, t, teuk_modes, ylms, phase_interp_t, phase_interp_coeffs, l_arr, m_arr, k_arr,
                              n_arr, frequencies, include_minus_m=True, separate_modes=False, dt=10.0, f_arr=None,
-                             mask_positive=False, _geodesic_status=None):
+                             mask_positive=False, host_out=None, _geodesic_status=None):
         """``sum`` with the trajectory's frequencies given instead of (M, a, p,
         e, xI): ``frequencies`` (3, len(t)) = (|f_phi|, f_theta, f_r) in Hz at
         the knots (an extension for callers whose trajectory already carries
         them).  Needs ``self.num_pts`` / ``self.num_pts_pad`` (set by
-        ``__call__``) unless f_arr is given."""
+        ``__call__``) unless f_arr is given.  ``host_out`` (extension): a
+        pinned complex128 CPU tensor of the output's shape that receives the
+        (h+, hx) result as well."""
         if separate_modes:
             raise ValueError("separate_modes=True is not supported: the reference kernel writes each mode at "
                              "mode_i * data_length + i of a data_length buffer (interpolate.cu:1512).")
@@ -184,6 +187,11 @@ class FDInterpolatedModeSum(SummationBase):
         out = torch.empty((2, cnt), dtype=torch.complex128, device=dev)
         _lib.call("few_fd_finalize", _ptr(wf), L, first, cnt, _ptr(out), st)
         self.waveform = out
+        if host_out is not None:
+            if (not isinstance(host_out, torch.Tensor) or host_out.device.type != "cpu" or not host_out.is_pinned()
+                    or host_out.dtype != torch.complex128 or tuple(host_out.shape) != tuple(out.shape)):
+                raise ValueError(f"host_out must be a pinned complex128 CPU tensor of shape {tuple(out.shape)}")
+            host_out.copy_(out, non_blocking=True)
 
         # the one synchronisation: the reference's errors
         if _geodesic_status is not None and int(_geodesic_status.item()) & 1:

@@ -200,3 +200,17 @@ def test_fd_matches_fft_of_time_domain(cuda):
     ov = (torch.vdot(a, b) / torch.sqrt(torch.vdot(a, a) * torch.vdot(b, b))).real.item()
     print(f"\nFD vs FFT(TD): 1 - overlap = {1 - ov:.3e}")
     assert 1 - ov < 1e-2
+
+
+def test_fd_host_out(cuda):
+    d = load("fd_schwarzschild")
+    fd = FDInterpolatedModeSum(pad_output=True)
+    args = (d["t"], d["teuk_modes"], d["ylms"], d["phase_t"], d["phase_coeffs"], d["l"], d["m"], d["k"], d["n"],
+            float(d["M"]), float(d["a"]), d["p"], d["e"], d["xI"])
+    ref = fd(*args, T=float(d["T"]), dt=float(d["dt"])).cpu().numpy()
+    h = torch.empty(ref.shape, dtype=torch.complex128).pin_memory()
+    out = fd(*args, T=float(d["T"]), dt=float(d["dt"]), host_out=h)
+    torch.cuda.synchronize()
+    assert rel(h.numpy(), out.cpu().numpy()) == 0.0 and rel(h.numpy(), ref) < 1e-14
+    with pytest.raises(ValueError):
+        fd(*args, T=float(d["T"]), dt=float(d["dt"]), host_out=torch.empty(ref.shape, dtype=torch.complex128))
