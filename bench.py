@@ -55,9 +55,9 @@ def parse():
     ap.add_argument("--no-aak", action="store_true", help="skip the AAK summation measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
-    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd"], default="forward",
-                    help="with --profile: forward calls, forward+backward through autograd, or the "
-                         "frequency-domain sum")
+    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd", "aak"], default="forward",
+                    help="with --profile: forward calls, forward+backward through autograd, the "
+                         "frequency-domain sum, or the AAK summation")
     ap.add_argument("--fd-modes", type=int, default=3843,
                     help="with --profile-form fd: the first modes of the one-year FD trajectory")
     return ap.parse_args()
@@ -697,6 +697,17 @@ def main():
             fd = FDInterpolatedModeSum(pad_output=True)
             for _ in range(args.warmup + args.steps):
                 fd(*fargs, T=fin.T, dt=fin.dt)
+            torch.cuda.synchronize()
+            return 0
+        if args.profile_form == "aak":
+            # the AAK summation on a 3e6 s trajectory (300,001 samples, 18 harmonics)
+            from fastemriwaveforms_b200 import AAKSummation
+            from fastemriwaveforms_b200 import synthetic as S
+
+            ain = S.aak_case(N=100, span=3e6, seed=55)
+            aak = AAKSummation()
+            for _ in range(args.warmup + args.steps):
+                aak(*ain.call_args(), T=ain.T, dt=ain.dt)
             torch.cuda.synchronize()
             return 0
         if args.profile_form == "fwd_bwd":
