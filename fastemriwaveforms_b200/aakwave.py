@@ -6,7 +6,8 @@ m1, a, dist, m2, qS, phiS, qK, phiK, nmodes, interp_t, interp_coeffs; mich,
 dt, integrate_backwards), the same pole shift of qS and qK, the same
 equatorial substitution Phi_theta := Phi_phi when |Y| == 1, and the waveform
 hI - i hII in ``self.waveform``.  The kernel is ``k_aak`` (``csrc/aak.cu``),
-reached through ``few_aak_waveform`` (the reference's ``get_waveform`` of
+reached through ``few_aak_sum`` on device tables (asynchronous);
+``few_aak_waveform`` is the reference-shaped entry (its ``get_waveform`` of
 ``gpuAAK.hh``).  The caller's ``interp_coeffs`` is not modified (the
 reference writes the substitution into it).
 """
@@ -18,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .summation import SummationBase, _ptr, _stream, _to_host
+from .summation import SummationBase, _ptr, _stream, _to_host, _upload
 
 logger = logging.getLogger("fastemriwaveforms_b200")
 
@@ -56,7 +57,27 @@ class AAKSummation(SummationBase):
             c = c.clone()
             c[:, 4] = c[:, 3]
         coeffs = c.permute(2, 0, 1).contiguous()  # (8, N-1, 6), the kernel's layout
-        it = np.ascontiguousarray(it)
-        _lib.call("few_aak_waveform", _ptr(self.waveform), _ptr(coeffs), float(m1), float(a), float(m2), float(qS),
-                  float(phiS), float(qK), float(phiK), float(dist), int(nmodes), int(bool(mich)), init_len,
-                  int(self.num_pts), float(dt), it.ctypes.data, _stream(dev))
+        first = aak_segments(it, int(self.num_pts), float(dt))
+        nseg = len(first) - 1
+        if nseg < 1:
+            return
+        t_d = _upload(np.ascontiguousarray(it), dev)
+        first_d = _upload(first, dev)
+        _lib.call("few_aak_sum", _ptr(self.waveform), _ptr(coeffs), init_len - 1, _ptr(t_d), _ptr(first_d), nseg,
+                  int(first[-1]), float(m1), float(a), float(m2), float(qS), float(phiS), float(qK), float(phiK),
+                  float(dist), int(nmodes), int(bool(mich)), float(dt), _stream(dev))
+
+
+def aak_segments(h_t: np.ndarray, out_len: int, dt: float) -> np.ndarray:
+    """First sample of each trajectory segment (gpuAAK.cu:495-519): ceil(t_j / dt)
+    while t_j < T = (out_len - 1) dt; the first knot at or past T closes the
+    list with out_len.  (nseg + 1,) int32."""
+    T = (out_len - 1) * dt
+    tail = np.asarray(h_t[1:], dtype=np.float64)
+    past = np.nonzero(tail >= T)[0]
+    if len(past):
+        k = int(past[0])
+        first = np.concatenate([[0], np.ceil(tail[:k] / dt), [out_len]])
+    else:
+        first = np.concatenate([[0], np.ceil(tail / dt)])
+    return first.astype(np.int32)

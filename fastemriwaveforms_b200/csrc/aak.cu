@@ -359,6 +359,35 @@ static int aak_segments(const double *h_t, int init_len, int out_len, double dt,
     return npts - 1;
 }
 
+// The kernel on device tables, without allocation or synchronisation (what
+// AAKSummation calls): t_knots [device] (>= nseg + 1), first [device]
+// (nseg + 1) from the segment rule below, coef [device] (8, cstride, 6).
+extern "C" FEW_API int few_aak_sum(void *waveform, const double *coef, int cstride, const double *t_knots,
+                                   const int *first, int nseg, int total, double M_phys, double S_phys, double mu,
+                                   double qS, double phiS, double qK, double phiK, double dist, int nmodes, int mich,
+                                   double delta_t, void *stream) {
+    few::clear_error();
+    if (nseg < 0 || cstride < nseg || total < 0 || nmodes < 0 || nmodes > 4096)
+        return few::fail(FEW_ERR_SIZE, "few_aak_sum: nseg=%d cstride=%d total=%d nmodes=%d", nseg, cstride, total,
+                         nmodes);
+    if (nseg == 0 || total == 0) return FEW_OK;
+    if (!waveform || !coef || !t_knots || !first) return few::fail(FEW_ERR_ARG, "few_aak_sum: null pointer");
+    few::aak::AakArgs A;
+    A.wf = static_cast<double2 *>(waveform);
+    A.coef = coef;
+    A.t = t_knots;
+    A.first = first;
+    A.nseg = nseg;
+    A.cstride = cstride;
+    A.nmodes = nmodes;
+    A.mich = mich;
+    A.M = M_phys; A.S = S_phys; A.mu = mu; A.qS = qS; A.phiS = phiS; A.qK = qK; A.phiK = phiK; A.dist = dist;
+    A.dt = delta_t;
+    few::aak::k_aak<<<(total + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
+    FEW_LAUNCH_CHECK("k_aak");
+    return FEW_OK;
+}
+
 // Drop-in for get_waveform of gpuAAK.hh:6-10 (AAKSummation's kernel call,
 // aakwave.py:175-192): interp_array [device] (8, init_len-1, 6) =
 // the trajectory's dense-output coefficients of (p, e, Y, Phi_phi, Phi_theta,

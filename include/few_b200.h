@@ -511,6 +511,14 @@ FEW_API int few_aak_waveform(void *waveform, const double *interp_array, double 
                              double qS, double phiS, double qK, double phiK, double dist, int nmodes, int mich,
                              int init_len, int out_len, double delta_t, const double *h_t, void *stream);
 
+/* The same kernel on device tables, asynchronous and without allocation:
+ * waveform [device]; coef [device] (8, cstride, 6); t_knots [device] (nseg+1,);
+ * first [device] (nseg+1,) the first sample of each segment by the rule above
+ * (first[nseg] = one past the last sample); total = first[nseg]. */
+FEW_API int few_aak_sum(void *waveform, const double *coef, int cstride, const double *t_knots, const int *first,
+                        int nseg, int total, double M_phys, double S_phys, double mu, double qS, double phiS,
+                        double qK, double phiK, double dist, int nmodes, int mich, double delta_t, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Measurement                                                              */
 /* ------------------------------------------------------------------------ */

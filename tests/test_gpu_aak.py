@@ -66,3 +66,20 @@ def test_aak_equatorial_poles_and_short_trajectory(cuda, oracle):
     long = run(S.aak_case(N=30, span=2e5, seed=54), False, T=3e5 / S.YRSID_SI, pad=True)
     last = int(2e5 / 10.0) + 1  # num_pts: the samples up to the last knot
     assert len(long) > last and np.all(long[last:] == 0) and np.all(long[:last] != 0)
+
+
+def test_aak_reference_shaped_entry(cuda):
+    """few_aak_waveform (the reference's get_waveform argument list, host knots)
+    gives the same samples as AAKSummation's asynchronous path."""
+    from fastemriwaveforms_b200 import _lib
+    from fastemriwaveforms_b200.summation import _ptr
+
+    inp = S.aak_case(N=40, span=3e5)
+    want = run(inp, True)
+    wf = torch.zeros(len(want), dtype=torch.complex128, device=cuda)
+    coef = torch.tensor(np.ascontiguousarray(np.transpose(inp.interp_coeffs, (2, 0, 1))), device=cuda)
+    t = np.ascontiguousarray(inp.t)
+    _lib.call("few_aak_waveform", _ptr(wf), _ptr(coef), inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, inp.qK, inp.phiK,
+              inp.dist, inp.nmodes, 1, len(t), len(want), inp.dt, t.ctypes.data,
+              torch.cuda.current_stream().cuda_stream)
+    assert np.array_equal(wf.cpu().numpy(), want)
