@@ -100,24 +100,31 @@ __device__ void bessel_band(int n, double x, double J[5]) {
 // scheduler to interleave.  The loop runs in three phases so that only the six
 // steps inside the bands capture values (with constant indices, so the bands
 // stay in registers).
-__device__ __forceinline__ void miller_step(int k, double t1, double t2, double &b1, double &bp1, double &s1,
+// One recurrence step of both chains at index k.  EVEN: k is even (b_k joins
+// the normalisation sum); CHECK: test for overflow after the step (every
+// other step suffices: two steps grow the values by less than 1e58 for any
+// argument the kernel sees).
+template <bool EVEN, bool CHECK>
+__device__ __forceinline__ void miller_step(double kf, double t1, double t2, double &b1, double &bp1, double &s1,
                                             double &b2, double &bp2, double &s2, double g1[5], double g2[5]) {
-    const double even = (k & 1) ? 0.0 : 1.0;
-    s1 += even * b1;
-    s2 += even * b2;
-    const double kf = (double)k;
+    if (EVEN) {
+        s1 += b1;
+        s2 += b2;
+    }
     const double m1 = kf * t1 * b1 - bp1, m2 = kf * t2 * b2 - bp2;
     bp1 = b1; b1 = m1;
     bp2 = b2; b2 = m2;
-    if (fabs(b1) > 1e250) {
-        b1 *= 1e-250; bp1 *= 1e-250; s1 *= 1e-250;
+    if (CHECK) {
+        if (fabs(b1) > 1e250) {
+            b1 *= 1e-250; bp1 *= 1e-250; s1 *= 1e-250;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) g1[q] *= 1e-250;
-    }
-    if (fabs(b2) > 1e250) {
-        b2 *= 1e-250; bp2 *= 1e-250; s2 *= 1e-250;
+            for (int q = 0; q < 5; ++q) g1[q] *= 1e-250;
+        }
+        if (fabs(b2) > 1e250) {
+            b2 *= 1e-250; bp2 *= 1e-250; s2 *= 1e-250;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) g2[q] *= 1e-250;
+            for (int q = 0; q < 5; ++q) g2[q] *= 1e-250;
+        }
     }
 }
 
@@ -133,18 +140,27 @@ __device__ void bessel_band2(int n, double x1, double x2, double J1[5], double J
     const double t1 = 2.0 / x1, t2 = 2.0 / x2;
     double bp1 = 0.0, b1 = 1.0, s1 = 0.0, bp2 = 0.0, b2 = 1.0, s2 = 0.0;
     double g1[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, g2[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int k = M; k > n + 3; --k) miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
-    // k = n+3 .. n-2: band 1 holds k = n-2+q (q = 0..4), band 2 holds k = n-1+q
+    // n is odd and M even: the steps pair up as (even k, odd k) in every phase
+    for (int k = M; k > n + 3; k -= 2) {
+        miller_step<true, false>((double)k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+        miller_step<false, true>((double)(k - 1), t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+    }
+    // k = n+3 .. n-2: band 1 holds k = n-2+q (q = 0..4), band 2 holds k = n-1+q;
+    // k = n-2+q is even exactly when q is odd
 #pragma unroll
     for (int q = 5; q >= 0; --q) {
         const int k = n - 2 + q;
         if (k >= 1) {
             if (q <= 4) g1[q] = b1;
             if (q >= 1) g2[q - 1] = b2;
-            miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+            if (q & 1) miller_step<true, false>((double)k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+            else miller_step<false, true>((double)k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
         }
     }
-    for (int k = n - 3; k >= 1; --k) miller_step(k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+    for (int k = n - 3; k >= 1; k -= 2) {
+        miller_step<true, false>((double)k, t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+        miller_step<false, true>((double)(k - 1), t1, t2, b1, bp1, s1, b2, bp2, s2, g1, g2);
+    }
     // k = 0 (b = b_0, bp = b_1) lies in band 1 when n <= 2 and in band 2 when n == 1
     if (n == 1) { g1[1] = b1; g2[0] = b2; }
     if (n == 2) g1[0] = b1;
