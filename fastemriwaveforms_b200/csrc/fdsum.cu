@@ -171,6 +171,14 @@ constexpr double kCbrt4 = 1.587401051968199475;      // 2^{2/3}
 struct SpaConsts {
     cx e23, e13, e34;  // e^{-2 pi i/3}, e^{-pi i/3}, e^{-3 pi i/4}
     double sqrt_half_pi;
+    // For a real argument r + 0i, the general csqrt_ and cpowr take the angle
+    // atan2(+0, r): +0 for r > 0 (sincos gives exactly (0, 1)) and pi for
+    // r < 0.  The sincos of the angles that follow from pi (pi/2 for the square
+    // root, p*pi for z^p) are computed once here with the same functions, so
+    // the real-argument paths below return the general functions' bits.
+    double half_s, half_c;    // sincos(pi / 2)
+    double third_s, third_c;  // sincos((1/3) pi)
+    double sixth_s, sixth_c;  // sincos((1/6) pi)
 };
 
 __device__ __forceinline__ SpaConsts spa_consts() {
@@ -179,12 +187,33 @@ __device__ __forceinline__ SpaConsts spa_consts() {
     k.e13 = cexp_(cdivr(cscale(mk(0.0, 1.0), -kPi), 3.0));
     k.e34 = cexp_(cscale(cscale(mk(-0.0, -1.0), 0.75), kPi));
     k.sqrt_half_pi = sqrt(0.5 * kPi);
+    const double pi_arg = atan2(0.0, -1.0);
+    sincos(pi_arg / 2.0, &k.half_s, &k.half_c);
+    sincos(__dmul_rn(1.0 / 3.0, pi_arg), &k.third_s, &k.third_c);
+    sincos(__dmul_rn(1.0 / 6.0, pi_arg), &k.sixth_s, &k.sixth_c);
     return k;
+}
+
+// csqrt_(r + 0i): the same bits without atan2 and sincos.
+__device__ __forceinline__ cx csqrt_real(double r, const SpaConsts &K) {
+    if (!isfinite(r)) return csqrt_(mk(r, 0.0));
+    const double rho = sqrt(hypot(r, 0.0));
+    if (r > 0.0 || (r == 0.0 && !signbit(r))) return mk(rho * 1.0, rho * 0.0);
+    return mk(rho * K.half_c, rho * K.half_s);
+}
+
+// cpowr(r + 0i, p) for p = 1/3 (third = true) or 1/6: exp(p log|r|) times the
+// phase factor of the angle 0 (r > 0) or p*pi (r < 0).
+__device__ __forceinline__ cx cpowr_real(double r, double p, bool third, const SpaConsts &K) {
+    if (!isfinite(r) || r == 0.0) return cpowr(mk(r, 0.0), p);
+    const double e = exp(p * log(hypot(r, 0.0)));
+    if (r > 0.0) return mk(e * 1.0, e * 0.0);
+    return third ? mk(e * K.third_c, e * K.third_s) : mk(e * K.sixth_c, e * K.sixth_s);
 }
 
 __device__ cx spa(double x, const SpaConsts &K) {
     if (fabs(x) <= 7.0) {
-        cx p6 = cpowr(mk(x, 0.0), 1.0 / 6.0);
+        cx p6 = cpowr_real(x, 1.0 / 6.0, false, K);
         cx pref1 = cdivr(cscale(cmul(cmul(cmul(cmul(cmul(K.e23, p6), p6), p6), p6), p6), kGammaM13), kCbrt2);
         cx pref2 = cdivr(cscale(cmul(K.e13, p6), kGammaP13), kCbrt4);
         double x2 = x * x;
@@ -207,12 +236,14 @@ __device__ cx spa(double x, const SpaConsts &K) {
 
 // Roots of a x^3 + b x^2 + c x + d by Cardano's formula with principal complex
 // branches (interpolate.cu:1113-1133); the real parts are returned.
-__device__ __forceinline__ void cube_roots(double a, double b, double c, double d, cx xi, double r[3]) {
+__device__ __forceinline__ void cube_roots(double a, double b, double c, double d, cx xi, double r[3],
+                                           const SpaConsts &K) {
     double b2 = b * b, b3 = b2 * b, a2 = a * a;
     double D0 = b2 - 3 * a * c;
     double D1 = 2 * b3 - 9 * a * b * c + 27 * a2 * d;
-    cx S = csqrt_(mk(D1 * D1 - 4 * (D0 * D0 * D0), 0.0));
-    cx C = cpowr(cdivr(mk(S.re + D1, S.im), 2.0), 1.0 / 3.0);
+    cx S = csqrt_real(D1 * D1 - 4 * (D0 * D0 * D0), K);
+    cx z = cdivr(mk(S.re + D1, S.im), 2.0);
+    cx C = (z.im == 0.0 && !signbit(z.im)) ? cpowr_real(z.re, 1.0 / 3.0, true, K) : cpowr(z, 1.0 / 3.0);
     double s = -(1.0 / (3 * a));
     cx D0c = mk(D0, 0.0);
     cx xC = cmul(xi, C);
@@ -514,7 +545,7 @@ __global__ void __launch_bounds__(256, MINB) k_fd_sum(SumArgs A) {
         double fc2 = m * fy[2 * A.fq] + k * fy[2 * A.fq + A.fp] + n * fy[2 * A.fq + 2 * A.fp];
         double fc3 = m * fy[3 * A.fq] + k * fy[3 * A.fq + A.fp] + n * fy[3 * A.fq + 2 * A.fp];
         double roots[3];
-        cube_roots(fc3, fc2, fc1, fyv - f, xi, roots);
+        cube_roots(fc3, fc2, fc1, fyv - f, xi, roots, SK);
         const double ts = A.t[seg], te = A.t[seg + 1];
         for (int r = 0; r < 3; ++r) {
             double x = roots[r];
@@ -550,7 +581,7 @@ __global__ void __launch_bounds__(256, MINB) k_fd_sum(SumArgs A) {
             }
             double arg = 2. * kPi * fdot * fdot * fdot / (3. * fddot * fddot);
             double pre = -1.0 * fdot / fabs(fddot) * 2. / sqrt(3.);
-            cx amp2 = cdiv(cscale(spa(arg, SK), pre), csqrt_(mk(arg, 0.0)));
+            cx amp2 = cdiv(cscale(spa(arg, SK), pre), csqrt_real(arg, SK));
             double ph = 2. * kPi * f * tt - phase;
             cx te_ = cmul(cmul(mk(Rre, Rim), amp2), cexp_i(ph));
             double2 yp = A.ylms[mode];
