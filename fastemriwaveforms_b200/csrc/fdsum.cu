@@ -197,7 +197,7 @@ __device__ __forceinline__ SpaConsts spa_consts() {
 // csqrt_(r + 0i): the same bits without atan2 and sincos.
 __device__ __forceinline__ cx csqrt_real(double r, const SpaConsts &K) {
     if (!isfinite(r)) return csqrt_(mk(r, 0.0));
-    const double rho = sqrt(hypot(r, 0.0));
+    const double rho = sqrt(fabs(r));  // hypot(r, +-0) is fabs(r) (CUDA's documented special case)
     if (r > 0.0 || (r == 0.0 && !signbit(r))) return mk(rho * 1.0, rho * 0.0);
     return mk(rho * K.half_c, rho * K.half_s);
 }
@@ -206,7 +206,7 @@ __device__ __forceinline__ cx csqrt_real(double r, const SpaConsts &K) {
 // phase factor of the angle 0 (r > 0) or p*pi (r < 0).
 __device__ __forceinline__ cx cpowr_real(double r, double p, bool third, const SpaConsts &K) {
     if (!isfinite(r) || r == 0.0) return cpowr(mk(r, 0.0), p);
-    const double e = exp(p * log(hypot(r, 0.0)));
+    const double e = exp(p * log(fabs(r)));  // hypot(r, +-0) is fabs(r)
     if (r > 0.0) return mk(e * 1.0, e * 0.0);
     return third ? mk(e * K.third_c, e * K.third_s) : mk(e * K.sixth_c, e * K.sixth_s);
 }
@@ -223,7 +223,10 @@ __device__ cx spa(double x, const SpaConsts &K) {
             s1 = c_spa.s1[j] + x2 * s1;
             s2 = c_spa.s2[j] + x2 * s2;
         }
-        cx ph = cexp_(cscale(mk(-0.0, -1.0), x));
+        // cexp_(-0 x - i x): exp(+-0) is exactly 1, so the factor is (cos x, -sin x)
+        double sx, cxv;
+        sincos(-x, &sx, &cxv);
+        cx ph = mk(cxv, sx);
         return cmul(ph, cadd(cscale(pref1, s1), cscale(pref2, s2)));
     }
     cx y = mk(1.0 / x, 0.0);
