@@ -55,9 +55,9 @@ def parse():
     ap.add_argument("--no-aak", action="store_true", help="skip the AAK summation measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps calls (for ncu captures); prints no JSON line")
-    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd", "aak"], default="forward",
+    ap.add_argument("--profile-form", choices=["forward", "fwd_bwd", "fd", "aak", "amplitude"], default="forward",
                     help="with --profile: forward calls, forward+backward through autograd, the "
-                         "frequency-domain sum, or the AAK summation")
+                         "frequency-domain sum, the AAK summation, or the amplitude grids")
     ap.add_argument("--fd-modes", type=int, default=3843,
                     help="with --profile-form fd: the first modes of the one-year FD trajectory")
     return ap.parse_args()
@@ -697,6 +697,20 @@ def main():
             fd = FDInterpolatedModeSum(pad_output=True)
             for _ in range(args.warmup + args.steps):
                 fd(*fargs, T=fin.T, dt=fin.dt)
+            torch.cuda.synchronize()
+            return 0
+        if args.profile_form == "amplitude":
+            # AmpInterp2D: 3843 modes x 2 bicubic grids of 40 x 40 knots at 1000 points
+            from fastemriwaveforms_b200 import AmpInterp2D
+            from fastemriwaveforms_b200 import synthetic as S
+
+            tw, tu, coeff = S.amplitude_grids(3843, nw=40, nu=40)
+            w, u = S.amplitude_points(1000)
+            amp = AmpInterp2D(tw, tu, coeff, None, None, None, None)
+            w_d = torch.tensor(w, device=dev)
+            u_d = torch.tensor(u, device=dev)
+            for _ in range(args.warmup + args.steps):
+                amp(w_d, u_d)
             torch.cuda.synchronize()
             return 0
         if args.profile_form == "aak":
