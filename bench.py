@@ -568,6 +568,16 @@ def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
              "e2e": {"ms": ems, "value": bins / (ems * 1e-3), "unit": "mode-bins/s", "h2d_bytes_per_step": int(h2d),
                      "d2h_bytes_per_step": int(h.numel() * 16)},
              "fp64_peak_tflops": fp64_tflops}
+    # FP64 work per (mode, bin) evaluation from the ncu capture in profiles/k_fd_sum_fd_full.md
+    # (DFMA x 2 + DADD + DMUL per bin visited)
+    flops_per_bin = 786.0
+    entry["roofline"] = {"bound": "fp64", "kernel": "k_fd_sum", "achieved": bins * flops_per_bin / (kms * 1e-3) / 1e12,
+                         "peak": fp64_tflops, "unit": "TFLOP/s",
+                         "frac": bins * flops_per_bin / (kms * 1e-3) / 1e12 / fp64_tflops,
+                         "peak_source": "measured in this run: few_probe_fp64_fma (FP64 FMA pipe)",
+                         "algorithmic": f"{flops_per_bin:.0f} FP64 flop per (mode, bin) evaluation (ncu count) x {bins}",
+                         "traffic": {"bytes_per_launch_300_modes": 70.5e6,
+                                     "source": "profiles/k_fd_sum_fd_full.md (300-mode capture)"}}
     if cpu:
         from oracle import oracle as O
 
@@ -597,7 +607,7 @@ def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
     return entry
 
 
-def bench_aak(dev, steps: int, cpu: bool):
+def bench_aak(dev, steps: int, cpu: bool, fp64_tflops: float | None = None):
     """AAK summation (AAKSummation): one year at dt = 10 s (3,150,001 samples),
     a 1000-knot trajectory with e 0.6 -> 0.35, 18 harmonics (the reference's
     int(30 e0)); device time of the call with the coefficients in HBM, and the
@@ -630,6 +640,14 @@ def bench_aak(dev, steps: int, cpu: bool):
                          "plain polarisations (mich=False)",
              "ms": ms, "value": L / (ms * 1e-3), "unit": "samples/s",
              "harmonic_value": L * inp.nmodes / (ms * 1e-3)}
+    if fp64_tflops:
+        # FP64 work per sample at 18 harmonics from the ncu capture in profiles/k_aak_one_year.md
+        flops_per_sample = 10152.0
+        ach = L * flops_per_sample / (ms * 1e-3) / 1e12
+        entry["roofline"] = {"bound": "fp64", "kernel": "k_aak", "achieved": ach, "peak": fp64_tflops,
+                             "unit": "TFLOP/s", "frac": ach / fp64_tflops,
+                             "peak_source": "measured in this run: few_probe_fp64_fma (FP64 FMA pipe)",
+                             "algorithmic": f"{flops_per_sample:.0f} FP64 flop per sample (ncu count, 18 harmonics)"}
     if cpu:
         from oracle import oracle as O
 
@@ -865,7 +883,8 @@ def main():
     amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
     fdsum = None if args.no_fd else bench_fd(dev, args.steps, fp64_tflops,
                                              cpu=(rank == 0 and not args.no_cpu_baseline))
-    aakw = None if args.no_aak else bench_aak(dev, args.steps, cpu=(rank == 0 and not args.no_cpu_baseline))
+    aakw = None if args.no_aak else bench_aak(dev, args.steps, cpu=(rank == 0 and not args.no_cpu_baseline),
+                                              fp64_tflops=fp64_tflops)
 
     # ---- roofline of the dominant kernel (the sum) ------------------------------------
     keys = fold.R * fold.NN
