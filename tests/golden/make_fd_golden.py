@@ -244,6 +244,55 @@ def modeselector_case():
     return {k: v.shape for k, v in out.items() if k.endswith("_l")}
 
 
+def _subset(inp, keep):
+    """The modes `keep` of a ModeSumInputs (amplitudes, both ylm halves, l m k n)."""
+    K = inp.teuk_modes.shape[1]
+    keep = np.asarray(keep)
+    sub = S.ModeSumInputs(t=inp.t, teuk_modes=np.ascontiguousarray(inp.teuk_modes[:, keep]),
+                          ylms=np.concatenate([inp.ylms[keep], inp.ylms[K + keep]]), phase_t=inp.phase_t,
+                          phase_coeffs=inp.phase_coeffs, l=inp.l[keep], m=inp.m[keep], k=inp.k[keep],
+                          n=inp.n[keep], dt=inp.dt, T=inp.T, name=inp.name, seed=inp.seed)
+    return sub
+
+
+def _turnovers(inp, fk):
+    """Interior turnovers of each mode's frequency on the reference's dense grid
+    (fdinterp.py:262-300), by the oracle's spline of the knot frequencies."""
+    K = inp.teuk_modes.shape[1]
+    fcoef = np.ascontiguousarray(np.transpose(O.interpolate_arrays(inp.t, fk, impl="ref"), (0, 2, 1)))
+    tn = np.linspace(inp.t.min(), inp.t.max(), 5000)
+    dense = O.spline_eval(inp.t, fcoef, tn)
+    m, k, n = (np.asarray(v, dtype=np.int64) for v in (inp.m, inp.k, inp.n))
+    per = m[:, None] * dense[0][None] + k[:, None] * dense[1][None] + n[:, None] * dense[2][None]
+    cnt = np.zeros(K, dtype=int)
+    for ext in (per.argmax(-1), per.argmin(-1)):
+        te = tn[ext]
+        cnt += ((te > 0.0) & (te < inp.t[-1])).astype(int)
+    return cnt
+
+
+def single_turnover_case(fdi, ims, freqs):
+    """A mode list with exactly one interior turnover over all modes, so the
+    reference's widening of that segment (fdinterp.py:318-376) takes effect:
+    one turning mode plus monotone ones, on the Schwarzschild trajectory."""
+    inp, tr = S.fd_case(K=77, N=50, span=1e6, seed=21, a=0.0, x=1.0, lmax=3, nmax=5, frequencies=freqs)
+    fk = np.asarray(freqs(tr.M, tr.a, tr.p, tr.e, tr.xI))
+    cnt = _turnovers(inp, fk)
+    turning = np.where(cnt == 1)[0]
+    mono = np.where(cnt == 0)[0]
+    for j in turning:
+        keep = np.concatenate([[j], mono[:11]])
+        sub = _subset(inp, keep)
+        if int(_turnovers(sub, fk).sum()) != 1:
+            continue
+        wf, freq, cap, lens = run_reference_fd(fdi, ims, sub, tr, sub.T, sub.dt)
+        start, end = O.fd_plan(sub.t, fk, np.ascontiguousarray(np.transpose(
+            O.interpolate_arrays(sub.t, fk, impl="ref"), (0, 2, 1))), sub.m, sub.k, sub.n, freq, False)
+        save_fd("fd_single_turnover.npz", sub, tr, wf, freq, cap, lens)
+        return int(j), len(keep)
+    raise RuntimeError("no mode list with a single interior turnover found")
+
+
 def main():
     O.build(ref=True)
     geo, ims, fdi = load_reference()
@@ -257,6 +306,9 @@ def main():
     wf, freq, cap, lens = run_reference_fd(fdi, ims, inp, tr, inp.T, inp.dt)
     save_fd("fd_schwarzschild.npz", inp, tr, wf, freq, cap, lens)
     print("fd_schwarzschild", wf.shape, float(np.abs(wf).max()))
+
+    # 1b. exactly one interior turnover: the widening of its segment applies
+    print("fd_single_turnover (mode, modes):", single_turnover_case(fdi, ims, freqs))
 
     # 2. Kerr prograde equatorial, user frequency grid (positive-side index rule)
     inp, tr = S.fd_case(K=66, N=40, span=8e5, seed=22, a=0.6, x=1.0, lmax=3, nmax=4, p_range=(11.0, 6.6),

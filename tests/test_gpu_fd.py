@@ -37,6 +37,7 @@ REL_FD_E2E = 1e-9      # end to end from (M, a, p, e, x): the geodesic frequenci
 
 CASES = {
     "fd_schwarzschild": dict(),
+    "fd_single_turnover": dict(),  # one interior turnover: its segment is widened
     "fd_kerr_farr": dict(f_arr=True),
     "fd_generic_pos": dict(include_minus_m=False, mask_positive=True),
 }

@@ -106,6 +106,7 @@ def test_interp2d_oracle_matches_reference_golden_and_scipy(oracle):
 
 FD_CASES = {
     "fd_schwarzschild": dict(),
+    "fd_single_turnover": dict(),
     "fd_kerr_farr": dict(f_arr=True),
     "fd_generic_pos": dict(include_minus_m=False, mask_positive=True),
 }
