@@ -19,12 +19,8 @@
 // sum's (m, nmodes) complex128 layout, grid 2j (real part) and 2j+1 (imaginary
 // part) of mode mode_idx[j] (the transpose and complex assembly that
 // AmpInterp2D.__call__ does on the host, ampinterp2d.py:186-189, fused into
-// the kernel).  Bicubic grids take the staged form (k_amp_interp2d_staged: a
-// CTA stages 4 modes' grids in shared memory and sweeps every point); other
-// degrees, or grids too large to stage, a tile of 32 points x 32 modes
-// (k_amp_interp2d, lane = point, output rows through a shared-memory transpose).
-#include <cstdint>
-
+// the kernel: a CTA evaluates a tile of 32 points x 32 modes, lane = point,
+// and writes each output row through a shared-memory transpose).
 #include "few_common.cuh"
 #include "few_internal.h"
 
@@ -215,56 +211,6 @@ __global__ void __launch_bounds__(kAmpThreads) k_amp_interp2d(Interp2DArgs a)
     }
 }
 
-// Fused layout, staged form (bicubic and other compile-time degrees): a CTA
-// owns kStageModes modes, copies their 2 * kStageModes coefficient grids into
-// shared memory once (every coefficient crosses HBM once, coalesced), then
-// each thread takes points i = threadIdx.x + k * blockDim.x, computes the
-// point's basis in registers and evaluates every staged mode at it with the
-// same arithmetic as eval_grid_k (same bits), writing the point's
-// kStageModes outputs as one contiguous run of the (m, nmodes) array.
-constexpr int kStageModes = 4;
-
-template <int KX, int KY>
-__global__ void __launch_bounds__(kAmpThreads) k_amp_interp2d_staged(Interp2DArgs a)
-{
-    extern __shared__ double2 s_c2[];  // (kStageModes, 2, len) doubles, as double2 pairs
-    double *s_c = reinterpret_cast<double *>(s_c2);
-    const int j0 = blockIdx.x * kStageModes;
-    const int nm = min(kStageModes, a.ngrid_or_modes - j0);
-    const int len = a.len_indiv_c;
-    // stage: mode q's two grids are contiguous (2 * len doubles) in c
-    for (int q = 0; q < nm; ++q) {
-        const int mode = a.mode_idx ? a.mode_idx[j0 + q] : j0 + q;
-        const double2 *src = reinterpret_cast<const double2 *>(a.c + (long long)mode * 2 * len);
-        double2 *dst = s_c2 + (long long)q * len;  // 2 * len doubles = len double2
-        for (int e = threadIdx.x; e < len; e += blockDim.x) dst[e] = src[e];
-    }
-    __syncthreads();
-    const int nky1 = a.ny - a.ky - 1;
-    double2 *out = static_cast<double2 *>(a.out);
-    for (int i = threadIdx.x; i < a.m; i += blockDim.x) {
-        double hx[kMaxDeg + 1], hy[kMaxDeg + 1];
-        const int lx = bspline_basis(a.tx, a.nx, KX, a.x[i], hx);
-        const int ly = bspline_basis(a.ty, a.ny, KY, a.y[i], hy);
-        double wx[KX + 1], wy[KY + 1];
-#pragma unroll
-        for (int q = 0; q <= KX; ++q) wx[q] = hx[q];
-#pragma unroll
-        for (int q = 0; q <= KY; ++q) wy[q] = hy[q];
-        double2 *orow = out + (long long)i * a.ngrid_or_modes + j0;
-#pragma unroll
-        for (int q = 0; q < kStageModes; ++q) {
-            if (q < nm) {
-                const double *cg = s_c + (long long)q * 2 * len;
-                double2 v;
-                v.x = eval_grid_k<KX, KY>(cg, nky1, lx, ly, wx, wy);
-                v.y = eval_grid_k<KX, KY>(cg + len, nky1, lx, ly, wx, wy);
-                orow[q] = v;
-            }
-        }
-    }
-}
-
 int check_interp2d(const char *who, const double *tx, int nx, const double *ty, int ny, const double *c, int kx,
                    int ky, const double *x, const double *y, int m, int n, int len_indiv_c, const void *out)
 {
@@ -311,16 +257,6 @@ extern "C" int few_amp_interp2d(void *out, const double *tx, int nx, const doubl
     few::Interp2DArgs a{tx, ty, c, x, y, mode_idx, out, nx, ny, kx, ky, m, nmodes, len_indiv_c};
     dim3 grid((m + few::kTileP - 1) / few::kTileP, (nmodes + few::kTileM - 1) / few::kTileM);
     if (grid.y > 65535) return few::fail(FEW_ERR_SIZE, "few_amp_interp2d: too many modes");
-    // bicubic with grids that fit kStageModes at a time in shared memory: the staged form
-    const size_t stage_bytes = (size_t)few::kStageModes * 2 * len_indiv_c * sizeof(double);
-    // (the staged copy reads the grids as 16-byte pairs: c must be 16-byte aligned)
-    if (kx == 3 && ky == 3 && stage_bytes <= 200 * 1024 && (reinterpret_cast<uintptr_t>(c) & 15) == 0) {
-        FEW_CUDA_TRY(few::ensure_smem_attr((const void *)few::k_amp_interp2d_staged<3, 3>, (int)stage_bytes));
-        const int blocks = (nmodes + few::kStageModes - 1) / few::kStageModes;
-        few::k_amp_interp2d_staged<3, 3><<<blocks, few::kAmpThreads, stage_bytes, (cudaStream_t)stream>>>(a);
-        FEW_LAUNCH_CHECK("k_amp_interp2d_staged");
-        return FEW_OK;
-    }
     if (kx == 3 && ky == 3)
         few::k_amp_interp2d<3, 3><<<grid, few::kAmpThreads, 0, (cudaStream_t)stream>>>(a);
     else
