@@ -176,6 +176,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
         const float2 Ep = anchor(Pp);
         const float2 Er = anchor(Pr);
         const float2 Et = a.use_theta ? anchor(Pt) : make_float2(1.f, 0.f);
+        const float2 Er2 = fcmul(Er, Er);
         float2 v[16];
 
         for (int k = 0; k < nch && !failed; ++k) {
@@ -195,9 +196,12 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                 cp_async_commit();
             }
             if (!second) {
+                // two interleaved chains (even and odd n') stepping by Er^2: half the
+                // dependent depth of one chain, and 8 FP32 steps from the anchor at most
                 v[0] = anchor((double)(nlo + 16 * nblk) * Pr);
+                v[1] = fcmul(v[0], Er);
 #pragma unroll
-                for (int q = 1; q < 16; ++q) v[q] = fcmul(v[q - 1], Er);
+                for (int q = 2; q < 16; ++q) v[q] = fcmul(v[q - 2], Er2);
 #pragma unroll
                 for (int q = 0; q < 16; ++q)
                     if (!valid || 16 * nblk + q >= NN) v[q] = make_float2(0.f, 0.f);
