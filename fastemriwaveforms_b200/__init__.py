@@ -7,6 +7,7 @@ kernels reached through the C ABI of ``libfew_b200.so`` (include/few_b200.h).
 """
 from .aakwave import AAKSummation
 from .amplitude import AmpInterp2D
+from .directmodesum import DirectModeSum
 from .fdinterp import FDInterpolatedModeSum
 from .geodesic import get_fundamental_frequencies
 from .modeselector import ModeSelector
@@ -14,5 +15,5 @@ from .summation import CubicSplineInterpolant, InterpolatedModeSum, SummationBas
 from .utility import get_mismatch, get_overlap
 from .ylm import GetYlms
 
-__all__ = ["AAKSummation", "AmpInterp2D", "CubicSplineInterpolant", "FDInterpolatedModeSum", "GetYlms", "InterpolatedModeSum",
+__all__ = ["AAKSummation", "AmpInterp2D", "CubicSplineInterpolant", "DirectModeSum", "FDInterpolatedModeSum", "GetYlms", "InterpolatedModeSum",
            "ModeSelector", "SummationBase", "get_fundamental_frequencies", "get_mismatch", "get_overlap"]

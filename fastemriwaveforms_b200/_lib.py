@@ -82,6 +82,7 @@ SIGNATURES = {
     "few_ylm": [_vp, _vp, _c_int, _c_int, _c_dbl, _c_dbl, _vp, _vp, _vp],
     "few_mode_snr2": [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp],
     "few_mode_keep": [_vp, _c_int, _c_dbl, _vp, _vp],
+    "few_direct_sum": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _vp, _vp],
     "few_aak_sum": [_vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl,
                     _c_dbl, _c_dbl, _c_int, _c_int, _c_dbl, _vp],
     "few_aak_waveform": [_vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_int, _c_int,

@@ -495,6 +495,18 @@ FEW_API int few_mode_snr2(const void *teuk, int N, int K, const void *ylms, cons
 FEW_API int few_mode_keep(const double *sorted_desc, int K, double threshold, int *keep, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Direct mode sum (DirectModeSum, src/few/summation/directmodesum.py)       */
+/* ------------------------------------------------------------------------ */
+
+/* out [device] (N,) complex = sum_j Y_j A_ij e^{-i phi_ij} + sum_{m_j > 0}
+ * (-1)^l_j Y_{K+j} conj(A_ij) e^{+i phi_ij}, phi_ij = (m_j Phi_phi,i +
+ * k_j Phi_theta,i) + n_j Phi_r,i (directmodesum.py:101-131): teuk [device]
+ * (N, K) complex, ylms [device] (2K) complex, phases [device] (3, N), l, m, k,
+ * n [device] (K,) int. */
+FEW_API int few_direct_sum(const void *teuk, const void *ylms, const double *phases, const int *l, const int *m,
+                           const int *k, const int *n, int N, int K, void *out, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* AAK summation (AAKSummation, src/few/summation/aakwave.py:12-196)         */
 /* ------------------------------------------------------------------------ */
 

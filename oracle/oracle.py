@@ -572,3 +572,18 @@ def aak_waveform(interp_t, interp_coeffs, M, S, mu, qS, phiS, qK, phiK, dist, nm
         hII += scale * (FpII * Ap + FcII * Ac)
     wf[idx] = hI - 1j * hII
     return wf
+
+
+def direct_sum(teuk, ylms, phases, l, m, k, n) -> np.ndarray:
+    """DirectModeSum.sum restated (src/few/summation/directmodesum.py:101-131):
+    the +m terms of every mode and the -m images of the m > 0 modes."""
+    teuk = np.asarray(teuk)
+    K = teuk.shape[1]
+    pp, pt, pr = (np.asarray(p, dtype=np.float64)[:, None] for p in phases)
+    m, k, n, l = (np.asarray(v)[None, :] for v in (m, k, n, l))
+    phase = m * pp + k * pt + n * pr
+    w1 = (np.asarray(ylms)[None, :K] * teuk * np.exp(-1j * phase)).sum(axis=1)
+    pos = m[0] > 0
+    w2 = ((-1.0) ** l[:, pos] * np.asarray(ylms)[None, K:][:, pos] * np.conj(teuk[:, pos])
+          * np.exp(1j * phase[:, pos])).sum(axis=1)
+    return w1 + w2

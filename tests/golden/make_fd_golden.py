@@ -14,6 +14,7 @@ defines them).  The rest runs unmodified:
 * the -2 spin-weighted harmonics of ``GetYlms`` (src/few/utils/ylm.py:17-276)
   and the selections of ``ModeSelector`` (src/few/utils/modeselector.py:252-490)
   on a fixed-amplitude generator;
+* ``DirectModeSum.sum`` (src/few/summation/directmodesum.py:30-131), numpy;
 * ``FDInterpolatedModeSum.sum`` (src/few/summation/fdinterp.py:138-542) with
   the reference's ``CubicSplineInterpolant`` (interpolatedmodesum.py:12-257),
   whose native ``interpolate_arrays`` and ``get_waveform_generic_fd`` are the
@@ -293,12 +294,37 @@ def single_turnover_case(fdi, ims, freqs):
     raise RuntimeError("no mode list with a single interior turnover found")
 
 
+def direct_sum_case():
+    """The reference's DirectModeSum (src/few/summation/directmodesum.py:30-131),
+    numpy all the way, on seeded dense amplitudes and phases: the reference
+    test's dummy case (tests/test_mode_summation.py:152-200) with random
+    harmonics, m = 0 modes and phases of ~1e6 rad."""
+    dms = _load("few.summation.directmodesum", os.path.join(REF, "summation/directmodesum.py"))
+    rng = np.random.default_rng(61)
+    t = np.linspace(0, 1e5, 20001)
+    K = 24
+    amp = (np.linspace(rng.uniform(-1, 1, (2, K)), rng.uniform(-1, 1, (2, K)), t.size, axis=-1))
+    teuk = np.ascontiguousarray((amp[0] + 1j * amp[1]).T)
+    phases = np.asarray([np.pi / 3 + 12.0 * t, np.pi / 6 + 2.0 * t, np.pi / 4 + 9.0 * t])
+    l = rng.integers(2, 6, K)
+    m = rng.integers(0, 5, K)
+    k = rng.integers(0, 2, K)
+    n = rng.integers(-3, 3, K)
+    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    fake = types.SimpleNamespace(xp=np)
+    dms.DirectModeSum.sum(fake, t, teuk, ylms, t, phases, l, m, k, n)
+    np.savez_compressed(os.path.join(HERE, "direct_sum.npz"), t=t, teuk=teuk, phases=phases, l=l, m=m, k=k, n=n,
+                        ylms=ylms, waveform=fake.waveform)
+    return fake.waveform.shape
+
+
 def main():
     O.build(ref=True)
     geo, ims, fdi = load_reference()
     print("geodesic rows:", geodesic_case(geo))
     print("ylm:", ylm_case())
     print("modeselector:", modeselector_case())
+    print("direct sum:", direct_sum_case())
     freqs = reference_frequencies(geo)
 
     # 1. Schwarzschild, eccentric, default frequency grid, +/- m

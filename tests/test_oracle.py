@@ -159,3 +159,9 @@ def test_aak_oracle_matches_reference_golden(oracle):
             again = oracle.aak_waveform(inp.t, inp.interp_coeffs, inp.m1, inp.a, inp.m2, inp.qS, inp.phiS, inp.qK,
                                         inp.phiK, inp.dist, inp.nmodes, bool(mich), L, inp.dt, impl="ref")
             assert np.array_equal(again, ref)
+
+
+def test_direct_sum_oracle_matches_reference_golden(oracle):
+    d = np.load(os.path.join(GOLDEN, "direct_sum.npz"))
+    got = oracle.direct_sum(d["teuk"], d["ylms"], d["phases"], d["l"], d["m"], d["k"], d["n"])
+    assert np.linalg.norm(got - d["waveform"]) <= 1e-13 * np.linalg.norm(d["waveform"])
