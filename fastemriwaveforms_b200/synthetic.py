@@ -503,3 +503,22 @@ def aak_case(N: int = 60, span: float = 1e6, seed: int = 51, e_range=(0.6, 0.35)
         nmodes = int(30 * e_range[0])
     return AAKInputs(t=t, interp_coeffs=coeffs, m1=1e6, a=a, dist=1.0, m2=10.0, qS=0.8, phiS=1.9, qK=2.1,
                      phiK=0.4, nmodes=nmodes, dt=dt, T=(span + dt) / YRSID_SI)
+
+
+def direct_case(samples: int = 20001, K: int = 24, seed: int = 61):
+    """Dense inputs of ``DirectModeSum`` in the style of the reference's test
+    (tests/test_mode_summation.py:152-200): linearly ramping complex amplitudes
+    (samples, K), linear phases reaching ~1e6 rad, random (l, m, k, n) with
+    m = 0 modes among them, complex-normal harmonics.  Returns
+    (t, teuk, ylms, phases (3, samples), l, m, k, n)."""
+    rng = np.random.default_rng(seed)
+    t = np.linspace(0, 1e5, samples)
+    amp = np.linspace(rng.uniform(-1, 1, (2, K)), rng.uniform(-1, 1, (2, K)), t.size, axis=-1)
+    teuk = np.ascontiguousarray((amp[0] + 1j * amp[1]).T)
+    phases = np.asarray([np.pi / 3 + 12.0 * t, np.pi / 6 + 2.0 * t, np.pi / 4 + 9.0 * t])
+    l = rng.integers(2, 6, K)
+    m = rng.integers(0, 5, K)
+    k = rng.integers(0, 2, K)
+    n = rng.integers(-3, 3, K)
+    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    return t, teuk, ylms, phases, l, m, k, n

@@ -296,25 +296,20 @@ def single_turnover_case(fdi, ims, freqs):
 
 def direct_sum_case():
     """The reference's DirectModeSum (src/few/summation/directmodesum.py:30-131),
-    numpy all the way, on seeded dense amplitudes and phases: the reference
-    test's dummy case (tests/test_mode_summation.py:152-200) with random
-    harmonics, m = 0 modes and phases of ~1e6 rad."""
+    numpy all the way, on synthetic.direct_case() (the reference test's dummy
+    case with random harmonics, m = 0 modes and phases of ~1e6 rad).  The
+    inputs are regenerated from their seed; the file keeps the output and a
+    digest of the inputs."""
+    import hashlib
+
     dms = _load("few.summation.directmodesum", os.path.join(REF, "summation/directmodesum.py"))
-    rng = np.random.default_rng(61)
-    t = np.linspace(0, 1e5, 20001)
-    K = 24
-    amp = (np.linspace(rng.uniform(-1, 1, (2, K)), rng.uniform(-1, 1, (2, K)), t.size, axis=-1))
-    teuk = np.ascontiguousarray((amp[0] + 1j * amp[1]).T)
-    phases = np.asarray([np.pi / 3 + 12.0 * t, np.pi / 6 + 2.0 * t, np.pi / 4 + 9.0 * t])
-    l = rng.integers(2, 6, K)
-    m = rng.integers(0, 5, K)
-    k = rng.integers(0, 2, K)
-    n = rng.integers(-3, 3, K)
-    ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
+    t, teuk, ylms, phases, l, m, k, n = S.direct_case()
     fake = types.SimpleNamespace(xp=np)
     dms.DirectModeSum.sum(fake, t, teuk, ylms, t, phases, l, m, k, n)
-    np.savez_compressed(os.path.join(HERE, "direct_sum.npz"), t=t, teuk=teuk, phases=phases, l=l, m=m, k=k, n=n,
-                        ylms=ylms, waveform=fake.waveform)
+    h = hashlib.sha256()
+    for a in (t, teuk, ylms, phases, l, m, k, n):
+        h.update(np.ascontiguousarray(a).tobytes())
+    np.savez_compressed(os.path.join(HERE, "direct_sum.npz"), waveform=fake.waveform, digest=h.hexdigest())
     return fake.waveform.shape
 
 

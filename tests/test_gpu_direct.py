@@ -10,14 +10,15 @@ import torch
 
 from conftest import GOLDEN
 from fastemriwaveforms_b200 import DirectModeSum
+from fastemriwaveforms_b200 import synthetic as S
 
 pytestmark = pytest.mark.gpu
 
 
 def test_direct_sum_matches_reference(cuda):
     d = np.load(os.path.join(GOLDEN, "direct_sum.npz"))
-    t = d["t"]
-    got = DirectModeSum()(t, d["teuk"], d["ylms"], t, d["phases"], d["l"], d["m"], d["k"], d["n"]).cpu().numpy()
+    t, teuk, ylms, phases, l, m, k, n = S.direct_case()
+    got = DirectModeSum()(t, teuk, ylms, t, phases, l, m, k, n).cpu().numpy()
     assert got.shape == d["waveform"].shape
     e = float(np.linalg.norm(got - d["waveform"]) / np.linalg.norm(d["waveform"]))
     print(f"\nDirectModeSum vs reference: rel L2 {e:.2e}")

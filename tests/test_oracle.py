@@ -162,6 +162,13 @@ def test_aak_oracle_matches_reference_golden(oracle):
 
 
 def test_direct_sum_oracle_matches_reference_golden(oracle):
+    import hashlib
+
     d = np.load(os.path.join(GOLDEN, "direct_sum.npz"))
-    got = oracle.direct_sum(d["teuk"], d["ylms"], d["phases"], d["l"], d["m"], d["k"], d["n"])
+    t, teuk, ylms, phases, l, m, k, n = S.direct_case()
+    h = hashlib.sha256()
+    for a in (t, teuk, ylms, phases, l, m, k, n):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == str(d["digest"])  # the inputs the golden output was made from
+    got = oracle.direct_sum(teuk, ylms, phases, l, m, k, n)
     assert np.linalg.norm(got - d["waveform"]) <= 1e-13 * np.linalg.norm(d["waveform"])
