@@ -642,7 +642,7 @@ def bench_aak(dev, steps: int, cpu: bool, fp64_tflops: float | None = None):
              "harmonic_value": L * inp.nmodes / (ms * 1e-3)}
     if fp64_tflops:
         # FP64 work per sample at 18 harmonics from the ncu capture in profiles/k_aak_one_year.md
-        flops_per_sample = 10152.0
+        flops_per_sample = 8792.0
         ach = L * flops_per_sample / (ms * 1e-3) / 1e12
         entry["roofline"] = {"bound": "fp64", "kernel": "k_aak", "achieved": ach, "peak": fp64_tflops,
                              "unit": "TFLOP/s", "frac": ach / fp64_tflops,
