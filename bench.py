@@ -861,7 +861,7 @@ def main():
     # mixed_fp64_adjoint: tensor-core forward, FP64 adjoint
     for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
                             ("mixed_fp64_adjoint", "mixed", "fp64")):
-        ms_fb, gt, gp = time_fwd_bwd(prec, inp, dev, max(2, args.steps // 2), 1, backward=bwd)
+        ms_fb, gt, gp = time_fwd_bwd(prec, inp, dev, max(2, args.steps // 2), 3, backward=bwd)
         fb[name] = {"ms_per_step": ms_fb}
         if name == "exact":
             g_ref = (gt, gp)
@@ -877,7 +877,7 @@ def main():
     fb_adj = {"workload": f"K={adj.num_modes}, N={adj.num_knots}, T={adj.out_len}"}
     for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
                             ("mixed_fp64_adjoint", "mixed", "fp64")):
-        fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 1, backward=bwd)[0]}
+        fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 3, backward=bwd)[0]}
 
     batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
     amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
@@ -895,7 +895,7 @@ def main():
     # DRAM bytes of one launch at this workload from an ncu capture (dram__bytes_read.sum +
     # dram__bytes_write.sum), summarised in profiles/; null for workloads not captured
     captured = args.workload == "plain_full" and args.precision == "faithful"
-    traffic = {"bytes_per_launch": 161.1e6, "source": "profiles/k_sum_folded_plain_full_faithful.md",
+    traffic = {"bytes_per_launch": 157.6e6, "source": "profiles/k_sum_folded_plain_full_faithful.md",
                "algorithmic_bytes": float(keys) * 64.0 * seg.nseg + 2.0 * 16.0 * T} if captured else None
     roofline = {"bound": "fp64", "kernel": "k_sum_folded", "achieved": achieved, "peak": fp64_tflops,
                 "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": traffic,
