@@ -215,23 +215,41 @@ struct AdjGArgs {
     double dt;
 };
 
-constexpr int kGTile = 24;  // samples per shared-memory tile
-constexpr int kGCols = 64;  // n' columns per CTA (one per thread of a row block)
-constexpr int kGRowBlocks = kAdjThreads / kGCols;  // 4 row blocks per CTA
+constexpr int kGThreads = 384;
+constexpr int kGPhase = kGThreads;  // samples whose phase data is staged at once (one per thread)
+constexpr int kGTile = 32;    // samples per phasor-table tile
+constexpr int kGCols = 64;    // n' columns per CTA (one per thread of a row block)
+constexpr int kGRowBlocks = kGThreads / kGCols;  // 6 row blocks per CTA
 
-// grid (nseg, row groups of 4*RB rows, column groups of 64): thread (row block
-// rb, column c) owns keys (r = group*4*RB + rb*RB + q, n' = c) for q < RB and
-// accumulates their four x^c sums over every sample of the segment.  The column
-// phasor v_{n'}(t_i) is read once per sample and used for RB rows; the row
-// factors g_i u_r(t_i) are warp-wide broadcasts.
+// Dynamic shared memory of k_adj_G<RB>: the phasor tables of one tile and the
+// phase data of kGPhase samples.
+constexpr size_t adj_g_smem(int rb)
+{
+    return (size_t)kGTile * kGRowBlocks * rb * sizeof(double2)  // g u_r
+           + (size_t)kGTile * kGCols * sizeof(double2)          // v_{n'}
+           + (size_t)kGPhase * 4 * sizeof(double2)              // Ep, Er, Et, g
+           + (size_t)kGPhase * 4 * sizeof(double);              // 1, x, x^2, x^3
+}
+
+// grid (nseg, row groups of 6*RB rows, column groups of 64), 384 threads (12
+// warps per SM at <= 170 registers): thread (row block rb, column c) owns keys
+// (r = group*6*RB + rb*RB + q, n' = c) for q < RB and
+// accumulates their four x^c sums over every sample of the segment.  Every
+// thread first evaluates the phases, sincos and g of one of the next kGPhase
+// samples; then, per tile of kGTile samples, the CTA builds the row factors
+// g_i u_r(t_i) and the column phasors v_{n'}(t_i), and each thread reads its
+// column phasor once per sample and uses it for RB rows (the row factors are
+// warp-wide broadcasts).  Samples are added in order: deterministic.
 template <int RB>
-__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_G(AdjGArgs a)
+__global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
 {
     constexpr int RG = kGRowBlocks * RB;  // rows per CTA
-    __shared__ double2 s_gu[kGTile][RG];
-    __shared__ double2 s_v[kGTile][kGCols];
-    __shared__ double s_x[kGTile][4];
-    __shared__ double2 s_E[kGTile][4];  // Ep, Er, Et, g
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 (*s_gu)[RG] = reinterpret_cast<double2 (*)[RG]>(smem_raw);
+    double2 (*s_v)[kGCols] = reinterpret_cast<double2 (*)[kGCols]>(smem_raw + (size_t)kGTile * RG * sizeof(double2));
+    double2 (*s_E)[4] = reinterpret_cast<double2 (*)[4]>(smem_raw + (size_t)kGTile * (RG + kGCols) * sizeof(double2));
+    double (*s_x)[4] = reinterpret_cast<double (*)[4]>(smem_raw + (size_t)(kGTile * (RG + kGCols) + kGPhase * 4) *
+                                                                      sizeof(double2));
     __shared__ int s_rm[RG], s_rk[RG];
     __shared__ double s_pc[24];
 
@@ -256,12 +274,12 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_G(AdjGArgs a)
     for (int q = 0; q < RB; ++q)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[q][c][0] = acc[q][c][1] = 0.0;
-    __syncthreads();
 
-    for (int i0 = lo; i0 < hi; i0 += kGTile) {
-        const int ns = min(kGTile, hi - i0);
-        if (tid < ns) {
-            const int i = i0 + tid;
+    for (int p0 = lo; p0 < hi; p0 += kGPhase) {
+        const int np = min(kGPhase, hi - p0);
+        __syncthreads();  // s_pc and the row tables are written; the previous batch's readers are done
+        if (tid < np) {
+            const int i = p0 + tid;
             const double t = rmul(a.dt, (double)i);
             const double x = rsub(t, t0);
             const double s = __ddiv_rn(rsub(t, pt0), pw);
@@ -284,42 +302,44 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_G(AdjGArgs a)
             s_x[tid][2] = x * x;
             s_x[tid][3] = x * x * x;
         }
-        __syncthreads();
-        // tables: g u_r for this CTA's rows, v_{n'} for its columns (runs of 8 by recurrence)
-        for (int w = tid; w < ns * RG; w += blockDim.x) {
-            const int j = w / RG, r = w - j * RG;
-            double2 uu = cpow_int(s_E[j][0], s_rm[r]);
-            if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[j][2], s_rk[r]));
-            s_gu[j][r] = cmul(s_E[j][3], uu);
-        }
-        for (int w = tid; w < ns * (kGCols / 8); w += blockDim.x) {
-            const int j = w / (kGCols / 8), b = w - j * (kGCols / 8);
-            const double2 Er = s_E[j][1];
-            double2 v = cpow_int(Er, a.nlo + c0 + 8 * b);
+        for (int i0 = 0; i0 < np; i0 += kGTile) {
+            const int ns = min(kGTile, np - i0);
+            __syncthreads();  // phase data written; the previous tile's readers are done
+            // tables: g u_r for this CTA's rows, v_{n'} for its columns (runs of 8 by recurrence)
+            for (int w = tid; w < ns * RG; w += blockDim.x) {
+                const int j = w / RG, r = w - j * RG;
+                double2 uu = cpow_int(s_E[i0 + j][0], s_rm[r]);
+                if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[i0 + j][2], s_rk[r]));
+                s_gu[j][r] = cmul(s_E[i0 + j][3], uu);
+            }
+            for (int w = tid; w < ns * (kGCols / 8); w += blockDim.x) {
+                const int j = w / (kGCols / 8), b = w - j * (kGCols / 8);
+                const double2 Er = s_E[i0 + j][1];
+                double2 v = cpow_int(Er, a.nlo + c0 + 8 * b);
 #pragma unroll
-            for (int c = 8 * b; c < 8 * b + 8; ++c) {
-                s_v[j][c] = v;
-                v = cmul(v, Er);
+                for (int c = 8 * b; c < 8 * b + 8; ++c) {
+                    s_v[j][c] = v;
+                    v = cmul(v, Er);
+                }
+            }
+            __syncthreads();
+            for (int j = 0; j < ns; ++j) {
+                const double2 v = s_v[j][col];
+                const double x1 = s_x[i0 + j][1], x2 = s_x[i0 + j][2], x3 = s_x[i0 + j][3];
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    const double2 z = cmul(s_gu[j][rb * RB + q], v);
+                    acc[q][0][0] += z.x;
+                    acc[q][0][1] += z.y;
+                    acc[q][1][0] = fma(x1, z.x, acc[q][1][0]);
+                    acc[q][1][1] = fma(x1, z.y, acc[q][1][1]);
+                    acc[q][2][0] = fma(x2, z.x, acc[q][2][0]);
+                    acc[q][2][1] = fma(x2, z.y, acc[q][2][1]);
+                    acc[q][3][0] = fma(x3, z.x, acc[q][3][0]);
+                    acc[q][3][1] = fma(x3, z.y, acc[q][3][1]);
+                }
             }
         }
-        __syncthreads();
-        for (int j = 0; j < ns; ++j) {
-            const double2 v = s_v[j][col];
-            const double x1 = s_x[j][1], x2 = s_x[j][2], x3 = s_x[j][3];
-#pragma unroll
-            for (int q = 0; q < RB; ++q) {
-                const double2 z = cmul(s_gu[j][rb * RB + q], v);
-                acc[q][0][0] += z.x;
-                acc[q][0][1] += z.y;
-                acc[q][1][0] = fma(x1, z.x, acc[q][1][0]);
-                acc[q][1][1] = fma(x1, z.y, acc[q][1][1]);
-                acc[q][2][0] = fma(x2, z.x, acc[q][2][0]);
-                acc[q][2][1] = fma(x2, z.y, acc[q][2][1]);
-                acc[q][3][0] = fma(x3, z.x, acc[q][3][0]);
-                acc[q][3][1] = fma(x3, z.y, acc[q][3][1]);
-            }
-        }
-        __syncthreads();
     }
     const int n = c0 + col;
     if (n < NN) {
@@ -808,7 +828,7 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     a.nkeys_pass = R * NN;
     a.dt = dt;
     const int colg = (NN + kGCols - 1) / kGCols;
-    // rows per CTA = 4 row blocks x RB; take the RB with the least padding
+    // rows per CTA = 6 row blocks x RB; take the RB with the least padding
     int best = 4, best_pad = 1 << 30;
     for (int rb : {4, 6, 8}) {
         const int rg = kGRowBlocks * rb;
@@ -820,9 +840,17 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     }
     const int rg = kGRowBlocks * best;
     dim3 grid(nseg, (R + rg - 1) / rg, colg);
-    if (best == 4) k_adj_G<4><<<grid, kAdjThreads, 0, st>>>(a);
-    else if (best == 6) k_adj_G<6><<<grid, kAdjThreads, 0, st>>>(a);
-    else k_adj_G<8><<<grid, kAdjThreads, 0, st>>>(a);
+    const size_t smem = adj_g_smem(best);
+    if (best == 4) {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G<4>, (int)smem));
+        k_adj_G<4><<<grid, kGThreads, smem, st>>>(a);
+    } else if (best == 6) {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G<6>, (int)smem));
+        k_adj_G<6><<<grid, kGThreads, smem, st>>>(a);
+    } else {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G<8>, (int)smem));
+        k_adj_G<8><<<grid, kGThreads, smem, st>>>(a);
+    }
     FEW_LAUNCH_CHECK("k_adj_G");
     return FEW_OK;
 }
