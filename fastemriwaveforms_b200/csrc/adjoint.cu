@@ -830,7 +830,7 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     const int colg = (NN + kGCols - 1) / kGCols;
     // rows per CTA = 6 row blocks x RB; take the RB with the least padding
     int best = 4, best_pad = 1 << 30;
-    for (int rb : {4, 6, 8}) {
+    for (int rb : {2, 4, 6, 8}) {
         const int rg = kGRowBlocks * rb;
         const int pad = (R + rg - 1) / rg * rg - R;
         if (pad < best_pad || (pad == best_pad && rb > best)) {
@@ -841,7 +841,10 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     const int rg = kGRowBlocks * best;
     dim3 grid(nseg, (R + rg - 1) / rg, colg);
     const size_t smem = adj_g_smem(best);
-    if (best == 4) {
+    if (best == 2) {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G<2>, (int)smem));
+        k_adj_G<2><<<grid, kGThreads, smem, st>>>(a);
+    } else if (best == 4) {
         FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G<4>, (int)smem));
         k_adj_G<4><<<grid, kGThreads, smem, st>>>(a);
     } else if (best == 6) {
