@@ -794,7 +794,7 @@ def main():
         pc_h = torch.from_numpy(inp.phase_coeffs).pin_memory()
         out_h = torch.empty(T, dtype=torch.complex128).pin_memory()
         host_args = (inp.t, teuk_h, ylms_h, inp.phase_t, pc_h, inp.l, inp.m, inp.k, inp.n)
-        for _ in range(2):
+        for _ in range(max(args.warmup, 3)):
             module(*host_args, T=inp.T, dt=inp.dt, host_out=out_h)
         torch.cuda.synchronize()
         barrier()
