@@ -56,7 +56,6 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *sW = reinterpret_cast<double2 *>(smem_raw);
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_rmd[kMaxRows], s_rkd[kMaxRows];  // the same as doubles: no conversion in the key loop
     __shared__ double s_pc[24];
     __shared__ double s_e[3][1024];  // dL/dPhi_f at each sample of the unit (units hold <= 1024 samples)
 
@@ -69,8 +68,6 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
         s_rm[r] = a.row_m[r];
         s_rk[r] = a.row_k[r];
-        s_rmd[r] = (double)a.row_m[r];
-        s_rkd[r] = (double)a.row_k[r];
     }
     if (threadIdx.x < 24) {
         const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
@@ -133,13 +130,13 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
                             Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
                             Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
                             const double2 P = cmul(U[q], Wx);
-                            const double mq = s_rmd[r0 + rb + q];
+                            const double mq = (double)s_rm[r0 + rb + q];
                             T.x += P.x;
                             T.y += P.y;
                             Tm.x = fma(mq, P.x, Tm.x);
                             Tm.y = fma(mq, P.y, Tm.y);
                             if (THETA) {
-                                const double kq = s_rkd[r0 + rb + q];
+                                const double kq = (double)s_rk[r0 + rb + q];
                                 Tk.x = fma(kq, P.x, Tk.x);
                                 Tk.y = fma(kq, P.y, Tk.y);
                             }
