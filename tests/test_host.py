@@ -160,3 +160,25 @@ def test_fd_dense_grid_is_numpy_linspace():
         mine = np.arange(DENSE_POINTS) * step + t0
         mine[-1] = t1
         assert np.array_equal(mine, np.linspace(t.min(), t.max(), DENSE_POINTS))
+
+
+def test_mode_selector_list_checks():
+    """ModeSelector's list checks and messages (the reference's
+    modeselector.py:144-171): bad strings, empty lists, duplicates, |m| > l,
+    l < 2; a negative m in the constructor's list only warns and sets the flag
+    that makes a later include_minus_mkn call fail."""
+    from fastemriwaveforms_b200 import ModeSelector
+
+    gen = S.FixedAmplitudes()
+    for bad, text in (("some", "must be either 'all', 'threshold', or None"),
+                      ([], "cannot be empty"),
+                      ([(2, 2, 0, 0), (2, 2, 0, 0)], "duplicate modes"),
+                      ([(2, 3, 0, 0)], "|m| > l"),
+                      ([(1, 0, 0, 0)], "l < 2")):
+        with pytest.raises(ValueError) as err:
+            ModeSelector(gen, mode_selection=bad, device="cpu")
+        assert text in str(err.value), (bad, str(err.value))
+    sel = ModeSelector(gen, mode_selection=[(2, -2, 0, 0)], device="cpu")
+    assert sel.negative_m_flag
+    with pytest.raises(ValueError, match="m >= 0 when include_minus_mkn = True"):
+        sel(np.zeros(4), 0.5, None, None, None, 1.0, 0.5)
