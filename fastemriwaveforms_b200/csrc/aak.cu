@@ -54,7 +54,7 @@ __device__ __forceinline__ void sincos_big(double ph, double *s, double *c) {
 // Miller's backward recurrence b_{k-1} = (2k/x) b_k - b_{k+1} from a start
 // index M = top + 16 + sqrt(30 top) above top = max(n + 2, x), normalised by
 // b_0 + 2 (b_2 + b_4 + ...).  The start's relative error is of order
-// (x/2)^{2M} / (M! (M-1)!): below 1e-50 for every x <= top <= 64.
+// (x/2)^{2M} / (M! (M-1)!): below 1e-38 for every x <= top <= 64.
 __device__ void bessel_band(int n, double x, double J[5]) {
     if (x == 0.0) {
 #pragma unroll
