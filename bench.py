@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--cpu-samples", type=int, default=60000,
                     help="output samples of the bounded single-core reference run (cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-window", type=int, default=32768,
+                    help="--impl reference: output samples per process per step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256,
                     help="waveforms of the uneven batch (T ~ logU[1e5, 3.15e6], N ~ U[50, 2000], K ~ U[200, 3843])")
@@ -163,11 +165,13 @@ def _cpu_impl():
 
 def cpu_baseline(inp, samples: int):
     """Single-threaded: the reference's spline build of all 2K amplitude series
-    plus its sum over the first `samples` output samples."""
+    plus its sum over the first `samples` output samples.  The spline build
+    serves the whole waveform, so `value` charges it pro rata (its time x
+    samples / T): the rate a whole-waveform call would have."""
     from oracle import oracle as O
 
     impl, kind = _cpu_impl()
-    K = inp.num_modes
+    K, T = inp.num_modes, inp.out_len
     t0 = time.perf_counter()
     y_all, pc, ylms = O.prepare_sum(inp)
     coeffs = O.spline_coeffs(inp.t, y_all, impl=impl)
@@ -175,10 +179,12 @@ def cpu_baseline(inp, samples: int):
     prob = O.window_problem(inp, coeffs, 0, samples)
     O.run_window(prob, impl)
     t2 = time.perf_counter()
-    value = K * samples / (t2 - t1)
+    spline_share = (t1 - t0) * samples / T
+    value = K * samples / (t2 - t1 + spline_share)
     return {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
             "sample": f"{samples} output samples x {K} modes of the same waveform (first samples); "
-                      f"sum {t2 - t1:.2f} s, spline build of all {2 * K} series {t1 - t0:.3f} s (not in value)",
+                      f"sum {t2 - t1:.2f} s plus the spline build of all {2 * K} series ({t1 - t0:.3f} s) "
+                      f"charged pro rata ({spline_share:.4f} s)",
             "cpu": _cpu_model()}
 
 
@@ -194,23 +200,66 @@ def _cpu_model():
 
 
 def _ref_worker(args):
-    """One process of the reference arm: window problems at its segment offset."""
-    impl, seed_off, j0, samples, steps = args
+    """One process of the reference arm: the reference's spline build of the
+    whole waveform (timed once), then one window of its own sample range per
+    step (windows tile the range and repeat once it is covered)."""
+    impl, windows, steps = args
     from oracle import oracle as O
 
-    inp = workload("plain_full", seed_off)
+    inp = workload("plain_full")
+    t0 = time.perf_counter()
     y_all, pc, ylms = O.prepare_sum(inp)
     coeffs = O.spline_coeffs(inp.t, y_all, impl=impl)
-    prob = O.window_problem(inp, coeffs, j0, samples)
+    spline_s = time.perf_counter() - t0
+    probs = [O.window_problem(inp, coeffs, j0, n) for j0, n in windows]
     times = []
-    for _ in range(steps):
+    for s in range(steps):
         t0 = time.perf_counter()
-        O.run_window(prob, impl)
+        O.run_window(probs[s % len(probs)], impl)
         times.append(time.perf_counter() - t0)
-    return times
+    return spline_s, times
+
+
+def reference_windows(inp, procs: int, window: int):
+    """Splits the waveform's knot segments into `procs` contiguous ranges of
+    about equal sample counts, and each range into windows of about `window`
+    samples that start at segment starts and tile the range exactly.
+    Returns [(share, [(j0, samples), ...])] per process."""
+    from oracle import oracle as O
+
+    start, nseg = O.find_start_inds(inp.t, inp.dt, inp.out_len)
+    start = [int(v) for v in start[:nseg + 1]]
+    T = start[nseg]
+    bounds = [0]
+    for p in range(1, procs):
+        target = p * T / procs
+        j = max(bounds[-1] + 1, min(nseg - (procs - p), next(j for j in range(nseg + 1) if start[j] >= target)))
+        bounds.append(j)
+    bounds.append(nseg)
+    out = []
+    for p in range(procs):
+        a, b = bounds[p], bounds[p + 1]
+        wins, j = [], a
+        while j < b:
+            k = j + 1
+            while k < b and start[k] - start[j] < window:
+                k += 1
+            wins.append((j, start[k] - start[j]))
+            j = k
+        out.append((start[b] - start[a], wins))
+    return out
 
 
 def run_reference(args):
+    """The reference's own CPU path (its interpolate.cu built from source) on
+    every host core, one process per core, over the same one-year workload.
+    The path is single-threaded, so the harness splits the waveform: process p
+    owns a contiguous range of knot segments (~T/P samples) and, per step,
+    runs the reference's get_waveform on the next window of that range
+    (windows tile the range; the whole waveform is covered every few steps).
+    Each process builds the whole spline once; its time is charged to every
+    step pro rata (window samples / the process's share), so the per-step rate
+    is that of a whole-waveform call split P ways."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -220,29 +269,38 @@ def run_reference(args):
     inp = workload(args.workload)
     K = inp.num_modes
     procs = os.cpu_count() or 1
-    samples = 20000 if args.workload == "plain_full" else 5000
-    from oracle import oracle as O
-
-    start, nseg = O.find_start_inds(inp.t, inp.dt, inp.out_len)
-    # spread the windows over the waveform, one per process, each at a segment start
-    js = [int(j) for j in np.linspace(0, nseg - 1, procs, endpoint=False)]
+    window = args.ref_window if args.workload == "plain_full" else 5000
+    plan = reference_windows(inp, procs, window)
     steps = args.warmup + args.steps
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(impl, 0, j, samples, steps) for j in js])
+        res = pool.map(_ref_worker, [(impl, wins, steps) for _, wins in plan])
     wall = time.perf_counter() - t0
-    # per step: the slowest process bounds the step
-    per_step = [max(r[s] for r in res) for s in range(args.warmup, steps)]
-    step_s = statistics.mean(per_step)
-    value = K * samples * procs / step_s
+    total_s, total_ms = 0.0, 0.0
+    covered = set()
+    for s in range(args.warmup, steps):
+        step_s, step_samples = 0.0, 0
+        for (share, wins), (spline_s, times) in zip(plan, res):
+            j0, n = wins[s % len(wins)]
+            covered.add(j0)
+            step_s = max(step_s, times[s] + spline_s * n / share)
+            step_samples += n
+        total_s += step_s
+        total_ms += K * step_samples
+    value = total_ms / total_s
+    nwin = sum(len(w) for _, w in plan)
+    spline_mean = statistics.mean(r[0] for r in res)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(inp, args, {"reference_window": f"{procs} processes x {samples} samples"}),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(inp, args),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": kind,
-                             "sample": f"{procs} windows of {samples} samples x {K} modes at spread knot segments, "
-                                       f"one process each (the reference path is single-threaded)",
+                             "sample": f"the whole waveform split into {procs} contiguous segment ranges, one "
+                                       f"process per core; per step every process runs the reference's "
+                                       f"get_waveform on the next ~{window}-sample window of its range "
+                                       f"({nwin} windows tile the waveform; {len(covered)} run in the timed "
+                                       f"steps); its whole-spline build ({spline_mean:.2f} s) charged pro rata",
                              "cpu": _cpu_model()},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
@@ -568,8 +626,8 @@ def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
              "e2e": {"ms": ems, "value": bins / (ems * 1e-3), "unit": "mode-bins/s", "h2d_bytes_per_step": int(h2d),
                      "d2h_bytes_per_step": int(h.numel() * 16)},
              "fp64_peak_tflops": fp64_tflops}
-    # FP64 work per (mode, bin) evaluation from the ncu capture in profiles/k_fd_sum_fd_full.md
-    # (DFMA x 2 + DADD + DMUL per bin visited)
+    # FP64 work per (mode, bin) evaluation from an ncu capture of k_fd_sum on the one-year
+    # trajectory (DFMA x 2 + DADD + DMUL per bin visited)
     flops_per_bin = 786.0
     entry["roofline"] = {"bound": "fp64", "kernel": "k_fd_sum", "achieved": bins * flops_per_bin / (kms * 1e-3) / 1e12,
                          "peak": fp64_tflops, "unit": "TFLOP/s",
@@ -577,7 +635,7 @@ def bench_fd(dev, steps: int, fp64_tflops: float, cpu: bool):
                          "peak_source": "measured in this run: few_probe_fp64_fma (FP64 FMA pipe)",
                          "algorithmic": f"{flops_per_bin:.0f} FP64 flop per (mode, bin) evaluation (ncu count) x {bins}",
                          "traffic": {"bytes_per_launch_300_modes": 70.5e6,
-                                     "source": "profiles/k_fd_sum_fd_full.md (300-mode capture)"}}
+                                     "source": "ncu capture of k_fd_sum, first 300 modes of the one-year case"}}
     if cpu:
         from oracle import oracle as O
 
@@ -641,7 +699,7 @@ def bench_aak(dev, steps: int, cpu: bool, fp64_tflops: float | None = None):
              "ms": ms, "value": L / (ms * 1e-3), "unit": "samples/s",
              "harmonic_value": L * inp.nmodes / (ms * 1e-3)}
     if fp64_tflops:
-        # FP64 work per sample at 18 harmonics from the ncu capture in profiles/k_aak_one_year.md
+        # FP64 work per sample at 18 harmonics from an ncu capture of k_aak (one-year case)
         flops_per_sample = 8792.0
         ach = L * flops_per_sample / (ms * 1e-3) / 1e12
         entry["roofline"] = {"bound": "fp64", "kernel": "k_aak", "achieved": ach, "peak": fp64_tflops,
@@ -660,6 +718,43 @@ def bench_aak(dev, steps: int, cpu: bool, fp64_tflops: float | None = None):
             entry["cpu_baseline"] = {"value": Ls / dt, "unit": "samples/s", "cores": 1, "kind": "reference",
                                      "sample": f"the reference's AAK kernel on the first {Ls} samples ({dt:.2f} s)"}
     return entry
+
+
+def _sig(x, digits: int = 4):
+    """Floats rounded to `digits` significant digits, recursively."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: _sig(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_sig(v, digits) for v in x]
+    return x
+
+
+def summary(faithful_ms, forms, fb, fb_adj, batched):
+    """The mixed-vs-FP64 figures in short form (ms per waveform, accuracy)."""
+    mixed = forms["mixed"]
+    out = {"forms": {"faithful": {"ms": faithful_ms}, "exact": {"ms": forms["exact"]["ms_per_step"]},
+                     "mixed": {"ms": mixed["ms_per_step"], "mismatch": mixed["mismatch_vs_faithful"],
+                               "rel_l2": mixed["rel_l2_vs_faithful"], "max_rel": mixed["max_rel_vs_faithful"],
+                               "tensor_frac": mixed["roofline"]["frac"]}},
+           "fwd_bwd": {k: {"ms": v["ms_per_step"], **({"grad_rel_l2_vs_exact": v["grad_rel_l2_vs_exact"]}
+                                                       if "grad_rel_l2_vs_exact" in v else {})}
+                       for k, v in fb.items()},
+           "fwd_bwd_adjoint_case": {k: (v["ms_per_step"] if isinstance(v, dict) else v) for k, v in fb_adj.items()}}
+    if batched:
+        loop, bm = batched["loop_plain_fp64"], batched["batched_mixed_graph"]
+        loop_fb = batched["loop_plain_fp64_fwd_bwd"]
+        out["batched"] = {"waveforms": batched["waveforms"], "mode_samples": float(batched["mode_samples"]),
+                          "loop_fp64": {"fwd_ms": loop["ms_total"], "fwd_p50_ms": loop["p50_ms"],
+                                        "fwd_p99_ms": loop["p99_ms"], "fwd_bwd_ms": loop_fb["ms_total"],
+                                        "fwd_bwd_p50_ms": loop_fb["p50_ms"], "fwd_bwd_p99_ms": loop_fb["p99_ms"]},
+                          "graph_mixed": {k: bm[k] for k in ("fwd_ms", "fwd_bwd_ms", "fwd_value", "fwd_bwd_value")
+                                          if k in bm}}
+        for k in ("fwd_p50_ms", "fwd_p99_ms", "fwd_done_p50_ms", "fwd_done_p99_ms"):
+            if k in bm:
+                out["batched"]["graph_mixed"][k] = bm[k]
+    return _sig(out)
 
 
 def peaks():
@@ -893,9 +988,9 @@ def main():
     achieved = sum_flops / (stage["sum"] * 1e-3) / 1e12
     spline_bytes = 40.0 * inp.num_knots * 2 * K
     # DRAM bytes of one launch at this workload from an ncu capture (dram__bytes_read.sum +
-    # dram__bytes_write.sum), summarised in profiles/; null for workloads not captured
+    # dram__bytes_write.sum); null for workloads not captured
     captured = args.workload == "plain_full" and args.precision == "faithful"
-    traffic = {"bytes_per_launch": 157.6e6, "source": "profiles/k_sum_folded_plain_full_faithful.md",
+    traffic = {"bytes_per_launch": 157.6e6, "source": "ncu capture of k_sum_folded (faithful, one-year workload)",
                "algorithmic_bytes": float(keys) * 64.0 * seg.nseg + 2.0 * 16.0 * T} if captured else None
     roofline = {"bound": "fp64", "kernel": "k_sum_folded", "achieved": achieved, "peak": fp64_tflops,
                 "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": traffic,
@@ -906,7 +1001,8 @@ def main():
                    "peak": pk["hbm_gbs"], "unit": "GB/s",
                    "frac": spline_bytes / (stage["spline"] * 1e-3) / 1e9 / pk["hbm_gbs"],
                    "peak_source": f"{pk_kind} hbm_gbs", "algorithmic": "40 B per (knot, series)",
-                   "traffic": ({"bytes_per_launch": 466.7e6, "source": "profiles/k_spline_build_factored_plain_full.md"}
+                   "traffic": ({"bytes_per_launch": 466.7e6,
+                                "source": "ncu capture of k_spline_build_factored (one-year workload)"}
                                if args.workload == "plain_full" else None),
                    "launch_ms": stage["spline"]}
 
@@ -917,12 +1013,18 @@ def main():
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(inp, min(args.cpu_samples, T) if args.workload == "plain_full" else min(5000, T))
+    # Key order: the contract's keys, then the rows around the path (long),
+    # then the full per-form records, and last a compact summary of the mixed
+    # and forward+backward figures, so that the end of the line carries them.
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(inp, args),
-            "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "roofline_spline": spline_roof,
-            "stage_ms": stage, "forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched, "amplitude": amplitude, "fd": fdsum, "aak": aakw, "cpu_baseline": cpu, "clocks": clk,
-            "device": torch.cuda.get_device_name(dev)}
+            "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "device": torch.cuda.get_device_name(dev),
+            "around_path": {"amplitude": amplitude, "fd": fdsum, "aak": aakw},
+            "roofline_spline": spline_roof, "stage_ms": stage,
+            "detail": {"forms": forms, "fwd_bwd": fb, "fwd_bwd_adjoint_case": fb_adj, "batched": batched}}
+    line.update(summary(ms_step, forms, fb, fb_adj, batched))
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

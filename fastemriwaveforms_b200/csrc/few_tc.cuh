@@ -166,20 +166,25 @@ struct MixedPipe {
     int pend0, pend1;
 };
 
-// Bounded wait for buffer b's outstanding MMAs.
+// Bounded wait for buffer b's outstanding MMAs.  On a timeout the commit
+// stays pending, so a later drain (the teardown's) waits for it again.
 __device__ __forceinline__ bool pipe_drain(MixedPipe &p, int b)
 {
     if (b == 0) {
         if (!p.pend0) return true;
         const bool ok = mbar_wait_bounded(&p.bar[0], p.ph0);
-        p.ph0 ^= 1u;
-        p.pend0 = 0;
+        if (ok) {
+            p.ph0 ^= 1u;
+            p.pend0 = 0;
+        }
         return ok;
     }
     if (!p.pend1) return true;
     const bool ok = mbar_wait_bounded(&p.bar[1], p.ph1);
-    p.ph1 ^= 1u;
-    p.pend1 = 0;
+    if (ok) {
+        p.ph1 ^= 1u;
+        p.pend1 = 0;
+    }
     return ok;
 }
 
@@ -205,14 +210,18 @@ __device__ __forceinline__ void mixed_setup(uint32_t *s_tmem, uint64_t *bars, in
     pp.pend0 = pp.pend1 = 0;
 }
 
-// After a timeout: let any MMA still in flight finish, then free TMEM.
+// End of a CTA: wait (bounded) for any MMA still in flight, then free TMEM.
+// When that wait itself times out, an MMA may still be writing the
+// accumulator, so the columns are left allocated rather than handed to the
+// next CTA, and the error word stays set.
 __device__ __forceinline__ void mixed_teardown(bool failed, MixedPipe &pp, int tmem_cols, int *err)
 {
-    if (failed && threadIdx.x == 0) atomicExch(err, 1);
-    pipe_drain(pp, 0);
-    pipe_drain(pp, 1);
+    const bool ok0 = pipe_drain(pp, 0);
+    const bool ok1 = pipe_drain(pp, 1);
     tc_fence_before();
-    __syncthreads();
+    const bool drained = __syncthreads_and(ok0 && ok1) != 0;
+    if ((failed || !drained) && threadIdx.x == 0) atomicExch(err, 1);
+    if (!drained) return;
     if ((threadIdx.x >> 5) == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(pp.tmem),

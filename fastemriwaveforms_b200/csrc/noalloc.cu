@@ -14,10 +14,13 @@
 // process exits.  Host code cannot use the array's name as a device address
 // (in host code it names a host-side stand-in), so the first call on each
 // device looks the address up once with cudaGetSymbolAddress, with that
-// device current, and passes it to the kernels.  The waveform is then built
-// in batches of knot segments: for each batch the folded coefficients of its
-// segments are written into the array and consumed by the sum kernel before
-// the next batch reuses the space, all in order on the caller's stream.
+// device current, and passes it to the kernels.  The address is kept for the
+// life of the process: after a cudaDeviceReset on that device (which unloads
+// the library's device code) the entry point must not be called again.  The
+// waveform is then built in batches of knot segments: for each batch the
+// folded coefficients of its segments are written into the array and consumed
+// by the sum kernel before the next batch reuses the space, all in order on
+// the caller's stream.  The caller's current device is restored on return.
 //
 // The kernels are the same ones few_get_waveform launches (k_fold_coeffs,
 // k_sum_folded); only where their scratch lives differs.
@@ -33,7 +36,8 @@ namespace few {
 
 namespace {
 
-constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // FEW_NOALLOC_SCRATCH_BYTES
+constexpr size_t kNoAllocScratchBytes = FEW_NOALLOC_SCRATCH_BYTES;
+static_assert(kNoAllocScratchBytes == (size_t(8) << 20), "the header states an 8 MiB scratch");
 constexpr int kMaxDevices = 64;
 
 // The one scratch array shared by every call on a device.  No byte of it needs
@@ -62,25 +66,14 @@ int scratch_address(int dev, unsigned char **out)
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-}  // namespace
-
-}  // namespace few
-
-extern "C" int few_get_waveform_noalloc(void *d_waveform, const double *interp_array, const double *phase_interp_t,
-                                        const double *phase_interp_coeffs, const int *d_m, const int *d_k,
-                                        const int *d_n, int init_len, int out_len, int num_teuk_modes,
-                                        const void *d_Ylms, double delta_t, const double *h_t, int dev, void *stream)
+// The body of few_get_waveform_noalloc, run with `dev` current.
+int get_waveform_noalloc(void *d_waveform, const double *interp_array, const double *phase_interp_t,
+                         const double *phase_interp_coeffs, const int *d_m, const int *d_k, const int *d_n,
+                         int init_len, int out_len, int num_teuk_modes, const void *d_Ylms, double delta_t,
+                         const double *h_t, int dev, void *stream)
 {
-    using namespace few;
-    clear_error();
-    if (!d_waveform || !interp_array || !phase_interp_t || !phase_interp_coeffs || !d_m || !d_k || !d_n || !d_Ylms ||
-        !h_t)
-        return fail(FEW_ERR_ARG, "few_get_waveform_noalloc: null pointer");
-    if (init_len < 2 || out_len < 1 || num_teuk_modes < 1)
-        return fail(FEW_ERR_SIZE, "few_get_waveform_noalloc: bad sizes");
     const int K = num_teuk_modes;
     cudaStream_t st = (cudaStream_t)stream;
-    FEW_CUDA_TRY(cudaSetDevice(dev));
     unsigned char *scratch = nullptr;
     int rc = scratch_address(dev, &scratch);
     if (rc) return rc;
@@ -193,5 +186,33 @@ extern "C" int few_get_waveform_noalloc(void *d_waveform, const double *interp_a
     cudaError_t e = cudaStreamSynchronize(st);
     if (status != FEW_OK) return status;
     if (e != cudaSuccess) return fail(FEW_ERR_CUDA, "few_get_waveform_noalloc: %s", cudaGetErrorString(e));
+    return FEW_OK;
+}
+
+}  // namespace
+}  // namespace few
+
+extern "C" int few_get_waveform_noalloc(void *d_waveform, const double *interp_array, const double *phase_interp_t,
+                                        const double *phase_interp_coeffs, const int *d_m, const int *d_k,
+                                        const int *d_n, int init_len, int out_len, int num_teuk_modes,
+                                        const void *d_Ylms, double delta_t, const double *h_t, int dev, void *stream)
+{
+    using namespace few;
+    clear_error();
+    if (!d_waveform || !interp_array || !phase_interp_t || !phase_interp_coeffs || !d_m || !d_k || !d_n || !d_Ylms ||
+        !h_t)
+        return fail(FEW_ERR_ARG, "few_get_waveform_noalloc: null pointer");
+    if (init_len < 2 || out_len < 1 || num_teuk_modes < 1)
+        return fail(FEW_ERR_SIZE, "few_get_waveform_noalloc: bad sizes");
+    // the work runs with `dev` current; the caller's current device is restored on return
+    int prev = 0;
+    FEW_CUDA_TRY(cudaGetDevice(&prev));
+    FEW_CUDA_TRY(cudaSetDevice(dev));
+    const int rc = get_waveform_noalloc(d_waveform, interp_array, phase_interp_t, phase_interp_coeffs, d_m, d_k, d_n,
+                                        init_len, out_len, num_teuk_modes, d_Ylms, delta_t, h_t, dev, stream);
+    const cudaError_t e = cudaSetDevice(prev);
+    if (rc != FEW_OK) return rc;
+    if (e != cudaSuccess)
+        return fail(FEW_ERR_CUDA, "few_get_waveform_noalloc: restoring device %d: %s", prev, cudaGetErrorString(e));
     return FEW_OK;
 }

@@ -26,7 +26,22 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libfew_ref.so")
-REFERENCE_ROOT = "/root/reference"
+
+
+def _reference_root() -> str:
+    """The reference checkout: $FEW_REFERENCE_ROOT, else the Makefile's REF default."""
+    env = os.environ.get("FEW_REFERENCE_ROOT")
+    if env:
+        return env
+    try:
+        out = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-ref"], capture_output=True,
+                             text=True, timeout=30)
+        return out.stdout.strip()
+    except (OSError, subprocess.SubprocessError):
+        return ""
+
+
+REFERENCE_ROOT = _reference_root()
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)

@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 from fastemriwaveforms_b200 import synthetic as S  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = "/root/reference/src/few"
+REF = os.path.join(O.REFERENCE_ROOT, "src", "few")
 MTSUN_SI = 4.9254909491978065e-06   # global.h:24
 YRSID_SI = 31558149.763545595       # global.h:23
 

@@ -61,7 +61,10 @@ def test_noalloc_matches_allocating_entry_point(case):
     second = call("few_get_waveform_noalloc", a, dev)
     assert rel_l2(first, ref) < TOL
     assert rel_l2(second, ref) < TOL
-    assert np.array_equal(first, second)
+    # the same kernels write every sample once from the same folded
+    # coefficients, so the batches of the fixed scratch change no bit
+    assert np.array_equal(first, ref)
+    assert np.array_equal(second, ref)
 
 
 def test_noalloc_rejects_what_does_not_fit():
