@@ -14,9 +14,12 @@ output 50 MB) exceeds the 126 MB L2, so no flush is needed between steps.
 Metric: mode-samples/s = K * samples / time.
   value  -- inputs already in HBM, device time of K steps (CUDA events, max over ranks)
   e2e    -- the same call from pinned host inputs, host<-device copy of the waveform, per step
-With N > 1 ranks (torchrun), every rank computes its own waveform (independent
-seeds): per-GPU work is fixed ("weak" scaling) and no collective touches the
-data path.
+With N > 1 ranks (torchrun) the default (--mode split) splits the one
+waveform across the ranks (ShardedInterpolatedModeSum: contiguous sample
+ranges, splines and fold built redundantly, the slices assembled by one NCCL
+all_gather, gradients summed by one all_reduce): total work is fixed
+("strong" scaling).  --mode replicas runs an independent waveform per rank
+instead ("weak" scaling, no collective on the data path).
 """
 from __future__ import annotations
 
@@ -50,6 +53,10 @@ def parse():
     ap.add_argument("--ref-window", type=int, default=32768,
                     help="--impl reference: output samples per process per step")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", choices=["split", "replicas"], default=None,
+                    help="with N > 1 ranks: split one waveform across the ranks (strong scaling, the default) or "
+                         "run an independent waveform per rank (weak scaling); --mode split on one GPU runs the "
+                         "split path in a one-rank group")
     ap.add_argument("--batch-count", type=int, default=256,
                     help="waveforms of the uneven batch (T ~ logU[1e5, 3.15e6], N ~ U[50, 2000], K ~ U[200, 3843])")
     ap.add_argument("--no-batch", action="store_true")
@@ -765,6 +772,97 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def run_split(args, world: int, rank: int, dev) -> int:
+    """One waveform split across `world` ranks: forward (slices gathered on
+    every rank), end to end from pinned host inputs, and forward + backward
+    (gradients all-reduced).  Device time, max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from fastemriwaveforms_b200.distributed import ShardedInterpolatedModeSum
+
+    inp = workload(args.workload)
+    K, T = inp.num_modes, inp.out_len
+    ims = ShardedInterpolatedModeSum(precision=args.precision, gather=True)
+    teuk_d = torch.from_numpy(inp.teuk_modes).to(dev)
+    ylms_d = torch.from_numpy(inp.ylms).to(dev)
+    pc_d = torch.from_numpy(inp.phase_coeffs).to(dev)
+    call_args = (inp.t, teuk_d, ylms_d, inp.phase_t, pc_d, inp.l, inp.m, inp.k, inp.n)
+
+    def timed(step, n):
+        dist.barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            step()
+        b.record()
+        torch.cuda.synchronize()
+        dist.barrier()
+        tm = torch.tensor([a.elapsed_time(b) / n], dtype=torch.float64, device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        return float(tm.item())
+
+    def fwd():
+        ims(*call_args, T=inp.T, dt=inp.dt)
+
+    for _ in range(max(args.warmup, 3)):
+        fwd()
+    clocks = ClockSampler(dev)
+    ms = timed(fwd, args.steps)
+    clk = clocks.stop()
+    e2e = None
+    if not args.no_e2e:
+        teuk_h = torch.from_numpy(inp.teuk_modes).pin_memory()
+        ylms_h = torch.from_numpy(inp.ylms).pin_memory()
+        pc_h = torch.from_numpy(inp.phase_coeffs).pin_memory()
+        out_h = torch.empty(T, dtype=torch.complex128).pin_memory()
+        host_args = (inp.t, teuk_h, ylms_h, inp.phase_t, pc_h, inp.l, inp.m, inp.k, inp.n)
+
+        def e2e_step():
+            h = ims(*host_args, T=inp.T, dt=inp.dt)
+            if rank == 0:
+                out_h.copy_(h[:T], non_blocking=True)
+
+        for _ in range(max(args.warmup, 3)):
+            e2e_step()
+        ems = timed(e2e_step, args.steps)
+        h2d = inp.teuk_modes.nbytes + inp.ylms.nbytes + inp.phase_coeffs.nbytes + inp.t.nbytes
+        e2e = {"value": K * T / (ems * 1e-3), "unit": METRIC, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(h2d * world), "d2h_bytes_per_step": int(T * 16)}
+    teuk_g = teuk_d.clone().requires_grad_(True)
+    pc_g = pc_d.clone().requires_grad_(True)
+    with torch.no_grad():
+        h_ref = ims(*call_args, T=inp.T, dt=inp.dt).clone()
+    upstream = torch.conj(h_ref)
+
+    def fwd_bwd():
+        teuk_g.grad = None
+        pc_g.grad = None
+        h = ims(inp.t, teuk_g, ylms_d, inp.phase_t, pc_g, inp.l, inp.m, inp.k, inp.n, T=inp.T, dt=inp.dt)
+        h.backward(upstream)
+
+    for _ in range(3):
+        fwd_bwd()
+    fb_ms = timed(fwd_bwd, max(2, args.steps // 2))
+    if rank == 0:
+        line = {"metric": METRIC, "value": K * T / (ms * 1e-3), "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {**config_of(inp, args),
+                           "parallelism": f"split x{world}: contiguous sample ranges per rank, splines and fold "
+                                          f"built on every rank, NCCL all_gather of the slices, gradient all_reduce"},
+                "e2e": e2e, "gpu_launches": 3 * args.steps * world, "cpu_baseline": None, "clocks": clk,
+                "device": torch.cuda.get_device_name(dev),
+                "fwd_bwd": {"ms_per_step": fb_ms, "value": K * T / (fb_ms * 1e-3),
+                            "note": "forward + backward through autograd, gradients all-reduced"}}
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -782,6 +880,18 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        if args.mode in (None, "split"):
+            return run_split(args, world, rank, dev)
+    elif args.mode == "split":
+        import socket
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if "MASTER_PORT" not in os.environ:
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120), device_id=dev)
+        return run_split(args, 1, 0, dev)
 
     def barrier():
         if world > 1:

@@ -87,6 +87,9 @@ SIGNATURES = {
                     _c_dbl, _c_dbl, _c_int, _c_int, _c_dbl, _vp],
     "few_aak_waveform": [_vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_int, _c_int,
                          _c_int, _c_int, _c_dbl, _vp, _vp],
+    "few_dopr853_dense": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
+                          _vp],
+    "few_dopr853_eval": [_vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp],
     "few_get_waveform_fd": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_dbl, _vp, _c_int, _c_int, _vp, _vp, _vp,
                             _c_int, _vp, _c_int, _c_int, _c_int, _vp],
 }

@@ -23,7 +23,8 @@ LIBNAME = "libfew_b200.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
 SOURCES = ["api.cu", "plan.cpp", "spline.cu", "modesum.cu", "probe.cu", "noalloc.cu", "adjoint.cu", "mixed.cu",
-           "mixed_adjoint.cu", "amplitude.cu", "geodesic.cu", "fdsum.cu", "ylm.cu", "modeselect.cu", "aak.cu", "directsum.cu"]
+           "mixed_adjoint.cu", "mixed_phase.cu", "amplitude.cu", "geodesic.cu", "fdsum.cu", "ylm.cu", "modeselect.cu", "aak.cu", "directsum.cu",
+           "dopr853.cu"]
 HEADERS = ["few_common.cuh", "few_internal.h", "few_tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

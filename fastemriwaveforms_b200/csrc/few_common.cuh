@@ -49,6 +49,7 @@ __device__ __forceinline__ double2 cpow_int(double2 z, int p)
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // Error of the rounded sum s = fl(a + b): a + b = s + err exactly (Knuth's TwoSum).
 __device__ __forceinline__ double two_sum_err(double a, double b, double s)

@@ -75,6 +75,55 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
 }
 
+// kind::i8 instruction descriptor: D s32, A and B signed 8-bit, both MN-major
+// (bit 15 / 16), M x N.
+__host__ __device__ constexpr uint32_t idesc_s8_mn(int M, int N)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+// One kind::i8 MMA (K = 32): D[s32] (+)= A[s8] B[s8], exact integer arithmetic.
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+    uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+// Signed base-128 digits of an integer |Y| <= 127 * 2^21: Y = d0 2^21 + d1 2^14
+// + d2 2^7 + d3 with d1..d3 in [-64, 63] and |d0| <= 127 (each digit fits an
+// int8).  Products of two such expansions, summed by the integer tensor core
+// level by level (level = digit index sum), are exact.
+__device__ __forceinline__ void digits4(int Y, int &d0, int &d1, int &d2, int &d3)
+{
+    d3 = ((Y + 64) & 127) - 64;
+    Y = (Y - d3) >> 7;
+    d2 = ((Y + 64) & 127) - 64;
+    Y = (Y - d2) >> 7;
+    d1 = ((Y + 64) & 127) - 64;
+    d0 = (Y - d1) >> 7;
+}
+
+// Low bytes of four ints packed little-endian into one word.
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d)
+{
+    return __byte_perm(__byte_perm((uint32_t)a, (uint32_t)b, 0x0040), __byte_perm((uint32_t)c, (uint32_t)d, 0x0040),
+                       0x5410);
+}
+
+// (re, im) byte pairs of a packed word -> (-im, re): the digits of z turned
+// into those of i z (negated digits represent the negated value exactly).
+__device__ __forceinline__ uint32_t rot_bytes(uint32_t w)
+{
+    const uint32_t t = __byte_perm(w, 0u, 0x2301);
+    return (__vneg4(t) & 0x00FF00FFu) | (t & 0xFF00FF00u);
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))

@@ -9,10 +9,8 @@
 // contraction over n' runs on the tensor cores as a real GEMM
 //     [Re v | Im v interleaved] (128 samples x 2 NNp)  x  B (2 NNp x 8R)
 // whose 8 columns per (m', k') row hold (Re Z_{c,r}, Im Z_{c,r}) for c = 0..3;
-// the epilogue applies tau^c (Horner) and u_r in FP32.  The phase adjoint uses
-// the same contraction with A = (v, tau v) and the 8 columns per row holding
-// (Y, Z) for c_b in {0, 2} (tau^c = tau^c_a tau^c_b, c_a from A), Z built from
-// n' W: Y_r = D0 + tau^2 D2, Z_r (the n'-weighted sum) likewise.
+// the epilogue applies tau^c (Horner) and u_r in FP32.  (The adjoints run in
+// exact integer arithmetic on the tensor cores: mixed_adjoint.cu, mixed_phase.cu.)
 //
 // Precision plan:
 //   * FP64: the phase polynomials, the per-sample anchors exp(-i Phi) and the
@@ -49,14 +47,12 @@ constexpr int kAStage = 2 * kMT * kKC * 2;  // A hi + lo planes of one stage (16
 // ---------------------------------------------------------------------------
 // B operand: per segment and K chunk, hi and lo bf16 tiles in the smem layout.
 // ---------------------------------------------------------------------------
-// Columns: 8 per (m', k') row r, slot = j % 8.  Sum: slot = 2 c + re/im.
-// Phase adjoint: slot = 4 yz + 2 cbl + re/im with c = c_a + 2 cbl and yz = 1
-// for the n'-weighted columns.  K chunk ch covers 16 n' (sum: block ch;
-// adjoint: block ch / 2 with c_a = ch % 2), element kk = 2 (n' - 16 block) + part.
-// One thread per 16-byte row of a core matrix (column j, K elements 8 kg ..
+// Columns: 8 per (m', k') row r, slot = j % 8 = 2 c + re/im.  K chunk ch
+// covers the 16 n' of block ch, element kk = 2 (n' - 16 ch) + part.  One
+// thread per 16-byte row of a core matrix (column j, K elements 8 kg ..
 // 8 kg + 7 = 4 n' x 2 parts); writes the hi and the lo chunk.
 __global__ void __launch_bounds__(256) k_fold_mixed(const double2 *__restrict__ W, const double *__restrict__ t_knots,
-                                                    int nseg, int R, int NN, int NB, int nchunks, int adj, int nlo,
+                                                    int nseg, int R, int NN, int NB, int nchunks,
                                                     __nv_bfloat16 *__restrict__ Bpk)
 {
     const long long per_chunk = (long long)NB * kKC;  // elements of one plane of one chunk
@@ -71,16 +67,7 @@ __global__ void __launch_bounds__(256) k_fold_mixed(const double2 *__restrict__ 
     const int s = (int)(rest / nchunks);
     const int r = j >> 3, slot = j & 7;
     const bool im_col = slot & 1;
-    int c, nblk;
-    bool zcol = false;
-    if (adj) {
-        nblk = ch >> 1;
-        c = (ch & 1) + 2 * ((slot >> 1) & 1);
-        zcol = (slot >> 2) != 0;
-    } else {
-        nblk = ch;
-        c = slot >> 1;
-    }
+    const int nblk = ch, c = slot >> 1;
     const double h = t_knots[s + 1] - t_knots[s];
     const double hc = (c == 0) ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
     float f[8];
@@ -89,9 +76,8 @@ __global__ void __launch_bounds__(256) k_fold_mixed(const double2 *__restrict__ 
         const int nidx = 16 * nblk + 4 * kg + q;
         double v0 = 0.0, v1 = 0.0;
         if (r < R && nidx < NN) {
-            const double scale = zcol ? (double)(nlo + nidx) : 1.0;
             const double2 w = W[(((long long)s * R + r) * NN + nidx) * 4 + c];
-            const double wr = w.x * hc * scale, wi = w.y * hc * scale;
+            const double wr = w.x * hc, wi = w.y * hc;
             v0 = im_col ? wi : wr;   // part 0: Re Z += Re v Re W ; Im Z += Re v Im W
             v1 = im_col ? wr : -wi;  // part 1: Re Z -= Im v Im W ; Im Z += Im v Re W
         }
@@ -117,29 +103,24 @@ struct MixedArgs {
     const int *row_m;
     const int *row_k;
     int *err;
-    const double2 *grad;  // phase adjoint: torch upstream gradient G (g = conj(G))
-    double *partial;      // phase adjoint: (nunits, 24) unit partials
     int N, R, nlo, NN, NNp, NB, nchunks, use_theta, tmem_cols;
     double dt;
 };
 
-__host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, bool adj, int &NNp, int &NB, int &nchunks)
+__host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, int &NNp, int &NB, int &nchunks)
 {
     NNp = (NN + 15) / 16 * 16;
     NB = (8 * R + 15) / 16 * 16;
-    nchunks = (adj ? 2 : 1) * NNp / 16;
+    nchunks = NNp / 16;
 }
 
 // One work unit (samples [lo, hi) of segment seg) on the tensor cores.
 // Returns false (for every thread) if a tensor-core wait timed out.
-template <bool ADJ>
 __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, MixedPipe &pp,
-                           int *s_rm, int *s_rk, double *s_pc, int unit = 0, float *s_e = nullptr,
-                           double *s_s = nullptr)
+                           int *s_rm, int *s_rk, double *s_pc)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int NB = a.NB;
-    double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // phase adjoint: this lane's share of 6 outputs
     const int bchunk = 2 * NB * kKC * 2;               // one B chunk: hi then lo planes
     const int stage = kAStage + bchunk;
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
@@ -181,8 +162,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
 
         for (int k = 0; k < nch && !failed; ++k) {
             const int b = k & 1;
-            const int nblk = ADJ ? (k >> 1) : k;
-            const bool second = ADJ && (k & 1);  // c_a = 1: A = tau v
+            const int nblk = k;
             // stage b is free once the MMAs of chunk k-2 are done
             if (__syncthreads_or(!pipe_drain(pp, b))) {
                 failed = true;
@@ -195,7 +175,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                 for (int q = tid; q < bchunk / 16; q += blockDim.x) cp_async16(sBb + 16 * q, src + 16 * q);
                 cp_async_commit();
             }
-            if (!second) {
+            {
                 // two interleaved chains (even and odd n') stepping by Er^2: half the
                 // dependent depth of one chain, and 8 FP32 steps from the anchor at most
                 v[0] = anchor((double)(nlo + 16 * nblk) * Pr);
@@ -206,7 +186,6 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                 for (int q = 0; q < 16; ++q)
                     if (!valid || 16 * nblk + q >= NN) v[q] = make_float2(0.f, 0.f);
             }
-            const float sc = second ? tau : 1.f;
             unsigned char *const aH = sAb, *const aL = sAb + kMT * kKC * 2;
 #pragma unroll
             for (int g = 0; g < 4; ++g) {  // 4 groups of 4 complex = 8 bf16 = 16 bytes
@@ -214,7 +193,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
 #pragma unroll
                 for (int e2 = 0; e2 < 4; ++e2) {
                     const float2 z = v[4 * g + e2];
-                    split2(sc * z.x, sc * z.y, h4[e2], l4[e2]);
+                    split2(z.x, z.y, h4[e2], l4[e2]);
                 }
                 const uint32_t off = tile_off(tid, 8 * g, kMT / 8);
                 *reinterpret_cast<uint4 *>(aH + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
@@ -262,8 +241,7 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
         const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
         float2 uu = make_float2(1.f, 0.f);
         int pm = 0x7fffffff, pk = 0x7fffffff;
-        const float tau2 = tau * tau;
-        float2 Sp = make_float2(0.f, 0.f), St = Sp, Sr = Sp;  // sum: Sp = h; adjoint: the three sums
+        float2 Sp = make_float2(0.f, 0.f);
         for (int c0 = 0; c0 < NB; c0 += 16) {
             float D[16];
             tmem_ld16(trow + c0, D);
@@ -282,86 +260,23 @@ __device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned
                     pm = mm;
                     pk = kk;
                     const float *d8 = D + 8 * q;
-                    if constexpr (!ADJ) {
-                        // Y = sum_c tau^c Z_c (Horner)
-                        const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
-                        const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
-                        Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
-                        Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
-                    } else {
-                        // dh/dPhi_phi = -i sum m' u Y, dh/dPhi_theta = -i sum k' u Y,
-                        // dh/dPhi_r = -i sum u Z
-                        const float2 Y = make_float2(fmaf(d8[2], tau2, d8[0]), fmaf(d8[3], tau2, d8[1]));
-                        const float2 Z = make_float2(fmaf(d8[6], tau2, d8[4]), fmaf(d8[7], tau2, d8[5]));
-                        const float2 P = fcmul(uu, Y);
-                        const float2 Q = fcmul(uu, Z);
-                        const float fm = (float)mm, fk = (float)kk;
-                        Sp.x = fmaf(fm, P.x, Sp.x);
-                        Sp.y = fmaf(fm, P.y, Sp.y);
-                        St.x = fmaf(fk, P.x, St.x);
-                        St.y = fmaf(fk, P.y, St.y);
-                        Sr.x += Q.x;
-                        Sr.y += Q.y;
-                    }
+                    // Y = sum_c tau^c Z_c (Horner)
+                    const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
+                    const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
+                    Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
+                    Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
                 }
             }
         }
-        if constexpr (!ADJ) {
-            if (valid) {
-                double2 o = a.wf[i];
-                o.x += (double)Sp.x;
-                o.y += (double)Sp.y;
-                a.wf[i] = o;
-            }
-        } else {
-            // e_f = Re(g dh/dPhi_f) = Im(g S_f), g = conj(G)
-            float ep = 0.f, et = 0.f, er = 0.f;
-            if (valid) {
-                const double2 Gt = a.grad[i];
-                const float gx = (float)Gt.x, gy = (float)Gt.y;
-                ep = gx * Sp.y - gy * Sp.x;
-                et = gx * St.y - gy * St.x;
-                er = gx * Sr.y - gy * Sr.x;
-            }
-            s_e[tid] = ep;
-            s_e[kMT + tid] = et;
-            s_e[2 * kMT + tid] = er;
-            s_s[tid] = s;
-            __syncthreads();
-            // project on b_q(s) = 1, s, s s1, s^2 s1, ... (factors s, s1 alternating):
-            // warp w accumulates outputs o = w + 4k (field o / 8, term o % 8)
-#pragma unroll
-            for (int m = 0; m < kMT / 32; ++m) {
-                const int jj = lane + 32 * m;
-                const double sj = s_s[jj], s1j = 1.0 - sj;
-                double bq[8];
-                bq[0] = 1.0;
-#pragma unroll
-                for (int q = 1; q < 8; ++q) bq[q] = bq[q - 1] * ((q & 1) ? sj : s1j);
-#pragma unroll
-                for (int kq = 0; kq < 6; ++kq) {
-                    const int o = warp + 4 * kq;
-                    const int f = o >> 3, q = o & 7;
-                    double bsel = bq[0];
-#pragma unroll
-                    for (int qq = 1; qq < 8; ++qq) bsel = (q == qq) ? bq[qq] : bsel;
-                    proj[kq] = fma(bsel, (double)s_e[f * kMT + jj], proj[kq]);
-                }
-            }
+        if (valid) {
+            double2 o = a.wf[i];
+            o.x += (double)Sp.x;
+            o.y += (double)Sp.y;
+            a.wf[i] = o;
         }
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
-    }
-    if constexpr (ADJ) {
-        if (!failed) {
-#pragma unroll
-            for (int kq = 0; kq < 6; ++kq) {
-                double v = proj[kq];
-                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-                if (lane == 0) a.partial[(long long)unit * 24 + warp + 4 * kq] = v;
-            }
-        }
     }
     cp_async_wait_all();
     return !failed;
@@ -378,7 +293,7 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
     mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
     const int u = blockIdx.x;
     const bool ok =
-        mixed_unit<false>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
+        mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
     mixed_teardown(!ok, pp, a.tmem_cols, a.err);
 }
 
@@ -405,8 +320,6 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.seg_info = d.seg_info;
         a.t_knots = d.t_knots;
         a.units = nullptr;
-        a.grad = nullptr;
-        a.partial = nullptr;
         a.row_m = d.row_m;
         a.row_k = d.row_k;
         a.err = err;
@@ -417,40 +330,19 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.use_theta = d.use_theta;
         a.dt = d.dt;
         a.tmem_cols = tmem_cols;
-        mixed_dims_core(d.R, d.NN, false, a.NNp, a.NB, a.nchunks);
-        ok = mixed_unit<false>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
+        mixed_dims_core(d.R, d.NN, a.NNp, a.NB, a.nchunks);
+        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
     }
     mixed_teardown(!ok, pp, tmem_cols, err);
 }
 
-// Phase adjoint on the tensor cores: the forward contraction with B holding
-// (Y_r, Z_r) column pairs (Z from n' W), an epilogue that forms dL/dPhi at each
-// sample and projects it on the phase basis; one CTA per work unit writes the
-// unit's 24 partials (field-major: phi, theta, r x 8 terms).
-__global__ void __launch_bounds__(kMT, 1) k_adj_phase_mixed(MixedArgs a)
-{
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_pc[24];
-    __shared__ float s_e[3 * kMT];
-    __shared__ double s_s[kMT];
-    MixedPipe pp;
-    mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
-    const int u = blockIdx.x;
-    const bool ok = mixed_unit<true>(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm,
-                                     s_rk, s_pc, u, s_e, s_s);
-    mixed_teardown(!ok, pp, a.tmem_cols, a.err);
-}
-
 }  // namespace
 
-// Tensor-core shapes of an R x NN fold grid (adj: the phase adjoint's operand).
-int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols, bool adj)
+// Tensor-core shapes of an R x NN fold grid.
+int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
 {
     if (R > 64) return fail(FEW_ERR_SIZE, "mixed form: %d (m, k) rows exceed the 64 the accumulator holds", R);
-    mixed_dims_core(R, NN, adj, *NNp, *NB, *nchunks);
+    mixed_dims_core(R, NN, *NNp, *NB, *nchunks);
     int cols = 32;
     while (cols < *NB) cols <<= 1;
     *tmem_cols = cols;
@@ -459,57 +351,25 @@ int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols, b
 
 size_t mixed_smem_bytes(int NB) { return (size_t)2 * (kAStage + 2 * NB * kKC * 2); }
 
-size_t mixed_bpk_bytes(int nseg, int R, int NN, bool adj)
+size_t mixed_bpk_bytes(int nseg, int R, int NN)
 {
     int NNp, NB, nch, cols;
-    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols, adj)) return 0;
+    if (mixed_dims(R, NN, &NNp, &NB, &nch, &cols)) return 0;
     return (size_t)nseg * nch * 2 * NB * kKC * sizeof(__nv_bfloat16);
 }
 
-int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, int nlo, bool adj, void *Bpk,
+int launch_fold_mixed(const double2 *W, const double *t_knots, int nseg, int R, int NN, void *Bpk,
                       cudaStream_t st)
 {
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols, adj);
+    int rc = mixed_dims(R, NN, &NNp, &NB, &nch, &cols);
     if (rc) return rc;
     const long long total = (long long)nseg * nch * (kKC / 8) * NB;
     if (total == 0) return FEW_OK;
     const int threads = 256;
     k_fold_mixed<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(W, t_knots, nseg, R, NN, NB, nch,
-                                                                                 adj ? 1 : 0, nlo, (__nv_bfloat16 *)Bpk);
+                                                                                 (__nv_bfloat16 *)Bpk);
     FEW_LAUNCH_CHECK("k_fold_mixed");
-    return FEW_OK;
-}
-
-int launch_adj_phase_mixed(const double2 *grad, const void *Bpk, const double *pc, int N, const double *seg_info,
-                           const double *t_knots, const int *units, int nunits, const int *row_m, const int *row_k,
-                           int R, int nlo, int NN, double dt, int use_theta, double *partial, int *err, cudaStream_t st)
-{
-    if (nunits == 0) return FEW_OK;
-    MixedArgs a;
-    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, true);
-    if (rc) return rc;
-    a.wf = nullptr;
-    a.Bpk = (const __nv_bfloat16 *)Bpk;
-    a.pc = pc;
-    a.seg_info = seg_info;
-    a.t_knots = t_knots;
-    a.units = units;
-    a.row_m = row_m;
-    a.row_k = row_k;
-    a.err = err;
-    a.grad = grad;
-    a.partial = partial;
-    a.N = N;
-    a.R = R;
-    a.nlo = nlo;
-    a.NN = NN;
-    a.use_theta = use_theta;
-    a.dt = dt;
-    const size_t smem = mixed_smem_bytes(a.NB);
-    FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_phase_mixed, (int)smem));
-    k_adj_phase_mixed<<<nunits, kMT, smem, st>>>(a);
-    FEW_LAUNCH_CHECK("k_adj_phase_mixed");
     return FEW_OK;
 }
 
@@ -519,11 +379,9 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
 {
     if (nunits == 0) return FEW_OK;
     MixedArgs a;
-    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols, false);
+    int rc = mixed_dims(R, NN, &a.NNp, &a.NB, &a.nchunks, &a.tmem_cols);
     if (rc) return rc;
     a.wf = wf;
-    a.grad = nullptr;
-    a.partial = nullptr;
     a.Bpk = (const __nv_bfloat16 *)Bpk;
     a.pc = pc;
     a.seg_info = seg_info;
@@ -550,7 +408,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
-    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols, false);
+    int rc = mixed_dims(max_R, 32, &NNp, &NB, &nch, &cols);
     if (rc) return rc;
     if (ctas <= 0) {
         int dev = 0, sms = 148;
@@ -583,12 +441,12 @@ extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, in
     few::clear_error();
     if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed: null pointer");
     if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed: bad sizes");
-    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, 0, false, Bpk, (cudaStream_t)stream);
+    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, Bpk, (cudaStream_t)stream);
 }
 
 extern "C" long long few_mixed_operand_bytes(int nseg, int R, int NN)
 {
-    return (long long)few::mixed_bpk_bytes(nseg, R, NN, false);
+    return (long long)few::mixed_bpk_bytes(nseg, R, NN);
 }
 
 extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs, int N, const double *seg_info,
@@ -604,30 +462,3 @@ extern "C" int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coef
                                  R, nlo, NN, dt, use_theta, err, (cudaStream_t)stream);
 }
 
-extern "C" long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN)
-{
-    return (long long)few::mixed_bpk_bytes(nseg, R, NN, true);
-}
-
-extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
-                                      void *stream)
-{
-    few::clear_error();
-    if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed_adjoint: null pointer");
-    if (nseg < 0 || R < 1 || NN < 1) return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: bad sizes");
-    return few::launch_fold_mixed((const double2 *)W, t_knots, nseg, R, NN, nlo, true, Bpk, (cudaStream_t)stream);
-}
-
-extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,
-                                       const double *seg_info, const double *t_knots, const int *units, int nunits,
-                                       const int *row_m, const int *row_k, int R, int nlo, int NN, double dt,
-                                       int use_theta, double *partial, int *err, void *stream)
-{
-    few::clear_error();
-    if (!grad || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !partial || !err)
-        return few::fail(FEW_ERR_ARG, "few_adjoint_phase_mixed: null pointer");
-    if (N < 2 || nunits < 0 || R < 1 || R > 64 || NN < 1)
-        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_mixed: bad sizes (R <= 64)");
-    return few::launch_adj_phase_mixed((const double2 *)grad, Bpk, phase_coeffs, N, seg_info, t_knots, units, nunits,
-                                       row_m, row_k, R, nlo, NN, dt, use_theta, partial, err, (cudaStream_t)stream);
-}

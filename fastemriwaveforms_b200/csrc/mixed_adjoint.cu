@@ -1,4 +1,5 @@
-// Amplitude adjoint of the mixed-precision mode sum on the tcgen05 tensor cores.
+// Amplitude adjoint of the mixed-precision mode sum on the tcgen05 tensor
+// cores, in exact integer arithmetic.
 //
 // Per knot segment s the gradient of L = Re sum_i g_i h_i with respect to the
 // folded coefficients is the contraction over the segment's samples
@@ -9,21 +10,34 @@
 // c_a in {0, 1} and c_b in {0, 2}, so each phasor is generated once per sample:
 //     D[(c_a, n')][(c_b, r, re/im)] += sum_{(i, part)} A[(c_a, n')][(i, part)] B[(i, part)][(c_b, r, re/im)]
 // with A = tau^c_a (Re v, Im v) and B = tau^c_b g (Re u, Im u | -Im u, Re u) for
-// part 0 | 1 (the product (v)(g u) written out in real arithmetic).  M = 2 x 64
-// n' rows per CTA (one CTA per 64 n' columns), N = (c_b, r, re/im) with 2R
-// padded to 8 (both c_b per CTA while N <= 256).  The samples are K: one CTA of
-// 8 warps owns one segment and loops over its samples in tiles of 32 (K = 64):
-// lane = sample, and the warps share the tile's operand groups (8 n' of A or 4
-// rows r of B, each written as 16-byte chunks of the MN-major no-swizzle layout:
-// core matrix = 8 K rows x 16 bytes, K groups 128 B apart, MN groups 1024 B
-// apart).  The FP64 phase prelude (phases, anchors, tau, g) is computed once per
-// sample, for 8 tiles at a time, into shared memory.  Operands are split into
-// bf16 hi + lo planes (three products hi*hi + hi*lo + lo*hi); FP32 accumulation
-// in TMEM over at most 1024 samples, then the accumulator is added into G in
-// FP64 and restarted, which keeps the FP32 rounding of long, oscillating
-// (cancelling) sums small.  Two operand buffers: while the tensor core consumes
-// tile k, the warps build tile k+1.  Every wait is bounded; a timeout sets the
-// error word, drains and frees TMEM.
+// part 0 | 1 (the product (v)(g u) written out in real arithmetic).
+//
+// Precision: the phasors, g and the powers of tau are formed in FP64 (one
+// FP64 sincos per phase and sample, FP64 recurrences), then every operand
+// value x is scaled to an integer Y = rint(x S) with |Y| <= 127 2^21 and
+// written as four signed base-128 digits (int8 planes 0..3, most significant
+// first); A's scale is fixed (|A| <= 1), B's is set per block of 1024
+// samples from the block's largest |g|.  The integer tensor core
+// (kind::i8, s32 accumulation) multiplies digit planes i and j into the
+// accumulator of level i + j (levels 0..3, ten products per K step); the
+// int32 sums are exact (no rounding anywhere in the contraction), and the
+// dropped levels >= 4 weigh below 2^-28 of the operands' scales.  After each
+// block the four levels are combined in FP64 and added into G.  The result
+// differs from the FP64 kernel only by the 2^-29 representation of the
+// operands, so its gradients carry FP64-level accuracy.
+//
+// Shape: M = 2 x 64 n' rows per CTA (one CTA per 64 n' columns), N = (c_b, r,
+// re/im) with 2R padded to 16 (both c_b per CTA while they fit one level
+// accumulator of 128 TMEM columns; the four levels fill the 512 columns).  The samples are K: one CTA of 8
+// warps owns one segment and loops over its samples in tiles of 32 (K = 64,
+// two MMA K steps): lane = sample, and the warps share the tile's operand
+// groups (16 n' of A or 8 rows r of B, each written as 16-byte chunks of the
+// MN-major no-swizzle layout: core matrix = 8 K rows x 16 bytes, K groups
+// 128 B apart, MN groups 1024 B apart).  The FP64 prelude (phasors, tau, g)
+// is computed once per sample, for 8 tiles at a time, into shared memory.  Two
+// operand buffers: while the tensor core consumes tile k, the warps build tile
+// k+1.  Every wait is bounded; a timeout sets the error word, drains and
+// frees TMEM.
 #include "few_common.cuh"
 #include "few_internal.h"
 #include "few_tc.cuh"
@@ -32,41 +46,41 @@ namespace few {
 
 namespace {
 
-constexpr int kGT = 32;            // samples per tile; K = 64 (sample x {Re, Im})
-constexpr int kGThreads = 256;     // 8 warps
-constexpr int kGPre = 8;           // tiles per prelude batch (kGPre * kGT = kGThreads samples)
-constexpr int kGPlaneA = 16 * 1024;  // one A plane: 16 MN groups (2 x 64 n') x 8 K groups x 128 B
-constexpr uint32_t kLBO = 128;     // K-group stride (bytes)
-constexpr uint32_t kSBO = 1024;    // MN-group stride (bytes)
-constexpr int kGFlush = 32;        // tiles accumulated in TMEM before each FP64 flush
+constexpr int kGT = 32;              // samples per tile; K = 64 (sample x {Re, Im})
+constexpr int kGThreads = 256;       // 8 warps
+constexpr int kGPre = 8;             // tiles per prelude batch (kGPre * kGT = kGThreads samples)
+constexpr int kGFlush = 32;          // tiles per block: one B scale, int32 sums well inside 2^31
+constexpr int kDigits = 4;           // base-128 digits per operand value
+constexpr int kPlaneA = 8 * 1024;    // one A digit plane: 8 MN groups (2 x 64 n') x 8 K groups x 128 B
+constexpr uint32_t kLBO = 128;       // K-group stride (bytes)
+constexpr uint32_t kSBO = 1024;      // MN-group stride (bytes)
+constexpr double kScaleA = 126.0 * 2097152.0;  // |A| <= 1 -> |Y| <= 126 2^21
+constexpr int kLevelCols = 128;      // TMEM columns per level accumulator (N <= 128)
 
-// Byte offset of (mn, k) in an MN-major, no-swizzle tile of K = 64.
-__device__ __forceinline__ uint32_t mn_off(int mn, int k)
+// Byte offset of (mn, k) in an MN-major, no-swizzle int8 tile of K = 64.
+__device__ __forceinline__ uint32_t mn_off8(int mn, int k)
 {
-    return (uint32_t)((mn >> 3) * kSBO + (k >> 3) * kLBO + (k & 7) * 16 + (mn & 7) * 2);
+    return (uint32_t)((mn >> 4) * kSBO + (k >> 3) * kLBO + (k & 7) * 16 + (mn & 15));
 }
 
-// Eight FP32 values -> one 16-byte hi chunk and one lo chunk.
-__device__ __forceinline__ void split8(const float *x, uint4 &hi, uint4 &lo)
-{
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) split2(x[2 * e], x[2 * e + 1], h[e], l[e]);
-    hi = make_uint4(h[0], h[1], h[2], h[3]);
-    lo = make_uint4(l[0], l[1], l[2], l[3]);
-}
-
-// (re, im) bf16 pair -> (-im, re): swap the halves, flip the new low half's
-// sign (the split is sign-symmetric, so this is the split of the negated value).
-__device__ __forceinline__ uint32_t rot_pair(uint32_t x) { return __byte_perm(x, 0u, 0x1032) ^ 0x8000u; }
-__device__ __forceinline__ uint4 rot4(uint4 v) { return make_uint4(rot_pair(v.x), rot_pair(v.y), rot_pair(v.z), rot_pair(v.w)); }
-
-// Per-sample values every operand group needs.
+// Per-sample values every operand group needs (FP64).
 struct GPrelude {
-    float2 Ep, Er, Et, g;
-    float tau, pad;
-    double Pr;
+    double2 v0;    // v_{n'} at this CTA's first n'
+    double2 Er, Er16, Ep, Et;
+    double2 g;     // conj of torch's upstream gradient
+    double tau;
 };
+
+// Digits of four values into the 4-byte lane q4 of 16-byte chunks: word[d] of
+// digit plane d.
+__device__ __forceinline__ void digit_words(const double *x, double scale, uint32_t *w)
+{
+    int d[4][4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) digits4(__double2int_rn(x[e] * scale), d[0][e], d[1][e], d[2][e], d[3][e]);
+#pragma unroll
+    for (int p = 0; p < kDigits; ++p) w[p] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+}
 
 struct AdjGMixedArgs {
     const double2 *grad;   // torch upstream gradient G; g = conj(G)
@@ -90,6 +104,8 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
     __shared__ double s_pc[24];
     __shared__ GPrelude s_pre[kGThreads];
+    __shared__ double s_gmax[kGThreads / 32];
+    __shared__ double s_scaleB;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int seg = blockIdx.x;
@@ -100,8 +116,8 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
     const long long nps = (long long)(a.N - 1) * 3;
-    const int nA = min(8, (NN - nrow0 + 7) >> 3);  // A groups: 8 n' each (both c_a)
-    const int nBg = CB >> 3;                         // B groups: 4 rows r each (all c_b of the CTA)
+    const int nA = (min(64, NN - nrow0) + 15) >> 4;  // A groups of 16 n' (each for both c_a)
+    const int nBg = CB >> 4;                         // B groups: 8 rows r (all c_b of the CTA)
     const int ngroups = nA + nBg;
 
     if (lo >= hi) {  // a segment without samples: zero gradient for this CTA's (n', c)
@@ -124,16 +140,15 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
     }
     // operand buffers start at zero: rows of A past NN and columns of B past
     // ncb * CB are never written
-    const int bplane = NB * 128;                      // one B plane: NB/8 N groups x 1024 B
-    const int smem_ops = 4 * kGPlaneA + 4 * bplane;
+    const int planeB = NB * 64;                          // one B digit plane: NB/16 MN groups x 1024 B
+    const int bufA = kDigits * kPlaneA, bufB = kDigits * planeB;
+    const int smem_ops = 2 * (bufA + bufB);
     for (int q = tid; q < smem_ops / 16; q += blockDim.x)
         reinterpret_cast<uint4 *>(smem_raw)[q] = make_uint4(0u, 0u, 0u, 0u);
     MixedPipe pp;
     mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);  // includes a __syncthreads
 
-    unsigned char *const sA = smem_raw;                  // [buffer][plane] 16 KB each
-    unsigned char *const sB = smem_raw + 4 * kGPlaneA;   // [buffer][plane] bplane each
-    const uint32_t idesc = idesc_bf16(128, NB) | (1u << 15) | (1u << 16);  // A and B MN-major
+    const uint32_t idesc = idesc_s8_mn(128, NB);
     const int k0 = 16 * (lane >> 3) + (lane & 7);  // K row of part 0 (part 1: +8)
     bool failed = false;
 
@@ -144,103 +159,155 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
             failed = true;
             break;
         }
+        if (it % kGFlush == 0) {
+            // B's scale for this block: its largest |g|
+            double gm = 0.0;
+            for (int i = base + tid; i < min(hi, base + kGFlush * kGT); i += kGThreads) {
+                const double2 Gt = a.grad[i];
+                gm = fmax(gm, sqrt(Gt.x * Gt.x + Gt.y * Gt.y));
+            }
+            for (int off = 16; off > 0; off >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, off));
+            if (lane == 0) s_gmax[warp] = gm;
+            __syncthreads();
+            if (tid == 0) {
+                double m = s_gmax[0];
+                for (int w = 1; w < kGThreads / 32; ++w) m = fmax(m, s_gmax[w]);
+                // |B| <= |g| (|u| = 1, tau <= 1); a hair of headroom for the FP64 rounding of g u
+                s_scaleB = m > 0.0 ? kScaleA / (m * (1.0 + 1e-12)) : 1.0;
+            }
+        }
         if (it % kGPre == 0) {
             // FP64 prelude for this thread's sample of the next kGPre tiles
-            // (phases as interpolate.cu:626-644, anchors reduced mod 2 pi)
+            // (phases as interpolate.cu:626-644, phasors by FP64 sincos)
             const int i = base + tid;
             const double t = (double)i * a.dt;
             const double s = (t - pt0) / pw;
             const double s1 = 1.0 - s;
             GPrelude pr;
-            const double Pr = phase_poly(s_pc + 16, s, s1);
-            pr.Pr = Pr;
-            pr.Er = anchor(Pr);
-            pr.Ep = anchor(phase_poly(s_pc, s, s1));
-            pr.Et = a.use_theta ? anchor(phase_poly(s_pc + 8, s, s1)) : make_float2(1.f, 0.f);
-            pr.tau = (float)((t - t0) / hs);
-            pr.pad = 0.f;
-            pr.g = make_float2(0.f, 0.f);
+            double sn, cs;
+            sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+            pr.Er = make_double2(cs, -sn);
+            sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+            pr.Ep = make_double2(cs, -sn);
+            if (a.use_theta) {
+                sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+                pr.Et = make_double2(cs, -sn);
+            } else {
+                pr.Et = make_double2(1.0, 0.0);
+            }
+            pr.v0 = cpow_int(pr.Er, a.nlo + nrow0);
+            double2 e16 = cmul(pr.Er, pr.Er);
+            e16 = cmul(e16, e16);
+            e16 = cmul(e16, e16);
+            pr.Er16 = cmul(e16, e16);
+            pr.tau = (t - t0) / hs;
+            pr.g = make_double2(0.0, 0.0);
             if (i < hi) {
                 const double2 Gt = a.grad[i];
-                pr.g = make_float2((float)Gt.x, (float)-Gt.y);
+                pr.g = make_double2(Gt.x, -Gt.y);
             }
             s_pre[tid] = pr;
-            __syncthreads();
         }
-        const GPrelude pr = s_pre[(it % kGPre) * kGT + lane];
-        unsigned char *const aH = sA + b * 2 * kGPlaneA, *const aL = aH + kGPlaneA;
-        unsigned char *const bH = sB + b * 2 * bplane, *const bL = bH + bplane;
+        __syncthreads();  // prelude and B scale visible
+        const GPrelude &pr = s_pre[(it % kGPre) * kGT + lane];
+        const double scaleB = s_scaleB;
+        unsigned char *const aBuf = smem_raw + b * (bufA + bufB);
+        unsigned char *const bBuf = aBuf + bufA;
         for (int gi = warp; gi < ngroups; gi += kGThreads / 32) {
             if (gi < nA) {
-                // A: tau^c_a v_{n'} for 8 n', c_a = 0 (rows 8 gi ..) and 1 (rows 64 + 8 gi ..)
-                const int n0 = nrow0 + 8 * gi;
-                float2 v = anchor((double)(a.nlo + n0) * pr.Pr);
-                float re[8], im[8];
+                // A: tau^c_a v_{n'} for 16 n' (MN 16 gi .. and 64 + 16 gi ..), 4 at a time
+                const int n0 = nrow0 + 16 * gi;
+                double2 v = pr.v0;
+                for (int q = 0; q < gi; ++q) v = cmul(v, pr.Er16);
+                const double tau = pr.tau;
+                uint32_t w[4][kDigits][4];  // [(c_a, part)][digit][word]
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const bool ok = n0 + q < NN;
-                    re[q] = ok ? v.x : 0.f;
-                    im[q] = ok ? v.y : 0.f;
-                    v = fcmul(v, pr.Er);
-                }
-                uint4 h4, l4;
+                for (int qb = 0; qb < 4; ++qb) {
+                    double re[4], im[4], tre[4], tim[4];
 #pragma unroll
-                for (int ca = 0; ca < 2; ++ca) {
-                    const int mn = 64 * ca + 8 * gi;
-                    split8(re, h4, l4);
-                    *reinterpret_cast<uint4 *>(aH + mn_off(mn, k0)) = h4;
-                    *reinterpret_cast<uint4 *>(aL + mn_off(mn, k0)) = l4;
-                    split8(im, h4, l4);
-                    *reinterpret_cast<uint4 *>(aH + mn_off(mn, k0 + 8)) = h4;
-                    *reinterpret_cast<uint4 *>(aL + mn_off(mn, k0 + 8)) = l4;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        re[q] *= pr.tau;
-                        im[q] *= pr.tau;
+                    for (int e = 0; e < 4; ++e) {
+                        const bool ok = n0 + 4 * qb + e < NN;
+                        re[e] = ok ? v.x : 0.0;
+                        im[e] = ok ? v.y : 0.0;
+                        tre[e] = tau * re[e];
+                        tim[e] = tau * im[e];
+                        v = cmul(v, pr.Er);
                     }
+                    uint32_t t4[kDigits];
+                    digit_words(re, kScaleA, t4);
+#pragma unroll
+                    for (int p = 0; p < kDigits; ++p) w[0][p][qb] = t4[p];
+                    digit_words(im, kScaleA, t4);
+#pragma unroll
+                    for (int p = 0; p < kDigits; ++p) w[1][p][qb] = t4[p];
+                    digit_words(tre, kScaleA, t4);
+#pragma unroll
+                    for (int p = 0; p < kDigits; ++p) w[2][p][qb] = t4[p];
+                    digit_words(tim, kScaleA, t4);
+#pragma unroll
+                    for (int p = 0; p < kDigits; ++p) w[3][p][qb] = t4[p];
+                }
+#pragma unroll
+                for (int p = 0; p < kDigits; ++p) {
+                    unsigned char *plane = aBuf + p * kPlaneA;
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(16 * gi, k0)) =
+                        make_uint4(w[0][p][0], w[0][p][1], w[0][p][2], w[0][p][3]);
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(16 * gi, k0 + 8)) =
+                        make_uint4(w[1][p][0], w[1][p][1], w[1][p][2], w[1][p][3]);
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(64 + 16 * gi, k0)) =
+                        make_uint4(w[2][p][0], w[2][p][1], w[2][p][2], w[2][p][3]);
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(64 + 16 * gi, k0 + 8)) =
+                        make_uint4(w[3][p][0], w[3][p][1], w[3][p][2], w[3][p][3]);
                 }
             } else {
-                // B: tau^c_b g u_r for 4 rows r, each c_b of the CTA
+                // B: tau^c_b g u_r for 8 rows r, each c_b of the CTA
                 const int rg = gi - nA;
-                float2 u4[4];
-                float2 uu = make_float2(1.f, 0.f);
+                double2 u8[8];
+                double2 uu = make_double2(1.0, 0.0);
                 int pm = 0x7fffffff, pk = 0x7fffffff;
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int r = 4 * rg + e;
-                    u4[e] = make_float2(0.f, 0.f);
+                for (int e = 0; e < 8; ++e) {
+                    const int r = 8 * rg + e;
+                    u8[e] = make_double2(0.0, 0.0);
                     if (r < R) {
                         const int mm = s_rm[r], kk = s_rk[r];
                         if (kk == pk && mm == pm + 1) {
-                            uu = fcmul(uu, pr.Ep);
+                            uu = cmul(uu, pr.Ep);
                         } else {
-                            uu = fcpow(pr.Ep, mm);
-                            if (kk) uu = fcmul(uu, fcpow(pr.Et, kk));
+                            uu = cpow_int(pr.Ep, mm);
+                            if (kk) uu = cmul(uu, cpow_int(pr.Et, kk));
                         }
                         pm = mm;
                         pk = kk;
-                        u4[e] = uu;
+                        u8[e] = uu;
                     }
                 }
-                const float t2 = pr.tau * pr.tau;
-                float2 gc = pr.g;
-                if (cbz) gc = make_float2(gc.x * t2, gc.y * t2);
+                const double t2 = pr.tau * pr.tau;
+                double2 gc = pr.g;
+                if (cbz) gc = make_double2(gc.x * t2, gc.y * t2);
                 for (int cl = 0; cl < ncb; ++cl) {
-                    float p0[8];
+                    uint32_t w0[kDigits][4];
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float2 w = fcmul(gc, u4[e]);
-                        p0[2 * e] = w.x;      // part 0 (Re v): column (c_b, r, 0) += Re v Re w, (c_b, r, 1) += Re v Im w
-                        p0[2 * e + 1] = w.y;  // part 1 (Im v) is (-Im w, Re w): rot4 of the same split
+                    for (int qb = 0; qb < 4; ++qb) {  // rows 2 qb, 2 qb + 1: (re, im, re, im)
+                        const double2 wa = cmul(gc, u8[2 * qb]), wb = cmul(gc, u8[2 * qb + 1]);
+                        const double x4[4] = {wa.x, wa.y, wb.x, wb.y};
+                        uint32_t t4[kDigits];
+                        digit_words(x4, scaleB, t4);
+#pragma unroll
+                        for (int p = 0; p < kDigits; ++p) w0[p][qb] = t4[p];
                     }
-                    uint4 h4, l4;
-                    split8(p0, h4, l4);
-                    const int mn = cl * CB + 8 * rg;
-                    *reinterpret_cast<uint4 *>(bH + mn_off(mn, k0)) = h4;
-                    *reinterpret_cast<uint4 *>(bL + mn_off(mn, k0)) = l4;
-                    *reinterpret_cast<uint4 *>(bH + mn_off(mn, k0 + 8)) = rot4(h4);
-                    *reinterpret_cast<uint4 *>(bL + mn_off(mn, k0 + 8)) = rot4(l4);
-                    gc = make_float2(gc.x * t2, gc.y * t2);
+                    const int mn = cl * CB + 16 * rg;
+#pragma unroll
+                    for (int p = 0; p < kDigits; ++p) {
+                        unsigned char *plane = bBuf + p * planeB;
+                        // part 0 (Re v): (Re w, Im w); part 1 (Im v): (-Im w, Re w)
+                        *reinterpret_cast<uint4 *>(plane + mn_off8(mn, k0)) =
+                            make_uint4(w0[p][0], w0[p][1], w0[p][2], w0[p][3]);
+                        *reinterpret_cast<uint4 *>(plane + mn_off8(mn, k0 + 8)) =
+                            make_uint4(rot_bytes(w0[p][0]), rot_bytes(w0[p][1]), rot_bytes(w0[p][2]),
+                                       rot_bytes(w0[p][3]));
+                    }
+                    gc = make_double2(gc.x * t2, gc.y * t2);
                 }
             }
         }
@@ -248,26 +315,32 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a_h = smem_u32(aH), a_l = smem_u32(aL);
-            const uint32_t b_h = smem_u32(bH), b_l = smem_u32(bL);
+            const uint32_t a0 = smem_u32(aBuf), b0 = smem_u32(bBuf);
+            const bool fresh = (it % kGFlush) == 0;
 #pragma unroll
-            for (int st = 0; st < 4; ++st) {  // K steps of 16 = K groups 2st, 2st+1
-                const uint32_t ko = st * 2 * kLBO;
-                const uint64_t da_h = smem_desc(a_h + ko, kLBO, kSBO), da_l = smem_desc(a_l + ko, kLBO, kSBO);
-                const uint64_t db_h = smem_desc(b_h + ko, kLBO, kSBO), db_l = smem_desc(b_l + ko, kLBO, kSBO);
-                mma_bf16(pp.tmem, da_h, db_h, idesc, ((it % kGFlush) | st) != 0);
-                mma_bf16(pp.tmem, da_h, db_l, idesc, 1u);
-                mma_bf16(pp.tmem, da_l, db_h, idesc, 1u);
+            for (int st = 0; st < 2; ++st) {  // K steps of 32 = K groups 4 st .. 4 st + 3
+                const uint32_t ko = st * 4 * kLBO;
+#pragma unroll
+                for (int lv = 0; lv < kDigits; ++lv) {
+#pragma unroll
+                    for (int i = 0; i <= lv; ++i) {
+                        const int j = lv - i;
+                        const uint64_t da = smem_desc(a0 + i * kPlaneA + ko, kLBO, kSBO);
+                        const uint64_t db = smem_desc(b0 + j * planeB + ko, kLBO, kSBO);
+                        mma_s8(pp.tmem + (uint32_t)(lv * kLevelCols), da, db, idesc,
+                               (fresh && st == 0 && i == 0) ? 0u : 1u);
+                    }
+                }
             }
             mma_commit(&pp.bar[b]);
         }
         if (b == 0) pp.pend0 = 1;
         else pp.pend1 = 1;
         if ((it % kGFlush) == kGFlush - 1 || base + kGT >= hi) {
-            // flush: every MMA done, then the accumulator (row (c_a, n'), column
-            // (c_b, r, re/im)) into G in FP64, stored by the first flush and added
-            // by the later ones; the next MMA restarts the accumulator.  Warps w
-            // and w+4 read the same TMEM lanes (32 (w % 4) ..) and share the columns.
+            // block done: every MMA finished, then the four levels combined in
+            // FP64 (row (c_a, n'), column (c_b, r, re/im)) and added into G (stored
+            // by the first block); the next MMA restarts the accumulators.
+            // Warps w and w+4 read the same TMEM lanes (32 (w % 4) ..) and share the columns.
             const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
             if (__syncthreads_or(!(ok0 && ok1))) {
                 failed = true;
@@ -275,14 +348,25 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
             }
             tc_fence_after();
             const bool first = it < kGFlush;
+            const double unit = 1.0 / (kScaleA * scaleB) * 4398046511104.0;  // 2^42 / (S_A S_B)
             const int quad = warp & 3;
             const int row = 32 * quad + lane;
             const int ca = row >> 6, n = nrow0 + (row & 63);
             const uint32_t trow = pp.tmem + ((uint32_t)(quad * 32) << 16);
             for (int j16 = warp >> 2; j16 < NB / 16; j16 += 2) {
-                float D[16];
-                tmem_ld16(trow + 16 * j16, D);
-                tmem_wait_ld();
+                double acc[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+                double wl = unit;
+#pragma unroll
+                for (int lv = 0; lv < kDigits; ++lv) {
+                    float D[16];
+                    tmem_ld16(trow + (uint32_t)(lv * kLevelCols + 16 * j16), D);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) acc[e] = fma((double)__float_as_int(D[e]), wl, acc[e]);
+                    wl *= 0.0078125;  // 2^-7 per level
+                }
                 if (n < NN) {
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
@@ -292,7 +376,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
                             const int c = ca + cbz + 2 * cl;
                             const double hc = c == 0 ? 1.0 : (c == 1 ? hs : (c == 2 ? hs * hs : hs * hs * hs));
                             double2 *gp = a.G + (((long long)seg * R + r) * NN + n) * 4 + c;
-                            double2 v = make_double2((double)D[2 * e] * hc, (double)D[2 * e + 1] * hc);
+                            double2 v = make_double2(acc[2 * e] * hc, acc[2 * e + 1] * hc);
                             if (!first) {
                                 const double2 o = *gp;
                                 v.x += o.x;
@@ -319,10 +403,12 @@ int launch_adj_G_mixed(const double2 *grad, const double *pc, int N, const doubl
 {
     if (nseg == 0) return FEW_OK;
     AdjGMixedArgs a;
-    a.CB = (2 * R + 7) / 8 * 8;  // columns per c_b: (r, re/im), padded to 8
-    a.ncb = 2 * a.CB <= 256 ? 2 : 1;
-    if (a.ncb * a.CB > 256) return fail(FEW_ERR_SIZE, "few_adjoint_G_mixed: %d rows exceed the 128 one MMA holds", R);
-    a.NB = (a.ncb * a.CB + 15) / 16 * 16;
+    a.CB = (2 * R + 15) / 16 * 16;  // columns per c_b: (r, re/im), padded to 16
+    // four level accumulators of kLevelCols columns each fill the 512 TMEM columns
+    a.ncb = 2 * a.CB <= kLevelCols ? 2 : 1;
+    if (a.ncb * a.CB > kLevelCols)
+        return fail(FEW_ERR_SIZE, "few_adjoint_G_mixed: %d rows exceed the 64 the accumulators hold", R);
+    a.NB = a.ncb * a.CB;
     a.grad = grad;
     a.pc = pc;
     a.seg_info = seg_info;
@@ -338,10 +424,8 @@ int launch_adj_G_mixed(const double2 *grad, const double *pc, int N, const doubl
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    int cols = 32;
-    while (cols < a.NB) cols <<= 1;
-    a.tmem_cols = cols;
-    const size_t smem = (size_t)4 * kGPlaneA + (size_t)4 * a.NB * 128;
+    a.tmem_cols = 512;
+    const size_t smem = (size_t)2 * (kDigits * kPlaneA + kDigits * a.NB * 64);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_adj_G_mixed, (int)smem));
     dim3 grid(nseg, (NN + 63) / 64, 2 / a.ncb);
     k_adj_G_mixed<<<grid, kGThreads, smem, st>>>(a);
@@ -359,8 +443,8 @@ extern "C" int few_adjoint_G_mixed(const void *grad, const double *phase_coeffs,
     few::clear_error();
     if (!grad || !phase_coeffs || !seg_info || !t_knots || !seg_start || !row_m || !row_k || !G || !err)
         return few::fail(FEW_ERR_ARG, "few_adjoint_G_mixed: null pointer");
-    if (N < 2 || nseg < 0 || nseg > N - 1 || R < 1 || R > 128 || NN < 1 || NN > 65535 * 64)
-        return few::fail(FEW_ERR_SIZE, "few_adjoint_G_mixed: bad sizes (R <= 128)");
+    if (N < 2 || nseg < 0 || nseg > N - 1 || R < 1 || R > 64 || NN < 1 || NN > 65535 * 64)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_G_mixed: bad sizes (R <= 64)");
     return few::launch_adj_G_mixed((const double2 *)grad, phase_coeffs, N, seg_info, t_knots, seg_start, nseg, row_m,
                                    row_k, R, nlo, NN, dt, use_theta, (double2 *)G, err, (cudaStream_t)stream);
 }

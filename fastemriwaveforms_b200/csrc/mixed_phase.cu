@@ -1,0 +1,475 @@
+// Phase adjoint of the mixed-precision mode sum on the tcgen05 tensor cores,
+// in exact integer arithmetic.
+//
+// The gradient of L = Re sum_i g_i h_i with respect to the phase coefficients
+// needs, per sample, dh/dPhi_phi = -i sum_r m'_r u_r Y_r, dh/dPhi_theta (k'_r
+// weights) and dh/dPhi_r = -i sum_r u_r Z_r, with
+//     Y_r(t) = sum_c tau^c sum_{n'} v_{n'}(t) W'[c][n'][r],   Z_r likewise with n' W'
+// (W' = W h_s^c, tau = (t - t_s)/h_s, v = exp(-i n' Phi_r), u = exp(-i (m' Phi_phi
+// + k' Phi_theta))); then e_f = Re(g dh/dPhi_f) is projected on the 8-term
+// basis b_q(s) and summed per work unit, exactly as the FP64 kernel
+// k_adj_phase does.  These sums cancel heavily (the coherent part of
+// conj(h) dh/dPhi is imaginary), so the per-sample values need close to FP64
+// accuracy: the contraction over n' runs on the integer tensor core.
+//
+//   A[i][(c_a, n', part)] = tau_i^c_a (Re v_{n'} | Im v_{n'})(t_i), c_a in {0, 1}
+//   B[(c_a, n', part)][(r, slot)] per segment, slot = 4 yz + 2 cbl + re/im:
+//       the real-arithmetic form of w = W'[c_a + 2 cbl][n'][r] (times n' for
+//       yz = 1): part Re v -> (Re w, Im w), part Im v -> (-Im w, Re w)
+//   D = A B  ->  (Y, Z) of each row for c_b = 2 cbl, and Y = D_0 + tau^2 D_2.
+//
+// Precision: v, u, g, tau in FP64 (FP64 sincos of each phase, FP64
+// recurrences); every operand value is scaled to an integer |Y| <= 126 2^21
+// (A: fixed scale, |A| <= 1; B: one scale per segment and column, from the
+// column's largest value) and split into four signed base-128 digits (int8
+// planes).  kind::i8 MMAs multiply digit planes i and j into the level i + j
+// accumulator (levels 0..3, ten products per K step, s32, exact); the levels
+// are combined in FP64 and the epilogue (u_r, the row sums, e_f, the
+// projection) runs in FP64.  The only error left is the 2^-29 representation
+// of the operands.
+//
+// Shape: one CTA of 128 threads per work unit (<= 1024 samples of one
+// segment), one sample row per thread per 128-sample tile; K = (c_a, n',
+// part) in steps of 32 (16 n' x {Re, Im}); the rows r are taken in passes of
+// at most 8 (N = 64 columns: four levels fill 256 TMEM columns, two CTAs per
+// SM).  A is generated per pass and K step by the threads while the B step
+// arrives by cp.async; two stages, an mbarrier per stage (tcgen05.commit).
+// Every wait is bounded; a timeout sets the error word and ends the kernel
+// after freeing TMEM.
+#include "few_common.cuh"
+#include "few_internal.h"
+#include "few_tc.cuh"
+
+namespace few {
+
+namespace {
+
+constexpr int kPT = 128;                            // samples per tile (MMA M)
+constexpr int kKS = 32;                             // K per MMA step: 16 n' x {Re, Im}
+constexpr int kDig = 4;                             // digits per operand value
+constexpr int kRowsPass = 8;                        // (m', k') rows per pass
+constexpr int kLvl = 64;                            // TMEM columns per level (8 rows x 8 slots)
+constexpr int kTmemCols = kDig * kLvl;              // 256
+constexpr int kAPlane = kPT * kKS;                  // A digit plane of a K step: 4 KB
+constexpr int kBPlane = 8 * kRowsPass * kKS;        // B digit plane of a K step and pass: 2 KB
+constexpr int kStage = kDig * (kAPlane + kBPlane);  // 24 KB
+constexpr double kScale = 126.0 * 2097152.0;        // |value| <= max -> |Y| <= 126 2^21
+constexpr int kMaxPhaseRows = 64;
+
+// Byte offset of (row, kk) in a K-major, no-swizzle int8 tile of one K step
+// (kk < 32): core matrices of 8 rows x 16 bytes, the two K halves 128 B apart
+// (LBO), 8-row groups 256 B apart (SBO).
+__host__ __device__ __forceinline__ uint32_t koff8(int row, int kk)
+{
+    return (uint32_t)((row >> 3) * 256 + ((kk >> 4) & 1) * 128 + (row & 7) * 16 + (kk & 15));
+}
+
+__host__ __device__ constexpr uint32_t idesc_s8_k(int M, int N)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Sixteen values -> their four digit chunks (16 bytes each, digit-plane order).
+__device__ __forceinline__ void digit_chunks(const double *x, double scale, uint4 *out)
+{
+    uint32_t w[kDig][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        int d[kDig][4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            digits4(__double2int_rn(x[4 * q + e] * scale), d[0][e], d[1][e], d[2][e], d[3][e]);
+#pragma unroll
+        for (int p = 0; p < kDig; ++p) w[p][q] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+    }
+#pragma unroll
+    for (int p = 0; p < kDig; ++p) out[p] = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+}
+
+// Per segment the packed operand is one block: the NBc column scales
+// (doubles), then the digit planes [K step][digit][NBc/8 column groups x 256 B].
+struct PhaseDims {
+    int NNp, nb, nks, Re, NBc;
+    long long dig_bytes;  // digit bytes of one segment
+    long long seg_bytes;  // the whole block of one segment (scales + digits)
+};
+
+__host__ __device__ inline PhaseDims phase_dims(int R, int NN)
+{
+    PhaseDims d;
+    d.NNp = (NN + 15) / 16 * 16;
+    d.nb = d.NNp / 16;
+    d.nks = 2 * d.nb;            // c_a in {0, 1}
+    d.Re = R + (R & 1);          // rows padded to even: every pass has N % 16 == 0
+    d.NBc = 8 * d.Re;
+    d.dig_bytes = (long long)d.nks * kDig * d.NBc * kKS;
+    d.seg_bytes = (long long)d.NBc * 8 + d.dig_bytes;  // both multiples of 16 bytes
+    return d;
+}
+
+// B operand: one warp per (segment, column): the column's values over K, their
+// largest magnitude (the column's scale), then the digit chunks.
+__global__ void __launch_bounds__(256) k_fold_phase_s8(const double2 *__restrict__ W,
+                                                       const double *__restrict__ t_knots, int nseg, int R, int NN,
+                                                       int nlo, unsigned char *__restrict__ Bpk)
+{
+    const PhaseDims pd = phase_dims(R, NN);
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (long long)nseg * pd.NBc) return;
+    const int s = (int)(w / pd.NBc), j = (int)(w % pd.NBc);
+    const int r = j >> 3, slot = j & 7;
+    const int ri = slot & 1, cbl = (slot >> 1) & 1, yz = slot >> 2;
+    const double h = t_knots[s + 1] - t_knots[s];
+    const int nchunks = 2 * pd.nks;  // 16 K values each
+    auto value = [&](int ks, int kk) -> double {
+        const int ca = ks / pd.nb, blk = ks % pd.nb;
+        const int n = 16 * blk + (kk >> 1), part = kk & 1;
+        if (r >= R || n >= NN) return 0.0;
+        const int c = ca + 2 * cbl;
+        const double hc = c == 0 ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
+        const double2 wv = W[(((long long)s * R + r) * NN + n) * 4 + c];
+        const double f = yz ? hc * (double)(nlo + n) : hc;
+        const double wr = wv.x * f, wi = wv.y * f;
+        return part == 0 ? (ri ? wi : wr) : (ri ? wr : -wi);
+    };
+    double m = 0.0;
+    for (int q = lane; q < nchunks; q += 32)
+        for (int e = 0; e < 16; ++e) m = fmax(m, fabs(value(q >> 1, 16 * (q & 1) + e)));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    const double scale = m > 0.0 ? kScale / (m * (1.0 + 1e-12)) : 1.0;
+    unsigned char *const block = Bpk + (long long)s * pd.seg_bytes;
+    if (lane == 0) reinterpret_cast<double *>(block)[j] = scale;
+    for (int q = lane; q < nchunks; q += 32) {
+        const int ks = q >> 1, half = q & 1;
+        double x[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) x[e] = value(ks, 16 * half + e);
+        uint4 ch[kDig];
+        digit_chunks(x, scale, ch);
+#pragma unroll
+        for (int p = 0; p < kDig; ++p) {
+            unsigned char *dst = block + (long long)pd.NBc * 8 + ((long long)ks * kDig + p) * pd.NBc * kKS +
+                                 koff8(j, 16 * half);
+            *reinterpret_cast<uint4 *>(dst) = ch[p];
+        }
+    }
+}
+
+struct PhaseArgs {
+    const double2 *grad;  // torch upstream gradient G; g = conj(G)
+    const unsigned char *Bpk;
+    const double *pc;
+    const double *seg_info;
+    const double *t_knots;
+    const int *units;
+    const int *row_m;
+    const int *row_k;
+    double *partial;      // (nunits, 24)
+    int *err;
+    int N, R, nlo, NN, use_theta;
+    double dt;
+};
+
+__global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_rm[kMaxPhaseRows], s_rk[kMaxPhaseRows];
+    __shared__ double s_pc[24];
+    __shared__ double s_scale[8 * kMaxPhaseRows];
+    __shared__ double s_e[3][kPT];
+    __shared__ double s_s[kPT];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int unit = blockIdx.x;
+    const int seg = a.units[3 * unit], lo = a.units[3 * unit + 1], hi = a.units[3 * unit + 2];
+    const PhaseDims pd = phase_dims(a.R, a.NN);
+    const int R = a.R, NN = a.NN, nks = pd.nks, nb = pd.nb;
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
+    const long long nps = (long long)(a.N - 1) * 3;
+
+    for (int r = tid; r < R; r += blockDim.x) {
+        s_rm[r] = a.row_m[r];
+        s_rk[r] = a.row_k[r];
+    }
+    const unsigned char *const block = a.Bpk + (long long)seg * pd.seg_bytes;
+    for (int j = tid; j < pd.NBc; j += blockDim.x) s_scale[j] = reinterpret_cast<const double *>(block)[j];
+    if (tid < 24) {
+        const int q = tid >> 3, c = tid & 7;
+        s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    MixedPipe pp;
+    mixed_setup(&s_tmem, s_bar, kTmemCols, pp);  // includes a __syncthreads
+
+    const unsigned char *const Bseg = block + (long long)pd.NBc * 8;
+    const int npass = (pd.Re + kRowsPass - 1) / kRowsPass;
+    const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
+    double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's share of the unit's 24 outputs
+    bool failed = false;
+    int kstep = 0;  // stage index runs on across tiles and passes
+
+    for (int base = lo; base < hi && !failed; base += kPT) {
+        const int i = base + tid;
+        const bool valid = i < hi;
+        // FP64 prelude (phases as interpolate.cu:626-644)
+        const double t = (double)i * a.dt;
+        const double tau = (t - t0) / hs;
+        const double s = (t - pt0) / pw;
+        const double s1 = 1.0 - s;
+        double sn, cs;
+        sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+        const double2 Ep = make_double2(cs, -sn);
+        sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+        const double2 Er = make_double2(cs, -sn);
+        double2 Et = make_double2(1.0, 0.0);
+        if (a.use_theta) {
+            sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+            Et = make_double2(cs, -sn);
+        }
+        const double2 vlo = cpow_int(Er, a.nlo);
+        const double tau2 = tau * tau;
+        double2 Sp = make_double2(0.0, 0.0), St = Sp, Sr = Sp;
+        double2 uu = make_double2(1.0, 0.0);
+        int pm = 0x7fffffff, pk = 0x7fffffff;
+
+        for (int pass = 0; pass < npass && !failed; ++pass) {
+            const int r0 = pass * kRowsPass, rows = min(kRowsPass, pd.Re - r0);
+            const int ncols = 8 * rows;
+            const uint32_t idesc = idesc_s8_k(kPT, ncols);
+            double2 v = vlo;
+            for (int ks = 0; ks < nks; ++ks, ++kstep) {
+                const int b = kstep & 1;
+                if (__syncthreads_or(!pipe_drain(pp, b))) {
+                    failed = true;
+                    break;
+                }
+                unsigned char *const sA = smem_raw + b * kStage;
+                unsigned char *const sB = sA + kDig * kAPlane;
+                // B step: this pass's rows of the four digit planes (rows * 256 bytes each)
+                {
+                    const int per_plane = rows * 16;  // 16-byte chunks
+                    for (int q = tid; q < kDig * per_plane; q += blockDim.x) {
+                        const int p = q / per_plane, c = q - p * per_plane;
+                        const unsigned char *src = Bseg + ((long long)ks * kDig + p) * pd.NBc * kKS + r0 * 256 + 16 * c;
+                        cp_async16(sB + p * kBPlane + 16 * c, src);
+                    }
+                    cp_async_commit();
+                }
+                // A step: tau^c_a v_{n'} for 16 n' (FP64 recurrence, restarted for each c_a)
+                {
+                    const int ca = ks / nb, blk = ks - ca * nb;
+                    if (blk == 0) v = vlo;
+                    double x[2 * 16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const bool ok = valid && (16 * blk + q < NN);
+                        const double f = ca ? tau : 1.0;
+                        x[2 * q] = ok ? f * v.x : 0.0;
+                        x[2 * q + 1] = ok ? f * v.y : 0.0;
+                        v = cmul(v, Er);
+                    }
+#pragma unroll
+                    for (int half = 0; half < 2; ++half) {
+                        uint4 ch[kDig];
+                        digit_chunks(x + 16 * half, kScale, ch);
+#pragma unroll
+                        for (int p = 0; p < kDig; ++p)
+                            *reinterpret_cast<uint4 *>(sA + p * kAPlane + koff8(tid, 16 * half)) = ch[p];
+                    }
+                }
+                cp_async_wait_all();
+                fence_async_smem();
+                __syncthreads();
+                if (tid == 0) {
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+                    for (int lv = 0; lv < kDig; ++lv) {
+#pragma unroll
+                        for (int ia = 0; ia <= lv; ++ia) {
+                            const int jb = lv - ia;
+                            const uint64_t da = smem_desc(a0 + ia * kAPlane, 128, 256);
+                            const uint64_t db = smem_desc(b0 + jb * kBPlane, 128, 256);
+                            mma_s8(pp.tmem + (uint32_t)(lv * kLvl), da, db, idesc, (ks == 0 && ia == 0) ? 0u : 1u);
+                        }
+                    }
+                    mma_commit(&pp.bar[b]);
+                }
+                if (b == 0) pp.pend0 = 1;
+                else pp.pend1 = 1;
+            }
+            if (failed) break;
+            const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
+            if (__syncthreads_or(!(ok0 && ok1))) {
+                failed = true;
+                break;
+            }
+            tc_fence_after();
+            // epilogue of the pass: the four levels of each row's 8 columns in FP64,
+            // (Y, Z) of each row, u_r, and the three weighted row sums
+            for (int rp = 0; rp < rows / 2; ++rp) {
+                int D[kDig][16];
+#pragma unroll
+                for (int lv = 0; lv < kDig; ++lv) {
+                    float f[16];
+                    tmem_ld16(trow + (uint32_t)(lv * kLvl + 16 * rp), f);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) D[lv][e] = __float_as_int(f[e]);
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int r = r0 + 2 * rp + q;
+                    if (r >= R) continue;
+                    double val[8];
+#pragma unroll
+                    for (int sl = 0; sl < 8; ++sl) {
+                        double acc = 0.0, wl = 4398046511104.0;  // 2^42
+#pragma unroll
+                        for (int lv = 0; lv < kDig; ++lv) {
+                            acc = fma((double)D[lv][8 * q + sl], wl, acc);
+                            wl *= 0.0078125;
+                        }
+                        val[sl] = acc / (kScale * s_scale[8 * r + sl]);
+                    }
+                    const int mm = s_rm[r], kk = s_rk[r];
+                    if (kk == pk && mm == pm + 1) {
+                        uu = cmul(uu, Ep);
+                    } else {
+                        uu = cpow_int(Ep, mm);
+                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
+                    }
+                    pm = mm;
+                    pk = kk;
+                    const double2 Y = make_double2(fma(val[2], tau2, val[0]), fma(val[3], tau2, val[1]));
+                    const double2 Z = make_double2(fma(val[6], tau2, val[4]), fma(val[7], tau2, val[5]));
+                    const double2 P = cmul(uu, Y), Q = cmul(uu, Z);
+                    Sp.x = fma((double)mm, P.x, Sp.x);
+                    Sp.y = fma((double)mm, P.y, Sp.y);
+                    St.x = fma((double)kk, P.x, St.x);
+                    St.y = fma((double)kk, P.y, St.y);
+                    Sr.x += Q.x;
+                    Sr.y += Q.y;
+                }
+            }
+            tc_fence_before();
+            __syncthreads();  // TMEM read before the next pass's first MMA overwrites it
+            tc_fence_after();
+        }
+        if (failed) break;
+        // e_f = Re(g dh/dPhi_f) = Im(g S_f), g = conj(G)
+        double ep = 0.0, et = 0.0, er = 0.0;
+        if (valid) {
+            const double2 Gt = a.grad[i];
+            ep = Gt.x * Sp.y - Gt.y * Sp.x;
+            et = Gt.x * St.y - Gt.y * St.x;
+            er = Gt.x * Sr.y - Gt.y * Sr.x;
+        }
+        s_e[0][tid] = ep;
+        s_e[1][tid] = et;
+        s_e[2][tid] = er;
+        s_s[tid] = s;
+        __syncthreads();
+        // project on b_q(s) = 1, s, s s1, s^2 s1, ... (factors s, s1 alternating):
+        // warp w accumulates outputs o = w + 4k (field o / 8, term o % 8)
+#pragma unroll
+        for (int m = 0; m < kPT / 32; ++m) {
+            const int jj = lane + 32 * m;
+            const double sj = s_s[jj], s1j = 1.0 - sj;
+            double bq[8];
+            bq[0] = 1.0;
+#pragma unroll
+            for (int q = 1; q < 8; ++q) bq[q] = bq[q - 1] * ((q & 1) ? sj : s1j);
+#pragma unroll
+            for (int kq = 0; kq < 6; ++kq) {
+                const int o = warp + 4 * kq;
+                const int f = o >> 3, q = o & 7;
+                double bsel = bq[0];
+#pragma unroll
+                for (int qq = 1; qq < 8; ++qq) bsel = (q == qq) ? bq[qq] : bsel;
+                proj[kq] = fma(bsel, s_e[f][jj], proj[kq]);
+            }
+        }
+        __syncthreads();  // s_e, s_s read before the next tile writes them
+    }
+    if (!failed) {
+#pragma unroll
+        for (int kq = 0; kq < 6; ++kq) {
+            double v = proj[kq];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0) a.partial[(long long)unit * 24 + warp + 4 * kq] = v;
+        }
+    }
+    cp_async_wait_all();
+    mixed_teardown(failed, pp, kTmemCols, a.err);
+}
+
+}  // namespace
+
+size_t phase_operand_bytes(int nseg, int R, int NN)
+{
+    if (R > kMaxPhaseRows) return 0;
+    return (size_t)nseg * (size_t)phase_dims(R, NN).seg_bytes;
+}
+
+}  // namespace few
+
+extern "C" long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN)
+{
+    if (nseg < 0 || R < 1 || NN < 1) return 0;
+    return (long long)few::phase_operand_bytes(nseg, R, NN);
+}
+
+extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
+                                      void *stream)
+{
+    few::clear_error();
+    if (!W || !t_knots || !Bpk) return few::fail(FEW_ERR_ARG, "few_fold_mixed_adjoint: null pointer");
+    if (nseg < 0 || R < 1 || R > few::kMaxPhaseRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: bad sizes (R <= %d)", few::kMaxPhaseRows);
+    if (nseg == 0) return FEW_OK;
+    const few::PhaseDims d = few::phase_dims(R, NN);
+    const long long threads = (long long)nseg * d.NBc * 32;
+    few::k_fold_phase_s8<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        (const double2 *)W, t_knots, nseg, R, NN, nlo, (unsigned char *)Bpk);
+    FEW_LAUNCH_CHECK("k_fold_phase_s8");
+    return FEW_OK;
+}
+
+extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,
+                                       const double *seg_info, const double *t_knots, const int *units, int nunits,
+                                       const int *row_m, const int *row_k, int R, int nlo, int NN, double dt,
+                                       int use_theta, double *partial, int *err, void *stream)
+{
+    few::clear_error();
+    if (!grad || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !partial || !err)
+        return few::fail(FEW_ERR_ARG, "few_adjoint_phase_mixed: null pointer");
+    if (N < 2 || nunits < 0 || R < 1 || R > few::kMaxPhaseRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_mixed: bad sizes (R <= %d)", few::kMaxPhaseRows);
+    if (nunits == 0) return FEW_OK;
+    few::PhaseArgs a;
+    a.grad = (const double2 *)grad;
+    a.Bpk = (const unsigned char *)Bpk;
+    a.pc = phase_coeffs;
+    a.seg_info = seg_info;
+    a.t_knots = t_knots;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.partial = partial;
+    a.err = err;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const int smem = 2 * few::kStage;
+    FEW_CUDA_TRY(few::ensure_smem_attr((const void *)few::k_adj_phase_s8, smem));
+    few::k_adj_phase_s8<<<nunits, few::kPT, smem, (cudaStream_t)stream>>>(a);
+    FEW_LAUNCH_CHECK("k_adj_phase_s8");
+    return FEW_OK;
+}

@@ -522,3 +522,42 @@ def direct_case(samples: int = 20001, K: int = 24, seed: int = 61):
     n = rng.integers(-3, 3, K)
     ylms = (rng.standard_normal(2 * K) + 1j * rng.standard_normal(2 * K)) / np.sqrt(2.0)
     return t, teuk, ylms, phases, l, m, k, n
+
+
+def toy_inspiral_ode(xp):
+    """A smooth inspiral-like ODE in the reference integrator's signature
+    ``ode(x, y, dydx, additionalArgs)`` (src/few/trajectory/dopr853.py:208),
+    batched over systems: y (8, nsys) = (p, e, x_I, Phi_phi, Phi_theta,
+    Phi_r, u, v), x (nsys,) the time in seconds; (u, v) is an oscillator of
+    period ~31 ks that wobbles e (so that the stepper takes ~1000 steps over
+    1e6 s).  ``xp`` is numpy (the reference's stepper) or torch (device
+    arrays).  Only +, -, *, / and sqrt appear, all correctly rounded on both,
+    and every division is array / array (torch turns a division by or of a
+    Python number into a multiplication by a reciprocal), so the two give the
+    same bits for the same inputs.
+
+        dp/dt   = -1e-6 (1 + 7.3 e^2) (12 / p)^3
+        de/dt   = -5e-8 e (12 / p)^4 + 1e-7 u
+        dx/dt   = -1e-8 (1 - x^2)
+        dPhi_phi/dt = w = 2 pi 1e-3 (12 / p)^(3/2)
+        dPhi_theta/dt = w (1 - 0.5 / p)
+        dPhi_r/dt   = w (1 - 6 / p) sqrt(1 - e^2)
+        du/dt = 2e-4 v,  dv/dt = -2e-4 u
+    """
+
+    def ode(x, y, dydx, additional_args):
+        p, e, xi, u, v = y[0], y[1], y[2], y[6], y[7]
+        one = xp.ones_like(p)
+        q = (12.0 * one) / p
+        q3 = q * q * q
+        w = 6.283185307179586e-3 * (q * xp.sqrt(q))
+        dydx[0] = -1e-6 * (1.0 + 7.3 * (e * e)) * q3
+        dydx[1] = -5e-8 * e * (q3 * q) + 1e-7 * u
+        dydx[2] = -1e-8 * (1.0 - xi * xi)
+        dydx[3] = w
+        dydx[4] = w * (1.0 - (0.5 * one) / p)
+        dydx[5] = w * (1.0 - (6.0 * one) / p) * xp.sqrt(1.0 - e * e)
+        dydx[6] = 2e-4 * v
+        dydx[7] = -2e-4 * u
+
+    return ode

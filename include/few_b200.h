@@ -308,29 +308,35 @@ FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, c
                           const int *seg_start, int nseg, const int *row_m, const int *row_k, int R, int nlo, int NN,
                           double dt, int use_theta, void *G, void *stream);
 
-/* Mixed-precision adjoint (tcgen05, split BF16, FP32 accumulation; no
- * counterpart in the reference).  Same quantities as few_adjoint_G and
- * few_adjoint_phase, computed with the precision plan of few_sum_mixed; err
- * [device] int is set to 1 if a tensor-core wait timed out. */
+/* Tensor-core adjoint (no counterpart in the reference).  Same quantities as
+ * few_adjoint_G and few_adjoint_phase, with the contractions on the tcgen05
+ * integer tensor cores in exact arithmetic: FP64 operands (phasors, g, powers
+ * of tau, folded coefficients) scaled to 28-bit integers and split into four
+ * int8 digits, digit products summed in int32 per level and combined in FP64;
+ * the results differ from the FP64 kernels by the 2^-29 representation of the
+ * operands only.  err [device] int is set to 1 if a tensor-core wait timed out. */
 
 /* few_adjoint_G on the tensor cores: the contraction over each segment's
- * samples with K = samples.  t_knots [device] (N,).  R <= 128. */
+ * samples with K = samples.  t_knots [device] (N,).  R <= 64. */
 FEW_API int few_adjoint_G_mixed(const void *grad, const double *phase_coeffs, int N, const double *seg_info,
                                 const double *t_knots, const int *seg_start, int nseg, const int *row_m,
                                 const int *row_k, int R, int nlo, int NN, double dt, int use_theta, void *G, int *err,
                                 void *stream);
 
-/* Bytes of the B operand of the mixed phase adjoint (0 if R > 64). */
+/* Bytes of the packed operand of the tensor-core phase adjoint (0 if R > 64):
+ * per segment the column scales and the int8 digit planes. */
 FEW_API long long few_mixed_adjoint_operand_bytes(int nseg, int R, int NN);
 
-/* Packs W into the phase adjoint's B operand: per (m', k') row the columns
- * (Re Y, Im Y) of few_fold_mixed and (Re Z, Im Z) from n' W (n' = nlo + column). */
+/* Packs W into the phase adjoint's operand: per (m', k') row 8 columns, the
+ * real form of W[c] h^c for c = c_a + {0, 2} (Y) and of n' W[c] h^c (Z,
+ * n' = nlo + column), each column scaled by its largest value and split into
+ * four int8 digits. */
 FEW_API int few_fold_mixed_adjoint(const void *W, const double *t_knots, int nseg, int R, int nlo, int NN, void *Bpk,
                                    void *stream);
 
-/* few_adjoint_phase on the tensor cores: the forward contraction against the
- * packed (Y, Z) operand, dL/dPhi per sample in the epilogue, projected on the
- * basis per work unit into partial [device] (nunits, 24).  R <= 64. */
+/* few_adjoint_phase on the tensor cores: the contraction over n' against the
+ * packed (Y, Z) operand, dL/dPhi per sample in an FP64 epilogue, projected on
+ * the basis per work unit into partial [device] (nunits, 24).  R <= 64. */
 FEW_API int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const double *phase_coeffs, int N,
                                     const double *seg_info, const double *t_knots, const int *units, int nunits,
                                     const int *row_m, const int *row_k, int R, int nlo, int NN, double dt,
@@ -533,6 +539,39 @@ FEW_API int few_aak_waveform(void *waveform, const double *interp_array, double 
 FEW_API int few_aak_sum(void *waveform, const double *coef, int cstride, const double *t_knots, const int *first,
                         int nseg, int total, double M_phys, double S_phys, double mu, double qS, double phiS,
                         double qK, double phiK, double dist, int nmodes, int mich, double delta_t, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Trajectory dense output (DOPR853), the producer of phase_interp_coeffs    */
+/* ------------------------------------------------------------------------ */
+
+/* One phase of DOPR853.prep_evaluate (src/few/trajectory/dopr853.py:621-758)
+ * over a batch of nsys steps of a node-component system; all pointers
+ * [device].  The basis of each step needs f at the step's end and at three
+ * extra stages, which the caller evaluates between the phases (the ODE is the
+ * trajectory's, not this library's):
+ *   phase 0: in x0, h0, y0, y1 (node, nsys), dydx1 = f(x1, y1), stages
+ *            (10, node, nsys) = k1..k10 as take_step leaves them (slots 2
+ *            and 3 hold stages 11 and 12); out rcont[..., 0..3], the stored
+ *            stages' part of rcont[..., 4..7], arg = stage 14's argument,
+ *            xarg (nsys,) its time;
+ *   phase 1: in k14 = f(xarg, arg); out arg, xarg of stage 15;
+ *   phase 2: in k14, k15; out arg, xarg of stage 16;
+ *   phase 3: in k14, k15, k16; completes rcont[..., 4..7].
+ * rcont (nsys, node, 8) is the reference's layout; its components 3..5 of a
+ * trajectory (Phi_phi, Phi_theta, Phi_r) are InterpolatedModeSum's
+ * phase_interp_coeffs.  Sums are rounded in the reference's order. */
+FEW_API int few_dopr853_dense(const double *x0, const double *h0, const double *x1, const double *y0,
+                              const double *y1, const double *dydx1, const double *stages, const double *k14,
+                              const double *k15, const double *k16, double *arg, double *xarg, double *rcont,
+                              int node, int nsys, int phase, void *stream);
+
+/* DOPR853.eval (order 0) and eval_derivative (orders 1..3)
+ * (dopr853.py:760-875): out [device] (npts, node) at t_new [device] (npts,)
+ * from coeffs [device] (nold-1, node, 8) on the knots t_old [device] (nold,).
+ * t_new must lie in [t_old[0], t_old[nold-1]] (the Python layer checks and
+ * raises ValueError as the reference does). */
+FEW_API int few_dopr853_eval(const double *t_new, int npts, const double *t_old, int nold, const double *coeffs,
+                             int node, int order, double *out, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Measurement                                                              */

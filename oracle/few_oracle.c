@@ -249,18 +249,35 @@ static void oracle_segment_f64(double *wf, const double *interp, const double *p
  * m*Phi_phi + k*Phi_theta + n*Phi_r, its sine/cosine, the amplitude and the
  * products are formed in long double.  This is the accuracy reference for the
  * recurrence form, which does not round the combined mode phase. */
+/* The 8-term basis in long double (the nested form of interpolate.cu:642-644). */
+static long double basis_ld(const double *c, long double s)
+{
+    long double s1 = 1.0L - s;
+    return c[0] + s * (c[1] + s1 * (c[2] + s * (c[3] + s1 * (c[4] + s * (c[5] + s1 * (c[6] + s * (long double)c[7]))))));
+}
+
+/* dpc (same layout as pc) and delta: when dpc is given, the phases are
+ * Phi + delta * dPhi evaluated in long double (a finite-difference probe whose
+ * step is not rounded into the large phase coefficients); otherwise Phi is
+ * evaluated in double exactly as the reference does. */
 static void oracle_segment_ext(double *wf, const double *interp, const double *pc,
                                const int *m_arr, const int *k_arr, const int *n_arr, int K,
                                const double *ylm, double dt, double start_t, int seg,
-                               int i_lo, int i_hi, int init_len, double pt0, double pwidth)
+                               int i_lo, int i_hi, int init_len, double pt0, double pwidth,
+                               const double *dpc, long double delta)
 {
     const size_t num_base = (size_t)init_len * (size_t)(2 * K);
     const size_t nps = (size_t)(init_len - 1) * 3;
-    double pp[8], pt[8], pr[8];
+    double pp[8], pt[8], pr[8], dp[8], dt8[8], dr[8];
     for (int c = 0; c < 8; ++c) {
         pp[c] = pc[c * nps + (size_t)seg * 3 + 0];
         pt[c] = pc[c * nps + (size_t)seg * 3 + 1];
         pr[c] = pc[c * nps + (size_t)seg * 3 + 2];
+        if (dpc) {
+            dp[c] = dpc[c * nps + (size_t)seg * 3 + 0];
+            dt8[c] = dpc[c * nps + (size_t)seg * 3 + 1];
+            dr[c] = dpc[c * nps + (size_t)seg * 3 + 2];
+        }
     }
     const double *cr[4], *ci[4];
     for (int c = 0; c < 4; ++c) {
@@ -272,9 +289,17 @@ static void oracle_segment_ext(double *wf, const double *interp, const double *p
         double x = t - start_t;
         double s = (t - pt0) / pwidth;
         double s1 = 1.0 - s;
-        double Pp = pp[0] + s * (pp[1] + s1 * (pp[2] + s * (pp[3] + s1 * (pp[4] + s * (pp[5] + s1 * (pp[6] + s * pp[7]))))));
-        double Pt = pt[0] + s * (pt[1] + s1 * (pt[2] + s * (pt[3] + s1 * (pt[4] + s * (pt[5] + s1 * (pt[6] + s * pt[7]))))));
-        double Pr = pr[0] + s * (pr[1] + s1 * (pr[2] + s * (pr[3] + s1 * (pr[4] + s * (pr[5] + s1 * (pr[6] + s * pr[7]))))));
+        long double Pp, Pt, Pr;
+        if (dpc) {
+            long double sl = ((long double)t - pt0) / pwidth;
+            Pp = basis_ld(pp, sl) + delta * basis_ld(dp, sl);
+            Pt = basis_ld(pt, sl) + delta * basis_ld(dt8, sl);
+            Pr = basis_ld(pr, sl) + delta * basis_ld(dr, sl);
+        } else {
+            Pp = pp[0] + s * (pp[1] + s1 * (pp[2] + s * (pp[3] + s1 * (pp[4] + s * (pp[5] + s1 * (pp[6] + s * pp[7]))))));
+            Pt = pt[0] + s * (pt[1] + s1 * (pt[2] + s * (pt[3] + s1 * (pt[4] + s * (pt[5] + s1 * (pt[6] + s * pt[7]))))));
+            Pr = pr[0] + s * (pr[1] + s1 * (pr[2] + s * (pr[3] + s1 * (pr[4] + s * (pr[5] + s1 * (pr[6] + s * pr[7]))))));
+        }
         long double X = x;
         long double tr = 0.0L, ti = 0.0L;
         for (int j = 0; j < K; ++j) {
@@ -307,10 +332,38 @@ static void oracle_segment_ext(double *wf, const double *interp, const double *p
  * extended = 0: double precision in the reference's operation order;
  * extended = 1: the long double restatement above.
  * Returns 0, or a negative code when the knots do not reach the output end. */
+static int get_waveform_impl(double *wf, const double *interp_array, const double *phase_interp_t,
+                             const double *phase_interp_coeffs, const int *m_arr, const int *k_arr,
+                             const int *n_arr, int init_len, int out_len, int K, const double *ylm,
+                             double dt, const double *h_t, int s_lo, int s_hi, int extended,
+                             const double *dpc, long double delta);
+
 int oracle_get_waveform(double *wf, const double *interp_array, const double *phase_interp_t,
                         const double *phase_interp_coeffs, const int *m_arr, const int *k_arr,
                         const int *n_arr, int init_len, int out_len, int K, const double *ylm,
                         double dt, const double *h_t, int s_lo, int s_hi, int extended)
+{
+    return get_waveform_impl(wf, interp_array, phase_interp_t, phase_interp_coeffs, m_arr, k_arr, n_arr, init_len,
+                             out_len, K, ylm, dt, h_t, s_lo, s_hi, extended, 0, 0.0L);
+}
+
+/* The long double sum with the phases Phi + delta * dPhi (dpc: the basis of a
+ * phase perturbation, laid out as phase_interp_coeffs), for finite
+ * differences of the phase inputs. */
+int oracle_get_waveform_dphase(double *wf, const double *interp_array, const double *phase_interp_t,
+                               const double *phase_interp_coeffs, const double *dpc, double delta,
+                               const int *m_arr, const int *k_arr, const int *n_arr, int init_len, int out_len,
+                               int K, const double *ylm, double dt, const double *h_t, int s_lo, int s_hi)
+{
+    return get_waveform_impl(wf, interp_array, phase_interp_t, phase_interp_coeffs, m_arr, k_arr, n_arr, init_len,
+                             out_len, K, ylm, dt, h_t, s_lo, s_hi, 1, dpc, (long double)delta);
+}
+
+static int get_waveform_impl(double *wf, const double *interp_array, const double *phase_interp_t,
+                             const double *phase_interp_coeffs, const int *m_arr, const int *k_arr,
+                             const int *n_arr, int init_len, int out_len, int K, const double *ylm,
+                             double dt, const double *h_t, int s_lo, int s_hi, int extended,
+                             const double *dpc, long double delta)
 {
     if (init_len < 2 || out_len < 1 || K < 1) return -1;
     int *start = (int *)malloc(sizeof(int) * (size_t)init_len);
@@ -324,7 +377,7 @@ int oracle_get_waveform(double *wf, const double *interp_array, const double *ph
         double pt0 = phase_interp_t[j], pw = phase_interp_t[j + 1] - phase_interp_t[j];
         if (extended)
             oracle_segment_ext(wf, interp_array, phase_interp_coeffs, m_arr, k_arr, n_arr, K, ylm,
-                               dt, h_t[j], j, a, b, init_len, pt0, pw);
+                               dt, h_t[j], j, a, b, init_len, pt0, pw, dpc, delta);
         else
             oracle_segment_f64(wf, interp_array, phase_interp_coeffs, m_arr, k_arr, n_arr, K, ylm,
                                dt, h_t[j], j, a, b, init_len, pt0, pw);

@@ -75,6 +75,10 @@ def _lib(impl: str):
         lib.oracle_get_waveform.argtypes = [_dp, _dp, _dp, _dp, _ip, _ip, _ip, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, _dp, ctypes.c_double, _dp, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int]
+        lib.oracle_get_waveform_dphase.restype = ctypes.c_int
+        lib.oracle_get_waveform_dphase.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_double, _ip, _ip, _ip,
+                                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double,
+                                                   _dp, ctypes.c_int, ctypes.c_int]
         lib.oracle_find_start_inds.restype = ctypes.c_int
         lib.oracle_find_start_inds.argtypes = [_ip, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int]
         lib.oracle_interp2d.argtypes = [_dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
@@ -177,13 +181,16 @@ def prepare_sum(inp):
 
 
 def mode_sum(inp, impl: str = "oracle", extended: bool = False, window=None,
-             coeffs: np.ndarray | None = None, out_len: int | None = None) -> np.ndarray:
+             coeffs: np.ndarray | None = None, out_len: int | None = None, dphase=None) -> np.ndarray:
     """The waveform of ``InterpolatedModeSum.__call__`` on the CPU.
 
     impl="oracle": the C restatement (``extended`` selects the long double
     form; ``window=(lo, hi)`` computes only those output samples, the rest
     stay zero).  impl="ref": the reference's own get_waveform (whole output).
-    ``coeffs`` optionally supplies amplitude spline coefficients (4, N, 2K)."""
+    ``coeffs`` optionally supplies amplitude spline coefficients (4, N, 2K).
+    ``dphase=(dcoeffs, delta)`` (long double form only) adds delta times the
+    phase basis dcoeffs (N-1, 3, 8) to the phases in long double: a phase
+    finite difference whose step is not rounded into the large coefficients."""
     from fastemriwaveforms_b200.synthetic import output_length
 
     K = inp.teuk_modes.shape[1]
@@ -202,7 +209,16 @@ def mode_sum(inp, impl: str = "oracle", extended: bool = False, window=None,
     ylm_flat = np.ascontiguousarray(ylms).view(np.float64)
     wf = np.zeros(out_len, dtype=np.complex128)
     lib = _lib(impl)
-    if impl == "oracle":
+    if impl == "oracle" and dphase is not None:
+        lo, hi = (0, out_len) if window is None else window
+        dpc_in, delta = dphase
+        dpc = np.ascontiguousarray(np.transpose(np.asarray(dpc_in, dtype=np.float64), (2, 0, 1)).reshape(-1))
+        st = lib.oracle_get_waveform_dphase(_p(wf.view(np.float64)), _p(interp), _p(pt), _p(pc), _p(dpc),
+                                            float(delta), _p(m, _ip), _p(k, _ip), _p(n, _ip), N, out_len, K,
+                                            _p(ylm_flat), float(inp.dt), _p(h_t), int(lo), int(hi))
+        if st != 0:
+            raise ValueError(f"oracle mode sum failed with status {st}")
+    elif impl == "oracle":
         lo, hi = (0, out_len) if window is None else window
         st = lib.oracle_get_waveform(_p(wf.view(np.float64)), _p(interp), _p(pt), _p(pc), _p(m, _ip), _p(k, _ip),
                                      _p(n, _ip), N, out_len, K, _p(ylm_flat), float(inp.dt), _p(h_t),
@@ -602,3 +618,81 @@ def direct_sum(teuk, ylms, phases, l, m, k, n) -> np.ndarray:
     w2 = ((-1.0) ** l[:, pos] * np.asarray(ylms)[None, K:][:, pos] * np.conj(teuk[:, pos])
           * np.exp(1j * phase[:, pos])).sum(axis=1)
     return w1 + w2
+
+
+# ---------------------------------------------------------------------------
+# DOPR853 dense output (src/few/trajectory/dopr853.py)
+# ---------------------------------------------------------------------------
+
+# Dense-output weights of DOP853 (Hairer, Norsett & Wanner; dopr853.py:130-181):
+# rows rcont5..8, columns k1, k6, k7, k8, k9, k10, k11, k12, f(x1), k14, k15, k16.
+DOPR853_D = np.array([
+    [-0.84289382761090128651353491142e01, 0.56671495351937776962531783590e00, -0.30689499459498916912797304727e01,
+     0.23846676565120698287728149680e01, 0.21170345824450282767155149946e01, -0.87139158377797299206789907490e00,
+     0.22404374302607882758541771650e01, 0.63157877876946881815570249290e00, -0.88990336451333310820698117400e-01,
+     0.18148505520854727256656404962e02, -0.91946323924783554000451984436e01, -0.44360363875948939664310572000e01],
+    [0.10427508642579134603413151009e02, 0.24228349177525818288430175319e03, 0.16520045171727028198505394887e03,
+     -0.37454675472269020279518312152e03, -0.22113666853125306036270938578e02, 0.77334326684722638389603898808e01,
+     -0.30674084731089398182061213626e02, -0.93321305264302278729567221706e01, 0.15697238121770843886131091075e02,
+     -0.31139403219565177677282850411e02, -0.93529243588444783865713862664e01, 0.35816841486394083752465898540e02],
+    [0.19985053242002433820987653617e02, -0.38703730874935176555105901742e03, -0.18917813819516756882830838328e03,
+     0.52780815920542364900561016686e03, -0.11573902539959630126141871134e02, 0.68812326946963000169666922661e01,
+     -0.10006050966910838403183860980e01, 0.77771377980534432092869265740e00, -0.27782057523535084065932004339e01,
+     -0.60196695231264120758267380846e02, 0.84320405506677161018159903784e02, 0.11992291136182789328035130030e02],
+    [-0.25693933462703749003312586129e02, -0.15418974869023643374053993627e03, -0.23152937917604549567536039109e03,
+     0.35763911791061412378285349910e03, 0.93405324183624310003907691704e02, -0.37458323136451633156875139351e02,
+     0.10409964950896230045147246184e03, 0.29840293426660503123344363579e02, -0.43533456590011143754432175058e02,
+     0.96324553959188282948394950600e02, -0.39177261675615439165231486172e02, -0.14972683625798562581422125276e03]])
+# extra stages 14..16 (dopr853.py:98-128): node, then couplings in the reference's summation order
+DOPR853_EXTRA = [
+    (0.1, [(0, 5.61675022830479523392909219681e-2), (6, 2.53500210216624811088794765333e-1),
+           (7, -2.46239037470802489917441475441e-1), (8, -1.24191423263816360469010140626e-1),
+           (9, 1.5329179827876569731206322685e-1), (1, 8.20105229563468988491666602057e-3),
+           (2, 7.56789766054569976138603589584e-3), ("f", -8.298e-3)]),
+    (0.2, [(0, 3.18346481635021405060768473261e-2), (5, 2.83009096723667755288322961402e-2),
+           (6, 5.35419883074385676223797384372e-2), (7, -5.49237485713909884646569340306e-2),
+           (1, -1.08347328697249322858509316994e-4), (2, 3.82571090835658412954920192323e-4),
+           ("f", -3.40465008687404560802977114492e-4), (14, 1.41312443674632500278074618366e-1)]),
+    (0.777777777777777777777777777778,
+     [(0, -4.28896301583791923408573538692e-1), (5, -4.69762141536116384314449447206e0),
+      (6, 7.68342119606259904184240953878e0), (7, 4.06898981839711007970213554331e0),
+      (8, 3.56727187455281109270669543021e-1), ("f", -1.39902416515901462129418009734e-3),
+      (14, 2.9475147891527723389556272149e0), (15, -9.15095847217987001081870187138e0)]),
+]
+
+
+def dopr853_prep_evaluate(x0, y0, h0, x1, y1, stages, ode, args=None):
+    """DOPR853.prep_evaluate (dopr853.py:621-758) restated in numpy, batched:
+    x0, h0, x1 (nsys,), y0, y1 (node, nsys), stages (10, node, nsys) as
+    take_step leaves them (slots 1, 2 = stages 11, 12); ``ode(x, y, dydx,
+    args)`` the right-hand side.  Every sum runs left to right as numpy
+    evaluates the reference's expressions.  Returns rcont (nsys, node, 8)."""
+    k = [np.asarray(s, dtype=np.float64) for s in stages]
+    f1 = np.zeros_like(y0)
+    ode(x1, y1, f1, args)
+    diff = y1 - y0
+    bspl = h0 * k[0] - diff
+    rc = [y0, diff, bspl, diff - h0 * f1 - bspl]
+    cols = [k[0], k[5], k[6], k[7], k[8], k[9], k[1], k[2]]
+    part = []
+    for q in range(4):
+        s = DOPR853_D[q][0] * cols[0]
+        for c in range(1, 8):
+            s = s + DOPR853_D[q][c] * cols[c]
+        part.append(s)
+    extra = {}
+    for node_c, terms in DOPR853_EXTRA:
+        s = None
+        for src, coef in terms:
+            v = f1 if src == "f" else (extra[src] if src in (14, 15) else k[src])
+            s = coef * v if s is None else s + coef * v
+        arg = y0 + h0 * s
+        out = np.zeros_like(y0)
+        ode(x0 + node_c * h0, arg, out, args)
+        extra[14 + len(extra)] = out
+    for q in range(4):
+        s = part[q]
+        for c, v in zip(range(8, 12), (f1, extra[14], extra[15], extra[16])):
+            s = s + DOPR853_D[q][c] * v
+        rc.append(h0 * s)
+    return np.array(rc).T

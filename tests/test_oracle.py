@@ -172,3 +172,27 @@ def test_direct_sum_oracle_matches_reference_golden(oracle):
     assert h.hexdigest() == str(d["digest"])  # the inputs the golden output was made from
     got = oracle.direct_sum(teuk, ylms, phases, l, m, k, n)
     assert np.linalg.norm(got - d["waveform"]) <= 1e-13 * np.linalg.norm(d["waveform"])
+
+
+def test_dopr853_dense_output_oracle_matches_reference_golden(oracle):
+    """The numpy restatement of DOPR853.prep_evaluate, batched over all the
+    steps at once, against the reference's own prep_evaluate_single run
+    after each step (tests/golden/make_dopr853_golden.py): bit for bit."""
+    d = np.load(os.path.join(GOLDEN, "dopr853_dense.npz"))
+    stages = np.transpose(d["stages"], (1, 2, 0))  # (10, node, nsys)
+    got = oracle.dopr853_prep_evaluate(d["x0"], d["y0"].T.copy(), d["h0"], d["x1"], d["y1"].T.copy(), stages,
+                                       S.toy_inspiral_ode(np))
+    assert np.array_equal(got, d["rcont"])
+
+
+def test_adjoint_fd_fixture_inputs_are_reproduced():
+    """The finite-difference fixture belongs to synthetic.adjoint_case's inputs."""
+    import hashlib
+
+    fx = np.load(os.path.join(GOLDEN, "adjoint_fd.npz"))
+    inp = S.adjoint_case(seed=int(fx["input_seed"]))
+    h = hashlib.sha256()
+    for a in (inp.t, inp.teuk_modes, inp.ylms, inp.phase_knots, inp.phase_coeffs, inp.m, inp.n):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest()[:32] == str(fx["digest"])
+    assert len(fx["fd"]) == 64 and set(fx["family"].tolist()) == {0, 1, 2, 3}
