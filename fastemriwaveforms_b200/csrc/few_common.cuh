@@ -58,6 +58,24 @@ __device__ __forceinline__ double two_sum_err(double a, double b, double s)
     return __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
 }
 
+// sin and cos of a large angle: Cody & Waite reduction mod 2 pi (2 pi split in
+// three parts, k*C1 and k*C2 exact for |k| < 2^21), then sincos on |r| <= pi,
+// which stays on the function's short path (large arguments take its slow,
+// table-driven reduction).
+__device__ __forceinline__ void sincos_reduced(double ph, double *s, double *c)
+{
+    const double kInv2Pi = 0.15915494309189535;
+    const double kC1 = 0x1.921fb54400000p+2, kC2 = 0x1.0b4611a600000p-32, kC3 = 0x1.3198a2e037073p-67;
+    double r = ph;
+    const double kq = rint(ph * kInv2Pi);
+    if (fabs(kq) < 2097152.0) {
+        r = __fma_rn(-kq, kC1, ph);
+        r = __fma_rn(-kq, kC2, r);
+        r = __fma_rn(-kq, kC3, r);
+    }
+    sincos(r, s, c);
+}
+
 // The 8-term dense-output phase polynomial in s, s1 = 1 - s, in the
 // operation order of src/few/cutils/interpolate.cu:642-644, every product and
 // sum rounded separately.

@@ -95,25 +95,40 @@ __device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a_desc, uint64_
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
 }
 
-// Signed base-128 digits of an integer |Y| <= 127 * 2^21: Y = d0 2^21 + d1 2^14
-// + d2 2^7 + d3 with d1..d3 in [-64, 63] and |d0| <= 127 (each digit fits an
-// int8).  Products of two such expansions, summed by the integer tensor core
-// level by level (level = digit index sum), are exact.
-__device__ __forceinline__ void digits4(int Y, int &d0, int &d1, int &d2, int &d3)
+// rint(x * scale) as an int32 (|x * scale| < 2^31) without a conversion
+// instruction: x * scale + 1.5 * 2^52, rounded once by the FMA, holds the
+// rounded integer in the low 32 bits of its significand.
+__device__ __forceinline__ int scaled_rint(double x, double scale)
 {
-    d3 = ((Y + 64) & 127) - 64;
-    Y = (Y - d3) >> 7;
-    d2 = ((Y + 64) & 127) - 64;
-    Y = (Y - d2) >> 7;
-    d1 = ((Y + 64) & 127) - 64;
-    d0 = (Y - d1) >> 7;
+    return __double2loint(__fma_rn(x, scale, 6755399441055744.0));
 }
 
-// Low bytes of four ints packed little-endian into one word.
-__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d)
+// Signed base-128 digits of integers |Y| <= 127 * 2^21: Y = d0 2^21 + d1 2^14
+// + d2 2^7 + d3 with d1..d3 in [-64, 63] and |d0| <= 127 (each digit fits an
+// int8).  Products of two such expansions, summed by the integer tensor core
+// level by level (level = digit index sum), are exact.  Four values at a
+// time, each digit plane packed into one word (byte e = value e): with the
+// bias 64 (1 + 2^7 + 2^14) added, the three low digits are plain 7-bit
+// fields minus 64 and the top digit is the arithmetic shift by 21.
+__device__ __forceinline__ void digit_words4(int y0, int y1, int y2, int y3, uint32_t *w)
 {
-    return __byte_perm(__byte_perm((uint32_t)a, (uint32_t)b, 0x0040), __byte_perm((uint32_t)c, (uint32_t)d, 0x0040),
-                       0x5410);
+    constexpr int kBias = 64 + (64 << 7) + (64 << 14);
+    y0 += kBias;
+    y1 += kBias;
+    y2 += kBias;
+    y3 += kBias;
+    const uint32_t lo01 = __byte_perm((uint32_t)y0, (uint32_t)y1, 0x0040);
+    const uint32_t lo23 = __byte_perm((uint32_t)y2, (uint32_t)y3, 0x0040);
+    w[3] = __vsub4(__byte_perm(lo01, lo23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
+    const uint32_t a01 = __byte_perm((uint32_t)(y0 >> 7), (uint32_t)(y1 >> 7), 0x0040);
+    const uint32_t a23 = __byte_perm((uint32_t)(y2 >> 7), (uint32_t)(y3 >> 7), 0x0040);
+    w[2] = __vsub4(__byte_perm(a01, a23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
+    const uint32_t b01 = __byte_perm((uint32_t)(y0 >> 14), (uint32_t)(y1 >> 14), 0x0040);
+    const uint32_t b23 = __byte_perm((uint32_t)(y2 >> 14), (uint32_t)(y3 >> 14), 0x0040);
+    w[1] = __vsub4(__byte_perm(b01, b23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
+    const uint32_t c01 = __byte_perm((uint32_t)(y0 >> 21), (uint32_t)(y1 >> 21), 0x0040);
+    const uint32_t c23 = __byte_perm((uint32_t)(y2 >> 21), (uint32_t)(y3 >> 21), 0x0040);
+    w[0] = __byte_perm(c01, c23, 0x5410);
 }
 
 // (re, im) byte pairs of a packed word -> (-im, re): the digits of z turned

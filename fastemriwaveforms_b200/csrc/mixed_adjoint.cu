@@ -75,11 +75,8 @@ struct GPrelude {
 // digit plane d.
 __device__ __forceinline__ void digit_words(const double *x, double scale, uint32_t *w)
 {
-    int d[4][4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) digits4(__double2int_rn(x[e] * scale), d[0][e], d[1][e], d[2][e], d[3][e]);
-#pragma unroll
-    for (int p = 0; p < kDigits; ++p) w[p] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+    digit_words4(scaled_rint(x[0], scale), scaled_rint(x[1], scale), scaled_rint(x[2], scale),
+                 scaled_rint(x[3], scale), w);
 }
 
 struct AdjGMixedArgs {
@@ -185,12 +182,12 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
             const double s1 = 1.0 - s;
             GPrelude pr;
             double sn, cs;
-            sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+            sincos_reduced(phase_poly(s_pc + 16, s, s1), &sn, &cs);
             pr.Er = make_double2(cs, -sn);
-            sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+            sincos_reduced(phase_poly(s_pc, s, s1), &sn, &cs);
             pr.Ep = make_double2(cs, -sn);
             if (a.use_theta) {
-                sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+                sincos_reduced(phase_poly(s_pc + 8, s, s1), &sn, &cs);
                 pr.Et = make_double2(cs, -sn);
             } else {
                 pr.Et = make_double2(1.0, 0.0);

@@ -12,11 +12,12 @@
 // conj(h) dh/dPhi is imaginary), so the per-sample values need close to FP64
 // accuracy: the contraction over n' runs on the integer tensor core.
 //
-//   A[i][(c_a, n', part)] = tau_i^c_a (Re v_{n'} | Im v_{n'})(t_i), c_a in {0, 1}
-//   B[(c_a, n', part)][(r, slot)] per segment, slot = 4 yz + 2 cbl + re/im:
-//       the real-arithmetic form of w = W'[c_a + 2 cbl][n'][r] (times n' for
-//       yz = 1): part Re v -> (Re w, Im w), part Im v -> (-Im w, Re w)
-//   D = A B  ->  (Y, Z) of each row for c_b = 2 cbl, and Y = D_0 + tau^2 D_2.
+//   A[i][(n', part)] = (Re v_{n'} | Im v_{n'})(t_i)
+//   B[(n', part)][(r, q)] per segment, q = 2 (4 yz + c) + re/im: the real
+//       form of w = W[c][n'][r] h_s^c (times n' for yz = 1): part Re v ->
+//       (Re w, Im w), part Im v -> (-Im w, Re w)
+//   D = A B  ->  Z_{c,r} and its n'-weighted twin for c = 0..3; the epilogue
+//       forms Y_r = sum_c tau^c Z_{c,r} (Horner, FP64).
 //
 // Precision: v, u, g, tau in FP64 (FP64 sincos of each phase, FP64
 // recurrences); every operand value is scaled to an integer |Y| <= 126 2^21
@@ -24,18 +25,18 @@
 // column's largest value) and split into four signed base-128 digits (int8
 // planes).  kind::i8 MMAs multiply digit planes i and j into the level i + j
 // accumulator (levels 0..3, ten products per K step, s32, exact); the levels
-// are combined in FP64 and the epilogue (u_r, the row sums, e_f, the
+// are combined in FP64 and the epilogue (tau^c, u_r, the row sums, e_f, the
 // projection) runs in FP64.  The only error left is the 2^-29 representation
 // of the operands.
 //
 // Shape: one CTA of 128 threads per work unit (<= 1024 samples of one
-// segment), one sample row per thread per 128-sample tile; K = (c_a, n',
-// part) in steps of 32 (16 n' x {Re, Im}); the rows r are taken in passes of
-// at most 8 (N = 64 columns: four levels fill 256 TMEM columns, two CTAs per
-// SM).  A is generated per pass and K step by the threads while the B step
-// arrives by cp.async; two stages, an mbarrier per stage (tcgen05.commit).
-// Every wait is bounded; a timeout sets the error word and ends the kernel
-// after freeing TMEM.
+// segment), one sample row per thread per 128-sample tile.  The tile's A
+// (K = 2 NNp: n' x {Re, Im}, in steps of 32) is generated once into shared
+// memory; the rows r are then taken in passes of 4 (N = 64 columns: the four
+// levels fill 256 TMEM columns, two CTAs per SM), each pass streaming its B
+// K steps by cp.async into two stages gated by an mbarrier per stage
+// (tcgen05.commit).  Every wait is bounded; a timeout sets the error word and
+// ends the kernel after freeing TMEM.
 #include "few_common.cuh"
 #include "few_internal.h"
 #include "few_tc.cuh"
@@ -47,14 +48,16 @@ namespace {
 constexpr int kPT = 128;                            // samples per tile (MMA M)
 constexpr int kKS = 32;                             // K per MMA step: 16 n' x {Re, Im}
 constexpr int kDig = 4;                             // digits per operand value
-constexpr int kRowsPass = 8;                        // (m', k') rows per pass
-constexpr int kLvl = 64;                            // TMEM columns per level (8 rows x 8 slots)
+constexpr int kRowsPass = 4;                        // (m', k') rows per pass
+constexpr int kColsRow = 16;                        // columns per row: (Y, Z) x c = 0..3 x re/im
+constexpr int kLvl = kColsRow * kRowsPass;          // TMEM columns per level (64)
 constexpr int kTmemCols = kDig * kLvl;              // 256
 constexpr int kAPlane = kPT * kKS;                  // A digit plane of a K step: 4 KB
-constexpr int kBPlane = 8 * kRowsPass * kKS;        // B digit plane of a K step and pass: 2 KB
-constexpr int kStage = kDig * (kAPlane + kBPlane);  // 24 KB
+constexpr int kBPlane = kLvl * kKS;                 // B digit plane of a K step and pass: 2 KB
+constexpr int kBStage = kDig * kBPlane;             // 8 KB
 constexpr double kScale = 126.0 * 2097152.0;        // |value| <= max -> |Y| <= 126 2^21
 constexpr int kMaxPhaseRows = 64;
+constexpr int kMaxPhaseNN = 128;                    // A of a tile (4 digits x 2 NNp x 128 B) <= 128 KB
 
 // Byte offset of (row, kk) in a K-major, no-swizzle int8 tile of one K step
 // (kk < 32): core matrices of 8 rows x 16 bytes, the two K halves 128 B apart
@@ -75,12 +78,11 @@ __device__ __forceinline__ void digit_chunks(const double *x, double scale, uint
     uint32_t w[kDig][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        int d[kDig][4];
+        uint32_t t[kDig];
+        digit_words4(scaled_rint(x[4 * q], scale), scaled_rint(x[4 * q + 1], scale),
+                     scaled_rint(x[4 * q + 2], scale), scaled_rint(x[4 * q + 3], scale), t);
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
-            digits4(__double2int_rn(x[4 * q + e] * scale), d[0][e], d[1][e], d[2][e], d[3][e]);
-#pragma unroll
-        for (int p = 0; p < kDig; ++p) w[p][q] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+        for (int p = 0; p < kDig; ++p) w[p][q] = t[p];
     }
 #pragma unroll
     for (int p = 0; p < kDig; ++p) out[p] = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
@@ -89,7 +91,7 @@ __device__ __forceinline__ void digit_chunks(const double *x, double scale, uint
 // Per segment the packed operand is one block: the NBc column scales
 // (doubles), then the digit planes [K step][digit][NBc/8 column groups x 256 B].
 struct PhaseDims {
-    int NNp, nb, nks, Re, NBc;
+    int NNp, nks, NBc;
     long long dig_bytes;  // digit bytes of one segment
     long long seg_bytes;  // the whole block of one segment (scales + digits)
 };
@@ -98,10 +100,8 @@ __host__ __device__ inline PhaseDims phase_dims(int R, int NN)
 {
     PhaseDims d;
     d.NNp = (NN + 15) / 16 * 16;
-    d.nb = d.NNp / 16;
-    d.nks = 2 * d.nb;            // c_a in {0, 1}
-    d.Re = R + (R & 1);          // rows padded to even: every pass has N % 16 == 0
-    d.NBc = 8 * d.Re;
+    d.nks = d.NNp / 16;          // K steps of 16 n' x {Re, Im}
+    d.NBc = kColsRow * R;
     d.dig_bytes = (long long)d.nks * kDig * d.NBc * kKS;
     d.seg_bytes = (long long)d.NBc * 8 + d.dig_bytes;  // both multiples of 16 bytes
     return d;
@@ -118,16 +118,14 @@ __global__ void __launch_bounds__(256) k_fold_phase_s8(const double2 *__restrict
     const int lane = threadIdx.x & 31;
     if (w >= (long long)nseg * pd.NBc) return;
     const int s = (int)(w / pd.NBc), j = (int)(w % pd.NBc);
-    const int r = j >> 3, slot = j & 7;
-    const int ri = slot & 1, cbl = (slot >> 1) & 1, yz = slot >> 2;
+    const int r = j / kColsRow, q16 = j % kColsRow;
+    const int ri = q16 & 1, c = (q16 >> 1) & 3, yz = q16 >> 3;
     const double h = t_knots[s + 1] - t_knots[s];
+    const double hc = c == 0 ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
     const int nchunks = 2 * pd.nks;  // 16 K values each
     auto value = [&](int ks, int kk) -> double {
-        const int ca = ks / pd.nb, blk = ks % pd.nb;
-        const int n = 16 * blk + (kk >> 1), part = kk & 1;
-        if (r >= R || n >= NN) return 0.0;
-        const int c = ca + 2 * cbl;
-        const double hc = c == 0 ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
+        const int n = 16 * ks + (kk >> 1), part = kk & 1;
+        if (n >= NN) return 0.0;
         const double2 wv = W[(((long long)s * R + r) * NN + n) * 4 + c];
         const double f = yz ? hc * (double)(nlo + n) : hc;
         const double wr = wv.x * f, wi = wv.y * f;
@@ -178,7 +176,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     __shared__ uint32_t s_tmem;
     __shared__ int s_rm[kMaxPhaseRows], s_rk[kMaxPhaseRows];
     __shared__ double s_pc[24];
-    __shared__ double s_scale[8 * kMaxPhaseRows];
+    __shared__ double s_inv[kColsRow * kMaxPhaseRows];  // 2^42 / (A scale x column scale)
     __shared__ double s_e[3][kPT];
     __shared__ double s_s[kPT];
 
@@ -186,7 +184,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     const int unit = blockIdx.x;
     const int seg = a.units[3 * unit], lo = a.units[3 * unit + 1], hi = a.units[3 * unit + 2];
     const PhaseDims pd = phase_dims(a.R, a.NN);
-    const int R = a.R, NN = a.NN, nks = pd.nks, nb = pd.nb;
+    const int R = a.R, NN = a.NN, nks = pd.nks;
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
     const long long nps = (long long)(a.N - 1) * 3;
@@ -196,7 +194,8 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
         s_rk[r] = a.row_k[r];
     }
     const unsigned char *const block = a.Bpk + (long long)seg * pd.seg_bytes;
-    for (int j = tid; j < pd.NBc; j += blockDim.x) s_scale[j] = reinterpret_cast<const double *>(block)[j];
+    for (int j = tid; j < pd.NBc; j += blockDim.x)
+        s_inv[j] = 4398046511104.0 / (kScale * reinterpret_cast<const double *>(block)[j]);
     if (tid < 24) {
         const int q = tid >> 3, c = tid & 7;
         s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
@@ -205,11 +204,13 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     mixed_setup(&s_tmem, s_bar, kTmemCols, pp);  // includes a __syncthreads
 
     const unsigned char *const Bseg = block + (long long)pd.NBc * 8;
-    const int npass = (pd.Re + kRowsPass - 1) / kRowsPass;
+    unsigned char *const sA = smem_raw;                                   // [digit][K step] planes
+    unsigned char *const sBst = smem_raw + (size_t)kDig * nks * kAPlane;  // [stage][digit] planes
+    const int npass = (R + kRowsPass - 1) / kRowsPass;
     const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
     double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's share of the unit's 24 outputs
     bool failed = false;
-    int kstep = 0;  // stage index runs on across tiles and passes
+    int kstep = 0;  // stage index runs on across passes and tiles
 
     for (int base = lo; base < hi && !failed; base += kPT) {
         const int i = base + tid;
@@ -220,78 +221,74 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
         const double s = (t - pt0) / pw;
         const double s1 = 1.0 - s;
         double sn, cs;
-        sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+        sincos_reduced(phase_poly(s_pc, s, s1), &sn, &cs);
         const double2 Ep = make_double2(cs, -sn);
-        sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+        sincos_reduced(phase_poly(s_pc + 16, s, s1), &sn, &cs);
         const double2 Er = make_double2(cs, -sn);
         double2 Et = make_double2(1.0, 0.0);
         if (a.use_theta) {
-            sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+            sincos_reduced(phase_poly(s_pc + 8, s, s1), &sn, &cs);
             Et = make_double2(cs, -sn);
         }
-        const double2 vlo = cpow_int(Er, a.nlo);
-        const double tau2 = tau * tau;
+        // A of the tile: v_{n'} for every n' (FP64 recurrence), digits into shared memory
+        // (the previous tile's MMAs are complete: its last pass drained both stages)
+        {
+            double2 v = cpow_int(Er, a.nlo);
+            for (int ks = 0; ks < nks; ++ks) {
+                double x[2 * 16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const bool ok = valid && (16 * ks + q < NN);
+                    x[2 * q] = ok ? v.x : 0.0;
+                    x[2 * q + 1] = ok ? v.y : 0.0;
+                    v = cmul(v, Er);
+                }
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    uint4 ch[kDig];
+                    digit_chunks(x + 16 * half, kScale, ch);
+#pragma unroll
+                    for (int p = 0; p < kDig; ++p)
+                        *reinterpret_cast<uint4 *>(sA + (p * nks + ks) * kAPlane + koff8(tid, 16 * half)) = ch[p];
+                }
+            }
+        }
         double2 Sp = make_double2(0.0, 0.0), St = Sp, Sr = Sp;
         double2 uu = make_double2(1.0, 0.0);
         int pm = 0x7fffffff, pk = 0x7fffffff;
 
         for (int pass = 0; pass < npass && !failed; ++pass) {
-            const int r0 = pass * kRowsPass, rows = min(kRowsPass, pd.Re - r0);
-            const int ncols = 8 * rows;
+            const int r0 = pass * kRowsPass, rows = min(kRowsPass, R - r0);
+            const int ncols = kColsRow * rows;
             const uint32_t idesc = idesc_s8_k(kPT, ncols);
-            double2 v = vlo;
             for (int ks = 0; ks < nks; ++ks, ++kstep) {
                 const int b = kstep & 1;
                 if (__syncthreads_or(!pipe_drain(pp, b))) {
                     failed = true;
                     break;
                 }
-                unsigned char *const sA = smem_raw + b * kStage;
-                unsigned char *const sB = sA + kDig * kAPlane;
-                // B step: this pass's rows of the four digit planes (rows * 256 bytes each)
-                {
-                    const int per_plane = rows * 16;  // 16-byte chunks
-                    for (int q = tid; q < kDig * per_plane; q += blockDim.x) {
-                        const int p = q / per_plane, c = q - p * per_plane;
-                        const unsigned char *src = Bseg + ((long long)ks * kDig + p) * pd.NBc * kKS + r0 * 256 + 16 * c;
-                        cp_async16(sB + p * kBPlane + 16 * c, src);
-                    }
-                    cp_async_commit();
+                unsigned char *const sB = sBst + b * kBStage;
+                // B step: this pass's rows of the four digit planes (rows x 512 bytes each)
+                const int per_plane = rows * (kColsRow / 8) * 16;  // 16-byte chunks
+                for (int q = tid; q < kDig * per_plane; q += blockDim.x) {
+                    const int p = q / per_plane, c = q - p * per_plane;
+                    const unsigned char *src =
+                        Bseg + ((long long)ks * kDig + p) * pd.NBc * kKS + (long long)r0 * kColsRow * kKS + 16 * c;
+                    cp_async16(sB + p * kBPlane + 16 * c, src);
                 }
-                // A step: tau^c_a v_{n'} for 16 n' (FP64 recurrence, restarted for each c_a)
-                {
-                    const int ca = ks / nb, blk = ks - ca * nb;
-                    if (blk == 0) v = vlo;
-                    double x[2 * 16];
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const bool ok = valid && (16 * blk + q < NN);
-                        const double f = ca ? tau : 1.0;
-                        x[2 * q] = ok ? f * v.x : 0.0;
-                        x[2 * q + 1] = ok ? f * v.y : 0.0;
-                        v = cmul(v, Er);
-                    }
-#pragma unroll
-                    for (int half = 0; half < 2; ++half) {
-                        uint4 ch[kDig];
-                        digit_chunks(x + 16 * half, kScale, ch);
-#pragma unroll
-                        for (int p = 0; p < kDig; ++p)
-                            *reinterpret_cast<uint4 *>(sA + p * kAPlane + koff8(tid, 16 * half)) = ch[p];
-                    }
-                }
+                cp_async_commit();
                 cp_async_wait_all();
-                fence_async_smem();
+                fence_async_smem();  // also publishes the A digits written above
                 __syncthreads();
                 if (tid == 0) {
                     tc_fence_after();
-                    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+                    const uint32_t a0 = smem_u32(sA) + ks * kAPlane, b0 = smem_u32(sB);
 #pragma unroll
                     for (int lv = 0; lv < kDig; ++lv) {
 #pragma unroll
                         for (int ia = 0; ia <= lv; ++ia) {
                             const int jb = lv - ia;
-                            const uint64_t da = smem_desc(a0 + ia * kAPlane, 128, 256);
+                            const uint64_t da = smem_desc(a0 + ia * nks * kAPlane, 128, 256);
                             const uint64_t db = smem_desc(b0 + jb * kBPlane, 128, 256);
                             mma_s8(pp.tmem + (uint32_t)(lv * kLvl), da, db, idesc, (ks == 0 && ia == 0) ? 0u : 1u);
                         }
@@ -308,52 +305,50 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
                 break;
             }
             tc_fence_after();
-            // epilogue of the pass: the four levels of each row's 8 columns in FP64,
-            // (Y, Z) of each row, u_r, and the three weighted row sums
-            for (int rp = 0; rp < rows / 2; ++rp) {
+            // epilogue of the pass, one row (16 columns) at a time: the four levels
+            // in FP64, Y and Z by Horner in tau, u_r, and the three weighted row sums
+            for (int rr = 0; rr < rows; ++rr) {
+                const int r = r0 + rr;
                 int D[kDig][16];
 #pragma unroll
                 for (int lv = 0; lv < kDig; ++lv) {
                     float f[16];
-                    tmem_ld16(trow + (uint32_t)(lv * kLvl + 16 * rp), f);
+                    tmem_ld16(trow + (uint32_t)(lv * kLvl + kColsRow * rr), f);
                     tmem_wait_ld();
 #pragma unroll
                     for (int e = 0; e < 16; ++e) D[lv][e] = __float_as_int(f[e]);
                 }
+                double val[16];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int r = r0 + 2 * rp + q;
-                    if (r >= R) continue;
-                    double val[8];
-#pragma unroll
-                    for (int sl = 0; sl < 8; ++sl) {
-                        double acc = 0.0, wl = 4398046511104.0;  // 2^42
-#pragma unroll
-                        for (int lv = 0; lv < kDig; ++lv) {
-                            acc = fma((double)D[lv][8 * q + sl], wl, acc);
-                            wl *= 0.0078125;
-                        }
-                        val[sl] = acc / (kScale * s_scale[8 * r + sl]);
-                    }
-                    const int mm = s_rm[r], kk = s_rk[r];
-                    if (kk == pk && mm == pm + 1) {
-                        uu = cmul(uu, Ep);
-                    } else {
-                        uu = cpow_int(Ep, mm);
-                        if (kk) uu = cmul(uu, cpow_int(Et, kk));
-                    }
-                    pm = mm;
-                    pk = kk;
-                    const double2 Y = make_double2(fma(val[2], tau2, val[0]), fma(val[3], tau2, val[1]));
-                    const double2 Z = make_double2(fma(val[6], tau2, val[4]), fma(val[7], tau2, val[5]));
-                    const double2 P = cmul(uu, Y), Q = cmul(uu, Z);
-                    Sp.x = fma((double)mm, P.x, Sp.x);
-                    Sp.y = fma((double)mm, P.y, Sp.y);
-                    St.x = fma((double)kk, P.x, St.x);
-                    St.y = fma((double)kk, P.y, St.y);
-                    Sr.x += Q.x;
-                    Sr.y += Q.y;
+                for (int q = 0; q < 16; ++q) {
+                    // the levels combined exactly in int64 (|sum| < 2^53), one conversion
+                    const long long acc = ((long long)D[0][q] << 21) + ((long long)D[1][q] << 14) +
+                                          ((long long)D[2][q] << 7) + (long long)D[3][q];
+                    val[q] = (double)acc * (s_inv[kColsRow * r + q] * 4.76837158203125e-07);  // 2^-21
                 }
+                // q = 2 (4 yz + c) + re/im
+                double2 Y = make_double2(val[6], val[7]), Z = make_double2(val[14], val[15]);
+#pragma unroll
+                for (int c = 2; c >= 0; --c) {
+                    Y = make_double2(fma(Y.x, tau, val[2 * c]), fma(Y.y, tau, val[2 * c + 1]));
+                    Z = make_double2(fma(Z.x, tau, val[8 + 2 * c]), fma(Z.y, tau, val[8 + 2 * c + 1]));
+                }
+                const int mm = s_rm[r], kk = s_rk[r];
+                if (kk == pk && mm == pm + 1) {
+                    uu = cmul(uu, Ep);
+                } else {
+                    uu = cpow_int(Ep, mm);
+                    if (kk) uu = cmul(uu, cpow_int(Et, kk));
+                }
+                pm = mm;
+                pk = kk;
+                const double2 P = cmul(uu, Y), Q = cmul(uu, Z);
+                Sp.x = fma((double)mm, P.x, Sp.x);
+                Sp.y = fma((double)mm, P.y, Sp.y);
+                St.x = fma((double)kk, P.x, St.x);
+                St.y = fma((double)kk, P.y, St.y);
+                Sr.x += Q.x;
+                Sr.y += Q.y;
             }
             tc_fence_before();
             __syncthreads();  // TMEM read before the next pass's first MMA overwrites it
@@ -447,8 +442,9 @@ extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const 
     few::clear_error();
     if (!grad || !Bpk || !phase_coeffs || !seg_info || !t_knots || !units || !row_m || !row_k || !partial || !err)
         return few::fail(FEW_ERR_ARG, "few_adjoint_phase_mixed: null pointer");
-    if (N < 2 || nunits < 0 || R < 1 || R > few::kMaxPhaseRows || NN < 1)
-        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_mixed: bad sizes (R <= %d)", few::kMaxPhaseRows);
+    if (N < 2 || nunits < 0 || R < 1 || R > few::kMaxPhaseRows || NN < 1 || NN > few::kMaxPhaseNN)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_phase_mixed: bad sizes (R <= %d, NN <= %d)", few::kMaxPhaseRows,
+                         few::kMaxPhaseNN);
     if (nunits == 0) return FEW_OK;
     few::PhaseArgs a;
     a.grad = (const double2 *)grad;
@@ -467,7 +463,7 @@ extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const 
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const int smem = 2 * few::kStage;
+    const int smem = few::kDig * few::phase_dims(R, NN).nks * few::kAPlane + 2 * few::kBStage;
     FEW_CUDA_TRY(few::ensure_smem_attr((const void *)few::k_adj_phase_s8, smem));
     few::k_adj_phase_s8<<<nunits, few::kPT, smem, (cudaStream_t)stream>>>(a);
     FEW_LAUNCH_CHECK("k_adj_phase_s8");
