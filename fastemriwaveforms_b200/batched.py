@@ -124,6 +124,9 @@ class BatchedInterpolatedModeSum:
             d["dt"] = p.dt
         self.descs = _upload(descs.view(np.uint8), dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        # time stamps (GPU global timer, ns): [0] start of the forward, [1 + w]
+        # completion of waveform w's sum, [1 + n + w] completion of its backward
+        self.stamps = torch.zeros(1 + 2 * len(self.preps), dtype=torch.int64, device=dev)
         self.mode_samples = sum(p.K * p.out_len for p in self.preps)
         seg_lens = [np.diff(p.seg.seg_start).mean() for p in self.preps if p.seg.nseg > 0]
         self._key = autotune.key_of(dev, self.precision, self.max_R, max_NN, float(np.mean(seg_lens)),
@@ -192,16 +195,16 @@ class BatchedInterpolatedModeSum:
                           st)
         self._join(main, side)
 
-    def _sum(self, units: torch.Tensor, ctas: int):
+    def _sum(self, units: torch.Tensor, ctas: int, done=None):
         st = _stream(self.device)
         nunits = units.numel() // 4
         if self.precision == "mixed":
             _lib.call("few_sum_mixed_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.max_R,
-                      ctas, _ptr(self.err), st)
+                      ctas, _ptr(self.err), done, st)
         else:
             mode = _lib.FEW_SUM_FAITHFUL if self.precision == "faithful" else _lib.FEW_SUM_EXACT
             _lib.call("few_sum_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.smem_bytes, mode,
-                      ctas, st)
+                      ctas, done, st)
 
     def _runner(self, chunk: int, per_sm: int):
         units = self._units(chunk)
@@ -213,10 +216,15 @@ class BatchedInterpolatedModeSum:
         return run
 
     def forward(self):
-        """All waveforms; returns the list of output tensors (views of one buffer)."""
+        """All waveforms; returns the list of output tensors (views of one buffer).
+        Time stamps: ``stamps[0]`` the start, ``stamps[1 + w]`` waveform w's
+        completion inside the persistent sum (see ``latencies``)."""
+        st = _stream(self.device)
+        self.stamps.zero_()
+        _lib.call("few_stamp", _ptr(self.stamps), st)
         self.out.zero_()
         self._prepare_operands()
-        self._sum(self.units, self.ctas_per_sm * self.sms)
+        self._sum(self.units, self.ctas_per_sm * self.sms, _ptr(self.stamps) + 8)
         return self.outputs
 
     def backward(self, grads):
@@ -225,11 +233,13 @@ class BatchedInterpolatedModeSum:
         streams; returns a list of (dL/d teuk_modes, dL/d phase_interp_coeffs)."""
         main, side = self._fork()
         out = []
+        n = len(self.preps)
         for i, (p, g) in enumerate(zip(self.preps, grads)):
             s = side[i % len(side)]
             with torch.cuda.stream(s):
                 p.st = s.cuda_stream
                 out.append(InterpolatedModeSum._backward(p, g, concurrent=False))
+                _lib.call("few_stamp", _ptr(self.stamps) + 8 * (1 + n + i), s.cuda_stream)
         self._join(main, side)
         if not torch.cuda.is_current_stream_capturing():
             for pair in out:  # made on side streams, used on the caller's stream
@@ -237,6 +247,18 @@ class BatchedInterpolatedModeSum:
                     if t is not None:
                         t.record_stream(main)
         return out
+
+    def latencies(self):
+        """Per-waveform times (ms) of the last forward (and backward) run, from
+        the forward's start: (forward completion (n,), backward completion
+        (n,) or None).  The forward times end when the waveform's last work
+        unit of the persistent sum finished; the backward times when its
+        adjoint chain finished."""
+        s = self.stamps.cpu().numpy()
+        n = len(self.preps)
+        fwd = (s[1:1 + n] - s[0]) * 1e-6
+        bwd = s[1 + n:]
+        return fwd, ((bwd - s[0]) * 1e-6 if np.all(bwd > 0) else None)
 
     def mixed_error(self) -> bool:
         """True if a tensor-core wait of the batched sum or of a mixed adjoint timed out."""

@@ -8,6 +8,14 @@
 
 namespace few {
 
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // ---------------------------------------------------------------------------
 // Complex FP64 helpers (double2: x = real, y = imaginary).  These are ordinary
 // FP64 expressions; nvcc may contract them into FMAs, which is intended.

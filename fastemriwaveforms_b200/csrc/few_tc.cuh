@@ -7,6 +7,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "few_common.cuh"
+
 namespace few {
 
 constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s of global time per wait
@@ -29,13 +31,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
 }
 
 // Bounded wait; false if the phase did not complete within kWaitLimitNs.

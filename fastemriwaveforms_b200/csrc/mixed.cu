@@ -301,7 +301,8 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
 // per CTA; units {waveform, segment, first, end} are taken in stride.
 __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_desc *__restrict__ descs,
                                                               const int *__restrict__ units4, int nunits,
-                                                              int tmem_cols, int *err)
+                                                              int tmem_cols, int *err,
+                                                              unsigned long long *__restrict__ done)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[2];
@@ -332,6 +333,7 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.tmem_cols = tmem_cols;
         mixed_dims_core(d.R, d.NN, a.NNp, a.NB, a.nchunks);
         ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
+        if (done && ok && threadIdx.x == 0) atomicMax(done + units4[4 * u], global_ns());  // unit complete
     }
     mixed_teardown(!ok, pp, tmem_cols, err);
 }
@@ -404,7 +406,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
 }
 
 int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int nunits, int max_R, int ctas, int *err,
-                             cudaStream_t st)
+                             unsigned long long *done, cudaStream_t st)
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
@@ -419,7 +421,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
     ctas = std::min(ctas, nunits);
     const size_t smem = mixed_smem_bytes(NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
-    k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err);
+    k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err, done);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");
     return FEW_OK;
 }
@@ -427,13 +429,13 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 }  // namespace few
 
 extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
-                                     int ctas, int *err, void *stream)
+                                     int ctas, int *err, unsigned long long *done, void *stream)
 {
     few::clear_error();
     if (!descs || !units4 || !err) return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: null pointer");
     if (nwave < 1 || nunits < 0 || max_R < 1 || max_R > 64)
         return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 64)");
-    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, err, (cudaStream_t)stream);
+    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, err, done, (cudaStream_t)stream);
 }
 
 extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream)

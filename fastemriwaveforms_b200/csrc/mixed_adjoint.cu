@@ -31,10 +31,12 @@
 // accumulator of 128 TMEM columns; the four levels fill the 512 columns).  The samples are K: one CTA of 8
 // warps owns one segment and loops over its samples in tiles of 32 (K = 64,
 // two MMA K steps): lane = sample, and the warps share the tile's operand
-// groups (16 n' of A or 8 rows r of B, each written as 16-byte chunks of the
-// MN-major no-swizzle layout: core matrix = 8 K rows x 16 bytes, K groups
-// 128 B apart, MN groups 1024 B apart).  The FP64 prelude (phasors, tau, g)
-// is computed once per sample, for 8 tiles at a time, into shared memory.  Two
+// groups (16 n' of A for one c_a, or 8 rows r of B for both c_b, each written
+// as whole 16-byte MN chunks, in the MN-major no-swizzle layout: core
+// matrix = 8 K rows x 16 bytes, K groups 128 B apart, MN groups 1024 B apart),
+// 12 warps so that every group of a tile has its own warp.  The FP64 prelude
+// (phasors, tau, g) is computed once per sample, for 12 tiles at a time, into
+// shared memory.  Two
 // operand buffers: while the tensor core consumes tile k, the warps build tile
 // k+1.  Every wait is bounded; a timeout sets the error word, drains and
 // frees TMEM.
@@ -47,8 +49,8 @@ namespace few {
 namespace {
 
 constexpr int kGT = 32;              // samples per tile; K = 64 (sample x {Re, Im})
-constexpr int kGThreads = 256;       // 8 warps
-constexpr int kGPre = 8;             // tiles per prelude batch (kGPre * kGT = kGThreads samples)
+constexpr int kGThreads = 384;       // 12 warps: one operand group each (8 of A, up to 4 of B)
+constexpr int kGPre = kGThreads / kGT;  // tiles per prelude batch (one sample per thread)
 constexpr int kGFlush = 32;          // tiles per block: one B scale, int32 sums well inside 2^31
 constexpr int kDigits = 4;           // base-128 digits per operand value
 constexpr int kPlaneA = 8 * 1024;    // one A digit plane: 8 MN groups (2 x 64 n') x 8 K groups x 128 B
@@ -66,7 +68,7 @@ __device__ __forceinline__ uint32_t mn_off8(int mn, int k)
 // Per-sample values every operand group needs (FP64).
 struct GPrelude {
     double2 v0;    // v_{n'} at this CTA's first n'
-    double2 Er, Er16, Ep, Et;
+    double2 Er, Er8, Ep, Et;
     double2 g;     // conj of torch's upstream gradient
     double tau;
 };
@@ -113,8 +115,9 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
     const long long nps = (long long)(a.N - 1) * 3;
-    const int nA = (min(64, NN - nrow0) + 15) >> 4;  // A groups of 16 n' (each for both c_a)
-    const int nBg = CB >> 4;                         // B groups: 8 rows r (all c_b of the CTA)
+    const int nA16 = (min(64, NN - nrow0) + 15) >> 4;  // 16-n' blocks of this CTA's rows
+    const int nA = 2 * nA16;                           // A groups: (16 n' block, c_a)
+    const int nBg = CB >> 4;                        // B groups: 8 rows r (all c_b of the CTA)
     const int ngroups = nA + nBg;
 
     if (lo >= hi) {  // a segment without samples: zero gradient for this CTA's (n', c)
@@ -193,10 +196,9 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
                 pr.Et = make_double2(1.0, 0.0);
             }
             pr.v0 = cpow_int(pr.Er, a.nlo + nrow0);
-            double2 e16 = cmul(pr.Er, pr.Er);
-            e16 = cmul(e16, e16);
-            e16 = cmul(e16, e16);
-            pr.Er16 = cmul(e16, e16);
+            double2 e8 = cmul(pr.Er, pr.Er);
+            e8 = cmul(e8, e8);
+            pr.Er8 = cmul(e8, e8);
             pr.tau = (t - t0) / hs;
             pr.g = make_double2(0.0, 0.0);
             if (i < hi) {
@@ -212,22 +214,21 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
         unsigned char *const bBuf = aBuf + bufA;
         for (int gi = warp; gi < ngroups; gi += kGThreads / 32) {
             if (gi < nA) {
-                // A: tau^c_a v_{n'} for 16 n' (MN 16 gi .. and 64 + 16 gi ..), 4 at a time
-                const int n0 = nrow0 + 16 * gi;
-                double2 v = pr.v0;
-                for (int q = 0; q < gi; ++q) v = cmul(v, pr.Er16);
-                const double tau = pr.tau;
-                uint32_t w[4][kDigits][4];  // [(c_a, part)][digit][word]
+                // A: tau^c_a v_{n'} for 16 n' and one c_a (MN 64 c_a + 16 blk ..): whole
+                // 16-byte MN chunks for both parts
+                const int blk = gi >> 1, ca = gi & 1;
+                const int n0 = nrow0 + 16 * blk;
+                double2 v = cmul(pr.v0, cpow_int(pr.Er8, 2 * blk));
+                const double f = ca ? pr.tau : 1.0;
+                uint32_t w[2][kDigits][4];  // [part][digit][word]
 #pragma unroll
                 for (int qb = 0; qb < 4; ++qb) {
-                    double re[4], im[4], tre[4], tim[4];
+                    double re[4], im[4];
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const bool ok = n0 + 4 * qb + e < NN;
-                        re[e] = ok ? v.x : 0.0;
-                        im[e] = ok ? v.y : 0.0;
-                        tre[e] = tau * re[e];
-                        tim[e] = tau * im[e];
+                        re[e] = ok ? f * v.x : 0.0;
+                        im[e] = ok ? f * v.y : 0.0;
                         v = cmul(v, pr.Er);
                     }
                     uint32_t t4[kDigits];
@@ -237,24 +238,15 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
                     digit_words(im, kScaleA, t4);
 #pragma unroll
                     for (int p = 0; p < kDigits; ++p) w[1][p][qb] = t4[p];
-                    digit_words(tre, kScaleA, t4);
-#pragma unroll
-                    for (int p = 0; p < kDigits; ++p) w[2][p][qb] = t4[p];
-                    digit_words(tim, kScaleA, t4);
-#pragma unroll
-                    for (int p = 0; p < kDigits; ++p) w[3][p][qb] = t4[p];
                 }
+                const int mn = 64 * ca + 16 * blk;
 #pragma unroll
                 for (int p = 0; p < kDigits; ++p) {
                     unsigned char *plane = aBuf + p * kPlaneA;
-                    *reinterpret_cast<uint4 *>(plane + mn_off8(16 * gi, k0)) =
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(mn, k0)) =
                         make_uint4(w[0][p][0], w[0][p][1], w[0][p][2], w[0][p][3]);
-                    *reinterpret_cast<uint4 *>(plane + mn_off8(16 * gi, k0 + 8)) =
+                    *reinterpret_cast<uint4 *>(plane + mn_off8(mn, k0 + 8)) =
                         make_uint4(w[1][p][0], w[1][p][1], w[1][p][2], w[1][p][3]);
-                    *reinterpret_cast<uint4 *>(plane + mn_off8(64 + 16 * gi, k0)) =
-                        make_uint4(w[2][p][0], w[2][p][1], w[2][p][2], w[2][p][3]);
-                    *reinterpret_cast<uint4 *>(plane + mn_off8(64 + 16 * gi, k0 + 8)) =
-                        make_uint4(w[3][p][0], w[3][p][1], w[3][p][2], w[3][p][3]);
                 }
             } else {
                 // B: tau^c_b g u_r for 8 rows r, each c_b of the CTA
@@ -337,7 +329,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
             // block done: every MMA finished, then the four levels combined in
             // FP64 (row (c_a, n'), column (c_b, r, re/im)) and added into G (stored
             // by the first block); the next MMA restarts the accumulators.
-            // Warps w and w+4 read the same TMEM lanes (32 (w % 4) ..) and share the columns.
+            // Warps w, w+4 and w+8 read the same TMEM lanes (32 (w % 4) ..) and share the columns.
             const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
             if (__syncthreads_or(!(ok0 && ok1))) {
                 failed = true;
@@ -350,7 +342,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G_mixed(AdjGMixedArgs a)
             const int row = 32 * quad + lane;
             const int ca = row >> 6, n = nrow0 + (row & 63);
             const uint32_t trow = pp.tmem + ((uint32_t)(quad * 32) << 16);
-            for (int j16 = warp >> 2; j16 < NB / 16; j16 += 2) {
+            for (int j16 = warp >> 2; j16 < NB / 16; j16 += kGThreads / 128) {
                 double acc[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e) acc[e] = 0.0;

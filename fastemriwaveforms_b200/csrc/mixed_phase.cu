@@ -33,10 +33,11 @@
 // segment), one sample row per thread per 128-sample tile.  The tile's A
 // (K = 2 NNp: n' x {Re, Im}, in steps of 32) is generated once into shared
 // memory; the rows r are then taken in passes of 4 (N = 64 columns: the four
-// levels fill 256 TMEM columns, two CTAs per SM), each pass streaming its B
-// K steps by cp.async into two stages gated by an mbarrier per stage
-// (tcgen05.commit).  Every wait is bounded; a timeout sets the error word and
-// ends the kernel after freeing TMEM.
+// levels fill 256 TMEM columns, two CTAs per SM).  A pass's B (every K step of
+// its rows) arrives by cp.async while the previous pass's epilogue runs; its
+// MMAs are issued at once and signal an mbarrier (tcgen05.commit).  Every
+// wait is bounded; a timeout sets the error word and ends the kernel after
+// freeing TMEM.
 #include "few_common.cuh"
 #include "few_internal.h"
 #include "few_tc.cuh"
@@ -54,7 +55,6 @@ constexpr int kLvl = kColsRow * kRowsPass;          // TMEM columns per level (6
 constexpr int kTmemCols = kDig * kLvl;              // 256
 constexpr int kAPlane = kPT * kKS;                  // A digit plane of a K step: 4 KB
 constexpr int kBPlane = kLvl * kKS;                 // B digit plane of a K step and pass: 2 KB
-constexpr int kBStage = kDig * kBPlane;             // 8 KB
 constexpr double kScale = 126.0 * 2097152.0;        // |value| <= max -> |Y| <= 126 2^21
 constexpr int kMaxPhaseRows = 64;
 constexpr int kMaxPhaseNN = 128;                    // A of a tile (4 digits x 2 NNp x 128 B) <= 128 KB
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     __shared__ uint32_t s_tmem;
     __shared__ int s_rm[kMaxPhaseRows], s_rk[kMaxPhaseRows];
     __shared__ double s_pc[24];
-    __shared__ double s_inv[kColsRow * kMaxPhaseRows];  // 2^42 / (A scale x column scale)
+    __shared__ double s_inv[kColsRow * kMaxPhaseRows];  // 2^21 / (A scale x column scale)
     __shared__ double s_e[3][kPT];
     __shared__ double s_s[kPT];
 
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     }
     const unsigned char *const block = a.Bpk + (long long)seg * pd.seg_bytes;
     for (int j = tid; j < pd.NBc; j += blockDim.x)
-        s_inv[j] = 4398046511104.0 / (kScale * reinterpret_cast<const double *>(block)[j]);
+        s_inv[j] = 2097152.0 / (kScale * reinterpret_cast<const double *>(block)[j]);
     if (tid < 24) {
         const int q = tid >> 3, c = tid & 7;
         s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
@@ -205,16 +205,30 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
 
     const unsigned char *const Bseg = block + (long long)pd.NBc * 8;
     unsigned char *const sA = smem_raw;                                   // [digit][K step] planes
-    unsigned char *const sBst = smem_raw + (size_t)kDig * nks * kAPlane;  // [stage][digit] planes
+    unsigned char *const sB = smem_raw + (size_t)kDig * nks * kAPlane;    // [digit][K step] planes of a pass
     const int npass = (R + kRowsPass - 1) / kRowsPass;
     const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
     double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's share of the unit's 24 outputs
     bool failed = false;
-    int kstep = 0;  // stage index runs on across passes and tiles
+
+    // B of a pass: its rows of every K step and digit plane (rows x 512 bytes each)
+    auto load_B = [&](int pass) {
+        const int r0 = pass * kRowsPass, rows = min(kRowsPass, R - r0);
+        const int per = rows * (kColsRow / 8) * 16;  // 16-byte chunks per (K step, digit)
+        for (int q = tid; q < nks * kDig * per; q += blockDim.x) {
+            const int kp = q / per, c = q - kp * per;  // kp = ks * kDig + digit
+            const int ks = kp / kDig, p = kp - ks * kDig;
+            const unsigned char *src =
+                Bseg + ((long long)ks * kDig + p) * pd.NBc * kKS + (long long)r0 * kColsRow * kKS + 16 * c;
+            cp_async16(sB + (p * nks + ks) * kBPlane + 16 * c, src);
+        }
+        cp_async_commit();
+    };
 
     for (int base = lo; base < hi && !failed; base += kPT) {
         const int i = base + tid;
         const bool valid = i < hi;
+        load_B(0);  // the buffer is free: the previous tile's MMAs were drained
         // FP64 prelude (phases as interpolate.cu:626-644)
         const double t = (double)i * a.dt;
         const double tau = (t - t0) / hs;
@@ -231,7 +245,6 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
             Et = make_double2(cs, -sn);
         }
         // A of the tile: v_{n'} for every n' (FP64 recurrence), digits into shared memory
-        // (the previous tile's MMAs are complete: its last pass drained both stages)
         {
             double2 v = cpow_int(Er, a.nlo);
             for (int ks = 0; ks < nks; ++ks) {
@@ -259,52 +272,34 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
 
         for (int pass = 0; pass < npass && !failed; ++pass) {
             const int r0 = pass * kRowsPass, rows = min(kRowsPass, R - r0);
-            const int ncols = kColsRow * rows;
-            const uint32_t idesc = idesc_s8_k(kPT, ncols);
-            for (int ks = 0; ks < nks; ++ks, ++kstep) {
-                const int b = kstep & 1;
-                if (__syncthreads_or(!pipe_drain(pp, b))) {
-                    failed = true;
-                    break;
-                }
-                unsigned char *const sB = sBst + b * kBStage;
-                // B step: this pass's rows of the four digit planes (rows x 512 bytes each)
-                const int per_plane = rows * (kColsRow / 8) * 16;  // 16-byte chunks
-                for (int q = tid; q < kDig * per_plane; q += blockDim.x) {
-                    const int p = q / per_plane, c = q - p * per_plane;
-                    const unsigned char *src =
-                        Bseg + ((long long)ks * kDig + p) * pd.NBc * kKS + (long long)r0 * kColsRow * kKS + 16 * c;
-                    cp_async16(sB + p * kBPlane + 16 * c, src);
-                }
-                cp_async_commit();
-                cp_async_wait_all();
-                fence_async_smem();  // also publishes the A digits written above
-                __syncthreads();
-                if (tid == 0) {
-                    tc_fence_after();
-                    const uint32_t a0 = smem_u32(sA) + ks * kAPlane, b0 = smem_u32(sB);
+            const uint32_t idesc = idesc_s8_k(kPT, kColsRow * rows);
+            cp_async_wait_all();
+            fence_async_smem();  // A and this pass's B visible to the tensor core
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+                for (int ks = 0; ks < nks; ++ks) {
 #pragma unroll
                     for (int lv = 0; lv < kDig; ++lv) {
 #pragma unroll
                         for (int ia = 0; ia <= lv; ++ia) {
                             const int jb = lv - ia;
-                            const uint64_t da = smem_desc(a0 + ia * nks * kAPlane, 128, 256);
-                            const uint64_t db = smem_desc(b0 + jb * kBPlane, 128, 256);
+                            const uint64_t da = smem_desc(a0 + (ia * nks + ks) * kAPlane, 128, 256);
+                            const uint64_t db = smem_desc(b0 + (jb * nks + ks) * kBPlane, 128, 256);
                             mma_s8(pp.tmem + (uint32_t)(lv * kLvl), da, db, idesc, (ks == 0 && ia == 0) ? 0u : 1u);
                         }
                     }
-                    mma_commit(&pp.bar[b]);
                 }
-                if (b == 0) pp.pend0 = 1;
-                else pp.pend1 = 1;
+                mma_commit(&pp.bar[0]);
             }
-            if (failed) break;
-            const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
-            if (__syncthreads_or(!(ok0 && ok1))) {
+            pp.pend0 = 1;
+            if (__syncthreads_or(!pipe_drain(pp, 0))) {
                 failed = true;
                 break;
             }
             tc_fence_after();
+            if (pass + 1 < npass) load_B(pass + 1);  // arrives while this pass's epilogue runs
             // epilogue of the pass, one row (16 columns) at a time: the four levels
             // in FP64, Y and Z by Horner in tau, u_r, and the three weighted row sums
             for (int rr = 0; rr < rows; ++rr) {
@@ -321,10 +316,15 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
                 double val[16];
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    // the levels combined exactly in int64 (|sum| < 2^53), one conversion
-                    const long long acc = ((long long)D[0][q] << 21) + ((long long)D[1][q] << 14) +
-                                          ((long long)D[2][q] << 7) + (long long)D[3][q];
-                    val[q] = (double)acc * (s_inv[kColsRow * r + q] * 4.76837158203125e-07);  // 2^-21
+                    // the levels combined in FP64 (each level's int32 exact as a double,
+                    // the sum exact below 2^53); int32 -> double without a conversion
+                    // instruction: 2^52 + 2^31 + D in the significand, minus the offset
+                    double lv[kDig];
+#pragma unroll
+                    for (int l = 0; l < kDig; ++l)
+                        lv[l] = __hiloint2double(0x43300000, D[l][q] ^ 0x80000000) - 4503601774854144.0;
+                    const double acc = fma(lv[0], 2097152.0, fma(lv[1], 16384.0, fma(lv[2], 128.0, lv[3])));
+                    val[q] = acc * s_inv[kColsRow * r + q];
                 }
                 // q = 2 (4 yz + c) + re/im
                 double2 Y = make_double2(val[6], val[7]), Z = make_double2(val[14], val[15]);
@@ -463,7 +463,7 @@ extern "C" int few_adjoint_phase_mixed(const void *grad, const void *Bpk, const 
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const int smem = few::kDig * few::phase_dims(R, NN).nks * few::kAPlane + 2 * few::kBStage;
+    const int smem = few::kDig * few::phase_dims(R, NN).nks * (few::kAPlane + few::kBPlane);
     FEW_CUDA_TRY(few::ensure_smem_attr((const void *)few::k_adj_phase_s8, smem));
     few::k_adj_phase_s8<<<nunits, few::kPT, smem, (cudaStream_t)stream>>>(a);
     FEW_LAUNCH_CHECK("k_adj_phase_s8");

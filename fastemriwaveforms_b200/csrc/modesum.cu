@@ -301,7 +301,8 @@ __global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_
 template <int RB, bool FAITHFUL, int SPT>
 __global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_sum_folded_batched(const few_wave_desc *__restrict__ descs,
                                                                        const int *__restrict__ units4, int nunits,
-                                                                       int smem_bytes)
+                                                                       int smem_bytes,
+                                                                       unsigned long long *__restrict__ done)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
@@ -326,6 +327,10 @@ __global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_
         a.rows_per_pass = max(1, min(d.R, smem_bytes / (d.NN * 4 * (int)sizeof(double2))));
         sum_unit<RB, FAITHFUL, SPT, true>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3],
                                     reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
+        if (done) {  // completion time of the waveform: the latest of its units
+            __syncthreads();
+            if (threadIdx.x == 0) atomicMax(done + w, global_ns());
+        }
     }
 }
 
@@ -369,10 +374,11 @@ SumShape sum_shape(int mode)
 
 template <int RB, bool F, int SPT>
 int launch_batched_t(const few_wave_desc *descs, const int *units4, int nunits, int smem_bytes, int ctas,
+                     unsigned long long *done,
                      cudaStream_t st)
 {
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_folded_batched<RB, F, SPT>, kSmemBudget));
-    k_sum_folded_batched<RB, F, SPT><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes);
+    k_sum_folded_batched<RB, F, SPT><<<ctas, kSumThreads, smem_bytes, st>>>(descs, units4, nunits, smem_bytes, done);
     FEW_LAUNCH_CHECK("k_sum_folded_batched");
     return FEW_OK;
 }
@@ -380,7 +386,7 @@ int launch_batched_t(const few_wave_desc *descs, const int *units4, int nunits, 
 }  // namespace
 
 int launch_sum_folded_batched(const few_wave_desc *descs, const int *units4, int nunits, int smem_bytes, int mode,
-                              int ctas, cudaStream_t st)
+                              int ctas, unsigned long long *done, cudaStream_t st)
 {
     if (nunits == 0) return FEW_OK;
     if (smem_bytes < 64 || smem_bytes > kSmemBudget)
@@ -396,16 +402,16 @@ int launch_sum_folded_batched(const few_wave_desc *descs, const int *units4, int
     const SumShape sh = sum_shape(mode);
     const bool F = mode == FEW_SUM_FAITHFUL;
     if (sh.rb == 4 && sh.spt == 2)
-        return F ? launch_batched_t<4, true, 2>(descs, units4, nunits, smem_bytes, ctas, st)
-                 : launch_batched_t<4, false, 2>(descs, units4, nunits, smem_bytes, ctas, st);
+        return F ? launch_batched_t<4, true, 2>(descs, units4, nunits, smem_bytes, ctas, done, st)
+                 : launch_batched_t<4, false, 2>(descs, units4, nunits, smem_bytes, ctas, done, st);
     if (sh.rb == 8 && sh.spt == 2)
-        return F ? launch_batched_t<8, true, 2>(descs, units4, nunits, smem_bytes, ctas, st)
-                 : launch_batched_t<8, false, 2>(descs, units4, nunits, smem_bytes, ctas, st);
+        return F ? launch_batched_t<8, true, 2>(descs, units4, nunits, smem_bytes, ctas, done, st)
+                 : launch_batched_t<8, false, 2>(descs, units4, nunits, smem_bytes, ctas, done, st);
     if (sh.rb == 4)
-        return F ? launch_batched_t<4, true, 1>(descs, units4, nunits, smem_bytes, ctas, st)
-                 : launch_batched_t<4, false, 1>(descs, units4, nunits, smem_bytes, ctas, st);
-    return F ? launch_batched_t<8, true, 1>(descs, units4, nunits, smem_bytes, ctas, st)
-             : launch_batched_t<8, false, 1>(descs, units4, nunits, smem_bytes, ctas, st);
+        return F ? launch_batched_t<4, true, 1>(descs, units4, nunits, smem_bytes, ctas, done, st)
+                 : launch_batched_t<4, false, 1>(descs, units4, nunits, smem_bytes, ctas, done, st);
+    return F ? launch_batched_t<8, true, 1>(descs, units4, nunits, smem_bytes, ctas, done, st)
+             : launch_batched_t<8, false, 1>(descs, units4, nunits, smem_bytes, ctas, done, st);
 }
 
 int launch_fold(const double *coeffs, const double2 *ylms, const int *key_ptr, const int *key_list, int K, int N,
@@ -473,13 +479,13 @@ extern "C" int few_fold_coeffs(const double *coeffs, const void *ylms, const int
 }
 
 extern "C" int few_sum_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int smem_bytes,
-                               int mode, int ctas, void *stream)
+                               int mode, int ctas, unsigned long long *done, void *stream)
 {
     few::clear_error();
     if (!descs || !units4) return few::fail(FEW_ERR_ARG, "few_sum_batched: null pointer");
     if (nwave < 1 || nunits < 0) return few::fail(FEW_ERR_SIZE, "few_sum_batched: bad sizes");
     if (mode != FEW_SUM_FAITHFUL && mode != FEW_SUM_EXACT) return few::fail(FEW_ERR_ARG, "few_sum_batched: bad mode");
-    return few::launch_sum_folded_batched(descs, units4, nunits, smem_bytes, mode, ctas, (cudaStream_t)stream);
+    return few::launch_sum_folded_batched(descs, units4, nunits, smem_bytes, mode, ctas, done, (cudaStream_t)stream);
 }
 
 extern "C" int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, int N, const double *seg_info,
@@ -494,4 +500,19 @@ extern "C" int few_sum_folded(void *wf, const void *W, const double *phase_coeff
     if (mode != FEW_SUM_FAITHFUL && mode != FEW_SUM_EXACT) return few::fail(FEW_ERR_ARG, "few_sum_folded: bad mode");
     return few::launch_sum_folded((double2 *)wf, (const double2 *)W, phase_coeffs, N, seg_info, units, nunits, row_m,
                                   row_k, R, nlo, NN, dt, mode, use_theta, (cudaStream_t)stream);
+}
+
+namespace few {
+namespace {
+__global__ void k_stamp(unsigned long long *dst) { *dst = global_ns(); }
+}  // namespace
+}  // namespace few
+
+extern "C" int few_stamp(unsigned long long *dst, void *stream)
+{
+    few::clear_error();
+    if (!dst) return few::fail(FEW_ERR_ARG, "few_stamp: null pointer");
+    few::k_stamp<<<1, 1, 0, (cudaStream_t)stream>>>(dst);
+    FEW_LAUNCH_CHECK("k_stamp");
+    return FEW_OK;
 }

@@ -647,6 +647,9 @@ class InterpolatedModeSum(SummationBase):
         each other on an SM)."""
         fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
         grad = grad[: p.out_len].to(torch.complex128).contiguous()
+        # the segment tables are uploaded on the caller's stream before the side
+        # stream forks from it: the phase branch reads them there
+        seg_start, _ = seg.backward_tables()
         both = need_teuk and need_pc and concurrent
         main = torch.cuda.current_stream(dev)
         side = None
@@ -658,7 +661,6 @@ class InterpolatedModeSum(SummationBase):
         if mixed and need_pc and fold.R > 64:
             raise ValueError("backward='mixed' supports at most 64 (m, k) rows for phase gradients")
         if need_teuk:
-            seg_start, _ = seg.backward_tables()
             G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
             if mixed:
                 _lib.call("few_adjoint_G_mixed", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(p.t_dev),

@@ -240,9 +240,16 @@ FEW_API int few_sum_folded(void *wf, const void *W, const double *phase_coeffs, 
  * first sample, end sample}, segments' samples as few_segment_plan makes
  * them (units of one waveform must not overlap).  smem_bytes: dynamic shared
  * memory per CTA (<= 200 KiB; the largest R*NN*64 of the batch, capped);
- * ctas: persistent CTAs (0: two per SM).  mode FEW_SUM_FAITHFUL or FEW_SUM_EXACT. */
+ * ctas: persistent CTAs (0: two per SM).  mode FEW_SUM_FAITHFUL or FEW_SUM_EXACT.
+ * done [device] (nwave,) or NULL: each waveform's completion time, the
+ * %globaltimer nanoseconds after its last work unit, merged with atomicMax
+ * (zero it first). */
 FEW_API int few_sum_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int smem_bytes,
-                            int mode, int ctas, void *stream);
+                            int mode, int ctas, unsigned long long *done, void *stream);
+
+/* Writes the GPU's %globaltimer (nanoseconds) into dst [device] when the
+ * stream reaches it: a time stamp that a CUDA graph can hold. */
+FEW_API int few_stamp(unsigned long long *dst, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Mixed-precision sum on tcgen05 tensor cores (no counterpart in the        */
@@ -275,9 +282,10 @@ FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs,
  * (nwave,) with Bpk set (few_fold_mixed per waveform); units4 [device]
  * (4*nunits,) = {waveform, segment, first sample, end sample}; max_R: the
  * largest R in the batch (<= 64, sizes shared memory and TMEM); ctas:
- * persistent CTAs (0: two per SM); err [device] int as in few_sum_mixed. */
+ * persistent CTAs (0: two per SM); err [device] int as in few_sum_mixed;
+ * done as in few_sum_batched. */
 FEW_API int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
-                                  int ctas, int *err, void *stream);
+                                  int ctas, int *err, unsigned long long *done, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Adjoint (no counterpart in the reference: it has no gradients)           */

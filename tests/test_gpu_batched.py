@@ -92,3 +92,48 @@ def test_batched_backward_matches_single(cuda, tmp_path, monkeypatch, precision)
         assert not b.mixed_error()
         assert torch.equal(gt, teuk.grad)
         assert torch.equal(gp, pc.grad)
+
+
+def test_per_waveform_completion_times(cuda, tmp_path, monkeypatch):
+    """The time stamps behind the batched p50/p99: every waveform's sum
+    completes after the forward's start, within the forward's span, and its
+    backward after every forward completion (the backward starts once the
+    persistent sum is done)."""
+    monkeypatch.setenv("FEW_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    batch = uneven_batch(count=5, seed=11)
+    b = BatchedInterpolatedModeSum(precision="mixed", chunk=1024, ctas_per_sm=2).setup(batch, requires_grad=True)
+    outs = b.forward()
+    b.backward([torch.conj(o).clone() for o in outs])
+    torch.cuda.synchronize()
+    fwd, bwd = b.latencies()
+    assert fwd.shape == (5,) and bwd is not None and bwd.shape == (5,)
+    assert np.all(fwd > 0) and np.all(np.isfinite(fwd))
+    assert np.all(bwd >= fwd.max())
+    assert bwd.max() < 60e3  # ms: the stamps are nanoseconds of the same clock
+
+
+def test_backward_tables_reach_the_side_stream(cuda):
+    """Many short forward + backward calls through one module (both gradients,
+    so the phase branch runs on the side stream): every call's gradients equal
+    a second run's bit for bit.  The side stream reads segment tables that the
+    backward uploads; they must be in place before it forks."""
+    rng = np.random.default_rng(4)
+    cases = []
+    for w in range(24):
+        K = int(rng.integers(5, 60))
+        N = int(rng.integers(6, 40))
+        cases.append(S.small_case(K=K, N=N, out_len=int(rng.integers(2000, 9000)), seed=100 + w, theta=False))
+    ims = InterpolatedModeSum(precision="exact")
+
+    def grads(inp):
+        teuk = torch.tensor(inp.teuk_modes, device=cuda, requires_grad=True)
+        pc = torch.tensor(inp.phase_coeffs, device=cuda, requires_grad=True)
+        h = ims(inp.t, teuk, inp.ylms, inp.phase_t, pc, inp.l, inp.m, inp.k, inp.n, T=inp.T, dt=inp.dt)
+        h.backward(torch.conj(h.detach()))
+        return teuk.grad, pc.grad
+
+    first = [grads(c) for c in cases]
+    torch.cuda.synchronize()
+    for c, (gt, gp) in zip(cases, first):
+        gt2, gp2 = grads(c)
+        assert torch.equal(gt, gt2) and torch.equal(gp, gp2)
