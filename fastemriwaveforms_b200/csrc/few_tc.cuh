@@ -90,48 +90,36 @@ __device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a_desc, uint64_
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
 }
 
-// rint(x * scale) as an int32 (|x * scale| < 2^31) without a conversion
-// instruction: x * scale + 1.5 * 2^52, rounded once by the FMA, holds the
-// rounded integer in the low 32 bits of its significand.
-__device__ __forceinline__ int scaled_rint(double x, double scale)
+// Signed base-256 digits.  An operand value x is scaled to an integer
+// |Y| <= 127 2^24 and written as Y = d0 2^24 + d1 2^16 + d2 2^8 + d3 with
+// |d0| <= 127 and d1..d3 in [-128, 127] (each an int8).  Products of two such
+// expansions, summed by the integer tensor core level by level (level = digit
+// index sum), are exact; levels >= 4 weigh below 2^-31 of the scales.
+//
+// The digits come straight out of the bytes of Y + kDigitBias (kDigitBias =
+// 128 (1 + 2^8 + 2^16)): its bytes 0..2 are d3..d1 + 128, its byte 3 is d0.
+// scaled_biased gives Y + kDigitBias as the low 32 bits of the FMA
+// x * scale + 1.5 * 2^52 + kDigitBias (rounded once: rint(x * scale)), so no
+// conversion instruction is needed.
+constexpr int kDigitBias = 128 + (128 << 8) + (128 << 16);
+constexpr double kDigitScale = 127.0 * 16777216.0;  // |x| <= 1 -> |Y| <= 127 2^24
+
+__device__ __forceinline__ uint32_t scaled_biased(double x, double scale)
 {
-    return __double2loint(__fma_rn(x, scale, 6755399441055744.0));
+    return (uint32_t)__double2loint(__fma_rn(x, scale, 6755399441055744.0 + (double)kDigitBias));
 }
 
-// Signed base-128 digits of integers |Y| <= 127 * 2^21: Y = d0 2^21 + d1 2^14
-// + d2 2^7 + d3 with d1..d3 in [-64, 63] and |d0| <= 127 (each digit fits an
-// int8).  Products of two such expansions, summed by the integer tensor core
-// level by level (level = digit index sum), are exact.  Four values at a
-// time, each digit plane packed into one word (byte e = value e): with the
-// bias 64 (1 + 2^7 + 2^14) added, the three low digits are plain 7-bit
-// fields minus 64 and the top digit is the arithmetic shift by 21.
-__device__ __forceinline__ void digit_words4(int y0, int y1, int y2, int y3, uint32_t *w)
-{
-    constexpr int kBias = 64 + (64 << 7) + (64 << 14);
-    y0 += kBias;
-    y1 += kBias;
-    y2 += kBias;
-    y3 += kBias;
-    const uint32_t lo01 = __byte_perm((uint32_t)y0, (uint32_t)y1, 0x0040);
-    const uint32_t lo23 = __byte_perm((uint32_t)y2, (uint32_t)y3, 0x0040);
-    w[3] = __vsub4(__byte_perm(lo01, lo23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
-    const uint32_t a01 = __byte_perm((uint32_t)(y0 >> 7), (uint32_t)(y1 >> 7), 0x0040);
-    const uint32_t a23 = __byte_perm((uint32_t)(y2 >> 7), (uint32_t)(y3 >> 7), 0x0040);
-    w[2] = __vsub4(__byte_perm(a01, a23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
-    const uint32_t b01 = __byte_perm((uint32_t)(y0 >> 14), (uint32_t)(y1 >> 14), 0x0040);
-    const uint32_t b23 = __byte_perm((uint32_t)(y2 >> 14), (uint32_t)(y3 >> 14), 0x0040);
-    w[1] = __vsub4(__byte_perm(b01, b23, 0x5410) & 0x7F7F7F7Fu, 0x40404040u);
-    const uint32_t c01 = __byte_perm((uint32_t)(y0 >> 21), (uint32_t)(y1 >> 21), 0x0040);
-    const uint32_t c23 = __byte_perm((uint32_t)(y2 >> 21), (uint32_t)(y3 >> 21), 0x0040);
-    w[0] = __byte_perm(c01, c23, 0x5410);
-}
+// The biased integer of -x from that of x: -Y + B = 2B - (Y + B).
+__device__ __forceinline__ uint32_t negated_biased(uint32_t y) { return 2u * (uint32_t)kDigitBias - y; }
 
-// (re, im) byte pairs of a packed word -> (-im, re): the digits of z turned
-// into those of i z (negated digits represent the negated value exactly).
-__device__ __forceinline__ uint32_t rot_bytes(uint32_t w)
+// Four biased values -> one word per digit plane (byte e = value e), plane 0
+// the most significant.
+__device__ __forceinline__ void digit_words8(uint32_t y0, uint32_t y1, uint32_t y2, uint32_t y3, uint32_t *w)
 {
-    const uint32_t t = __byte_perm(w, 0u, 0x2301);
-    return (__vneg4(t) & 0x00FF00FFu) | (t & 0xFF00FF00u);
+    w[0] = __byte_perm(__byte_perm(y0, y1, 0x0073), __byte_perm(y2, y3, 0x0073), 0x5410);
+    w[1] = __byte_perm(__byte_perm(y0, y1, 0x0062), __byte_perm(y2, y3, 0x0062), 0x5410) ^ 0x80808080u;
+    w[2] = __byte_perm(__byte_perm(y0, y1, 0x0051), __byte_perm(y2, y3, 0x0051), 0x5410) ^ 0x80808080u;
+    w[3] = __byte_perm(__byte_perm(y0, y1, 0x0040), __byte_perm(y2, y3, 0x0040), 0x5410) ^ 0x80808080u;
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar)

@@ -20,13 +20,13 @@
 //       forms Y_r = sum_c tau^c Z_{c,r} (Horner, FP64).
 //
 // Precision: v, u, g, tau in FP64 (FP64 sincos of each phase, FP64
-// recurrences); every operand value is scaled to an integer |Y| <= 126 2^21
+// recurrences); every operand value is scaled to an integer |Y| <= 127 2^24
 // (A: fixed scale, |A| <= 1; B: one scale per segment and column, from the
-// column's largest value) and split into four signed base-128 digits (int8
+// column's largest value) and split into four signed base-256 digits (int8
 // planes).  kind::i8 MMAs multiply digit planes i and j into the level i + j
 // accumulator (levels 0..3, ten products per K step, s32, exact); the levels
 // are combined in FP64 and the epilogue (tau^c, u_r, the row sums, e_f, the
-// projection) runs in FP64.  The only error left is the 2^-29 representation
+// projection) runs in FP64.  The only error left is the 2^-32 representation
 // of the operands.
 //
 // Shape: one CTA of 128 threads per work unit (<= 1024 samples of one
@@ -55,7 +55,7 @@ constexpr int kLvl = kColsRow * kRowsPass;          // TMEM columns per level (6
 constexpr int kTmemCols = kDig * kLvl;              // 256
 constexpr int kAPlane = kPT * kKS;                  // A digit plane of a K step: 4 KB
 constexpr int kBPlane = kLvl * kKS;                 // B digit plane of a K step and pass: 2 KB
-constexpr double kScale = 126.0 * 2097152.0;        // |value| <= max -> |Y| <= 126 2^21
+constexpr double kScale = kDigitScale;               // |value| <= max -> |Y| <= 127 2^24
 constexpr int kMaxPhaseRows = 64;
 constexpr int kMaxPhaseNN = 128;                    // A of a tile (4 digits x 2 NNp x 128 B) <= 128 KB
 
@@ -79,8 +79,8 @@ __device__ __forceinline__ void digit_chunks(const double *x, double scale, uint
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         uint32_t t[kDig];
-        digit_words4(scaled_rint(x[4 * q], scale), scaled_rint(x[4 * q + 1], scale),
-                     scaled_rint(x[4 * q + 2], scale), scaled_rint(x[4 * q + 3], scale), t);
+        digit_words8(scaled_biased(x[4 * q], scale), scaled_biased(x[4 * q + 1], scale),
+                     scaled_biased(x[4 * q + 2], scale), scaled_biased(x[4 * q + 3], scale), t);
 #pragma unroll
         for (int p = 0; p < kDig; ++p) w[p][q] = t[p];
     }
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     __shared__ uint32_t s_tmem;
     __shared__ int s_rm[kMaxPhaseRows], s_rk[kMaxPhaseRows];
     __shared__ double s_pc[24];
-    __shared__ double s_inv[kColsRow * kMaxPhaseRows];  // 2^21 / (A scale x column scale)
+    __shared__ double s_inv[kColsRow * kMaxPhaseRows];  // 2^24 / (A scale x column scale)
     __shared__ double s_e[3][kPT];
     __shared__ double s_s[kPT];
 
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     }
     const unsigned char *const block = a.Bpk + (long long)seg * pd.seg_bytes;
     for (int j = tid; j < pd.NBc; j += blockDim.x)
-        s_inv[j] = 2097152.0 / (kScale * reinterpret_cast<const double *>(block)[j]);
+        s_inv[j] = 16777216.0 / (kScale * reinterpret_cast<const double *>(block)[j]);
     if (tid < 24) {
         const int q = tid >> 3, c = tid & 7;
         s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
 #pragma unroll
                     for (int l = 0; l < kDig; ++l)
                         lv[l] = __hiloint2double(0x43300000, D[l][q] ^ 0x80000000) - 4503601774854144.0;
-                    const double acc = fma(lv[0], 2097152.0, fma(lv[1], 16384.0, fma(lv[2], 128.0, lv[3])));
+                    const double acc = fma(lv[0], 16777216.0, fma(lv[1], 65536.0, fma(lv[2], 256.0, lv[3])));
                     val[q] = acc * s_inv[kColsRow * r + q];
                 }
                 // q = 2 (4 yz + c) + re/im

@@ -291,14 +291,14 @@ __global__ void __launch_bounds__(32 * kScanChunks) k_spline_build_factored(
         const double tt = (sN2 + s_last - 2 * dl) * ih;
         const double c1 = sN2, c2 = (dl - sN2) * ih - tt, c3 = tt * ih;
         const long long off = i * os_i, offe = (long long)(N - 1) * os_i;
-        o0[off] = yl;
-        o1[off] = c1;
-        o2[off] = c2;
-        o3[off] = c3;
-        o0[offe] = yc;
-        o1[offe] = c1 + 2 * c2 * xx + 3 * c3 * xx * xx;
-        o2[offe] = (2. * c2 + 6. * c3 * xx) / 2.;
-        o3[offe] = c3;
+        __stcs(o0 + off, yl);
+        __stcs(o1 + off, c1);
+        __stcs(o2 + off, c2);
+        __stcs(o3 + off, c3);
+        __stcs(o0 + offe, yc);
+        __stcs(o1 + offe, c1 + 2 * c2 * xx + 3 * c3 * xx * xx);
+        __stcs(o2 + offe, (2. * c2 + 6. * c3 * xx) / 2.);
+        __stcs(o3 + offe, c3);
         s_ip1 = sN2;
         yr = yl;
         top = N - 3;
@@ -324,10 +324,12 @@ __global__ void __launch_bounds__(32 * kScanChunks) k_spline_build_factored(
                 const double s_i = fma(fq[q], cb, rv[q]);
                 const double dl = (yr - yv[q]) * fh[q];
                 const double tt = (s_i + s_ip1 - 2 * dl) * fh[q];
-                o0[off] = yv[q];
-                o1[off] = s_i;
-                o2[off] = (dl - s_i) * fh[q] - tt;
-                o3[off] = tt * fh[q];
+                // final coefficients: streaming stores (evict first), so that they do
+                // not push the sweep temporaries and y out of L2
+                __stcs(o0 + off, yv[q]);
+                __stcs(o1 + off, s_i);
+                __stcs(o2 + off, (dl - s_i) * fh[q] - tt);
+                __stcs(o3 + off, tt * fh[q]);
                 s_ip1 = s_i;
                 yr = yv[q];
             }
