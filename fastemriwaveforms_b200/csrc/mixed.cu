@@ -22,14 +22,15 @@
 //
 // Layout: A and B tiles are K-major, no swizzle: 8x8 bf16 core matrices of
 // 128 contiguous bytes; stride 128 B between the two K halves of a K=16 step
-// (LBO) and 256 B between 8-row groups (SBO).  One CTA of 128 threads owns a
-// work unit (<= 1024 samples of one segment); each thread owns one sample row of
-// a 128-sample tile.  K runs in chunks of 32 (16 n' x {Re, Im}); two stages:
-// while the tensor cores run chunk k's MMAs (2 K-steps x 3 split products per
-// group of <= 256 columns), the threads write chunk k+1 of A and its B chunk
-// arrives by cp.async; an mbarrier per stage (tcgen05.commit) gates reuse.
-// Every wait is bounded and a timeout sets an error word and ends the kernel
-// after freeing TMEM.
+// (LBO) and 256 B between 8-row groups (SBO).  A CTA of 8 producer warps and one
+// MMA warp owns a work unit (<= 1024 samples of one segment) at a time, in
+// 128-sample tiles; two producer threads share a sample row.  K runs in chunks
+// of 32 (16 n' x {Re, Im}) through a two-stage ring: the producer half h writes
+// the A chunks k = h, h + 2, ... into stage h while the MMA warp brings each
+// chunk's B into its stage with one bulk copy and issues its MMAs (2 K-steps x
+// 3 split products per group of <= 256 columns); mbarriers gate every hand-off
+// (details at the kernels).  Every wait is bounded and a timeout sets an error
+// word and ends the kernel, freeing TMEM only once the MMAs have drained.
 #include <cuda_bf16.h>
 
 #include "few_common.cuh"
@@ -114,205 +115,347 @@ __host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, int &NNp
     nchunks = NNp / 16;
 }
 
-// One work unit (samples [lo, hi) of segment seg) on the tensor cores.
-// Returns false (for every thread) if a tensor-core wait timed out.
-__device__ bool mixed_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, MixedPipe &pp,
-                           int *s_rm, int *s_rk, double *s_pc)
-{
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int NB = a.NB;
-    const int bchunk = 2 * NB * kKC * 2;               // one B chunk: hi then lo planes
-    const int stage = kAStage + bchunk;
-    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
-    const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
-    const int R = a.R, NN = a.NN, nlo = a.nlo, nch = a.nchunks;
-    const long long nps = (long long)(a.N - 1) * 3;
+// ---------------------------------------------------------------------------
+// Warp-specialized sum: 8 producer warps and one MMA warp per CTA.
+// ---------------------------------------------------------------------------
+// Producer warp w owns TMEM lane quarter w & 3 (samples 32 (w & 3) .. +31 of a
+// 128-sample tile) and half h = w >> 2: half h writes the A chunks k = h, h + 2,
+// ... of every tile into A stage h and reads accumulator column groups
+// [h G/2, ...) in the epilogue, so two threads share a sample and the two A
+// stages are filled at the same time.  The B chunks go through their own ring
+// of nbs (2..4) slots: lane 0 of the MMA warp brings each chunk in with one bulk
+// copy nbs - 1 chunks ahead of its MMAs, waits for the chunk's A stage, issues
+// the MMAs and commits them to the A stage's and the B slot's "empty" barriers,
+// and after a tile's last chunk to "accumulator full".  Barriers: full[b] (4
+// producer arrivals), empty[b] (MMA commit), bfull[s] (the bulk copy's bytes),
+// bempty[s] (MMA commit), accf (MMA commit), acce (8 producer arrivals once the
+// accumulator has been read).  Every wait is bounded; a timeout sets the CTA's
+// fail word, after which no role waits again, every producer still reaches
+// every named barrier and arrival, and the MMA warp stops issuing.
+constexpr int kSumProd = 8;                        // producer warps: two per TMEM lane quarter
+constexpr int kSumProdThreads = 32 * kSumProd;     // 256
+constexpr int kSumThreads = kSumProdThreads + 32;  // + the MMA warp
+constexpr int kMaxBSlots = 4;
 
-    for (int r = tid; r < R; r += blockDim.x) {
-        s_rm[r] = a.row_m[r];
-        s_rk[r] = a.row_k[r];
+struct SumShared {
+    uint64_t full[2], empty[2], bfull[kMaxBSlots], bempty[kMaxBSlots], accf, acce, done;
+    uint32_t tmem;
+    int fail;
+    int rm[kMaxRows], rk[kMaxRows];
+    double pc[24];
+    float2 part[2][kMT];  // half 1's epilogue sums, by tile parity
+};
+
+// Ring layout of the dynamic shared memory: two A stages, then nbs B slots.
+struct SumRing {
+    int nbs;       // B slots
+    int bslot;     // bytes per B slot (>= every unit's chunk)
+};
+
+// Phases a role has consumed so far (registers; the same sequence in every role).
+struct SumRole {
+    uint32_t n0, n1;    // fills of A stage 0 and stage 1
+    uint32_t tiles;     // accumulator uses
+    uint32_t gi, gc;    // MMA warp: B chunks issued / consumed (all units)
+    bool dead;
+};
+
+__device__ __forceinline__ void sum_prod_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kSumProdThreads) : "memory"); }
+
+__device__ __forceinline__ void sum_setup(SumShared &s, int tmem_cols, SumRole &ro)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                     "r"((uint32_t)tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (tid < 24) {
-        const int q = tid >> 3, c = tid & 7;
-        s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&s.full[b], kSumProd / 2);
+            mbar_init(&s.empty[b], 1);
+        }
+        for (int q = 0; q < kMaxBSlots; ++q) {
+            mbar_init(&s.bfull[q], 1);
+            mbar_init(&s.bempty[q], 1);
+        }
+        mbar_init(&s.accf, 1);
+        mbar_init(&s.acce, kSumProd);
+        mbar_init(&s.done, 1);
+        s.fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const __nv_bfloat16 *Bseg = a.Bpk + (long long)seg * nch * 2 * NB * kKC;
-    bool failed = false;
+    ro.n0 = ro.n1 = ro.tiles = ro.gi = ro.gc = 0;
+    ro.dead = false;
+}
 
-    for (int base = lo; base < hi && !failed; base += kMT) {
-        const int i = base + tid;
+// End of a CTA: the MMA warp waits (bounded) for every MMA and bulk copy it
+// issued; TMEM is freed only if that drain completed (otherwise an MMA may
+// still be writing the accumulator and the columns stay allocated), and the
+// error word is set on any timeout.
+__device__ __forceinline__ void sum_teardown(SumShared &s, SumRole &ro, const SumRing &rg, int tmem_cols, int *err)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    bool drained = true;
+    if (warp == kSumProd && lane == 0) {
+        mma_commit(&s.done);
+        drained = mbar_wait_bounded(&s.done, 0);
+        for (uint32_t g = ro.gc; g < ro.gi; ++g)  // copies issued but not yet observed
+            drained = mbar_wait_bounded(&s.bfull[g % rg.nbs], (g / rg.nbs) & 1u) && drained;
+    }
+    tc_fence_before();
+    drained = __syncthreads_and(drained) != 0;
+    if ((s.fail || !drained) && threadIdx.x == 0) atomicExch(err, 1);
+    if (drained && warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"((uint32_t)tmem_cols)
+                     : "memory");
+    }
+}
+
+// MMA warp: bulk copy of B chunk k of the unit's segment into the next slot,
+// once the MMAs of that slot's previous chunk are done.
+__device__ __forceinline__ bool sum_issue_b(const unsigned char *Bseg, int k, uint32_t bchunk,
+                                            unsigned char *smem_raw, const SumRing &rg, SumShared &s, SumRole &ro)
+{
+    const uint32_t g = ro.gi, slot = g % rg.nbs, use = g / rg.nbs;
+    if (use >= 1 && !mbar_wait_bounded(&s.bempty[slot], (use - 1) & 1u)) return false;
+    mbar_arrive_expect_tx(&s.bfull[slot], bchunk);
+    bulk_copy_g2s(smem_raw + 2 * kAStage + slot * rg.bslot, Bseg + (size_t)k * bchunk, bchunk, &s.bfull[slot]);
+    ro.gi = g + 1;
+    return true;
+}
+
+// MMA warp, lane 0: the B chunks and the MMAs of every tile of one unit.
+__device__ void sum_mma_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, const SumRing &rg,
+                             SumShared &s, SumRole &ro)
+{
+    const int NB = a.NB, nch = a.nchunks;
+    const uint32_t bchunk = (uint32_t)(2 * NB * kKC * 2);  // hi then lo planes
+    const unsigned char *Bseg = reinterpret_cast<const unsigned char *>(a.Bpk) + (size_t)seg * nch * bchunk;
+    const int nfill = (hi - lo + kMT - 1) / kMT * nch;     // (tile, chunk) pairs of the unit
+    const int ahead = rg.nbs - 1;
+    bool ok = !*(volatile int *)&s.fail;
+    for (int f = 0; f < min(ahead, nfill) && ok; ++f) ok = sum_issue_b(Bseg, f % nch, bchunk, smem_raw, rg, s, ro);
+    for (int f = 0; f < nfill && ok; ++f) {
+        const int k = f % nch, b = k & 1;
+        const uint32_t n = b ? ro.n1 : ro.n0;
+        ok = !*(volatile int *)&s.fail;
+        // the accumulator is free once every producer has read the previous tile
+        if (ok && k == 0 && ro.tiles >= 1) ok = mbar_wait_bounded(&s.acce, (ro.tiles - 1) & 1u);
+        const uint32_t g = ro.gc, slot = g % rg.nbs;
+        if (ok) ok = mbar_wait_bounded(&s.bfull[slot], (g / rg.nbs) & 1u);
+        if (!ok) break;
+        ro.gc = g + 1;
+        ok = mbar_wait_bounded(&s.full[b], n & 1u);
+        if (!ok) break;
+        if (b) ro.n1 = n + 1;
+        else ro.n0 = n + 1;
+        tc_fence_after();
+        const uint32_t a_h = smem_u32(smem_raw + b * kAStage), a_l = a_h + kMT * kKC * 2;
+        const uint32_t b_h = smem_u32(smem_raw + 2 * kAStage + slot * rg.bslot), b_l = b_h + NB * kKC * 2;
+#pragma unroll
+        for (int st = 0; st < kKC / 16; ++st) {
+            const uint64_t da_h = smem_desc(a_h + st * (kMT / 8) * 256, 128, 256);
+            const uint64_t da_l = smem_desc(a_l + st * (kMT / 8) * 256, 128, 256);
+            for (int n0 = 0; n0 < NB; n0 += 256) {  // column groups of <= 256 (one MMA each)
+                const int nq = min(256, NB - n0);
+                const uint32_t idesc = idesc_bf16(kMT, nq);
+                const uint32_t boff = st * (NB / 8) * 256 + (n0 / 8) * 256;
+                const uint64_t db_h = smem_desc(b_h + boff, 128, 256);
+                const uint64_t db_l = smem_desc(b_l + boff, 128, 256);
+                const uint32_t d = s.tmem + (uint32_t)n0;
+                mma_bf16(d, da_h, db_h, idesc, (k | st) != 0);
+                mma_bf16(d, da_h, db_l, idesc, 1u);
+                mma_bf16(d, da_l, db_h, idesc, 1u);
+            }
+        }
+        mma_commit(&s.empty[b]);
+        mma_commit(&s.bempty[slot]);
+        if (k == nch - 1) {
+            mma_commit(&s.accf);
+            ro.tiles++;
+        }
+        // next copy: into the slot of chunk f - 1, whose MMAs were issued one step ago
+        if (f + ahead < nfill) ok = sum_issue_b(Bseg, (f + ahead) % nch, bchunk, smem_raw, rg, s, ro);
+    }
+    if (!ok) {
+        ro.dead = true;
+        atomicExch(&s.fail, 1);
+    }
+}
+
+// Producer warps: one unit's A chunks and epilogues.  Every producer runs every
+// tile of the unit and reaches every named barrier and arrival; after a failed
+// wait it only skips the work.
+__device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, SumShared &s,
+                              SumRole &ro)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int h = warp >> 2, row = 32 * (warp & 3) + lane;  // half; sample row = TMEM lane
+    const int NB = a.NB, R = a.R, nlo = a.nlo, nch = a.nchunks;
+    const long long nps = (long long)(a.N - 1) * 3;
+    sum_prod_sync();  // the previous unit's readers of the row tables are done
+    for (int r = tid; r < R; r += kSumProdThreads) {
+        s.rm[r] = a.row_m[r];
+        s.rk[r] = a.row_k[r];
+    }
+    if (tid < 24) {
+        const int q = tid >> 3, c = tid & 7;
+        s.pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    sum_prod_sync();
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
+    const int ng = NB / 16, gs = (ng + 1) / 2;  // 16-column groups; half 0 takes [0, gs)
+    const int g_lo = h ? gs : 0, g_hi = h ? ng : gs;
+    unsigned char *const aH = smem_raw + h * kAStage, *const aL = aH + kMT * kKC * 2;
+
+    for (int base = lo; base < hi; base += kMT) {
+        const int i = base + row;
         const bool valid = i < hi;
-        // FP64 prelude: phases (interpolate.cu:626-644) and anchors
+        // the output sample, read early (half 0 adds both halves' sums into it)
+        double2 o = make_double2(0.0, 0.0);
+        if (!h && valid) o = a.wf[i];
+        // FP64 prelude: phases (interpolate.cu:626-644) and anchors.  Rows past the
+        // unit (and n' past NN, whose B rows are zero) hold finite phasors whose
+        // products are discarded or vanish, so nothing is masked.
         const double t = (double)i * a.dt;
-        const double x = t - t0;
-        const float tau = (float)(x / hs);
-        const double s = (t - pt0) / pw;
-        const double s1 = 1.0 - s;
-        const double Pp = phase_poly(s_pc, s, s1);
-        const double Pr = phase_poly(s_pc + 16, s, s1);
-        const double Pt = a.use_theta ? phase_poly(s_pc + 8, s, s1) : 0.0;
-        const float2 Ep = anchor(Pp);
+        const float tau = (float)((t - t0) / hs);
+        const double sp = (t - pt0) / pw;
+        const double sp1 = 1.0 - sp;
+        const double Pr = phase_poly(s.pc + 16, sp, sp1);
         const float2 Er = anchor(Pr);
-        const float2 Et = a.use_theta ? anchor(Pt) : make_float2(1.f, 0.f);
         const float2 Er2 = fcmul(Er, Er);
-        float2 v[16];
-
-        for (int k = 0; k < nch && !failed; ++k) {
-            const int b = k & 1;
-            const int nblk = k;
-            // stage b is free once the MMAs of chunk k-2 are done
-            if (__syncthreads_or(!pipe_drain(pp, b))) {
-                failed = true;
-                break;
+        for (int k = h; k < nch; k += 2) {
+            const uint32_t n = h ? ro.n1 : ro.n0;
+            bool dead = ro.dead || *(volatile int *)&s.fail;
+            if (!dead && n >= 1 && !mbar_wait_bounded(&s.empty[h], (n - 1) & 1u)) {
+                atomicExch(&s.fail, 1);
+                dead = true;
             }
-            unsigned char *const sAb = smem_raw + b * stage;
-            unsigned char *const sBb = sAb + kAStage;
-            {
-                const unsigned char *src = reinterpret_cast<const unsigned char *>(Bseg + (long long)k * 2 * NB * kKC);
-                for (int q = tid; q < bchunk / 16; q += blockDim.x) cp_async16(sBb + 16 * q, src + 16 * q);
-                cp_async_commit();
-            }
-            {
+            ro.dead = __any_sync(0xffffffffu, dead);
+            if (!ro.dead) {
                 // two interleaved chains (even and odd n') stepping by Er^2: half the
                 // dependent depth of one chain, and 8 FP32 steps from the anchor at most
-                v[0] = anchor((double)(nlo + 16 * nblk) * Pr);
+                float2 v[16];
+                v[0] = anchor((double)(nlo + 16 * k) * Pr);
                 v[1] = fcmul(v[0], Er);
 #pragma unroll
                 for (int q = 2; q < 16; ++q) v[q] = fcmul(v[q - 2], Er2);
 #pragma unroll
-                for (int q = 0; q < 16; ++q)
-                    if (!valid || 16 * nblk + q >= NN) v[q] = make_float2(0.f, 0.f);
-            }
-            unsigned char *const aH = sAb, *const aL = sAb + kMT * kKC * 2;
+                for (int g = 0; g < 4; ++g) {  // 4 groups of 4 complex = 8 bf16 = 16 bytes
+                    uint32_t h4[4], l4[4];
 #pragma unroll
-            for (int g = 0; g < 4; ++g) {  // 4 groups of 4 complex = 8 bf16 = 16 bytes
-                uint32_t h4[4], l4[4];
-#pragma unroll
-                for (int e2 = 0; e2 < 4; ++e2) {
-                    const float2 z = v[4 * g + e2];
-                    split2(z.x, z.y, h4[e2], l4[e2]);
+                    for (int e2 = 0; e2 < 4; ++e2) split2(v[4 * g + e2].x, v[4 * g + e2].y, h4[e2], l4[e2]);
+                    const uint32_t off = tile_off(row, 8 * g, kMT / 8);
+                    *reinterpret_cast<uint4 *>(aH + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
+                    *reinterpret_cast<uint4 *>(aL + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
                 }
-                const uint32_t off = tile_off(tid, 8 * g, kMT / 8);
-                *reinterpret_cast<uint4 *>(aH + off) = make_uint4(h4[0], h4[1], h4[2], h4[3]);
-                *reinterpret_cast<uint4 *>(aL + off) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
             }
-            cp_async_wait_all();
             fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                tc_fence_after();
-                const uint32_t a_h = smem_u32(aH), a_l = smem_u32(aL);
-                const uint32_t b_h = smem_u32(sBb), b_l = b_h + NB * kKC * 2;
-#pragma unroll
-                for (int st = 0; st < kKC / 16; ++st) {
-                    const uint64_t da_h = smem_desc(a_h + st * (kMT / 8) * 256, 128, 256);
-                    const uint64_t da_l = smem_desc(a_l + st * (kMT / 8) * 256, 128, 256);
-                    for (int n0 = 0; n0 < NB; n0 += 256) {  // column groups of <= 256 (one MMA each)
-                        const int nq = min(256, NB - n0);
-                        const uint32_t idesc = idesc_bf16(kMT, nq);
-                        const uint32_t boff = st * (NB / 8) * 256 + (n0 / 8) * 256;
-                        const uint64_t db_h = smem_desc(b_h + boff, 128, 256);
-                        const uint64_t db_l = smem_desc(b_l + boff, 128, 256);
-                        const uint32_t d = pp.tmem + (uint32_t)n0;
-                        mma_bf16(d, da_h, db_h, idesc, (k | st) != 0);
-                        mma_bf16(d, da_h, db_l, idesc, 1u);
-                        mma_bf16(d, da_l, db_h, idesc, 1u);
-                    }
-                }
-                mma_commit(&pp.bar[b]);
-            }
-            if (b == 0) pp.pend0 = 1;
-            else pp.pend1 = 1;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s.full[h]);
+            if (h) ro.n1 = n + 1;
+            else ro.n0 = n + 1;
         }
-        if (failed) break;
-        // all MMAs of the tile done before the accumulator is read
-        const bool ok0 = pipe_drain(pp, 0), ok1 = pipe_drain(pp, 1);
-        if (__syncthreads_or(!(ok0 && ok1))) {
-            failed = true;
-            break;
+        // accumulator of this tile: this thread's row (TMEM lane), half h's column
+        // groups; two (m', k') rows of 8 columns per 16-column load, two loads in
+        // flight; u_r by one multiplication when m' steps by one
+        bool dead = ro.dead || *(volatile int *)&s.fail;
+        if (!dead && !mbar_wait_bounded(&s.accf, ro.tiles & 1u)) {
+            atomicExch(&s.fail, 1);
+            dead = true;
         }
-        // epilogue: this thread's accumulator row (TMEM lane = tid); two (m', k')
-        // rows of 8 columns per 16-column load; u_r by one multiplication when m'
-        // steps by one
+        ro.dead = __any_sync(0xffffffffu, dead);
         tc_fence_after();
-        const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
-        float2 uu = make_float2(1.f, 0.f);
-        int pm = 0x7fffffff, pk = 0x7fffffff;
         float2 Sp = make_float2(0.f, 0.f);
-        for (int c0 = 0; c0 < NB; c0 += 16) {
-            float D[16];
-            tmem_ld16(trow + c0, D);
-            tmem_wait_ld();
+        if (!ro.dead && g_lo < g_hi) {
+            const double Pp = phase_poly(s.pc, sp, sp1);
+            const float2 Ep = anchor(Pp);
+            const float2 Et = a.use_theta ? anchor(phase_poly(s.pc + 8, sp, sp1)) : make_float2(1.f, 0.f);
+            const uint32_t trow = s.tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+            float2 uu = make_float2(1.f, 0.f);
+            int pm = 0x7fffffff, pk = 0x7fffffff;
+            for (int g0 = g_lo; g0 < g_hi; g0 += 2) {
+                float D[32];
+                tmem_ld16(trow + 16 * g0, D);
+                if (g0 + 1 < g_hi) tmem_ld16(trow + 16 * (g0 + 1), D + 16);
+                tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int r = (c0 >> 3) + q;
-                if (r < R) {
-                    const int mm = s_rm[r], kk = s_rk[r];
-                    if (kk == pk && mm == pm + 1) {
-                        uu = fcmul(uu, Ep);
-                    } else {
-                        uu = fcpow(Ep, mm);
-                        if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                for (int q = 0; q < 4; ++q) {
+                    const int r = 2 * g0 + q;
+                    if (r < R && (q < 2 || g0 + 1 < g_hi)) {
+                        const int mm = s.rm[r], kk = s.rk[r];
+                        if (kk == pk && mm == pm + 1) {
+                            uu = fcmul(uu, Ep);
+                        } else {
+                            uu = fcpow(Ep, mm);
+                            if (kk) uu = fcmul(uu, fcpow(Et, kk));
+                        }
+                        pm = mm;
+                        pk = kk;
+                        const float *d8 = D + 8 * q;
+                        // Y = sum_c tau^c Z_c (Horner)
+                        const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
+                        const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
+                        Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
+                        Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
                     }
-                    pm = mm;
-                    pk = kk;
-                    const float *d8 = D + 8 * q;
-                    // Y = sum_c tau^c Z_c (Horner)
-                    const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
-                    const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
-                    Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
-                    Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
                 }
             }
-        }
-        if (valid) {
-            double2 o = a.wf[i];
-            o.x += (double)Sp.x;
-            o.y += (double)Sp.y;
-            a.wf[i] = o;
         }
         tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s.acce);
+        if (h) s.part[ro.tiles & 1u][row] = Sp;
+        sum_prod_sync();
+        if (!h && valid && !ro.dead) {
+            const float2 o2 = s.part[ro.tiles & 1u][row];
+            o.x += (double)(Sp.x + o2.x);
+            o.y += (double)(Sp.y + o2.y);
+            a.wf[i] = o;
+        }
+        ro.tiles++;
     }
-    cp_async_wait_all();
-    return !failed;
 }
 
-__global__ void __launch_bounds__(kMT, 1) k_sum_mixed(MixedArgs a)
+__global__ void __launch_bounds__(kSumThreads, 2) k_sum_mixed(MixedArgs a, SumRing rg)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_pc[24];
-    MixedPipe pp;
-    mixed_setup(&s_tmem, s_bar, a.tmem_cols, pp);
+    __shared__ SumShared s;
+    SumRole ro;
+    sum_setup(s, a.tmem_cols, ro);
     const int u = blockIdx.x;
-    const bool ok =
-        mixed_unit(a, a.units[3 * u], a.units[3 * u + 1], a.units[3 * u + 2], smem_raw, pp, s_rm, s_rk, s_pc);
-    mixed_teardown(!ok, pp, a.tmem_cols, a.err);
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    if ((int)(threadIdx.x >> 5) == kSumProd) {
+        if ((threadIdx.x & 31) == 0) sum_mma_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
+        __syncwarp();
+    } else {
+        sum_prod_unit(a, seg, lo, hi, smem_raw, s, ro);
+    }
+    sum_teardown(s, ro, rg, a.tmem_cols, a.err);
 }
 
 // Persistent form over many waveforms: TMEM and the mbarriers are set up once
-// per CTA; units {waveform, segment, first, end} are taken in stride.
-__global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_desc *__restrict__ descs,
-                                                              const int *__restrict__ units4, int nunits,
-                                                              int tmem_cols, int *err,
-                                                              unsigned long long *__restrict__ done)
+// per CTA; units {waveform, segment, first, end} are taken in stride.  The B
+// slots keep the size of the largest chunk (max_NB) for every unit, so that a
+// unit with a wider B never writes where the previous unit's MMAs may still
+// read.
+__global__ void __launch_bounds__(kSumThreads, 2) k_sum_mixed_batched(const few_wave_desc *__restrict__ descs,
+                                                                      const int *__restrict__ units4, int nunits,
+                                                                      SumRing rg, int tmem_cols, int *err,
+                                                                      unsigned long long *__restrict__ done)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
-    __shared__ double s_pc[24];
-    MixedPipe pp;
-    mixed_setup(&s_tmem, s_bar, tmem_cols, pp);
-    bool ok = true;
-    for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+    __shared__ SumShared s;
+    SumRole ro;
+    sum_setup(s, tmem_cols, ro);
+    const bool mma = (int)(threadIdx.x >> 5) == kSumProd;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const few_wave_desc d = descs[units4[4 * u]];
         MixedArgs a;
         a.wf = (double2 *)d.wf;
@@ -332,10 +475,19 @@ __global__ void __launch_bounds__(kMT, 1) k_sum_mixed_batched(const few_wave_des
         a.dt = d.dt;
         a.tmem_cols = tmem_cols;
         mixed_dims_core(d.R, d.NN, a.NNp, a.NB, a.nchunks);
-        ok = mixed_unit(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3], smem_raw, pp, s_rm, s_rk, s_pc);
-        if (done && ok && threadIdx.x == 0) atomicMax(done + units4[4 * u], global_ns());  // unit complete
+        const int seg = units4[4 * u + 1], lo = units4[4 * u + 2], hi = units4[4 * u + 3];
+        if (mma) {
+            if ((threadIdx.x & 31) == 0 && !ro.dead) sum_mma_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
+        } else {
+            sum_prod_unit(a, seg, lo, hi, smem_raw, s, ro);
+            if (done) {
+                sum_prod_sync();  // every output row of the unit written
+                if (threadIdx.x == 0 && !ro.dead) atomicMax(done + units4[4 * u], global_ns());  // unit complete
+            }
+        }
     }
-    mixed_teardown(!ok, pp, tmem_cols, err);
+    if (mma) __syncwarp();
+    sum_teardown(s, ro, rg, tmem_cols, err);
 }
 
 }  // namespace
@@ -351,7 +503,21 @@ int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
     return FEW_OK;
 }
 
-size_t mixed_smem_bytes(int NB) { return (size_t)2 * (kAStage + 2 * NB * kKC * 2); }
+// B slots of the sum's ring for chunks of NB columns: as many (2..4) as keep two
+// CTAs per SM (<= 110 KB of dynamic shared memory with the two A stages), and
+// the dynamic shared memory that takes.
+SumRing mixed_ring(int NB)
+{
+    SumRing rg;
+    rg.bslot = 2 * NB * kKC * 2;
+    rg.nbs = std::max(2, std::min(kMaxBSlots, (110 * 1024 - 2 * kAStage) / rg.bslot));
+    return rg;
+}
+size_t mixed_smem_bytes(int NB)
+{
+    const SumRing rg = mixed_ring(NB);
+    return (size_t)2 * kAStage + (size_t)rg.nbs * rg.bslot;
+}
 
 size_t mixed_bpk_bytes(int nseg, int R, int NN)
 {
@@ -400,7 +566,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
     a.dt = dt;
     const size_t smem = mixed_smem_bytes(a.NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed, (int)smem));
-    k_sum_mixed<<<nunits, kMT, smem, st>>>(a);
+    k_sum_mixed<<<nunits, kSumThreads, smem, st>>>(a, mixed_ring(a.NB));
     FEW_LAUNCH_CHECK("k_sum_mixed");
     return FEW_OK;
 }
@@ -421,7 +587,7 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
     ctas = std::min(ctas, nunits);
     const size_t smem = mixed_smem_bytes(NB);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
-    k_sum_mixed_batched<<<ctas, kMT, smem, st>>>(descs, units4, nunits, cols, err, done);
+    k_sum_mixed_batched<<<ctas, kSumThreads, smem, st>>>(descs, units4, nunits, mixed_ring(NB), cols, err, done);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");
     return FEW_OK;
 }

@@ -55,7 +55,7 @@ constexpr int kProdThreads = 32 * kProd;
 constexpr int kGPre = kProd;         // tiles per prelude batch (one sample per producer thread)
 constexpr int kStages = 2;           // operand ring
 constexpr int kGFlush = 32;          // tiles per block: one B scale, int32 sums well inside 2^31
-constexpr int kDigits = 4;           // base-128 digits per operand value
+constexpr int kDigits = 4;           // base-256 digits per operand value
 constexpr int kPlaneA = 8 * 1024;    // one A digit plane: 8 MN groups (2 x 64 n') x 8 K groups x 128 B
 constexpr uint32_t kLBO = 128;       // K-group stride (bytes)
 constexpr uint32_t kSBO = 1024;      // MN-group stride (bytes)
@@ -86,10 +86,6 @@ __device__ __forceinline__ void digit_words(const double *x, double scale, uint3
 // Producer-only named barrier (the MMA warp does not take part).
 __device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kProdThreads) : "memory"); }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 struct AdjGMixedArgs {
     const double2 *grad;   // torch upstream gradient G; g = conj(G)

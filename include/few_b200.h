@@ -319,10 +319,10 @@ FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, c
 /* Tensor-core adjoint (no counterpart in the reference).  Same quantities as
  * few_adjoint_G and few_adjoint_phase, with the contractions on the tcgen05
  * integer tensor cores in exact arithmetic: FP64 operands (phasors, g, powers
- * of tau, folded coefficients) scaled to 28-bit integers and split into four
- * int8 digits, digit products summed in int32 per level and combined in FP64;
- * the results differ from the FP64 kernels by the 2^-29 representation of the
- * operands only.  err [device] int is set to 1 if a tensor-core wait timed out. */
+ * of tau, folded coefficients) scaled to 32-bit integers and split into four
+ * signed base-256 int8 digits, digit products summed in int32 per level and
+ * combined in FP64; the results differ from the FP64 kernels by the 2^-32
+ * representation of the operands only.  err [device] int is set to 1 if a tensor-core wait timed out. */
 
 /* few_adjoint_G on the tensor cores: the contraction over each segment's
  * samples with K = samples.  t_knots [device] (N,).  R <= 64. */

@@ -2,7 +2,7 @@
 adjoint against the FP64 adjoint kernels, and the gradients of a mixed
 forward + mixed backward against the FP64 backward.  Both contractions run in
 exact integer arithmetic on the tensor cores (FP64 operands as four int8
-digits, int32 accumulation), so the only differences from FP64 are the 2^-29
+digits, int32 accumulation), so the only differences from FP64 are the 2^-32
 representation of the operands; the relative errors are printed."""
 import numpy as np
 import pytest
@@ -15,9 +15,9 @@ from fastemriwaveforms_b200.summation import _ptr
 
 pytestmark = pytest.mark.gpu
 
-REL_G = 1e-7           # G array (nseg, R, NN, 4) vs the FP64 kernel, relative L2
-REL_GRAD_TEUK = 1e-7   # dL/d teuk_modes vs the FP64 backward, relative L2
-REL_GRAD_PC = 1e-7     # dL/d phase_interp_coeffs vs the FP64 backward, relative L2
+REL_G = 1e-8           # G array (nseg, R, NN, 4) vs the FP64 kernel, relative L2 (measured <= 9e-10)
+REL_GRAD_TEUK = 3e-8   # dL/d teuk_modes vs the FP64 backward, relative L2 (measured <= 4.2e-9)
+REL_GRAD_PC = 3e-8     # dL/d phase_interp_coeffs vs the FP64 backward, relative L2 (measured <= 1.5e-9)
 
 
 def rel(a, b):

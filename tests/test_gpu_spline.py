@@ -84,7 +84,7 @@ def test_complex_strided_input_matches_real_rows(cuda, oracle):
     assert coeff_err(out.cpu().numpy(), ref) < 1e-12
 
 
-@pytest.mark.parametrize("N,ni,seed", [(4, 5, 0), (7, 3, 1), (1000, 7686, 2), (2000, 100, 3)])
+@pytest.mark.parametrize("N,ni,seed", [(4, 5, 0), (7, 3, 1), (1000, 7686, 2), (2000, 100, 3), (3001, 22, 4)])
 def test_factored_build_matches_generic(cuda, oracle, N, ni, seed):
     """The shared-knot path (host factorization) agrees with the per-series
     kernel and the oracle, on the complex (N, K) view InterpolatedModeSum uses."""
@@ -108,6 +108,28 @@ def test_factored_build_matches_generic(cuda, oracle, N, ni, seed):
     if N <= 1000:
         y_all = np.concatenate([teuk.T.real, teuk.T.imag])
         assert coeff_err(fact.cpu().numpy(), oracle.spline_coeffs(t, y_all)) < 1e-11
+
+
+@pytest.mark.parametrize("N,ni", [(5, 1), (64, 13), (1000, 300)])
+def test_factored_build_real_series(cuda, N, ni):
+    """The shared-knot build on a plain (ninterps, length) array (no complex
+    split: series in consecutive lanes) equals the per-series kernel."""
+    rng = np.random.default_rng(N + ni)
+    t = np.cumsum(np.concatenate([[0.0], rng.uniform(0.2, 3.0, N - 1)]))
+    y = rng.standard_normal((ni, N))
+    td = torch.from_numpy(t).to(cuda)
+    yd = torch.from_numpy(y).to(cuda)
+    st = torch.cuda.current_stream().cuda_stream
+    generic = torch.empty((4, N, ni), dtype=torch.float64, device=cuda)
+    _lib.call("few_spline_build", td.data_ptr(), 0, yd.data_ptr(), 1, N, ni, 0, ni, N, generic.data_ptr(),
+              _lib.FEW_LAYOUT_KNOT_MAJOR, st)
+    from fastemriwaveforms_b200.summation import spline_factor_table
+
+    fac = spline_factor_table(t, cuda)
+    fact = torch.empty_like(generic)
+    _lib.call("few_spline_build_factored", fac.data_ptr(), yd.data_ptr(), 1, N, ni, 0, ni, N, fact.data_ptr(),
+              _lib.FEW_LAYOUT_KNOT_MAJOR, st)
+    assert coeff_err(fact.cpu().numpy(), generic.cpu().numpy()) < 1e-11
 
 
 def test_reference_shaped_interpolate_arrays(cuda, oracle):
