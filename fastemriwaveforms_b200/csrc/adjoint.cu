@@ -33,7 +33,6 @@ namespace few {
 namespace {
 
 constexpr int kAdjThreads = 256;
-constexpr int kRowBlock = 8;
 constexpr int kSmemBudget = 200 * 1024;
 
 struct AdjPhaseArgs {
@@ -50,38 +49,56 @@ struct AdjPhaseArgs {
 };
 
 // dL/dPhi at every sample of the unit, projected on the phase basis.
+//
+// Shared memory holds the folded coefficients of this pass's rows in blocks of
+// RB rows (rows past R zero-filled), each block laid out (n', row, c): the
+// 4 RB double2 values one column n' needs are contiguous, so every load of the
+// key loop is at an immediate offset from one pointer.  The per-row factors
+// (u_r, m'_r, k'_r) are formed once per block.  s_e (after the blocks) holds
+// dL/dPhi_f per sample of the unit for the fields in use (phi, r, and theta).
 template <int RB, bool THETA>
 __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
 {
+    constexpr int NF = THETA ? 3 : 2;  // fields: 0 phi, 1 r, 2 theta
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *sW = reinterpret_cast<double2 *>(smem_raw);
-    __shared__ int s_rm[kMaxRows], s_rk[kMaxRows];
+    __shared__ int s_rm[kMaxRows + 8], s_rk[kMaxRows + 8];
     __shared__ double s_pc[24];
-    __shared__ double s_e[3][1024];  // dL/dPhi_f at each sample of the unit (units hold <= 1024 samples)
 
     const int u = blockIdx.x;
     const int seg = a.units[3 * u], lo = a.units[3 * u + 1];
     const int hi = min(a.units[3 * u + 2], lo + 1024);  // units hold at most 1024 samples (checked on the host)
     const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
     const int R = a.R, NN = a.NN, nlo = a.nlo;
+    const int rpp = a.rows_per_pass;  // a multiple of RB
+    double2 *sW = reinterpret_cast<double2 *>(smem_raw);
+    double (*s_e)[1024] = reinterpret_cast<double (*)[1024]>(smem_raw + (size_t)rpp * NN * 4 * sizeof(double2));
     const long long nps = (long long)(a.N - 1) * 3;
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
-        s_rm[r] = a.row_m[r];
-        s_rk[r] = a.row_k[r];
+    const int Rp = (R + RB - 1) / RB * RB;
+    for (int r = threadIdx.x; r < Rp; r += blockDim.x) {
+        s_rm[r] = r < R ? a.row_m[r] : 0;  // padded rows: u = 1 against zero coefficients
+        s_rk[r] = r < R ? a.row_k[r] : 0;
     }
     if (threadIdx.x < 24) {
         const int q = threadIdx.x >> 3, c = threadIdx.x & 7;
         s_pc[threadIdx.x] = a.pc[c * nps + (long long)seg * 3 + q];
     }
-    for (int q = threadIdx.x; q < hi - lo; q += blockDim.x) s_e[0][q] = s_e[1][q] = s_e[2][q] = 0.0;
+    for (int q = threadIdx.x; q < hi - lo; q += blockDim.x)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s_e[f][q] = 0.0;
 
-    for (int r0 = 0; r0 < R; r0 += a.rows_per_pass) {
-        const int nrp = min(a.rows_per_pass, R - r0);
+    for (int r0 = 0; r0 < Rp; r0 += rpp) {
+        const int nrp = min(rpp, Rp - r0);  // a multiple of RB
         __syncthreads();
         {
+            // (row, n', c) in global order -> (block, n', row in block, c) in shared
             const double2 *src = a.W + ((long long)seg * R + r0) * NN * 4;
             const int count = nrp * NN * 4;
-            for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
+            for (int e = threadIdx.x; e < count; e += blockDim.x) {
+                const int rr = e / (NN * 4), rem = e - rr * (NN * 4);
+                const int n = rem >> 2, c = rem & 3;
+                const int blk = rr / RB, q = rr - blk * RB;
+                sW[(((long long)blk * NN + n) * RB + q) * 4 + c] = (r0 + rr < R) ? src[e] : make_double2(0.0, 0.0);
+            }
         }
         __syncthreads();
         for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
@@ -91,7 +108,6 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
             const double s1 = rsub(1.0, s);
             const double Pp = phase_poly(s_pc, s, s1);
             const double Pr = phase_poly(s_pc + 16, s, s1);
-            const double Pt = THETA ? phase_poly(s_pc + 8, s, s1) : 0.0;
             double sn, cs;
             sincos(Pp, &sn, &cs);
             const double2 Ep = make_double2(cs, -sn);
@@ -99,50 +115,45 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
             const double2 Er = make_double2(cs, -sn);
             double2 Et = make_double2(1.0, 0.0);
             if (THETA) {
-                sincos(Pt, &sn, &cs);
+                sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
                 Et = make_double2(cs, -sn);
             }
             const double2 V0 = cpow_int(Er, nlo);
             double2 Dp = make_double2(0.0, 0.0), Dr = Dp, Dt = Dp;
             for (int rb = 0; rb < nrp; rb += RB) {
                 double2 U[RB];
+                double mq[RB], kq[RB];
 #pragma unroll
                 for (int q = 0; q < RB; ++q) {
-                    U[q] = make_double2(0.0, 0.0);
-                    if (rb + q < nrp) {
-                        const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
-                        double2 uu = cpow_int(Ep, mm);
-                        if (THETA && kk) uu = cmul(uu, cpow_int(Et, kk));
-                        U[q] = uu;
-                    }
+                    const int mm = s_rm[r0 + rb + q], kk = s_rk[r0 + rb + q];
+                    double2 uu = cpow_int(Ep, mm);
+                    if (THETA && kk) uu = cmul(uu, cpow_int(Et, kk));
+                    U[q] = uu;
+                    mq[q] = (double)mm;
+                    kq[q] = (double)kk;
                 }
                 double2 v = V0;
-                const double2 *wrow = sW + (long long)rb * NN * 4;
-                for (int c = 0; c < NN; ++c) {
+                double dn = (double)nlo;
+                const double2 *wb = sW + (long long)rb * NN * 4;  // block (rb / RB): (n', row, c)
+                for (int n = 0; n < NN; ++n) {
+                    const double2 *wn = wb + n * (RB * 4);
                     double2 T = make_double2(0.0, 0.0), Tm = T, Tk = T;
-                    const double2 *wc = wrow + c * 4;
 #pragma unroll
                     for (int q = 0; q < RB; ++q) {
-                        if (rb + q < nrp) {
-                            const double2 *w = wc + (long long)q * NN * 4;
-                            const double2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
-                            double2 Wx;
-                            Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
-                            Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
-                            const double2 P = cmul(U[q], Wx);
-                            const double mq = (double)s_rm[r0 + rb + q];
-                            T.x += P.x;
-                            T.y += P.y;
-                            Tm.x = fma(mq, P.x, Tm.x);
-                            Tm.y = fma(mq, P.y, Tm.y);
-                            if (THETA) {
-                                const double kq = (double)s_rk[r0 + rb + q];
-                                Tk.x = fma(kq, P.x, Tk.x);
-                                Tk.y = fma(kq, P.y, Tk.y);
-                            }
+                        const double2 w0 = wn[4 * q], w1 = wn[4 * q + 1], w2 = wn[4 * q + 2], w3 = wn[4 * q + 3];
+                        double2 Wx;
+                        Wx.x = fma(fma(fma(w3.x, x, w2.x), x, w1.x), x, w0.x);
+                        Wx.y = fma(fma(fma(w3.y, x, w2.y), x, w1.y), x, w0.y);
+                        const double2 P = cmul(U[q], Wx);
+                        T.x += P.x;
+                        T.y += P.y;
+                        Tm.x = fma(mq[q], P.x, Tm.x);
+                        Tm.y = fma(mq[q], P.y, Tm.y);
+                        if (THETA) {
+                            Tk.x = fma(kq[q], P.x, Tk.x);
+                            Tk.y = fma(kq[q], P.y, Tk.y);
                         }
                     }
-                    const double dn = (double)(nlo + c);
                     const double2 vT = cmul(v, T);
                     const double2 vTm = cmul(v, Tm);
                     Dp.x += vTm.x;
@@ -155,36 +166,38 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_adj_phase(AdjPhaseArgs a)
                         Dt.y += vTk.y;
                     }
                     v = cmul(v, Er);
+                    dn += 1.0;
                 }
             }
             // dh/dPhi = -i D; dL/dPhi = Re(g (-i D)) = Im(g D) with g = conj(G)
             const double2 G = a.grad[i];
-            const double ep = G.x * Dp.y - G.y * Dp.x;
-            const double er = G.x * Dr.y - G.y * Dr.x;
-            const double et = G.x * Dt.y - G.y * Dt.x;
             // partial over this pass's rows; passes add in a fixed order
-            s_e[0][i - lo] += ep;
-            s_e[1][i - lo] += et;
-            s_e[2][i - lo] += er;
+            s_e[0][i - lo] += G.x * Dp.y - G.y * Dp.x;
+            s_e[1][i - lo] += G.x * Dr.y - G.y * Dr.x;
+            if (THETA) s_e[2][i - lo] += G.x * Dt.y - G.y * Dt.x;
         }
     }
     __syncthreads();
     // project on the basis b_q(s) = 1, s, s s1, s^2 s1, s^2 s1^2, s^3 s1^2, s^3 s1^3,
-    // s^4 s1^3: warp w produces outputs w, w+8, w+16 (24 = 3 fields x 8 terms)
+    // s^4 s1^3: warp w produces outputs w, w+8, w+16 (24 = 3 fields x 8 terms;
+    // output field order phi, theta, r)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int o = warp; o < 24; o += nwarp) {
         const int f = o >> 3, q = o & 7;
+        const int fe = f == 0 ? 0 : (f == 2 ? 1 : 2);  // s_e row of output field f
         double v = 0.0;
-        for (int j = lane; j < hi - lo; j += 32) {
-            const double t = rmul(a.dt, (double)(lo + j));
-            const double s = __ddiv_rn(rsub(t, pt0), pw);
-            const double s1 = rsub(1.0, s);
-            double b = 1.0;
-            // b_q: alternate factors s, s1 starting with s
-            for (int k = 0; k < q; ++k) b *= (k & 1) ? s1 : s;
-            v = fma(s_e[f][j], b, v);
+        if (fe < NF) {
+            for (int j = lane; j < hi - lo; j += 32) {
+                const double t = rmul(a.dt, (double)(lo + j));
+                const double s = __ddiv_rn(rsub(t, pt0), pw);
+                const double s1 = rsub(1.0, s);
+                double b = 1.0;
+                // b_q: alternate factors s, s1 starting with s
+                for (int k = 0; k < q; ++k) b *= (k & 1) ? s1 : s;
+                v = fma(s_e[fe][j], b, v);
+            }
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         }
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if (lane == 0) a.partial[(long long)u * 24 + o] = v;
     }
 }
@@ -780,21 +793,24 @@ int launch_adj_phase(const double2 *grad, const double2 *W, const double *pc, in
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
+    // rows in blocks of 7 or 8 (the one that pads R less; 8 on a tie), as many
+    // blocks per pass as fit beside the per-sample field array
     const long long row_bytes = (long long)NN * 4 * sizeof(double2);
-    const int rpp = (int)std::min<long long>(R, kSmemBudget / row_bytes);
-    if (rpp < 1) return fail(FEW_ERR_SIZE, "adjoint: NN=%d too large for one row in shared memory", NN);
-    a.rows_per_pass = rpp;
-    if (use_theta) {
-        FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          kSmemBudget));
-        k_adj_phase<kRowBlock, true><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
-    } else {
-        FEW_CUDA_TRY(cudaFuncSetAttribute(k_adj_phase<kRowBlock, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          kSmemBudget));
-        k_adj_phase<kRowBlock, false><<<nunits, kAdjThreads, (size_t)rpp * row_bytes, st>>>(a);
-    }
-    FEW_LAUNCH_CHECK("k_adj_phase");
-    return FEW_OK;
+    const int rb = ((R + 6) / 7 * 7 < (R + 7) / 8 * 8) ? 7 : 8;
+    const int Rp = (R + rb - 1) / rb * rb;
+    const long long e_bytes = (long long)(use_theta ? 3 : 2) * 1024 * sizeof(double);
+    const int blocks = (int)std::min<long long>(Rp / rb, (kSmemBudget - e_bytes) / (row_bytes * rb));
+    if (blocks < 1) return fail(FEW_ERR_SIZE, "adjoint: NN=%d too large for one row block in shared memory", NN);
+    a.rows_per_pass = blocks * rb;
+    const size_t smem = (size_t)(a.rows_per_pass * row_bytes + e_bytes);
+    auto go = [&](auto kern) -> int {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)kern, (int)smem));
+        kern<<<nunits, kAdjThreads, smem, st>>>(a);
+        FEW_LAUNCH_CHECK("k_adj_phase");
+        return FEW_OK;
+    };
+    if (rb == 7) return use_theta ? go(k_adj_phase<7, true>) : go(k_adj_phase<7, false>);
+    return use_theta ? go(k_adj_phase<8, true>) : go(k_adj_phase<8, false>);
 }
 
 int launch_adj_phase_reduce(const double *partial, const int *seg_units, int nseg, double *grad_pc, cudaStream_t st)
