@@ -2,10 +2,13 @@
 
 Tunable shape: the work-unit length (output samples per unit, which sets how
 often a CTA reloads a segment's folded coefficients and how evenly the units
-spread) and the number of persistent CTAs per SM.  Each candidate is timed with
-CUDA events on the caller's real batch (the sum kernel only; the rest of the
-forward does not depend on the choice) and the fastest is cached in a JSON file
-keyed by GPU name, precision and the batch's shape buckets.
+spread), the number of persistent CTAs per SM and, for the tensor-core sum, the
+depth of its B-operand pipeline (bulk-copy slots the MMA warp keeps in flight
+ahead of the MMAs; deeper rings hide more copy latency but take shared memory
+that a second CTA per SM needs).  Each candidate is timed with CUDA events on
+the caller's real batch (the sum kernel only; the rest of the forward does not
+depend on the choice) and the fastest is cached in a JSON file keyed by GPU
+name, precision and the batch's shape buckets.
 
 Cache location: $FEW_B200_TUNE_CACHE, else ~/.cache/fastemriwaveforms_b200/tune.json.
 """
@@ -20,6 +23,8 @@ import torch
 
 CHUNKS = (256, 512, 1024)
 CTAS_PER_SM = (1, 2, 3)
+MIXED_CTAS_PER_SM = (1, 2)   # 288-thread CTAs of ~100 KB shared memory: at most two resident per SM
+B_STAGES = (2, 3, 4)
 _lock = threading.Lock()
 
 
@@ -90,17 +95,22 @@ def time_ms(fn, reps: int = 3) -> float:
     return times[len(times) // 2]
 
 
-def tune(key: str, make_runner, candidates=None) -> dict:
-    """Time make_runner(chunk, ctas_per_sm)() for every candidate and cache the best."""
-    if candidates is None:
-        candidates = [(c, m) for c in CHUNKS for m in CTAS_PER_SM]
+def candidates_for(precision: str) -> list:
+    """The shapes tried for a precision: dicts of make_runner's keyword arguments."""
+    if precision == "mixed":
+        return [{"chunk": c, "ctas_per_sm": m, "bstages": b} for c in CHUNKS for m in MIXED_CTAS_PER_SM
+                for b in B_STAGES]
+    return [{"chunk": c, "ctas_per_sm": m} for c in CHUNKS for m in CTAS_PER_SM]
+
+
+def tune(key: str, make_runner, candidates) -> dict:
+    """Time make_runner(**shape)() for every candidate shape and cache the best."""
     results = []
-    for chunk, per_sm in candidates:
-        run = make_runner(chunk, per_sm)
-        results.append((time_ms(run), chunk, per_sm))
-    results.sort()
-    best_ms, chunk, per_sm = results[0]
-    choice = {"chunk": chunk, "ctas_per_sm": per_sm, "ms": best_ms,
-              "tried": [{"chunk": c, "ctas_per_sm": m, "ms": t} for t, c, m in results]}
+    for shape in candidates:
+        run = make_runner(**shape)
+        results.append((time_ms(run), shape))
+    results.sort(key=lambda r: r[0])
+    best_ms, best = results[0]
+    choice = dict(best, ms=best_ms, tried=[dict(sh, ms=t) for t, sh in results])
     record(key, choice)
     return choice

@@ -75,6 +75,7 @@ int launch_spline_adjoint_factored(const double *fac, double *gc, double *gy, lo
 constexpr int kFacWidth = 16;       // doubles per row of the shared spline factorization
 constexpr int kScanChunks = 8;      // knot chunks of the scan form of the spline sweeps (warps per CTA)
 constexpr int kMaxRows = 256;        // distinct (m', k') rows of a fold plan
+constexpr int kMaxBStages = 4;       // B-operand bulk-copy slots of the tensor-core sum
 constexpr int kDefaultChunk = 1024;  // output samples per work unit of the sum
 
 }  // namespace few

@@ -135,7 +135,7 @@ __host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, int &NNp
 constexpr int kSumProd = 8;                        // producer warps: two per TMEM lane quarter
 constexpr int kSumProdThreads = 32 * kSumProd;     // 256
 constexpr int kSumThreads = kSumProdThreads + 32;  // + the MMA warp
-constexpr int kMaxBSlots = 4;
+constexpr int kMaxBSlots = kMaxBStages;
 
 struct SumShared {
     uint64_t full[2], empty[2], bfull[kMaxBSlots], bempty[kMaxBSlots], accf, acce, done;
@@ -308,8 +308,11 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
         s.pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
     }
     sum_prod_sync();
-    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
-    const double hs = a.t_knots[seg + 1] - a.t_knots[seg];
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1];
+    // reciprocals once per unit: s and tau by multiplication (within an ulp of the
+    // quotients, far below this form's FP32 phasor error)
+    const double ipw = 1.0 / a.seg_info[3 * seg + 2];
+    const double ihs = 1.0 / (a.t_knots[seg + 1] - a.t_knots[seg]);
     const int ng = NB / 16, gs = (ng + 1) / 2;  // 16-column groups; half 0 takes [0, gs)
     const int g_lo = h ? gs : 0, g_hi = h ? ng : gs;
     unsigned char *const aH = smem_raw + h * kAStage, *const aL = aH + kMT * kKC * 2;
@@ -324,12 +327,15 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
         // unit (and n' past NN, whose B rows are zero) hold finite phasors whose
         // products are discarded or vanish, so nothing is masked.
         const double t = (double)i * a.dt;
-        const float tau = (float)((t - t0) / hs);
-        const double sp = (t - pt0) / pw;
+        const float tau = (float)((t - t0) * ihs);
+        const double sp = (t - pt0) * ipw;
         const double sp1 = 1.0 - sp;
         const double Pr = phase_poly(s.pc + 16, sp, sp1);
         const float2 Er = anchor(Pr);
         const float2 Er2 = fcmul(Er, Er);
+        // the epilogue's phasors, ahead of the chunk loop so that their latency is hidden
+        const float2 Ep = anchor(phase_poly(s.pc, sp, sp1));
+        const float2 Et = a.use_theta ? anchor(phase_poly(s.pc + 8, sp, sp1)) : make_float2(1.f, 0.f);
         for (int k = h; k < nch; k += 2) {
             const uint32_t n = h ? ro.n1 : ro.n0;
             bool dead = ro.dead || *(volatile int *)&s.fail;
@@ -372,11 +378,8 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
         }
         ro.dead = __any_sync(0xffffffffu, dead);
         tc_fence_after();
-        float2 Sp = make_float2(0.f, 0.f);
+        float2 Sp = make_float2(0.f, 0.f), Sq = Sp;  // even and odd rows: two accumulation chains
         if (!ro.dead && g_lo < g_hi) {
-            const double Pp = phase_poly(s.pc, sp, sp1);
-            const float2 Ep = anchor(Pp);
-            const float2 Et = a.use_theta ? anchor(phase_poly(s.pc + 8, sp, sp1)) : make_float2(1.f, 0.f);
             const uint32_t trow = s.tmem + ((uint32_t)(32 * (warp & 3)) << 16);
             float2 uu = make_float2(1.f, 0.f);
             int pm = 0x7fffffff, pk = 0x7fffffff;
@@ -402,11 +405,14 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
                         // Y = sum_c tau^c Z_c (Horner)
                         const float yr = fmaf(fmaf(fmaf(d8[6], tau, d8[4]), tau, d8[2]), tau, d8[0]);
                         const float yi = fmaf(fmaf(fmaf(d8[7], tau, d8[5]), tau, d8[3]), tau, d8[1]);
-                        Sp.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, Sp.x));
-                        Sp.y = fmaf(uu.x, yi, fmaf(uu.y, yr, Sp.y));
+                        float2 &S = (q & 1) ? Sq : Sp;
+                        S.x = fmaf(uu.x, yr, fmaf(-uu.y, yi, S.x));
+                        S.y = fmaf(uu.x, yi, fmaf(uu.y, yr, S.y));
                     }
                 }
             }
+            Sp.x += Sq.x;
+            Sp.y += Sq.y;
         }
         tc_fence_before();
         __syncwarp();
@@ -506,18 +512,15 @@ int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
 // B slots of the sum's ring for chunks of NB columns: as many (2..4) as keep two
 // CTAs per SM (<= 110 KB of dynamic shared memory with the two A stages), and
 // the dynamic shared memory that takes.
-SumRing mixed_ring(int NB)
+// nbs > 0 asks for that many slots instead.
+SumRing mixed_ring(int NB, int nbs = 0)
 {
     SumRing rg;
     rg.bslot = 2 * NB * kKC * 2;
-    rg.nbs = std::max(2, std::min(kMaxBSlots, (110 * 1024 - 2 * kAStage) / rg.bslot));
+    rg.nbs = nbs > 0 ? nbs : std::max(2, std::min(kMaxBSlots, (110 * 1024 - 2 * kAStage) / rg.bslot));
     return rg;
 }
-size_t mixed_smem_bytes(int NB)
-{
-    const SumRing rg = mixed_ring(NB);
-    return (size_t)2 * kAStage + (size_t)rg.nbs * rg.bslot;
-}
+size_t mixed_smem_bytes(const SumRing &rg) { return (size_t)2 * kAStage + (size_t)rg.nbs * rg.bslot; }
 
 size_t mixed_bpk_bytes(int nseg, int R, int NN)
 {
@@ -564,15 +567,16 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
-    const size_t smem = mixed_smem_bytes(a.NB);
+    const SumRing rg = mixed_ring(a.NB);
+    const size_t smem = mixed_smem_bytes(rg);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed, (int)smem));
-    k_sum_mixed<<<nunits, kSumThreads, smem, st>>>(a, mixed_ring(a.NB));
+    k_sum_mixed<<<nunits, kSumThreads, smem, st>>>(a, rg);
     FEW_LAUNCH_CHECK("k_sum_mixed");
     return FEW_OK;
 }
 
-int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int nunits, int max_R, int ctas, int *err,
-                             unsigned long long *done, cudaStream_t st)
+int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int nunits, int max_R, int ctas,
+                             int bstages, int *err, unsigned long long *done, cudaStream_t st)
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
@@ -585,9 +589,13 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
         ctas = 2 * sms;
     }
     ctas = std::min(ctas, nunits);
-    const size_t smem = mixed_smem_bytes(NB);
+    const SumRing rg = mixed_ring(NB, bstages);
+    const size_t smem = mixed_smem_bytes(rg);
+    if (smem > 227 * 1024)
+        return fail(FEW_ERR_SIZE, "few_sum_mixed_batched: %d B stages of %d bytes exceed shared memory", rg.nbs,
+                    rg.bslot);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
-    k_sum_mixed_batched<<<ctas, kSumThreads, smem, st>>>(descs, units4, nunits, mixed_ring(NB), cols, err, done);
+    k_sum_mixed_batched<<<ctas, kSumThreads, smem, st>>>(descs, units4, nunits, rg, cols, err, done);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");
     return FEW_OK;
 }
@@ -595,13 +603,16 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 }  // namespace few
 
 extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
-                                     int ctas, int *err, unsigned long long *done, void *stream)
+                                     int ctas, int bstages, int *err, unsigned long long *done, void *stream)
 {
     few::clear_error();
     if (!descs || !units4 || !err) return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: null pointer");
     if (nwave < 1 || nunits < 0 || max_R < 1 || max_R > 64)
         return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 64)");
-    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, err, done, (cudaStream_t)stream);
+    if (bstages != 0 && (bstages < 2 || bstages > few::kMaxBStages))
+        return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: bstages=%d not in 2..%d", bstages, few::kMaxBStages);
+    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, bstages, err, done,
+                                         (cudaStream_t)stream);
 }
 
 extern "C" int few_fold_mixed(const void *W, const double *t_knots, int nseg, int R, int NN, void *Bpk, void *stream)
