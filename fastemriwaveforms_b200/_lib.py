@@ -56,7 +56,7 @@ SIGNATURES = {
     "few_sum_mixed": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
                       _vp, _vp],
     "few_sum_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
-    "few_sum_mixed_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp],
+    "few_sum_mixed_batched": [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp],
     "few_stamp": [_vp, _vp],
     "few_adjoint_G_mixed": [_vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int,
                             _vp, _vp, _vp],

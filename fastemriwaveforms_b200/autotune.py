@@ -3,9 +3,11 @@
 Tunable shape: the work-unit length (output samples per unit, which sets how
 often a CTA reloads a segment's folded coefficients and how evenly the units
 spread), the number of persistent CTAs per SM and, for the tensor-core sum, the
-depth of its B-operand pipeline (bulk-copy slots the MMA warp keeps in flight
-ahead of the MMAs; deeper rings hide more copy latency but take shared memory
-that a second CTA per SM needs).  Each candidate is timed with CUDA events on
+shape of its operand pipeline: A stages per producer half (with two, a half
+writes its next chunk while the tensor cores read the previous one) and B
+bulk-copy slots the MMA warp keeps in flight ahead of the MMAs.  Deeper
+pipelines hide more latency but take shared memory that a second CTA per SM
+needs.  Each candidate is timed with CUDA events on
 the caller's real batch (the sum kernel only; the rest of the forward does not
 depend on the choice) and the fastest is cached in a JSON file keyed by GPU
 name, precision and the batch's shape buckets.
@@ -23,7 +25,9 @@ import torch
 
 CHUNKS = (256, 512, 1024)
 CTAS_PER_SM = (1, 2, 3)
+MIXED_CHUNKS = (512, 1024)
 MIXED_CTAS_PER_SM = (1, 2)   # 288-thread CTAs of ~100 KB shared memory: at most two resident per SM
+A_STAGES = (1, 2)
 B_STAGES = (2, 3, 4)
 _lock = threading.Lock()
 
@@ -98,8 +102,8 @@ def time_ms(fn, reps: int = 3) -> float:
 def candidates_for(precision: str) -> list:
     """The shapes tried for a precision: dicts of make_runner's keyword arguments."""
     if precision == "mixed":
-        return [{"chunk": c, "ctas_per_sm": m, "bstages": b} for c in CHUNKS for m in MIXED_CTAS_PER_SM
-                for b in B_STAGES]
+        return [{"chunk": c, "ctas_per_sm": m, "astages": a, "bstages": b} for c in MIXED_CHUNKS
+                for m in MIXED_CTAS_PER_SM for a in A_STAGES for b in B_STAGES]
     return [{"chunk": c, "ctas_per_sm": m} for c in CHUNKS for m in CTAS_PER_SM]
 
 

@@ -47,10 +47,11 @@ class BatchedInterpolatedModeSum:
     args:
         precision: "mixed" (tensor cores), "exact" or "faithful" (FP64).
         autotune: choose the unit length, CTAs per SM and (tensor cores) the
-            B-operand pipeline depth by timing (cached).
-        chunk, ctas_per_sm: fixed shape (overrides the autotuner); bstages: fixed
-            B-operand pipeline depth (2..4; default: the tuned one, or as many
-            slots as keep two CTAs per SM when chunk and ctas_per_sm are given).
+            operand pipeline shape by timing (cached).
+        chunk, ctas_per_sm: fixed shape (overrides the autotuner); astages,
+            bstages: fixed operand pipeline (A stages per producer half, 1 or 2;
+            B bulk-copy slots, 2..4; default: the tuned ones, or the library's
+            choice when chunk and ctas_per_sm are given).
         backward: "mixed" or "fp64" adjoint (default: "mixed" for precision="mixed").
         streams: side streams over which the per-waveform spline builds, folds
             and adjoints are spread (they are small launches; running several
@@ -59,7 +60,7 @@ class BatchedInterpolatedModeSum:
 
     def __init__(self, precision: str = "mixed", device=None, autotune: bool = True, chunk: int | None = None,
                  ctas_per_sm: int | None = None, backward: str | None = None, streams: int = 8,
-                 bstages: int | None = None):
+                 astages: int | None = None, bstages: int | None = None):
         if precision not in ("mixed", "exact", "faithful"):
             raise ValueError("precision must be 'mixed', 'exact' or 'faithful'")
         self.precision = precision
@@ -78,6 +79,9 @@ class BatchedInterpolatedModeSum:
         self.ctas_per_sm = ctas_per_sm
         if bstages is not None and not 2 <= bstages <= 4:
             raise ValueError("bstages must be 2, 3 or 4")
+        if astages is not None and astages not in (1, 2):
+            raise ValueError("astages must be 1 or 2")
+        self.astages = astages
         self.bstages = bstages
         self.graph = None
         self.tuning = None
@@ -139,19 +143,21 @@ class BatchedInterpolatedModeSum:
         self._key = autotune.key_of(dev, self.precision, self.max_R, max_NN, float(np.mean(seg_lens)),
                                     len(self.preps))
         self.sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        chunk, per_sm, bst = self.chunk, self.ctas_per_sm, self.bstages
+        chunk, per_sm, ast, bst = self.chunk, self.ctas_per_sm, self.astages, self.bstages
         if chunk is None or per_sm is None:
             cached = autotune.lookup(self._key) if self.autotune else None
             if cached is None and self.autotune:
                 self._prepare_operands()
                 cached = autotune.tune(self._key, self._runner, autotune.candidates_for(self.precision))
             if cached is None:
-                cached = {"chunk": 1024, "ctas_per_sm": 2, "bstages": 0}
+                cached = {"chunk": 1024, "ctas_per_sm": 2, "astages": 0, "bstages": 0}
             self.tuning = cached
             chunk = chunk or cached["chunk"]
             per_sm = per_sm or cached["ctas_per_sm"]
+            ast = ast or cached.get("astages", 0)
             bst = bst or cached.get("bstages", 0)
-        self.chunk, self.ctas_per_sm, self.bstages = int(chunk), int(per_sm), int(bst or 0)
+        self.chunk, self.ctas_per_sm = int(chunk), int(per_sm)
+        self.astages, self.bstages = int(ast or 0), int(bst or 0)
         self.units = self._units(self.chunk)
         return self
 
@@ -203,24 +209,26 @@ class BatchedInterpolatedModeSum:
                           st)
         self._join(main, side)
 
-    def _sum(self, units: torch.Tensor, ctas: int, done=None, bstages: int | None = None):
+    def _sum(self, units: torch.Tensor, ctas: int, done=None, astages: int | None = None,
+             bstages: int | None = None):
         st = _stream(self.device)
         nunits = units.numel() // 4
         if self.precision == "mixed":
+            ast = self.astages if astages is None else astages
             bst = self.bstages if bstages is None else bstages
             _lib.call("few_sum_mixed_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.max_R,
-                      ctas, int(bst or 0), _ptr(self.err), done, st)
+                      ctas, int(ast or 0), int(bst or 0), _ptr(self.err), done, st)
         else:
             mode = _lib.FEW_SUM_FAITHFUL if self.precision == "faithful" else _lib.FEW_SUM_EXACT
             _lib.call("few_sum_batched", _ptr(self.descs), len(self.preps), _ptr(units), nunits, self.smem_bytes, mode,
                       ctas, done, st)
 
-    def _runner(self, chunk: int, ctas_per_sm: int, bstages: int = 0):
+    def _runner(self, chunk: int, ctas_per_sm: int, astages: int = 0, bstages: int = 0):
         units = self._units(chunk)
 
         def run():
             self.out.zero_()
-            self._sum(units, ctas_per_sm * self.sms, bstages=bstages)
+            self._sum(units, ctas_per_sm * self.sms, astages=astages, bstages=bstages)
 
         return run
 

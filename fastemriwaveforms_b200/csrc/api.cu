@@ -48,7 +48,7 @@ cudaError_t ensure_smem_attr(const void *kernel, int bytes)
 
 extern "C" const char *few_last_error(void) { return few::g_last_error; }
 
-extern "C" int few_abi_version(void) { return 3; }
+extern "C" int few_abi_version(void) { return 4; }
 
 extern "C" int few_interpolate_arrays(const double *t_arr, double *interp_array, int ninterps, int length, double *B,
                                       double *upper_diag, double *diag, double *lower_diag, void *stream)

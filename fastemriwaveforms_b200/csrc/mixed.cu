@@ -120,14 +120,15 @@ __host__ __device__ __forceinline__ void mixed_dims_core(int R, int NN, int &NNp
 // ---------------------------------------------------------------------------
 // Producer warp w owns TMEM lane quarter w & 3 (samples 32 (w & 3) .. +31 of a
 // 128-sample tile) and half h = w >> 2: half h writes the A chunks k = h, h + 2,
-// ... of every tile into A stage h and reads accumulator column groups
-// [h G/2, ...) in the epilogue, so two threads share a sample and the two A
-// stages are filled at the same time.  The B chunks go through their own ring
-// of nbs (2..4) slots: lane 0 of the MMA warp brings each chunk in with one bulk
-// copy nbs - 1 chunks ahead of its MMAs, waits for the chunk's A stage, issues
-// the MMAs and commits them to the A stage's and the B slot's "empty" barriers,
-// and after a tile's last chunk to "accumulator full".  Barriers: full[b] (4
-// producer arrivals), empty[b] (MMA commit), bfull[s] (the bulk copy's bytes),
+// ... of every tile into its nas (1 or 2) A stages in turn (with two, it writes
+// the next chunk while the tensor cores still read the previous one) and reads
+// accumulator column groups [h G/2, ...) in the epilogue; two threads share a
+// sample.  The B chunks go through their own ring of nbs (2..4) slots: lane 0 of
+// the MMA warp brings each chunk in with one bulk copy nbs - 1 chunks ahead of
+// its MMAs, waits for the chunk's A stage, issues the MMAs and commits them to
+// the A stage's and the B slot's "empty" barriers, and after a tile's last chunk
+// to "accumulator full".  Barriers: full[b] (4 producer arrivals) and empty[b]
+// (MMA commit) per A stage, bfull[s] (the bulk copy's bytes),
 // bempty[s] (MMA commit), accf (MMA commit), acce (8 producer arrivals once the
 // accumulator has been read).  Every wait is bounded; a timeout sets the CTA's
 // fail word, after which no role waits again, every producer still reaches
@@ -136,25 +137,31 @@ constexpr int kSumProd = 8;                        // producer warps: two per TM
 constexpr int kSumProdThreads = 32 * kSumProd;     // 256
 constexpr int kSumThreads = kSumProdThreads + 32;  // + the MMA warp
 constexpr int kMaxBSlots = kMaxBStages;
+constexpr int kMaxAStages = 4;     // two per producer half
+constexpr int kMixedMaxRows = 64;  // (m', k') rows the accumulator holds
 
 struct SumShared {
-    uint64_t full[2], empty[2], bfull[kMaxBSlots], bempty[kMaxBSlots], accf, acce, done;
+    uint64_t full[kMaxAStages], empty[kMaxAStages], bfull[kMaxBSlots], bempty[kMaxBSlots], accf, acce, done;
     uint32_t tmem;
     int fail;
-    int rm[kMaxRows], rk[kMaxRows];
+    int rm[kMixedMaxRows], rk[kMixedMaxRows];
     double pc[24];
     float2 part[2][kMT];  // half 1's epilogue sums, by tile parity
 };
 
-// Ring layout of the dynamic shared memory: two A stages, then nbs B slots.
+// Ring layout of the dynamic shared memory: 2 nas A stages, then nbs B slots.
 struct SumRing {
+    int nas;       // A stages per producer half (1 or 2)
     int nbs;       // B slots
     int bslot;     // bytes per B slot (>= every unit's chunk)
 };
 
+// A stage of chunk k of a tile: half k & 1, its stages taken in turn.
+__device__ __forceinline__ int sum_stage(int k, int nas) { return nas == 2 ? 2 * (k & 1) + ((k >> 1) & 1) : (k & 1); }
+
 // Phases a role has consumed so far (registers; the same sequence in every role).
 struct SumRole {
-    uint32_t n0, n1;    // fills of A stage 0 and stage 1
+    uint32_t par, used; // A stage b: bit b = parity of its fills so far / filled at least once
     uint32_t tiles;     // accumulator uses
     uint32_t gi, gc;    // MMA warp: B chunks issued / consumed (all units)
     bool dead;
@@ -171,7 +178,7 @@ __device__ __forceinline__ void sum_setup(SumShared &s, int tmem_cols, SumRole &
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kMaxAStages; ++b) {
             mbar_init(&s.full[b], kSumProd / 2);
             mbar_init(&s.empty[b], 1);
         }
@@ -188,7 +195,7 @@ __device__ __forceinline__ void sum_setup(SumShared &s, int tmem_cols, SumRole &
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    ro.n0 = ro.n1 = ro.tiles = ro.gi = ro.gc = 0;
+    ro.par = ro.used = ro.tiles = ro.gi = ro.gc = 0;
     ro.dead = false;
 }
 
@@ -224,7 +231,8 @@ __device__ __forceinline__ bool sum_issue_b(const unsigned char *Bseg, int k, ui
     const uint32_t g = ro.gi, slot = g % rg.nbs, use = g / rg.nbs;
     if (use >= 1 && !mbar_wait_bounded(&s.bempty[slot], (use - 1) & 1u)) return false;
     mbar_arrive_expect_tx(&s.bfull[slot], bchunk);
-    bulk_copy_g2s(smem_raw + 2 * kAStage + slot * rg.bslot, Bseg + (size_t)k * bchunk, bchunk, &s.bfull[slot]);
+    bulk_copy_g2s(smem_raw + 2 * rg.nas * kAStage + slot * rg.bslot, Bseg + (size_t)k * bchunk, bchunk,
+                  &s.bfull[slot]);
     ro.gi = g + 1;
     return true;
 }
@@ -241,8 +249,8 @@ __device__ void sum_mma_unit(const MixedArgs &a, int seg, int lo, int hi, unsign
     bool ok = !*(volatile int *)&s.fail;
     for (int f = 0; f < min(ahead, nfill) && ok; ++f) ok = sum_issue_b(Bseg, f % nch, bchunk, smem_raw, rg, s, ro);
     for (int f = 0; f < nfill && ok; ++f) {
-        const int k = f % nch, b = k & 1;
-        const uint32_t n = b ? ro.n1 : ro.n0;
+        const int k = f % nch, b = sum_stage(k, rg.nas);
+        const uint32_t pb = (ro.par >> b) & 1u;
         ok = !*(volatile int *)&s.fail;
         // the accumulator is free once every producer has read the previous tile
         if (ok && k == 0 && ro.tiles >= 1) ok = mbar_wait_bounded(&s.acce, (ro.tiles - 1) & 1u);
@@ -250,13 +258,12 @@ __device__ void sum_mma_unit(const MixedArgs &a, int seg, int lo, int hi, unsign
         if (ok) ok = mbar_wait_bounded(&s.bfull[slot], (g / rg.nbs) & 1u);
         if (!ok) break;
         ro.gc = g + 1;
-        ok = mbar_wait_bounded(&s.full[b], n & 1u);
+        ok = mbar_wait_bounded(&s.full[b], pb);
         if (!ok) break;
-        if (b) ro.n1 = n + 1;
-        else ro.n0 = n + 1;
+        ro.par ^= 1u << b;
         tc_fence_after();
         const uint32_t a_h = smem_u32(smem_raw + b * kAStage), a_l = a_h + kMT * kKC * 2;
-        const uint32_t b_h = smem_u32(smem_raw + 2 * kAStage + slot * rg.bslot), b_l = b_h + NB * kKC * 2;
+        const uint32_t b_h = smem_u32(smem_raw + 2 * rg.nas * kAStage + slot * rg.bslot), b_l = b_h + NB * kKC * 2;
 #pragma unroll
         for (int st = 0; st < kKC / 16; ++st) {
             const uint64_t da_h = smem_desc(a_h + st * (kMT / 8) * 256, 128, 256);
@@ -291,8 +298,8 @@ __device__ void sum_mma_unit(const MixedArgs &a, int seg, int lo, int hi, unsign
 // Producer warps: one unit's A chunks and epilogues.  Every producer runs every
 // tile of the unit and reaches every named barrier and arrival; after a failed
 // wait it only skips the work.
-__device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, SumShared &s,
-                              SumRole &ro)
+__device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsigned char *smem_raw, const SumRing &rg,
+                              SumShared &s, SumRole &ro)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int h = warp >> 2, row = 32 * (warp & 3) + lane;  // half; sample row = TMEM lane
@@ -315,7 +322,6 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
     const double ihs = 1.0 / (a.t_knots[seg + 1] - a.t_knots[seg]);
     const int ng = NB / 16, gs = (ng + 1) / 2;  // 16-column groups; half 0 takes [0, gs)
     const int g_lo = h ? gs : 0, g_hi = h ? ng : gs;
-    unsigned char *const aH = smem_raw + h * kAStage, *const aL = aH + kMT * kKC * 2;
 
     for (int base = lo; base < hi; base += kMT) {
         const int i = base + row;
@@ -337,13 +343,16 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
         const float2 Ep = anchor(phase_poly(s.pc, sp, sp1));
         const float2 Et = a.use_theta ? anchor(phase_poly(s.pc + 8, sp, sp1)) : make_float2(1.f, 0.f);
         for (int k = h; k < nch; k += 2) {
-            const uint32_t n = h ? ro.n1 : ro.n0;
+            const int b = sum_stage(k, rg.nas);
+            const uint32_t pb = (ro.par >> b) & 1u;
             bool dead = ro.dead || *(volatile int *)&s.fail;
-            if (!dead && n >= 1 && !mbar_wait_bounded(&s.empty[h], (n - 1) & 1u)) {
+            // the stage is free once the MMAs of its previous fill are done
+            if (!dead && ((ro.used >> b) & 1u) && !mbar_wait_bounded(&s.empty[b], pb ^ 1u)) {
                 atomicExch(&s.fail, 1);
                 dead = true;
             }
             ro.dead = __any_sync(0xffffffffu, dead);
+            unsigned char *const aH = smem_raw + b * kAStage, *const aL = aH + kMT * kKC * 2;
             if (!ro.dead) {
                 // two interleaved chains (even and odd n') stepping by Er^2: half the
                 // dependent depth of one chain, and 8 FP32 steps from the anchor at most
@@ -364,9 +373,9 @@ __device__ void sum_prod_unit(const MixedArgs &a, int seg, int lo, int hi, unsig
             }
             fence_async_smem();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&s.full[h]);
-            if (h) ro.n1 = n + 1;
-            else ro.n0 = n + 1;
+            if (lane == 0) mbar_arrive(&s.full[b]);
+            ro.par ^= 1u << b;
+            ro.used |= 1u << b;
         }
         // accumulator of this tile: this thread's row (TMEM lane), half h's column
         // groups; two (m', k') rows of 8 columns per 16-column load, two loads in
@@ -441,7 +450,7 @@ __global__ void __launch_bounds__(kSumThreads, 2) k_sum_mixed(MixedArgs a, SumRi
         if ((threadIdx.x & 31) == 0) sum_mma_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
         __syncwarp();
     } else {
-        sum_prod_unit(a, seg, lo, hi, smem_raw, s, ro);
+        sum_prod_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
     }
     sum_teardown(s, ro, rg, a.tmem_cols, a.err);
 }
@@ -485,7 +494,7 @@ __global__ void __launch_bounds__(kSumThreads, 2) k_sum_mixed_batched(const few_
         if (mma) {
             if ((threadIdx.x & 31) == 0 && !ro.dead) sum_mma_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
         } else {
-            sum_prod_unit(a, seg, lo, hi, smem_raw, s, ro);
+            sum_prod_unit(a, seg, lo, hi, smem_raw, rg, s, ro);
             if (done) {
                 sum_prod_sync();  // every output row of the unit written
                 if (threadIdx.x == 0 && !ro.dead) atomicMax(done + units4[4 * u], global_ns());  // unit complete
@@ -509,18 +518,22 @@ int mixed_dims(int R, int NN, int *NNp, int *NB, int *nchunks, int *tmem_cols)
     return FEW_OK;
 }
 
-// B slots of the sum's ring for chunks of NB columns: as many (2..4) as keep two
-// CTAs per SM (<= 110 KB of dynamic shared memory with the two A stages), and
-// the dynamic shared memory that takes.
-// nbs > 0 asks for that many slots instead.
-SumRing mixed_ring(int NB, int nbs = 0)
+// Ring shape of the sum for chunks of NB columns.  By default one A stage per
+// producer half and as many B slots (2..4) as keep two CTAs per SM (<=
+// kTwoCtaBytes of dynamic shared memory): at the one-year 3843-mode workload this
+// measured 0.75 ms against 0.77 ms for two A stages per half with two B slots,
+// and the autotuner's search over both agrees.  nas, nbs > 0 ask for a shape.
+constexpr int kTwoCtaBytes = 112 * 1024;
+size_t mixed_smem_bytes(const SumRing &rg) { return (size_t)2 * rg.nas * kAStage + (size_t)rg.nbs * rg.bslot; }
+SumRing mixed_ring(int NB, int nbs = 0, int nas = 0)
 {
     SumRing rg;
     rg.bslot = 2 * NB * kKC * 2;
-    rg.nbs = nbs > 0 ? nbs : std::max(2, std::min(kMaxBSlots, (110 * 1024 - 2 * kAStage) / rg.bslot));
+    rg.nas = nas > 0 ? nas : 1;
+    rg.nbs = nbs > 0 ? nbs
+                     : std::max(2, std::min(kMaxBSlots, (kTwoCtaBytes - 2 * rg.nas * kAStage) / rg.bslot));
     return rg;
 }
-size_t mixed_smem_bytes(const SumRing &rg) { return (size_t)2 * kAStage + (size_t)rg.nbs * rg.bslot; }
 
 size_t mixed_bpk_bytes(int nseg, int R, int NN)
 {
@@ -576,7 +589,7 @@ int launch_sum_mixed(double2 *wf, const void *Bpk, const double *pc, int N, cons
 }
 
 int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int nunits, int max_R, int ctas,
-                             int bstages, int *err, unsigned long long *done, cudaStream_t st)
+                             int astages, int bstages, int *err, unsigned long long *done, cudaStream_t st)
 {
     if (nunits == 0) return FEW_OK;
     int NNp, NB, nch, cols;
@@ -589,11 +602,11 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
         ctas = 2 * sms;
     }
     ctas = std::min(ctas, nunits);
-    const SumRing rg = mixed_ring(NB, bstages);
+    const SumRing rg = mixed_ring(NB, bstages, astages);
     const size_t smem = mixed_smem_bytes(rg);
-    if (smem > 227 * 1024)
-        return fail(FEW_ERR_SIZE, "few_sum_mixed_batched: %d B stages of %d bytes exceed shared memory", rg.nbs,
-                    rg.bslot);
+    if (smem > 220 * 1024)
+        return fail(FEW_ERR_SIZE, "few_sum_mixed_batched: %d A stages per half and %d B stages of %d bytes exceed "
+                    "shared memory", rg.nas, rg.nbs, rg.bslot);
     FEW_CUDA_TRY(ensure_smem_attr((const void *)k_sum_mixed_batched, (int)smem));
     k_sum_mixed_batched<<<ctas, kSumThreads, smem, st>>>(descs, units4, nunits, rg, cols, err, done);
     FEW_LAUNCH_CHECK("k_sum_mixed_batched");
@@ -603,7 +616,8 @@ int launch_sum_mixed_batched(const few_wave_desc *descs, const int *units4, int 
 }  // namespace few
 
 extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
-                                     int ctas, int bstages, int *err, unsigned long long *done, void *stream)
+                                     int ctas, int astages, int bstages, int *err, unsigned long long *done,
+                                     void *stream)
 {
     few::clear_error();
     if (!descs || !units4 || !err) return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: null pointer");
@@ -611,7 +625,9 @@ extern "C" int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, cons
         return few::fail(FEW_ERR_SIZE, "few_sum_mixed_batched: bad sizes (max_R <= 64)");
     if (bstages != 0 && (bstages < 2 || bstages > few::kMaxBStages))
         return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: bstages=%d not in 2..%d", bstages, few::kMaxBStages);
-    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, bstages, err, done,
+    if (astages != 0 && astages != 1 && astages != 2)
+        return few::fail(FEW_ERR_ARG, "few_sum_mixed_batched: astages=%d not 1 or 2", astages);
+    return few::launch_sum_mixed_batched(descs, units4, nunits, max_R, ctas, astages, bstages, err, done,
                                          (cudaStream_t)stream);
 }
 

@@ -282,11 +282,13 @@ FEW_API int few_sum_mixed(void *wf, const void *Bpk, const double *phase_coeffs,
  * (nwave,) with Bpk set (few_fold_mixed per waveform); units4 [device]
  * (4*nunits,) = {waveform, segment, first sample, end sample}; max_R: the
  * largest R in the batch (<= 64, sizes shared memory and TMEM); ctas:
- * persistent CTAs (0: two per SM); bstages: depth of the B-operand ring, 2..4
- * bulk-copy slots (0: as many as keep two CTAs per SM); err [device] int as in
- * few_sum_mixed; done as in few_sum_batched. */
+ * persistent CTAs (0: two per SM); astages: A-operand stages per producer half
+ * (1 or 2; 0: 1); bstages: depth of the B-operand ring, 2..4 bulk-copy slots
+ * (0: as many as keep two CTAs per SM); err [device] int as in few_sum_mixed;
+ * done as in few_sum_batched.  Results do not depend on the stage counts. */
 FEW_API int few_sum_mixed_batched(const few_wave_desc *descs, int nwave, const int *units4, int nunits, int max_R,
-                                  int ctas, int bstages, int *err, unsigned long long *done, void *stream);
+                                  int ctas, int astages, int bstages, int *err, unsigned long long *done,
+                                  void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Adjoint (no counterpart in the reference: it has no gradients)           */

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_text():
     lib = _lib.load()
-    assert lib.few_abi_version() == 3
+    assert lib.few_abi_version() == 4
     rc = lib.few_spline_build(None, 0, None, 1, 1, 1, 0, 1, 10, None, 0, None)
     assert rc == _lib.FEW_ERR_ARG
     assert "null" in _lib.last_error()

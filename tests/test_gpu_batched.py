@@ -49,25 +49,27 @@ def test_batched_equals_single(cuda, tmp_path, monkeypatch, precision):
         assert np.array_equal(got, ref)
     cache = json.loads((tmp_path / "tune.json").read_text())
     assert b._key in cache and cache[b._key]["chunk"] in (256, 512, 1024)
-    if precision == "mixed":  # the tensor-core shape search includes the B pipeline depth
-        assert cache[b._key]["bstages"] in (2, 3, 4)
-        assert {t["bstages"] for t in cache[b._key]["tried"]} == {2, 3, 4}
+    if precision == "mixed":  # the tensor-core shape search includes the operand pipeline
+        assert cache[b._key]["astages"] in (1, 2) and cache[b._key]["bstages"] in (2, 3, 4)
+        tried = cache[b._key]["tried"]
+        assert {(t["astages"], t["bstages"]) for t in tried} == {(a, c) for a in (1, 2) for c in (2, 3, 4)}
 
 
-def test_mixed_pipeline_depth_does_not_change_results(cuda, tmp_path, monkeypatch):
-    """Every B-operand ring depth and CTA count gives bitwise the same waveforms."""
+def test_mixed_pipeline_shape_does_not_change_results(cuda, tmp_path, monkeypatch):
+    """Every operand pipeline shape and CTA count gives bitwise the same waveforms."""
     monkeypatch.setenv("FEW_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     batch = uneven_batch(count=5, seed=9)
     ref = None
-    for bst, per_sm in ((2, 2), (3, 2), (4, 1), (4, 2)):
-        b = BatchedInterpolatedModeSum(precision="mixed", chunk=512, ctas_per_sm=per_sm, bstages=bst).setup(batch)
+    for ast, bst, per_sm in ((1, 2, 2), (1, 3, 2), (1, 4, 1), (2, 2, 2), (2, 3, 2), (2, 4, 1)):
+        b = BatchedInterpolatedModeSum(precision="mixed", chunk=512, ctas_per_sm=per_sm, astages=ast,
+                                       bstages=bst).setup(batch)
         outs = [o.cpu().numpy() for o in b.forward()]
         torch.cuda.synchronize()
         assert not b.mixed_error()
         if ref is None:
             ref = outs
         for a, c in zip(ref, outs):
-            assert np.array_equal(a, c), (bst, per_sm)
+            assert np.array_equal(a, c), (ast, bst, per_sm)
 
 
 def test_graph_capture_replay_and_update(cuda, tmp_path, monkeypatch):
