@@ -407,12 +407,51 @@ def time_fwd_bwd(precision, inp, dev, steps, warmup, backward=None):
     return a.elapsed_time(b) / steps, teuk.grad.detach().clone(), pc.grad.detach().clone()
 
 
-def bench_batched(count: int, dev, steps: int):
+def time_forward(precision, inp, dev, steps, warmup):
+    """Forward only, inputs on the device: device time per call (ms)."""
+    import torch
+
+    from fastemriwaveforms_b200 import InterpolatedModeSum
+
+    ims = InterpolatedModeSum(precision=precision)
+    args = [inp.t, torch.from_numpy(inp.teuk_modes).to(dev), torch.from_numpy(inp.ylms).to(dev), inp.phase_t,
+            torch.from_numpy(inp.phase_coeffs).to(dev), inp.l, inp.m, inp.k, inp.n]
+    for _ in range(warmup):
+        ims(*args, T=inp.T, dt=inp.dt)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        ims(*args, T=inp.T, dt=inp.dt)
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def cpu_batch_subset(cases, samples: int):
+    """The reference's CPU path (one core) on the first waveforms of the batch,
+    each on its first `samples` output samples with its whole spline build
+    charged pro rata (as cpu_baseline): aggregate mode-samples/s."""
+    ms, sec = 0.0, 0.0
+    for c in cases:
+        n = min(samples, c.out_len)
+        r = cpu_baseline(c, n)
+        ms += c.num_modes * n
+        sec += c.num_modes * n / r["value"]
+    return {"value": ms / sec, "unit": METRIC, "cores": 1, "kind": r["kind"],
+            "sample": f"{len(cases)} waveforms of the batch (K {min(c.num_modes for c in cases)}-"
+                      f"{max(c.num_modes for c in cases)}), the first {samples} samples of each, "
+                      f"their spline builds charged pro rata ({sec:.2f} s)"}
+
+
+def bench_batched(count: int, dev, steps: int, cpu: bool = False):
     """Uneven batch (T ~ logU[1e5, 3.15e6] samples, N ~ U[50, 2000], K ~ U[200, 3843]):
     looping InterpolatedModeSum (plain FP64, one call per waveform; forward, and
     forward + backward through autograd) vs the persistent batched launch in a
     CUDA graph (mixed form with the tensor-core adjoint), upstream gradient
-    conj(h) per waveform."""
+    conj(h) per waveform; with cpu, the reference's CPU path on an 8-waveform
+    subset (cpu_batch_subset)."""
     import torch
 
     from fastemriwaveforms_b200 import InterpolatedModeSum
@@ -421,6 +460,7 @@ def bench_batched(count: int, dev, steps: int):
 
     cases = S.batch_cases(count=count, seed=5)
     ms_total = sum(c.num_modes * c.out_len for c in cases)
+    cpu_subset = cpu_batch_subset(cases[:8], 20000) if cpu else None
     loop = InterpolatedModeSum(precision="faithful")
     loop_fb = InterpolatedModeSum(precision="exact", backward="fp64")
     dev_args = []
@@ -460,6 +500,8 @@ def bench_batched(count: int, dev, steps: int):
                 "p99_ms": pw[min(len(pw) - 1, int(0.99 * len(pw)))]}
 
     out = {"waveforms": count, "mode_samples": ms_total, "loop_plain_fp64": timed(fwd)}
+    if cpu_subset:
+        out["cpu_subset"] = cpu_subset
     for a_ in dev_args:
         a_[1].requires_grad_(True)
         a_[4].requires_grad_(True)
@@ -757,7 +799,11 @@ def summary(faithful_ms, forms, fb, fb_adj, batched):
            "fwd_bwd": {k: {"ms": v["ms_per_step"], **({"grad_rel_l2_vs_exact": v["grad_rel_l2_vs_exact"]}
                                                        if "grad_rel_l2_vs_exact" in v else {})}
                        for k, v in fb.items()},
-           "fwd_bwd_adjoint_case": {k: (v["ms_per_step"] if isinstance(v, dict) else v) for k, v in fb_adj.items()}}
+           "fwd_bwd_adjoint_case": {k: v["ms_per_step"] for k, v in fb_adj.items()
+                                    if isinstance(v, dict) and "ms_per_step" in v},
+           "fwd_adjoint_case": dict(fb_adj["forward_ms"],
+                                    **({"cpu_1core_ms": fb_adj["cpu_forward_ms_whole"]}
+                                       if "cpu_forward_ms_whole" in fb_adj else {}))}
     if batched:
         loop, bm = batched["loop_plain_fp64"], batched["batched_mixed_graph"]
         loop_fb = batched["loop_plain_fp64_fwd_bwd"]
@@ -770,6 +816,8 @@ def summary(faithful_ms, forms, fb, fb_adj, batched):
         for k in ("fwd_p50_ms", "fwd_p99_ms", "fwd_bwd_p50_ms", "fwd_bwd_p99_ms"):
             if k in bm:
                 out["batched"]["graph_mixed"][k] = bm[k]
+        if "cpu_subset" in batched:
+            out["batched"]["cpu_1core_subset_value"] = batched["cpu_subset"]["value"]
     return _sig(out)
 
 
@@ -1092,8 +1140,14 @@ def main():
     for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
                             ("mixed_fp64_adjoint", "mixed", "fp64")):
         fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 3, backward=bwd)[0]}
+    fb_adj["forward_ms"] = {p: time_forward(p, adj, dev, max(3, args.steps), 3) for p in ("faithful", "exact", "mixed")}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c = cpu_baseline(adj, 60000)
+        fb_adj["cpu_forward"] = c
+        fb_adj["cpu_forward_ms_whole"] = adj.num_modes * adj.out_len / c["value"] * 1e3  # rate x whole waveform
 
-    batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2))
+    batched = None if args.no_batch else bench_batched(args.batch_count, dev, max(2, args.steps // 2),
+                                                       cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     amplitude = bench_amplitude(dev, args.steps, pk, pk_kind, cpu=(rank == 0 and not args.no_cpu_baseline))
     fdsum = None if args.no_fd else bench_fd(dev, args.steps, fp64_tflops,
                                              cpu=(rank == 0 and not args.no_cpu_baseline))
@@ -1120,7 +1174,7 @@ def main():
                    "peak": pk["hbm_gbs"], "unit": "GB/s",
                    "frac": spline_bytes / (stage["spline"] * 1e-3) / 1e9 / pk["hbm_gbs"],
                    "peak_source": f"{pk_kind} hbm_gbs", "algorithmic": "40 B per (knot, series)",
-                   "traffic": ({"bytes_per_launch": 466.7e6,
+                   "traffic": ({"bytes_per_launch": 423.9e6,
                                 "source": "ncu capture of k_spline_build_factored (one-year workload)"}
                                if args.workload == "plain_full" else None),
                    "launch_ms": stage["spline"]}
