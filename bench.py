@@ -407,7 +407,7 @@ def time_fwd_bwd(precision, inp, dev, steps, warmup, backward=None):
     return a.elapsed_time(b) / steps, teuk.grad.detach().clone(), pc.grad.detach().clone()
 
 
-def time_forward(precision, inp, dev, steps, warmup):
+def time_forward_form(precision, inp, dev, steps, warmup):
     """Forward only, inputs on the device: device time per call (ms)."""
     import torch
 
@@ -1140,7 +1140,8 @@ def main():
     for name, prec, bwd in (("exact", "exact", "fp64"), ("mixed", "mixed", "mixed"),
                             ("mixed_fp64_adjoint", "mixed", "fp64")):
         fb_adj[name] = {"ms_per_step": time_fwd_bwd(prec, adj, dev, max(2, args.steps // 2), 3, backward=bwd)[0]}
-    fb_adj["forward_ms"] = {p: time_forward(p, adj, dev, max(3, args.steps), 3) for p in ("faithful", "exact", "mixed")}
+    fb_adj["forward_ms"] = {p: time_forward_form(p, adj, dev, max(3, args.steps), 3)
+                            for p in ("faithful", "exact", "mixed")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         c = cpu_baseline(adj, 60000)
         fb_adj["cpu_forward"] = c
