@@ -107,49 +107,85 @@ __host__ __device__ inline PhaseDims phase_dims(int R, int NN)
     return d;
 }
 
-// B operand: one warp per (segment, column): the column's values over K, their
-// largest magnitude (the column's scale), then the digit chunks.
-__global__ void __launch_bounds__(256) k_fold_phase_s8(const double2 *__restrict__ W,
-                                                       const double *__restrict__ t_knots, int nseg, int R, int NN,
-                                                       int nlo, unsigned char *__restrict__ Bpk)
+// B operand: one CTA of 4 NNp threads per (segment, row).  A row's 16 columns
+// are (yz, c, re/im) combinations of the same 4 NN complex coefficients, so the
+// CTA stages the row's w = W[c][n'] h_s^c (and n' w) in shared memory, takes
+// the column scales from the largest |Re w|, |Im w| per (yz, c) (both re/im
+// columns of a pair see the same magnitudes), and then each thread writes the
+// four digit chunks of one (column, K step, K half).
+constexpr int kFoldThreads = 4 * kMaxPhaseNN;  // the largest CTA
+
+__global__ void __launch_bounds__(kFoldThreads) k_fold_phase_s8(const double2 *__restrict__ W,
+                                                                const double *__restrict__ t_knots, int nseg, int R,
+                                                                int NN, int nlo, unsigned char *__restrict__ Bpk)
 {
+    __shared__ double2 s_w[2][kMaxPhaseNN][4];  // [yz][n'][c]
+    __shared__ double s_m[kFoldThreads / 32][8];
+    __shared__ double s_scale[8];               // per (yz, c)
     const PhaseDims pd = phase_dims(R, NN);
-    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= (long long)nseg * pd.NBc) return;
-    const int s = (int)(w / pd.NBc), j = (int)(w % pd.NBc);
-    const int r = j / kColsRow, q16 = j % kColsRow;
-    const int ri = q16 & 1, c = (q16 >> 1) & 3, yz = q16 >> 3;
+    const int s = blockIdx.x, r = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double h = t_knots[s + 1] - t_knots[s];
-    const double hc = c == 0 ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
-    const int nchunks = 2 * pd.nks;  // 16 K values each
-    auto value = [&](int ks, int kk) -> double {
-        const int n = 16 * ks + (kk >> 1), part = kk & 1;
-        if (n >= NN) return 0.0;
-        const double2 wv = W[(((long long)s * R + r) * NN + n) * 4 + c];
-        const double f = yz ? hc * (double)(nlo + n) : hc;
-        const double wr = wv.x * f, wi = wv.y * f;
-        return part == 0 ? (ri ? wi : wr) : (ri ? wr : -wi);
-    };
-    double m = 0.0;
-    for (int q = lane; q < nchunks; q += 32)
-        for (int e = 0; e < 16; ++e) m = fmax(m, fabs(value(q >> 1, 16 * (q & 1) + e)));
-    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
-    const double scale = m > 0.0 ? kScale / (m * (1.0 + 1e-12)) : 1.0;
     unsigned char *const block = Bpk + (long long)s * pd.seg_bytes;
-    if (lane == 0) reinterpret_cast<double *>(block)[j] = scale;
-    for (int q = lane; q < nchunks; q += 32) {
-        const int ks = q >> 1, half = q & 1;
-        double x[16];
+    const int nchunk = kColsRow * pd.nks * 2;  // (column, K step, K half) chunks of a row
+    {
+        // stage: thread (n', c) of n' < NNp (zero past NN); local maxima per (yz, c)
+        double m0 = 0.0, m1 = 0.0;
+        const int c = tid & 3, n = tid >> 2;
+        if (n < pd.NNp) {
+            const double hc = c == 0 ? 1.0 : (c == 1 ? h : (c == 2 ? h * h : h * h * h));
+            double2 w0 = make_double2(0.0, 0.0), w1 = w0;
+            if (n < NN) {
+                const double2 wv = W[(((long long)s * R + r) * NN + n) * 4 + c];
+                const double f1 = hc * (double)(nlo + n);
+                w0 = make_double2(wv.x * hc, wv.y * hc);
+                w1 = make_double2(wv.x * f1, wv.y * f1);
+            }
+            s_w[0][n][c] = w0;
+            s_w[1][n][c] = w1;
+            m0 = fmax(fabs(w0.x), fabs(w0.y));
+            m1 = fmax(fabs(w1.x), fabs(w1.y));
+        }
+        // maxima over n' for each c: lanes with the same c are 4 apart
+        for (int off = 4; off < 32; off <<= 1) {
+            m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, off));
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, off));
+        }
+        if (lane < 4) {
+            s_m[warp][lane] = m0;       // yz = 0, c = lane
+            s_m[warp][4 + lane] = m1;   // yz = 1
+        }
+        __syncthreads();
+        if (tid < 8) {
+            double m = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_m[w][tid]);
+            s_scale[tid] = m > 0.0 ? kScale / (m * (1.0 + 1e-12)) : 1.0;
+        }
+        __syncthreads();
+        if (tid < kColsRow) {
+            const int yz = tid >> 3, cc = (tid >> 1) & 3;
+            reinterpret_cast<double *>(block)[r * kColsRow + tid] = s_scale[4 * yz + cc];
+        }
+        for (int q = tid; q < nchunk; q += blockDim.x) {
+            const int q16 = q % kColsRow, rest = q / kColsRow;
+            const int ks = rest >> 1, half = rest & 1;
+            const int ri = q16 & 1, cc = (q16 >> 1) & 3, yz = q16 >> 3;
+            const int j = r * kColsRow + q16;
+            double x[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) x[e] = value(ks, 16 * half + e);
-        uint4 ch[kDig];
-        digit_chunks(x, scale, ch);
+            for (int e = 0; e < 8; ++e) {
+                const double2 w = s_w[yz][16 * ks + 8 * half + e][cc];
+                // part 0 (Re v): (Re w, Im w); part 1 (Im v): (-Im w, Re w)
+                x[2 * e] = ri ? w.y : w.x;
+                x[2 * e + 1] = ri ? w.x : -w.y;
+            }
+            uint4 ch[kDig];
+            digit_chunks(x, s_scale[4 * yz + cc], ch);
 #pragma unroll
-        for (int p = 0; p < kDig; ++p) {
-            unsigned char *dst = block + (long long)pd.NBc * 8 + ((long long)ks * kDig + p) * pd.NBc * kKS +
-                                 koff8(j, 16 * half);
-            *reinterpret_cast<uint4 *>(dst) = ch[p];
+            for (int p = 0; p < kDig; ++p) {
+                unsigned char *dst = block + (long long)pd.NBc * 8 + ((long long)ks * kDig + p) * pd.NBc * kKS +
+                                     koff8(j, 16 * half);
+                *reinterpret_cast<uint4 *>(dst) = ch[p];
+            }
         }
     }
 }
@@ -426,9 +462,10 @@ extern "C" int few_fold_mixed_adjoint(const void *W, const double *t_knots, int 
     if (nseg < 0 || R < 1 || R > few::kMaxPhaseRows || NN < 1)
         return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: bad sizes (R <= %d)", few::kMaxPhaseRows);
     if (nseg == 0) return FEW_OK;
-    const few::PhaseDims d = few::phase_dims(R, NN);
-    const long long threads = (long long)nseg * d.NBc * 32;
-    few::k_fold_phase_s8<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+    if (NN > few::kMaxPhaseNN)
+        return few::fail(FEW_ERR_SIZE, "few_fold_mixed_adjoint: NN=%d > %d", NN, few::kMaxPhaseNN);
+    const dim3 grid(nseg, R);
+    few::k_fold_phase_s8<<<grid, 4 * few::phase_dims(R, NN).NNp, 0, (cudaStream_t)stream>>>(
         (const double2 *)W, t_knots, nseg, R, NN, nlo, (unsigned char *)Bpk);
     FEW_LAUNCH_CHECK("k_fold_phase_s8");
     return FEW_OK;
