@@ -117,10 +117,9 @@ FEW_API int few_get_waveform(void *d_waveform, const double *interp_array, const
  * (R * NN * 64 bytes plus the fold tables, R the (m, k) rows and NN the n
  * range of the mode list) are rejected with FEW_ERR_SIZE and a message.
  * The first call on each device looks up the array's device address (with
- * that device made current) and keeps it for the life of the process; make
- * that first call before any stream capture, and do not call the entry point
- * on a device again after a cudaDeviceReset of it.  The caller's current
- * device is restored on return.
+ * that device made current) and keeps it for the life of the process; do not
+ * call the entry point on a device again after a cudaDeviceReset of it.  The
+ * caller's current device is restored on return.
  * All calls on a device share the array, so calls that overlap on the GPU
  * (other threads, other streams) race and must be serialised by the caller;
  * each call writes every scratch byte it reads, so nothing needs clearing.
