@@ -230,29 +230,46 @@ struct AdjGArgs {
 
 constexpr int kGThreads = 384;
 constexpr int kGPhase = kGThreads;  // samples whose phase data is staged at once (one per thread)
-constexpr int kGTile = 32;    // samples per phasor-table tile
+constexpr int kGTile = 64;    // samples per phasor-table tile
 constexpr int kGCols = 64;    // n' columns per CTA (one per thread of a row block)
 constexpr int kGRowBlocks = kGThreads / kGCols;  // 6 row blocks per CTA
 
-// Dynamic shared memory of k_adj_G<RB>: the phasor tables of one tile and the
-// phase data of kGPhase samples.
+constexpr int kGPow = 16;     // per tile sample and phasor: E^0..E^7, then E^0, E^8, ..., E^56
+
+// Dynamic shared memory of k_adj_G<RB>: the phasor tables of one tile, the
+// small power tables of its samples, and the phase data of kGPhase samples.
 constexpr size_t adj_g_smem(int rb)
 {
     return (size_t)kGTile * kGRowBlocks * rb * sizeof(double2)  // g u_r
            + (size_t)kGTile * kGCols * sizeof(double2)          // v_{n'}
-           + (size_t)kGPhase * 4 * sizeof(double2)              // Ep, Er, Et, g
+           + (size_t)kGTile * 2 * kGPow * sizeof(double2)       // powers of e^{-i Phi_phi}, e^{-i Phi_r}
+           + (size_t)kGPhase * 5 * sizeof(double2)              // Ep, Er, Et, g, v at this CTA's first n'
            + (size_t)kGPhase * 4 * sizeof(double);              // 1, x, x^2, x^3
+}
+
+// E^p from a sample's power table (E^0..E^7, E^0, E^8, ..., E^56): two factors
+// for |p| < 64 (a power by squaring past that), the conjugate for p < 0.
+__device__ __forceinline__ double2 pow_from_table(const double2 *T, int p)
+{
+    const int q = p < 0 ? -p : p;
+    double2 z = q < 64 ? cmul(T[8 + (q >> 3)], T[q & 7]) : cpow_int(T[1], q);
+    if (p < 0) z.y = -z.y;
+    return z;
 }
 
 // grid (nseg, row groups of 6*RB rows, column groups of 64), 384 threads (12
 // warps per SM at <= 170 registers): thread (row block rb, column c) owns keys
 // (r = group*6*RB + rb*RB + q, n' = c) for q < RB and
 // accumulates their four x^c sums over every sample of the segment.  Every
-// thread first evaluates the phases, sincos and g of one of the next kGPhase
-// samples; then, per tile of kGTile samples, the CTA builds the row factors
-// g_i u_r(t_i) and the column phasors v_{n'}(t_i), and each thread reads its
-// column phasor once per sample and uses it for RB rows (the row factors are
-// warp-wide broadcasts).  Samples are added in order: deterministic.
+// thread first evaluates the phases, sincos, g and v at the CTA's first n' of
+// one of the next kGPhase samples; then, per tile of kGTile samples, 2 kGTile
+// threads build each sample's small power tables of e^{-i Phi_phi} and
+// e^{-i Phi_r} (E^0..E^7 and E^8k), the CTA fills the row factors g_i u_r(t_i)
+// and the column phasors v_{n'}(t_i) from them (each entry two or three
+// independent complex products, no long dependent chains), and each thread
+// reads its column phasor once per sample and uses it for RB rows (the row
+// factors are warp-wide broadcasts).  Samples are added in order:
+// deterministic.
 template <int RB>
 __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
 {
@@ -260,9 +277,12 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 (*s_gu)[RG] = reinterpret_cast<double2 (*)[RG]>(smem_raw);
     double2 (*s_v)[kGCols] = reinterpret_cast<double2 (*)[kGCols]>(smem_raw + (size_t)kGTile * RG * sizeof(double2));
-    double2 (*s_E)[4] = reinterpret_cast<double2 (*)[4]>(smem_raw + (size_t)kGTile * (RG + kGCols) * sizeof(double2));
-    double (*s_x)[4] = reinterpret_cast<double (*)[4]>(smem_raw + (size_t)(kGTile * (RG + kGCols) + kGPhase * 4) *
-                                                                      sizeof(double2));
+    double2 (*s_P)[2][kGPow] =  // [tile sample][phi, r][power]
+        reinterpret_cast<double2 (*)[2][kGPow]>(smem_raw + (size_t)kGTile * (RG + kGCols) * sizeof(double2));
+    double2 (*s_E)[5] = reinterpret_cast<double2 (*)[5]>(smem_raw + (size_t)kGTile * (RG + kGCols + 2 * kGPow) *
+                                                                         sizeof(double2));
+    double (*s_x)[4] = reinterpret_cast<double (*)[4]>(
+        smem_raw + (size_t)(kGTile * (RG + kGCols + 2 * kGPow) + kGPhase * 5) * sizeof(double2));
     __shared__ int s_rm[RG], s_rk[RG];
     __shared__ double s_pc[24];
 
@@ -310,6 +330,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
             }
             const double2 G = a.grad[i];
             s_E[tid][3] = make_double2(G.x, -G.y);  // g = conj(G)
+            s_E[tid][4] = cpow_int(s_E[tid][1], a.nlo + c0);
             s_x[tid][0] = 1.0;
             s_x[tid][1] = x;
             s_x[tid][2] = x * x;
@@ -318,22 +339,37 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
         for (int i0 = 0; i0 < np; i0 += kGTile) {
             const int ns = min(kGTile, np - i0);
             __syncthreads();  // phase data written; the previous tile's readers are done
-            // tables: g u_r for this CTA's rows, v_{n'} for its columns (runs of 8 by recurrence)
+            // small power tables of each sample's e^{-i Phi_phi} (f = 0) and e^{-i Phi_r} (f = 1)
+            if (tid < 2 * ns) {
+                const int j = tid >> 1, f = tid & 1;
+                const double2 E = s_E[i0 + j][f];
+                double2 *T = s_P[j][f];
+                double2 z = make_double2(1.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    T[q] = z;
+                    z = cmul(z, E);
+                }
+                const double2 E8 = z;
+                z = make_double2(1.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    T[8 + q] = z;
+                    z = cmul(z, E8);
+                }
+            }
+            __syncthreads();
+            // tables: g u_r for this CTA's rows, v_{n'} = v_{c0} E_r^{n' - c0} for its columns
             for (int w = tid; w < ns * RG; w += blockDim.x) {
                 const int j = w / RG, r = w - j * RG;
-                double2 uu = cpow_int(s_E[i0 + j][0], s_rm[r]);
+                double2 uu = pow_from_table(s_P[j][0], s_rm[r]);
                 if (s_rk[r]) uu = cmul(uu, cpow_int(s_E[i0 + j][2], s_rk[r]));
                 s_gu[j][r] = cmul(s_E[i0 + j][3], uu);
             }
-            for (int w = tid; w < ns * (kGCols / 8); w += blockDim.x) {
-                const int j = w / (kGCols / 8), b = w - j * (kGCols / 8);
-                const double2 Er = s_E[i0 + j][1];
-                double2 v = cpow_int(Er, a.nlo + c0 + 8 * b);
-#pragma unroll
-                for (int c = 8 * b; c < 8 * b + 8; ++c) {
-                    s_v[j][c] = v;
-                    v = cmul(v, Er);
-                }
+            for (int w = tid; w < ns * kGCols; w += blockDim.x) {
+                const int j = w / kGCols, c = w - j * kGCols;
+                const double2 *T = s_P[j][1];
+                s_v[j][c] = cmul(s_E[i0 + j][4], cmul(T[8 + (c >> 3)], T[c & 7]));
             }
             __syncthreads();
             for (int j = 0; j < ns; ++j) {
