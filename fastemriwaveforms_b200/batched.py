@@ -112,7 +112,8 @@ class BatchedInterpolatedModeSum:
         max_NN = max(p.fold.NN for p in self.preps)
         if self.precision == "mixed" and self.max_R > 64:
             raise ValueError("precision='mixed' supports at most 64 (m, k) rows")
-        self.smem_bytes = int(min(200 * 1024, max(p.fold.R * p.fold.NN * 64 for p in self.preps)))
+        # the FP64 kernels keep a segment's rows in shared memory in blocks of up to 8 rows
+        self.smem_bytes = int(min(200 * 1024, max((p.fold.R + 7) // 8 * 8 * p.fold.NN * 64 for p in self.preps)))
         descs = np.zeros(len(self.preps), DESC_DTYPE)
         for i, p in enumerate(self.preps):
             p.coeffs = torch.empty((4, p.N, 2 * p.K), dtype=torch.float64, device=dev)

@@ -98,6 +98,15 @@ struct SumArgs {
     double dt;
 };
 
+// Rows per pass of the folded sum: all R when their blocks of RB rows fit in
+// smem_bytes, else the most whole blocks that fit (0 if not even one does).
+__host__ __device__ inline int sum_rows_per_pass(int R, int NN, int RB, int smem_bytes)
+{
+    const int fit = smem_bytes / (NN * 4 * (int)sizeof(double2));  // rows whose coefficients fit
+    if ((R + RB - 1) / RB * RB <= fit) return R;
+    return fit / RB * RB;
+}
+
 // One work unit (samples [lo, hi) of segment seg) of the folded sum; the
 // block's shared memory holds the segment's W rows.  Each thread carries SPT
 // samples (i, i + blockDim, ...) through the key loop together, so every
@@ -138,9 +147,16 @@ __device__ __forceinline__ void sum_unit(const SumArgs &a, int seg, int lo, int 
         const int nrp = min(a.rows_per_pass, R - r0);
         __syncthreads();  // previous pass finished reading sW
         {
+            // rows (row, n', c) in global order -> blocks of RB rows, each laid out
+            // (n', row in block, c): the 4 RB coefficients one column needs are
+            // contiguous (the last block of a pass may be partly unused)
             const double2 *src = a.W + ((long long)seg * R + r0) * NN * 4;
             const int count = nrp * NN * 4;
-            for (int q = threadIdx.x; q < count; q += blockDim.x) sW[q] = src[q];
+            for (int e = threadIdx.x; e < count; e += blockDim.x) {
+                const int rr = e / (NN * 4), rem = e - rr * (NN * 4);
+                const int blk = rr / RB, q = rr - blk * RB;
+                sW[((blk * NN) + (rem >> 2)) * (RB * 4) + q * 4 + (rem & 3)] = src[e];
+            }
         }
         __syncthreads();
         for (int ib = lo + threadIdx.x; ib < hi; ib += SPT * blockDim.x) {
@@ -240,11 +256,11 @@ __device__ __forceinline__ void sum_unit(const SumArgs &a, int seg, int lo, int 
                         }
                         T[sm] = make_double2(0.0, 0.0);
                     }
-                    const double2 *wc = wrow + c * 4;
+                    const double2 *wc = wrow + c * (RB * 4);
 #pragma unroll
                     for (int q = 0; q < RB; ++q) {
                         if (rb + q < nrp) {
-                            const double2 *w = wc + (long long)q * NN * 4;
+                            const double2 *w = wc + q * 4;
                             const double2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
 #pragma unroll
                             for (int sm = 0; sm < SPT; ++sm) {
@@ -324,7 +340,7 @@ __global__ void __launch_bounds__(kSumThreads, (SPT == 1 || RB <= 4) ? 2 : 1) k_
         a.NN = d.NN;
         a.use_theta = d.use_theta;
         a.dt = d.dt;
-        a.rows_per_pass = max(1, min(d.R, smem_bytes / (d.NN * 4 * (int)sizeof(double2))));
+        a.rows_per_pass = sum_rows_per_pass(d.R, d.NN, RB, smem_bytes);
         sum_unit<RB, FAITHFUL, SPT, true>(a, units4[4 * u + 1], units4[4 * u + 2], units4[4 * u + 3],
                                     reinterpret_cast<double2 *>(smem_raw), s_rm, s_rk, s_pc);
         if (done) {  // completion time of the waveform: the latest of its units
@@ -447,11 +463,12 @@ int launch_sum_folded(double2 *wf, const double2 *W, const double *pc, int N, co
     a.use_theta = use_theta;
     a.dt = dt;
     const long long row_bytes = (long long)NN * 4 * sizeof(double2);
-    int rpp = (int)std::min<long long>(R, kSmemBudget / row_bytes);
-    if (rpp < 1) return fail(FEW_ERR_SIZE, "few_sum_folded: NN=%d too large for one row in shared memory", NN);
-    a.rows_per_pass = rpp;
-    const size_t smem = (size_t)rpp * row_bytes;
     const SumShape sh = sum_shape(mode);
+    const int rpp = sum_rows_per_pass(R, NN, sh.rb, kSmemBudget);
+    if (rpp < 1)
+        return fail(FEW_ERR_SIZE, "few_sum_folded: NN=%d too large for one row block in shared memory", NN);
+    a.rows_per_pass = rpp;
+    const size_t smem = (size_t)((rpp + sh.rb - 1) / sh.rb * sh.rb) * row_bytes;
     if (sh.rb == 4 && sh.spt == 2)
         return mode == FEW_SUM_FAITHFUL ? launch_sum_t<4, true, 2>(a, nunits, smem, st)
                                         : launch_sum_t<4, false, 2>(a, nunits, smem, st);

@@ -24,7 +24,7 @@ def run(inp, precision):
     return wf.cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["theta", "m0", "plain_small", "plain_full", "many_rows"])
+@pytest.mark.parametrize("case", ["theta", "m0", "plain_small", "plain_full", "many_rows", "wide_n"])
 def test_mixed_matches_fp64(cuda, case):
     if case == "theta":
         inp, _ = load_case("sum_small_theta.npz")
@@ -34,6 +34,8 @@ def test_mixed_matches_fp64(cuda, case):
         inp = S.plain_small()
     elif case == "many_rows":
         inp = S.many_rows_case()  # 63 (m', k') rows: two MMA column groups
+    elif case == "wide_n":
+        inp = S.many_rows_case(mmax=2, kmax=0, nmax=60, seed=13)  # NN = 121: eight K chunks
     else:
         inp = S.plain_full()
     ref = run(inp, "exact")

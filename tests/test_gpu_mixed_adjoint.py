@@ -52,6 +52,8 @@ CASES = {
     "plain_full": lambda: S.plain_full(seed=2),
     "small_theta": lambda: S.small_case(K=40, N=30, out_len=20000, seed=5, theta=True),
     "many_rows": lambda: S.many_rows_case(),  # 63 rows: two MMA column groups in the phase adjoint
+    # n' = -60..60 (NN = 121): eight K steps of 16 n' in the phase adjoint, two 64-n' blocks in G
+    "wide_n": lambda: S.many_rows_case(mmax=2, kmax=0, nmax=60, seed=13),
 }
 
 
