@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
     unsigned char *const sA = smem_raw;                                   // [digit][K step] planes
     unsigned char *const sB = smem_raw + (size_t)kDig * nks * kAPlane;    // [digit][K step] planes of a pass
     const int npass = (R + kRowsPass - 1) / kRowsPass;
+    const bool pair_levels = nks <= 4;  // K = 32 nks <= 128: level pairs fit in int32
     const uint32_t trow = pp.tmem + ((uint32_t)(warp * 32) << 16);
     double proj[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's share of the unit's 24 outputs
     bool failed = false;
@@ -352,14 +353,26 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
                 double val[16];
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    // the levels combined in FP64 (each level's int32 exact as a double,
-                    // the sum exact below 2^53); int32 -> double without a conversion
-                    // instruction: 2^52 + 2^31 + D in the significand, minus the offset
-                    double lv[kDig];
+                    // the levels combined exactly: a level sums (level + 1) K digit
+                    // products of magnitude <= 2^14, so with K <= 128 (nks <= 4) the
+                    // pairs D0 2^8 + D1 and D2 2^8 + D3 stay below 2^31 in int32 and two
+                    // int32 -> double steps and one FMA give the same double as four and
+                    // three (every partial sum is an integer below 2^53).  int32 -> double
+                    // without a conversion instruction: 2^52 + 2^31 + D in the
+                    // significand, minus the offset.
+                    double acc;
+                    if (pair_levels) {
+                        const int hi2 = D[0][q] * 256 + D[1][q], lo2 = D[2][q] * 256 + D[3][q];
+                        const double dh = __hiloint2double(0x43300000, hi2 ^ 0x80000000) - 4503601774854144.0;
+                        const double dl = __hiloint2double(0x43300000, lo2 ^ 0x80000000) - 4503601774854144.0;
+                        acc = fma(dh, 65536.0, dl);
+                    } else {
+                        double lv[kDig];
 #pragma unroll
-                    for (int l = 0; l < kDig; ++l)
-                        lv[l] = __hiloint2double(0x43300000, D[l][q] ^ 0x80000000) - 4503601774854144.0;
-                    const double acc = fma(lv[0], 16777216.0, fma(lv[1], 65536.0, fma(lv[2], 256.0, lv[3])));
+                        for (int l = 0; l < kDig; ++l)
+                            lv[l] = __hiloint2double(0x43300000, D[l][q] ^ 0x80000000) - 4503601774854144.0;
+                        acc = fma(lv[0], 16777216.0, fma(lv[1], 65536.0, fma(lv[2], 256.0, lv[3])));
+                    }
                     val[q] = acc * s_inv[kColsRow * r + q];
                 }
                 // q = 2 (4 yz + c) + re/im
