@@ -341,15 +341,16 @@ __global__ void __launch_bounds__(kPT, 2) k_adj_phase_s8(PhaseArgs a)
             // in FP64, Y and Z by Horner in tau, u_r, and the three weighted row sums
             for (int rr = 0; rr < rows; ++rr) {
                 const int r = r0 + rr;
+                // the four levels of the row: four loads in flight, one wait
+                float F[kDig][16];
+#pragma unroll
+                for (int lv = 0; lv < kDig; ++lv) tmem_ld16(trow + (uint32_t)(lv * kLvl + kColsRow * rr), F[lv]);
+                tmem_wait_ld();
                 int D[kDig][16];
 #pragma unroll
-                for (int lv = 0; lv < kDig; ++lv) {
-                    float f[16];
-                    tmem_ld16(trow + (uint32_t)(lv * kLvl + kColsRow * rr), f);
-                    tmem_wait_ld();
+                for (int lv = 0; lv < kDig; ++lv)
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) D[lv][e] = __float_as_int(f[e]);
-                }
+                    for (int e = 0; e < 16; ++e) D[lv][e] = __float_as_int(F[lv][e]);
                 double val[16];
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
