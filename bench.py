@@ -1164,7 +1164,7 @@ def main():
     # DRAM bytes of one launch at this workload from an ncu capture (dram__bytes_read.sum +
     # dram__bytes_write.sum); null for workloads not captured
     captured = args.workload == "plain_full" and args.precision == "faithful"
-    traffic = {"bytes_per_launch": 157.6e6, "source": "ncu capture of k_sum_folded (faithful, one-year workload)",
+    traffic = {"bytes_per_launch": 161.0e6, "source": "ncu capture of k_sum_folded (faithful, one-year workload)",
                "algorithmic_bytes": float(keys) * 64.0 * seg.nseg + 2.0 * 16.0 * T} if captured else None
     roofline = {"bound": "fp64", "kernel": "k_sum_folded", "achieved": achieved, "peak": fp64_tflops,
                 "unit": "TFLOP/s", "frac": achieved / fp64_tflops, "traffic": traffic,
