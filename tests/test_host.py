@@ -182,3 +182,24 @@ def test_mode_selector_list_checks():
     assert sel.negative_m_flag
     with pytest.raises(ValueError, match="m >= 0 when include_minus_mkn = True"):
         sel(np.zeros(4), 0.5, None, None, None, 1.0, 0.5)
+
+
+def test_autotune_shape_search_and_cache(tmp_path, monkeypatch):
+    """The tuner's shape lists (the tensor-core sum's operand pipeline included)
+    and its JSON cache: the fastest candidate is kept with every timing."""
+    from fastemriwaveforms_b200 import autotune
+
+    mixed = autotune.candidates_for("mixed")
+    assert {(c["astages"], c["bstages"]) for c in mixed} == {(a, b) for a in (1, 2) for b in (2, 3, 4)}
+    assert all(set(c) == {"chunk", "ctas_per_sm", "astages", "bstages"} for c in mixed)
+    fp64 = autotune.candidates_for("exact")
+    assert len(fp64) == len(autotune.CHUNKS) * len(autotune.CTAS_PER_SM)
+    assert all(set(c) == {"chunk", "ctas_per_sm"} for c in fp64)
+
+    monkeypatch.setenv("FEW_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(autotune, "time_ms", lambda fn, reps=3: fn())
+    cost = {1: 3.0, 2: 1.0, 3: 2.0}
+    choice = autotune.tune("k", lambda chunk, ctas_per_sm: (lambda: cost[ctas_per_sm] + chunk * 1e-6), fp64)
+    assert choice["ctas_per_sm"] == 2 and choice["chunk"] == min(autotune.CHUNKS)
+    assert len(choice["tried"]) == len(fp64)
+    assert autotune.lookup("k")["ctas_per_sm"] == 2
