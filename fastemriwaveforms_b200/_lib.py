@@ -48,6 +48,9 @@ SIGNATURES = {
                           _vp, _vp],
     "few_adjoint_phase_reduce": [_vp, _vp, _c_int, _vp, _vp],
     "few_adjoint_G": [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp, _vp],
+    "few_adjoint_joint_scratch": [_c_int, _c_int, _c_int],
+    "few_adjoint_joint": [_vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_int, _c_int,
+                          _c_dbl, _c_int, _vp, _vp, _vp, _vp],
     "few_unfold": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
     "few_spline_adjoint_factored": [_vp, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
     "few_spline_adjoint": [_vp, _c_ll, _vp, _vp, _c_ll, _c_ll, _c_int, _c_ll, _c_int, _c_int, _c_int, _vp],
@@ -95,7 +98,7 @@ SIGNATURES = {
                             _c_int, _vp, _c_int, _c_int, _c_int, _vp],
 }
 _RESTYPE = {"few_last_error": ctypes.c_char_p, "few_mixed_operand_bytes": ctypes.c_longlong,
-            "few_mixed_adjoint_operand_bytes": ctypes.c_longlong}
+            "few_mixed_adjoint_operand_bytes": ctypes.c_longlong, "few_adjoint_joint_scratch": ctypes.c_longlong}
 
 _lock = threading.Lock()
 _lib = None

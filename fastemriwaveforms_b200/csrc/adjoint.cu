@@ -404,6 +404,321 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Joint FP64 adjoint: G and the phase-coefficient gradients from one pass.
+//
+// For key (r, n') let z_i = g_i u_r(t_i) v_n(t_i) (n = nlo + n') and let
+// sigma_i = x_i / w (x = t - t0, w the phase step of the segment).  The kernel
+// accumulates per key the eleven moments M_p = sum_i sigma_i^p z_i, p = 0..10,
+// over the segment's samples; both gradients are linear in them:
+//   G[c] = w^c M_c  (c = 0..3), and
+//   dL/dcoef_{f,q} = sum_keys wt_f Im( sum_c W_c w^c sum_j beta_qj M_{j+c} ),
+// with wt_f = m', k' or n for the fields phi, theta, r, W_c the forward's folded
+// coefficients and beta_qj the coefficients of the basis term b_q(s) as a
+// polynomial in sigma (s = sigma - (pt0 - t0) / w).  The second line holds
+// because dL/dPhi_f(t_i) = Im(g_i D_f(t_i)) with D_f = sum_keys wt_f u v^n W(x),
+// and b_q(s) x^c is a polynomial of degree q + c <= 10 in sigma.  Per (key,
+// sample) that is one complex product and eleven complex accumulations (26 FP64
+// operations) where the two separate kernels take 12 (G) plus about 17 (the
+// per-sample phase sums), and the phasors are formed once.
+// ---------------------------------------------------------------------------
+constexpr int kJMom = 11;  // moments sigma^0 .. sigma^10
+
+struct AdjJointArgs {
+    const double2 *grad;
+    const double2 *W;      // (nseg, R, NN, 4) the forward's folded coefficients
+    const double *pc;
+    const double *seg_info;
+    const int *units;      // (nunits, 3): segment, first sample, end sample (<= 1024 samples)
+    const int *row_m;
+    const int *row_k;
+    double2 *Gpart;        // (nunits, R, NN, 4) each unit's share of G, or null
+    double *partial;       // (nunits * blocks per unit, 24) or null
+    int N, R, nlo, NN, use_theta;
+    double dt;
+};
+
+// Dynamic shared memory of k_adj_joint: the tile tables of k_adj_G plus the
+// powers sigma^1..sigma^10 of the tile's samples and sigma of the staged ones
+// (nrb row blocks of rb rows by cols columns; nrb * cols samples staged).
+constexpr size_t adj_joint_smem(int nrb, int rb, int cols)
+{
+    return (size_t)kGTile * nrb * rb * sizeof(double2)         // g u_r
+           + (size_t)kGTile * cols * sizeof(double2)            // v_{n'}
+           + (size_t)kGTile * 2 * kGPow * sizeof(double2)       // powers of e^{-i Phi_phi}, e^{-i Phi_r}
+           + (size_t)nrb * cols * 5 * sizeof(double2)           // Ep, Er, Et, g, v at this CTA's first n'
+           + (size_t)kGTile * 5 * sizeof(double2)               // (sigma^(2h+1), sigma^(2h+2)), h < 5
+           + (size_t)nrb * cols * sizeof(double);               // sigma
+}
+
+// grid (work units, row groups of NRB*RB rows, column groups of COLS),
+// NRB*COLS threads.  A work unit is at most 1024 samples of one segment, so
+// the CTAs are of like size whatever the knot spacing.  The work split and the
+// per-tile tables are k_adj_G's (the power tables built two threads per sample
+// and phasor); each thread keeps the 11 moments of its RB keys in registers,
+// samples added in order (deterministic).  The epilogue writes the unit's
+// share of G and reduces the keys' phase terms over the CTA into one row of 24
+// partials (field-major: phi, theta, r; 8 basis terms each).
+template <int NRB, int RB, int COLS, int UNR>
+__global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
+{
+    constexpr int NT = NRB * COLS;  // threads; also the samples staged per phase batch
+    constexpr int RG = NRB * RB;    // rows per CTA
+    static_assert(NT >= 5 * kGTile, "the tile tables need 5 x 64 threads");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char *sp = smem_raw;
+    double2 (*s_gu)[RG] = reinterpret_cast<double2 (*)[RG]>(sp);
+    sp += (size_t)kGTile * RG * sizeof(double2);
+    double2 (*s_v)[COLS] = reinterpret_cast<double2 (*)[COLS]>(sp);
+    sp += (size_t)kGTile * COLS * sizeof(double2);
+    double2 (*s_P)[2][kGPow] = reinterpret_cast<double2 (*)[2][kGPow]>(sp);
+    sp += (size_t)kGTile * 2 * kGPow * sizeof(double2);
+    double2 (*s_E)[5] = reinterpret_cast<double2 (*)[5]>(sp);
+    sp += (size_t)NT * 5 * sizeof(double2);
+    double2 (*s_sig)[5] = reinterpret_cast<double2 (*)[5]>(sp);
+    sp += (size_t)kGTile * 5 * sizeof(double2);
+    double *s_sx = reinterpret_cast<double *>(sp);
+    __shared__ int s_rm[RG], s_rk[RG];
+    __shared__ double s_pc[24];
+    __shared__ double s_beta[8][8];
+    __shared__ double s_red[NT / 32][24];
+
+    const int R = a.R, NN = a.NN;
+    const int u = blockIdx.x;
+    const int seg = a.units[3 * u], lo = a.units[3 * u + 1], hi = a.units[3 * u + 2];
+    const int r0 = blockIdx.y * RG, c0 = blockIdx.z * COLS;
+    const double t0 = a.seg_info[3 * seg], pt0 = a.seg_info[3 * seg + 1], pw = a.seg_info[3 * seg + 2];
+    const long long nps = (long long)(a.N - 1) * 3;
+    const int tid = threadIdx.x;
+    const int col = tid % COLS, rb = tid / COLS;
+    for (int r = tid; r < RG; r += blockDim.x) {
+        s_rm[r] = (r0 + r < R) ? a.row_m[r0 + r] : 0;
+        s_rk[r] = (r0 + r < R) ? a.row_k[r0 + r] : 0;
+    }
+    if (tid < 24) {
+        const int q = tid >> 3, c = tid & 7;
+        s_pc[tid] = a.pc[c * nps + (long long)seg * 3 + q];
+    }
+    if (tid == 32) {
+        // b_q = prod_{k < q} (k even ? s : s1) as polynomials in sigma, with
+        // s = sigma - d and s1 = (1 + d) - sigma
+        const double d = (pt0 - t0) / pw;
+        double b[8] = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) s_beta[q][j] = b[j];
+            const double al = (q & 1) ? -1.0 : 1.0, ga = (q & 1) ? 1.0 + d : -d;
+#pragma unroll
+            for (int j = 7; j >= 0; --j) b[j] = ga * b[j] + (j ? al * b[j - 1] : 0.0);
+        }
+    }
+    double2 acc[RB][kJMom];
+#pragma unroll
+    for (int q = 0; q < RB; ++q)
+#pragma unroll
+        for (int p = 0; p < kJMom; ++p) acc[q][p] = make_double2(0.0, 0.0);
+
+    for (int p0 = lo; p0 < hi; p0 += NT) {
+        const int np = min(NT, hi - p0);
+        __syncthreads();  // s_pc and the row tables are written; the previous batch's readers are done
+        if (tid < np) {
+            const int i = p0 + tid;
+            const double t = rmul(a.dt, (double)i);
+            const double x = rsub(t, t0);
+            const double s = __ddiv_rn(rsub(t, pt0), pw);
+            const double s1 = rsub(1.0, s);
+            double sn, cs;
+            sincos(phase_poly(s_pc, s, s1), &sn, &cs);
+            s_E[tid][0] = make_double2(cs, -sn);
+            sincos(phase_poly(s_pc + 16, s, s1), &sn, &cs);
+            s_E[tid][1] = make_double2(cs, -sn);
+            if (a.use_theta) {
+                sincos(phase_poly(s_pc + 8, s, s1), &sn, &cs);
+                s_E[tid][2] = make_double2(cs, -sn);
+            } else {
+                s_E[tid][2] = make_double2(1.0, 0.0);
+            }
+            const double2 G = a.grad[i];
+            s_E[tid][3] = make_double2(G.x, -G.y);  // g = conj(G)
+            s_E[tid][4] = cpow_int(s_E[tid][1], a.nlo + c0);
+            s_sx[tid] = __ddiv_rn(x, pw);
+        }
+        for (int i0 = 0; i0 < np; i0 += kGTile) {
+            const int ns = min(kGTile, np - i0);
+            __syncthreads();  // phase data written; the previous tile's readers are done
+            if (tid < 4 * ns) {
+                // two threads per (sample, phasor): half h writes E^{4h..4h+3} and
+                // E^{8 (4h..4h+3)}, every entry at most seven products from E
+                const int j = tid >> 2, f = (tid >> 1) & 1, h = tid & 1;
+                const double2 E = s_E[i0 + j][f];
+                double2 *T = s_P[j][f];
+                const double2 E2 = cmul(E, E), E4 = cmul(E2, E2), E8 = cmul(E4, E4);
+                const double2 E16 = cmul(E8, E8), E32 = cmul(E16, E16);
+                const double2 b1 = h ? E4 : make_double2(1.0, 0.0), b8 = h ? E32 : make_double2(1.0, 0.0);
+                T[4 * h] = b1;
+                T[4 * h + 1] = h ? cmul(b1, E) : E;
+                T[4 * h + 2] = h ? cmul(b1, E2) : E2;
+                T[4 * h + 3] = cmul(h ? cmul(b1, E2) : E2, E);
+                T[8 + 4 * h] = b8;
+                T[8 + 4 * h + 1] = h ? cmul(b8, E8) : E8;
+                T[8 + 4 * h + 2] = h ? cmul(b8, E16) : E16;
+                T[8 + 4 * h + 3] = cmul(h ? cmul(b8, E16) : E16, E8);
+            } else if (tid >= 4 * kGTile && tid < 4 * kGTile + ns) {
+                const int j = tid - 4 * kGTile;
+                const double sg = s_sx[i0 + j];
+                double *row = reinterpret_cast<double *>(s_sig[j]);
+                double pp = sg;
+#pragma unroll
+                for (int q = 0; q < 10; ++q) {
+                    row[q] = pp;
+                    pp *= sg;
+                }
+            }
+            __syncthreads();
+            {
+                // written through restrict pointers, so the loads of one entry need
+                // not wait for the stores of the previous one
+                const double2 *__restrict__ tP = &s_P[0][0][0];
+                const double2 *__restrict__ tE = &s_E[i0][0];
+                double2 *__restrict__ tgu = &s_gu[0][0];
+                double2 *__restrict__ tv = &s_v[0][0];
+                for (int w = tid; w < ns * RG; w += NT) {
+                    const int j = w / RG, r = w - j * RG;
+                    double2 uu = pow_from_table(tP + (2 * j) * kGPow, s_rm[r]);
+                    if (s_rk[r]) uu = cmul(uu, cpow_int(tE[5 * j + 2], s_rk[r]));
+                    tgu[w] = cmul(tE[5 * j + 3], uu);
+                }
+                for (int w = tid; w < ns * COLS; w += NT) {
+                    const int j = w / COLS, c = w - j * COLS;
+                    const double2 *T = tP + (2 * j + 1) * kGPow;
+                    tv[w] = cmul(tE[5 * j + 4], cmul(T[8 + (c >> 3)], T[c & 7]));
+                }
+            }
+            __syncthreads();
+#pragma unroll UNR
+            for (int j = 0; j < ns; ++j) {
+                const double2 v = s_v[j][col];
+                double2 z[RB];
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    z[q] = cmul(s_gu[j][rb * RB + q], v);
+                    acc[q][0].x += z[q].x;
+                    acc[q][0].y += z[q].y;
+                }
+#pragma unroll
+                for (int h = 0; h < 5; ++h) {
+                    const double2 sg = s_sig[j][h];
+#pragma unroll
+                    for (int q = 0; q < RB; ++q) {
+                        acc[q][2 * h + 1].x = fma(sg.x, z[q].x, acc[q][2 * h + 1].x);
+                        acc[q][2 * h + 1].y = fma(sg.x, z[q].y, acc[q][2 * h + 1].y);
+                        acc[q][2 * h + 2].x = fma(sg.y, z[q].x, acc[q][2 * h + 2].x);
+                        acc[q][2 * h + 2].y = fma(sg.y, z[q].y, acc[q][2 * h + 2].y);
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();  // the row and basis tables are visible even to a segment without samples
+    // epilogue: G, then this thread's phase terms
+    const double w1 = pw, w2 = pw * pw, w3 = w2 * pw;
+    const int n = c0 + col;
+    double ph[3][8];
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) ph[f][q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < RB; ++q) {
+        const int r = r0 + rb * RB + q;
+        if (r >= R || n >= NN) continue;
+        const long long key = ((long long)seg * R + r) * NN + n;
+        if (a.Gpart) {  // this unit's share of G; k_adj_joint_reduce_G adds a segment's units
+            double2 *g = a.Gpart + (((long long)u * R + r) * NN + n) * 4;
+            g[0] = acc[q][0];
+            g[1] = make_double2(acc[q][1].x * w1, acc[q][1].y * w1);
+            g[2] = make_double2(acc[q][2].x * w2, acc[q][2].y * w2);
+            g[3] = make_double2(acc[q][3].x * w3, acc[q][3].y * w3);
+        }
+        if (a.partial) {
+            const double2 *Wk = a.W + key * 4;
+            const double2 W0 = Wk[0], W1 = Wk[1], W2 = Wk[2], W3 = Wk[3];
+            const double2 om[4] = {W0, make_double2(W1.x * w1, W1.y * w1), make_double2(W2.x * w2, W2.y * w2),
+                                   make_double2(W3.x * w3, W3.y * w3)};
+            double iq[8];  // Im sum_c om_c M_{j+c}
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                double v = 0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) v = fma(om[c].x, acc[q][j + c].y, fma(om[c].y, acc[q][j + c].x, v));
+                iq[j] = v;
+            }
+            const double wm = (double)s_rm[rb * RB + q];
+            const double wk = a.use_theta ? (double)s_rk[rb * RB + q] : 0.0;
+            const double wn = (double)(a.nlo + n);
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                double y = 0.0;
+#pragma unroll
+                for (int j = 0; j <= b; ++j) y = fma(s_beta[b][j], iq[j], y);
+                ph[0][b] = fma(wm, y, ph[0][b]);
+                ph[1][b] = fma(wk, y, ph[1][b]);
+                ph[2][b] = fma(wn, y, ph[2][b]);
+            }
+        }
+    }
+    if (!a.partial) return;
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            double v = ph[f][q];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) s_red[warp][f * 8 + q] = v;
+        }
+    __syncthreads();
+    if (tid < 24) {
+        double v = 0.0;
+        for (int w = 0; w < NT / 32; ++w) v += s_red[w][tid];
+        const long long cta = ((long long)blockIdx.x * gridDim.y + blockIdx.y) * gridDim.z + blockIdx.z;
+        a.partial[cta * 24 + tid] = v;
+    }
+}
+
+// grad_pc[s][e] = sum over the segment's units and their CTAs of the partials,
+// in order.
+__global__ void k_adj_joint_reduce(const double *__restrict__ partial, const int *__restrict__ seg_units, int nblk,
+                                   int nseg, double *__restrict__ grad_pc)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nseg * 24) return;
+    const int s = idx / 24, e = idx - s * 24;
+    double v = 0.0;
+    for (long long b = (long long)seg_units[s] * nblk; b < (long long)seg_units[s + 1] * nblk; ++b)
+        v += partial[b * 24 + e];
+    grad_pc[idx] = v;
+}
+
+// G[s][key][c] = sum of the segment's unit shares, in unit order.
+__global__ void k_adj_joint_reduce_G(const double2 *__restrict__ Gpart, const int *__restrict__ seg_units, int nseg,
+                                     long long per_unit, double2 *__restrict__ G)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nseg * per_unit) return;
+    const int s = (int)(idx / per_unit);
+    const long long e = idx - (long long)s * per_unit;
+    double2 v = make_double2(0.0, 0.0);
+    for (int u = seg_units[s]; u < seg_units[s + 1]; ++u) {
+        const double2 g = Gpart[(long long)u * per_unit + e];
+        v.x += g.x;
+        v.y += g.y;
+    }
+    G[idx] = v;
+}
+
 // Transpose of the fold: dL/d coefficient (4, N, 2K); knots >= nseg get 0.
 __global__ void k_unfold(const double2 *__restrict__ G, const double2 *__restrict__ ylms,
                          const int *__restrict__ key_plus, const int *__restrict__ key_minus, int K, int N, int nseg,
@@ -910,6 +1225,104 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     return FEW_OK;
 }
 
+// Shape of the joint adjoint's CTA: NRB row blocks of 2 rows by COLS columns,
+// the candidate that pads the (row, column) keys least, the first listed on a
+// tie.  With fewer columns per CTA the row and column tables cover fewer
+// entries per key (12 x 32: 24 + 32 per sample for 768 keys; 6 x 64: 12 + 64
+// for 768 keys).
+struct JointShape {
+    int nrb, cols;
+};
+constexpr JointShape kJointShapes[] = {{12, 32}, {11, 32}, {6, 64}, {5, 64}};
+
+static JointShape joint_shape(int R, int NN)
+{
+    JointShape best = kJointShapes[0];
+    long long best_keys = -1;
+    for (const JointShape &c : kJointShapes) {
+        const int rg = 2 * c.nrb;
+        const long long keys = (long long)((R + rg - 1) / rg * rg) * ((NN + c.cols - 1) / c.cols * c.cols);
+        if (best_keys < 0 || keys < best_keys) {
+            best = c;
+            best_keys = keys;
+        }
+    }
+    return best;
+}
+
+long long adj_joint_blocks(int R, int NN)
+{
+    const JointShape sh = joint_shape(R, NN);
+    return (long long)((R + 2 * sh.nrb - 1) / (2 * sh.nrb)) * ((NN + sh.cols - 1) / sh.cols);
+}
+
+long long adj_joint_scratch(int nunits, int R, int NN)
+{
+    // each unit's share of G (R NN 4 complex), then the CTAs' phase partials
+    return (long long)nunits * R * NN * 8 + (long long)nunits * adj_joint_blocks(R, NN) * 24;
+}
+
+int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, int N, const double *seg_info,
+                     const int *units, int nunits, const int *seg_units, int nseg, const int *row_m, const int *row_k,
+                     int R, int nlo, int NN, double dt, int use_theta, double2 *G, double *grad_pc, double *scratch,
+                     cudaStream_t st)
+{
+    if (nunits == 0 || nseg == 0) return FEW_OK;
+    double2 *Gpart = reinterpret_cast<double2 *>(scratch);
+    double *partial = scratch + (long long)nunits * R * NN * 8;
+    AdjJointArgs a;
+    a.grad = grad;
+    a.W = W;
+    a.pc = pc;
+    a.seg_info = seg_info;
+    a.units = units;
+    a.row_m = row_m;
+    a.row_k = row_k;
+    a.Gpart = G ? Gpart : nullptr;
+    a.partial = grad_pc ? partial : nullptr;
+    a.N = N;
+    a.R = R;
+    a.nlo = nlo;
+    a.NN = NN;
+    a.use_theta = use_theta;
+    a.dt = dt;
+    const JointShape sh = joint_shape(R, NN);
+    const int rg = 2 * sh.nrb, nt = sh.nrb * sh.cols;
+    dim3 grid(nunits, (R + rg - 1) / rg, (NN + sh.cols - 1) / sh.cols);
+    const size_t smem = adj_joint_smem(sh.nrb, 2, sh.cols);
+    auto go = [&](auto kern) -> int {
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)kern, (int)smem));
+        kern<<<grid, nt, smem, st>>>(a);
+        FEW_LAUNCH_CHECK("k_adj_joint");
+        return FEW_OK;
+    };
+    int rc;
+    if (sh.nrb == 12)
+        rc = go(k_adj_joint<12, 2, 32, 2>);
+    else if (sh.nrb == 11)
+        rc = go(k_adj_joint<11, 2, 32, 2>);
+    else if (sh.nrb == 6)
+        rc = go(k_adj_joint<6, 2, 64, 2>);
+    else
+        rc = go(k_adj_joint<5, 2, 64, 2>);
+    if (rc != FEW_OK) return rc;
+    const int threads = 256;
+    if (G) {
+        const long long per_unit = (long long)R * NN * 4;
+        const long long total = (long long)nseg * per_unit;
+        k_adj_joint_reduce_G<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(Gpart, seg_units, nseg,
+                                                                                             per_unit, G);
+        FEW_LAUNCH_CHECK("k_adj_joint_reduce_G");
+    }
+    if (grad_pc) {
+        const int nblk = (int)(grid.y * grid.z);
+        k_adj_joint_reduce<<<(nseg * 24 + threads - 1) / threads, threads, 0, st>>>(partial, seg_units, nblk, nseg,
+                                                                                  grad_pc);
+        FEW_LAUNCH_CHECK("k_adj_joint_reduce");
+    }
+    return FEW_OK;
+}
+
 int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, const int *key_minus, int K, int N,
                   int nseg, int nkeys, double *gcoef, cudaStream_t st)
 {
@@ -981,6 +1394,29 @@ extern "C" int few_adjoint_G(const void *grad, const double *phase_coeffs, int N
         return few::fail(FEW_ERR_SIZE, "few_adjoint_G: bad sizes");
     return few::launch_adj_G((const double2 *)grad, phase_coeffs, N, seg_info, seg_start, nseg, row_m, row_k, R, nlo,
                              NN, dt, use_theta, (double2 *)G, (cudaStream_t)stream);
+}
+
+extern "C" long long few_adjoint_joint_scratch(int nunits, int R, int NN)
+{
+    if (nunits < 1 || R < 1 || NN < 1) return 0;
+    return few::adj_joint_scratch(nunits, R, NN);
+}
+
+extern "C" int few_adjoint_joint(const void *grad, const void *W, const double *phase_coeffs, int N,
+                                 const double *seg_info, const int *units, int nunits, const int *seg_units, int nseg,
+                                 const int *row_m, const int *row_k, int R, int nlo, int NN, double dt, int use_theta,
+                                 void *G, double *grad_pc, double *scratch, void *stream)
+{
+    few::clear_error();
+    if (!grad || !phase_coeffs || !seg_info || !units || !seg_units || !row_m || !row_k || !scratch)
+        return few::fail(FEW_ERR_ARG, "few_adjoint_joint: null pointer");
+    if (!G && !grad_pc) return few::fail(FEW_ERR_ARG, "few_adjoint_joint: neither G nor grad_pc given");
+    if (grad_pc && !W) return few::fail(FEW_ERR_ARG, "few_adjoint_joint: grad_pc needs W");
+    if (N < 2 || nunits < 0 || nseg < 0 || nseg > N - 1 || R < 1 || R > few::kMaxRows || NN < 1)
+        return few::fail(FEW_ERR_SIZE, "few_adjoint_joint: bad sizes");
+    return few::launch_adj_joint((const double2 *)grad, (const double2 *)W, phase_coeffs, N, seg_info, units, nunits,
+                                 seg_units, nseg, row_m, row_k, R, nlo, NN, dt, use_theta, (double2 *)G, grad_pc,
+                                 scratch, (cudaStream_t)stream);
 }
 
 extern "C" int few_unfold(const void *G, const void *ylms, const int *key_plus, const int *key_minus, int K, int N,

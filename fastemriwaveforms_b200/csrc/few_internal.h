@@ -64,6 +64,12 @@ int launch_adj_phase_reduce(const double *partial, const int *seg_units, int nse
 int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg_info, const int *seg_start, int nseg,
                  const int *row_m, const int *row_k, int R, int nlo, int NN, double dt, int use_theta, double2 *G,
                  cudaStream_t st);
+long long adj_joint_blocks(int R, int NN);
+long long adj_joint_scratch(int nunits, int R, int NN);
+int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, int N, const double *seg_info,
+                     const int *units, int nunits, const int *seg_units, int nseg, const int *row_m, const int *row_k,
+                     int R, int nlo, int NN, double dt, int use_theta, double2 *G, double *grad_pc, double *scratch,
+                     cudaStream_t st);
 int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, const int *key_minus, int K, int N,
                   int nseg, int nkeys, double *gcoef, cudaStream_t st);
 int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *gy, long long sk, long long sp,

@@ -642,14 +642,19 @@ class InterpolatedModeSum(SummationBase):
     @staticmethod
     def _backward(p, grad, need_teuk=True, need_pc=True, concurrent=True):
         """Adjoint kernels: (dL/d teuk_modes (N, K) complex, dL/d phase_interp_coeffs (N-1, 3, 8)).
-        With both gradients wanted and ``concurrent``, the phase branch runs on a
-        second stream beside the amplitude branch (the two kernels leave room for
-        each other on an SM)."""
+        Both FP64 gradients come from one joint pass.  With both gradients wanted
+        from the tensor-core kernels and ``concurrent``, the phase branch runs on
+        a second stream beside the amplitude branch."""
         fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
         grad = grad[: p.out_len].to(torch.complex128).contiguous()
         # the segment tables are uploaded on the caller's stream before the side
         # stream forks from it: the phase branch reads them there
         seg_start, _ = seg.backward_tables()
+        mixed = getattr(p, "bwd_mixed", False)
+        if mixed and need_pc and fold.R > 64:
+            raise ValueError("backward='mixed' supports at most 64 (m, k) rows for phase gradients")
+        if need_teuk and need_pc and not mixed:
+            return InterpolatedModeSum._joint_backward(p, grad)
         both = need_teuk and need_pc and concurrent
         main = torch.cuda.current_stream(dev)
         side = None
@@ -657,9 +662,6 @@ class InterpolatedModeSum(SummationBase):
             side = _side_stream(dev)
             side.wait_stream(main)
         g_teuk = g_pc = None
-        mixed = getattr(p, "bwd_mixed", False)
-        if mixed and need_pc and fold.R > 64:
-            raise ValueError("backward='mixed' supports at most 64 (m, k) rows for phase gradients")
         if need_teuk:
             G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
             if mixed:
@@ -670,12 +672,7 @@ class InterpolatedModeSum(SummationBase):
                 _lib.call("few_adjoint_G", _ptr(grad), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg_start),
                           seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN, p.dt,
                           fold.use_theta, _ptr(G), st)
-            gcoef = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
-            _lib.call("few_unfold", _ptr(G), _ptr(p.ylm), _ptr(fold.d_key_plus), _ptr(fold.d_key_minus), K, N,
-                      seg.nseg, fold.R * fold.NN, _ptr(gcoef), st)
-            g_teuk = torch.empty((N, K), dtype=torch.complex128, device=dev)
-            _lib.call("few_spline_adjoint_factored", _ptr(p.fac), _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N,
-                      0, st)
+            g_teuk = InterpolatedModeSum._amplitude_backward(p, G)
         if need_pc:
             with torch.cuda.stream(side) if both else torch.cuda.stream(main):
                 g_pc = InterpolatedModeSum._phase_backward(p, grad, mixed, side.cuda_stream if both else st)
@@ -684,6 +681,33 @@ class InterpolatedModeSum(SummationBase):
                 if not torch.cuda.is_current_stream_capturing():
                     g_pc.record_stream(main)
         return g_teuk, g_pc
+
+    @staticmethod
+    def _amplitude_backward(p, G):
+        """dL/d teuk_modes (N, K) from G (nseg, R, NN, 4): the transposes of the fold and the spline."""
+        fold, seg, N, K, st, dev = p.fold, p.seg, p.N, p.K, p.st, p.dev
+        gcoef = torch.empty((4, N, 2 * K), dtype=torch.float64, device=dev)
+        _lib.call("few_unfold", _ptr(G), _ptr(p.ylm), _ptr(fold.d_key_plus), _ptr(fold.d_key_minus), K, N,
+                  seg.nseg, fold.R * fold.NN, _ptr(gcoef), st)
+        g_teuk = torch.empty((N, K), dtype=torch.complex128, device=dev)
+        _lib.call("few_spline_adjoint_factored", _ptr(p.fac), _ptr(gcoef), _ptr(g_teuk), 2 * K, 2, K, 1, 2 * K, N,
+                  0, st)
+        return g_teuk
+
+    @staticmethod
+    def _joint_backward(p, grad):
+        """Both FP64 gradients from one pass (few_adjoint_joint): the per-key
+        moments give G and the phase-coefficient gradients together."""
+        fold, seg, N, st, dev = p.fold, p.seg, p.N, p.st, p.dev
+        _, seg_units = seg.backward_tables()
+        G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
+        g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
+        nscratch = int(_lib.load().few_adjoint_joint_scratch(max(seg.nunits, 1), fold.R, fold.NN))
+        scratch = torch.empty(max(nscratch, 1), dtype=torch.float64, device=dev)
+        _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg.d_units),
+                  seg.nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+                  fold.NN, p.dt, fold.use_theta, _ptr(G), _ptr(g_pc), _ptr(scratch), st)
+        return InterpolatedModeSum._amplitude_backward(p, G), g_pc
 
     @staticmethod
     def _phase_backward(p, grad, mixed, st):

@@ -318,6 +318,25 @@ FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, c
                           const int *seg_start, int nseg, const int *row_m, const int *row_k, int R, int nlo, int NN,
                           double dt, int use_theta, void *G, void *stream);
 
+/* Both FP64 adjoints from one pass over the samples.  Per key and work unit
+ * the kernel sums the moments M_p = sum_i sigma_i^p g_i exp(-i phase_key(t_i)),
+ * p = 0..10, sigma = x / (phase step); G[c] = step^c M_c, and the phase
+ * gradients are the keys' moments contracted with the folded coefficients W
+ * [device] (nseg, R, NN, 4) and the basis terms written as polynomials in
+ * sigma.  units [device] (nunits, 3) and seg_units [device] (nseg+1,) as for
+ * few_adjoint_phase and few_adjoint_phase_reduce (units of at most 1024
+ * samples, those of a segment consecutive).  G [device] as few_adjoint_G, or
+ * null; grad_pc [device] (nseg, 3, 8) as few_adjoint_phase_reduce writes it,
+ * or null (not both null); scratch [device] few_adjoint_joint_scratch(nunits,
+ * R, NN) doubles (each unit's share of G and the CTAs' phase partials, summed
+ * per segment in a fixed order).  Agrees with the two separate kernels to
+ * rounding (the sums are regrouped). */
+FEW_API long long few_adjoint_joint_scratch(int nunits, int R, int NN);
+FEW_API int few_adjoint_joint(const void *grad, const void *W, const double *phase_coeffs, int N,
+                              const double *seg_info, const int *units, int nunits, const int *seg_units, int nseg,
+                              const int *row_m, const int *row_k, int R, int nlo, int NN, double dt, int use_theta,
+                              void *G, double *grad_pc, double *scratch, void *stream);
+
 /* Tensor-core adjoint (no counterpart in the reference).  Same quantities as
  * few_adjoint_G and few_adjoint_phase, with the contractions on the tcgen05
  * integer tensor cores in exact arithmetic: FP64 operands (phasors, g, powers
