@@ -1308,11 +1308,8 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
     if (rc != FEW_OK) return rc;
     const int threads = 256;
     if (G) {
-        const long long per_unit = (long long)R * NN * 4;
-        const long long total = (long long)nseg * per_unit;
-        k_adj_joint_reduce_G<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(Gpart, seg_units, nseg,
-                                                                                             per_unit, G);
-        FEW_LAUNCH_CHECK("k_adj_joint_reduce_G");
+        const int rg_ = launch_reduce_unit_G(Gpart, seg_units, nseg, (long long)R * NN * 4, G, st);
+        if (rg_ != FEW_OK) return rg_;
     }
     if (grad_pc) {
         const int nblk = (int)(grid.y * grid.z);
@@ -1320,6 +1317,18 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
                                                                                   grad_pc);
         FEW_LAUNCH_CHECK("k_adj_joint_reduce");
     }
+    return FEW_OK;
+}
+
+int launch_reduce_unit_G(const double2 *Gpart, const int *seg_units, int nseg, long long per_unit, double2 *G,
+                         cudaStream_t st)
+{
+    const long long total = (long long)nseg * per_unit;
+    if (total == 0) return FEW_OK;
+    const int threads = 256;
+    k_adj_joint_reduce_G<<<(unsigned)((total + threads - 1) / threads), threads, 0, st>>>(Gpart, seg_units, nseg,
+                                                                                         per_unit, G);
+    FEW_LAUNCH_CHECK("k_adj_joint_reduce_G");
     return FEW_OK;
 }
 

@@ -70,6 +70,10 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
                      const int *units, int nunits, const int *seg_units, int nseg, const int *row_m, const int *row_k,
                      int R, int nlo, int NN, double dt, int use_theta, double2 *G, double *grad_pc, double *scratch,
                      cudaStream_t st);
+// G[s] = sum of the per-unit shares Gpart[u] (per_unit complex values each) over
+// the segment's units seg_units[s] .. seg_units[s+1]-1, in unit order.
+int launch_reduce_unit_G(const double2 *Gpart, const int *seg_units, int nseg, long long per_unit, double2 *G,
+                         cudaStream_t st);
 int launch_unfold(const double2 *G, const double2 *ylms, const int *key_plus, const int *key_minus, int K, int N,
                   int nseg, int nkeys, double *gcoef, cudaStream_t st);
 int launch_spline_adjoint(const double *t, long long t_rs, double *gc, double *gy, long long sk, long long sp,
