@@ -400,6 +400,29 @@ class _SegmentPlan:
             self._bwd = (t[: self.nseg + 1], t[self.nseg + 1:])
         return self._bwd
 
+    def balanced_units(self, chunk: int = 1024):
+        """Device (units (n, 3), seg_units (nseg+1,)) int32 for the joint adjoint:
+        each segment's samples cut into ceil(len / chunk) parts of equal length
+        (within one sample), so no work unit is a short remainder."""
+        if not hasattr(self, "_bal"):
+            lo = self.seg_start[: self.nseg].astype(np.int64)
+            hi = self.seg_start[1: self.nseg + 1].astype(np.int64)
+            n = np.maximum(hi - lo, 0)
+            parts = (n + chunk - 1) // chunk
+            seg_units = np.zeros(self.nseg + 1, np.int32)
+            seg_units[1:] = np.cumsum(parts)
+            total = int(seg_units[-1])
+            seg = np.repeat(np.arange(self.nseg), parts)
+            k = np.arange(total) - np.repeat(seg_units[:-1], parts)
+            P = np.repeat(parts, parts)
+            a = np.repeat(lo, parts) + (k * np.repeat(n, parts)) // np.maximum(P, 1)
+            b = np.repeat(lo, parts) + ((k + 1) * np.repeat(n, parts)) // np.maximum(P, 1)
+            units = np.stack([seg, a, b], axis=1).astype(np.int32).reshape(-1)
+            host = np.concatenate([units, seg_units])
+            t = _upload(host, self._device)
+            self._bal = (t[: 3 * total], t[3 * total:], total)
+        return self._bal
+
 
 class _Prepared:
     """Inputs, plans and device tensors of one call (kept for the backward)."""
@@ -699,13 +722,13 @@ class InterpolatedModeSum(SummationBase):
         """Both FP64 gradients from one pass (few_adjoint_joint): the per-key
         moments give G and the phase-coefficient gradients together."""
         fold, seg, N, st, dev = p.fold, p.seg, p.N, p.st, p.dev
-        _, seg_units = seg.backward_tables()
+        units, seg_units, nunits = seg.balanced_units()
         G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
         g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
-        nscratch = int(_lib.load().few_adjoint_joint_scratch(max(seg.nunits, 1), fold.R, fold.NN))
+        nscratch = int(_lib.load().few_adjoint_joint_scratch(max(nunits, 1), fold.R, fold.NN))
         scratch = torch.empty(max(nscratch, 1), dtype=torch.float64, device=dev)
-        _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(seg.d_units),
-                  seg.nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
+        _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(units),
+                  nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
                   fold.NN, p.dt, fold.use_theta, _ptr(G), _ptr(g_pc), _ptr(scratch), st)
         return InterpolatedModeSum._amplitude_backward(p, G), g_pc
 

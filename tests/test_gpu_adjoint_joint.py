@@ -1,5 +1,5 @@
 """The joint FP64 adjoint (few_adjoint_joint: eleven moments per key and
-segment, from which G and the phase-coefficient gradients both follow) against
+work unit, from which G and the phase-coefficient gradients both follow) against
 the two separate FP64 adjoint kernels (few_adjoint_G, few_adjoint_phase and its
 reduction).  The joint pass regroups the same sums, so the two agree to
 rounding; the cases cover the theta phase on and off, several row and column
@@ -62,15 +62,19 @@ def _separate(p, grad):
     return G.cpu().numpy()[: seg.nseg], g_pc.cpu().numpy()
 
 
-def _joint(p, grad, want_G=True, want_pc=True):
+def _joint(p, grad, want_G=True, want_pc=True, balanced=True):
     fold, seg = p.fold, p.seg
-    _, seg_units = seg.backward_tables()
+    if balanced:
+        units, seg_units, nunits = seg.balanced_units()
+    else:
+        units, nunits = seg.d_units, seg.nunits
+        _, seg_units = seg.backward_tables()
     G = torch.full((max(seg.nseg, 1), fold.R, fold.NN, 4), np.nan, dtype=torch.complex128, device=grad.device)
     g_pc = torch.zeros((p.N - 1, 3, 8), dtype=torch.float64, device=grad.device)
-    n = int(_lib.load().few_adjoint_joint_scratch(max(seg.nunits, 1), fold.R, fold.NN))
+    n = int(_lib.load().few_adjoint_joint_scratch(max(nunits, 1), fold.R, fold.NN))
     scratch = torch.full((max(n, 1),), np.nan, dtype=torch.float64, device=grad.device)
-    _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), p.N, _ptr(seg.d_seg_info), _ptr(seg.d_units),
-              seg.nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN,
+    _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), p.N, _ptr(seg.d_seg_info), _ptr(units),
+              nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo, fold.NN,
               p.dt, fold.use_theta, _ptr(G) if want_G else 0, _ptr(g_pc) if want_pc else 0, _ptr(scratch), p.st)
     return G.cpu().numpy()[: seg.nseg], g_pc.cpu().numpy()
 
@@ -103,6 +107,10 @@ def test_joint_adjoint_single_outputs_and_determinism(cuda):
     _, pc_only = _joint(p, grad, want_G=False)
     assert np.array_equal(G_only, G)
     assert np.array_equal(pc_only, pc)
+    # the forward's work units (a short remainder per segment) regroup the same sums
+    G_u, pc_u = _joint(p, grad, balanced=False)
+    assert np.abs(G_u - G).max() <= TOL_G * np.abs(G).max()
+    assert np.abs(pc_u - pc).max() <= TOL_PC * np.abs(pc).max()
 
 
 def test_joint_adjoint_argument_errors(cuda):
