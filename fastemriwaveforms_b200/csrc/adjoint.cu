@@ -441,13 +441,13 @@ struct AdjJointArgs {
 // Dynamic shared memory of k_adj_joint: the tile tables of k_adj_G plus the
 // powers sigma^1..sigma^10 of the tile's samples and sigma of the staged ones
 // (nrb row blocks of rb rows by cols columns; nrb * cols samples staged).
-constexpr size_t adj_joint_smem(int nrb, int rb, int cols)
+constexpr size_t adj_joint_smem(int nrb, int rb, int cols, int tile)
 {
-    return (size_t)kGTile * nrb * rb * sizeof(double2)         // g u_r
-           + (size_t)kGTile * cols * sizeof(double2)            // v_{n'}
-           + (size_t)kGTile * 2 * kGPow * sizeof(double2)       // powers of e^{-i Phi_phi}, e^{-i Phi_r}
+    return (size_t)tile * nrb * rb * sizeof(double2)           // g u_r
+           + (size_t)tile * cols * sizeof(double2)              // v_{n'}
+           + (size_t)tile * 2 * kGPow * sizeof(double2)         // powers of e^{-i Phi_phi}, e^{-i Phi_r}
            + (size_t)nrb * cols * 5 * sizeof(double2)           // Ep, Er, Et, g, v at this CTA's first n'
-           + (size_t)kGTile * 5 * sizeof(double2)               // (sigma^(2h+1), sigma^(2h+2)), h < 5
+           + (size_t)tile * 5 * sizeof(double2)                 // (sigma^(2h+1), sigma^(2h+2)), h < 5
            + (size_t)nrb * cols * sizeof(double);               // sigma
 }
 
@@ -459,24 +459,23 @@ constexpr size_t adj_joint_smem(int nrb, int rb, int cols)
 // samples added in order (deterministic).  The epilogue writes the unit's
 // share of G and reduces the keys' phase terms over the CTA into one row of 24
 // partials (field-major: phi, theta, r; 8 basis terms each).
-template <int NRB, int RB, int COLS, int UNR>
+template <int NRB, int RB, int COLS, int UNR, int TILE>
 __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
 {
     constexpr int NT = NRB * COLS;  // threads; also the samples staged per phase batch
     constexpr int RG = NRB * RB;    // rows per CTA
-    static_assert(NT >= 5 * kGTile, "the tile tables need 5 x 64 threads");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *sp = smem_raw;
     double2 (*s_gu)[RG] = reinterpret_cast<double2 (*)[RG]>(sp);
-    sp += (size_t)kGTile * RG * sizeof(double2);
+    sp += (size_t)TILE * RG * sizeof(double2);
     double2 (*s_v)[COLS] = reinterpret_cast<double2 (*)[COLS]>(sp);
-    sp += (size_t)kGTile * COLS * sizeof(double2);
+    sp += (size_t)TILE * COLS * sizeof(double2);
     double2 (*s_P)[2][kGPow] = reinterpret_cast<double2 (*)[2][kGPow]>(sp);
-    sp += (size_t)kGTile * 2 * kGPow * sizeof(double2);
+    sp += (size_t)TILE * 2 * kGPow * sizeof(double2);
     double2 (*s_E)[5] = reinterpret_cast<double2 (*)[5]>(sp);
     sp += (size_t)NT * 5 * sizeof(double2);
     double2 (*s_sig)[5] = reinterpret_cast<double2 (*)[5]>(sp);
-    sp += (size_t)kGTile * 5 * sizeof(double2);
+    sp += (size_t)TILE * 5 * sizeof(double2);
     double *s_sx = reinterpret_cast<double *>(sp);
     __shared__ int s_rm[RG], s_rk[RG];
     __shared__ double s_pc[24];
@@ -544,35 +543,38 @@ __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
             s_E[tid][4] = cpow_int(s_E[tid][1], a.nlo + c0);
             s_sx[tid] = __ddiv_rn(x, pw);
         }
-        for (int i0 = 0; i0 < np; i0 += kGTile) {
-            const int ns = min(kGTile, np - i0);
+        for (int i0 = 0; i0 < np; i0 += TILE) {
+            const int ns = min(TILE, np - i0);
             __syncthreads();  // phase data written; the previous tile's readers are done
-            if (tid < 4 * ns) {
-                // two threads per (sample, phasor): half h writes E^{4h..4h+3} and
-                // E^{8 (4h..4h+3)}, every entry at most seven products from E
-                const int j = tid >> 2, f = (tid >> 1) & 1, h = tid & 1;
-                const double2 E = s_E[i0 + j][f];
-                double2 *T = s_P[j][f];
-                const double2 E2 = cmul(E, E), E4 = cmul(E2, E2), E8 = cmul(E4, E4);
-                const double2 E16 = cmul(E8, E8), E32 = cmul(E16, E16);
-                const double2 b1 = h ? E4 : make_double2(1.0, 0.0), b8 = h ? E32 : make_double2(1.0, 0.0);
-                T[4 * h] = b1;
-                T[4 * h + 1] = h ? cmul(b1, E) : E;
-                T[4 * h + 2] = h ? cmul(b1, E2) : E2;
-                T[4 * h + 3] = cmul(h ? cmul(b1, E2) : E2, E);
-                T[8 + 4 * h] = b8;
-                T[8 + 4 * h + 1] = h ? cmul(b8, E8) : E8;
-                T[8 + 4 * h + 2] = h ? cmul(b8, E16) : E16;
-                T[8 + 4 * h + 3] = cmul(h ? cmul(b8, E16) : E16, E8);
-            } else if (tid >= 4 * kGTile && tid < 4 * kGTile + ns) {
-                const int j = tid - 4 * kGTile;
-                const double sg = s_sx[i0 + j];
-                double *row = reinterpret_cast<double *>(s_sig[j]);
-                double pp = sg;
+            // power tables (two work items per sample and phasor: half h writes
+            // E^{4h..4h+3} and E^{8 (4h..4h+3)}, every entry at most seven products
+            // from E), then the sigma powers (one item per sample)
+            for (int k = tid; k < 5 * ns; k += NT) {
+                if (k < 4 * ns) {
+                    const int j = k >> 2, f = (k >> 1) & 1, h = k & 1;
+                    const double2 E = s_E[i0 + j][f];
+                    double2 *T = s_P[j][f];
+                    const double2 E2 = cmul(E, E), E4 = cmul(E2, E2), E8 = cmul(E4, E4);
+                    const double2 E16 = cmul(E8, E8), E32 = cmul(E16, E16);
+                    const double2 b1 = h ? E4 : make_double2(1.0, 0.0), b8 = h ? E32 : make_double2(1.0, 0.0);
+                    T[4 * h] = b1;
+                    T[4 * h + 1] = h ? cmul(b1, E) : E;
+                    T[4 * h + 2] = h ? cmul(b1, E2) : E2;
+                    T[4 * h + 3] = cmul(h ? cmul(b1, E2) : E2, E);
+                    T[8 + 4 * h] = b8;
+                    T[8 + 4 * h + 1] = h ? cmul(b8, E8) : E8;
+                    T[8 + 4 * h + 2] = h ? cmul(b8, E16) : E16;
+                    T[8 + 4 * h + 3] = cmul(h ? cmul(b8, E16) : E16, E8);
+                } else {
+                    const int j = k - 4 * ns;
+                    const double sg = s_sx[i0 + j];
+                    double *row = reinterpret_cast<double *>(s_sig[j]);
+                    double pp = sg;
 #pragma unroll
-                for (int q = 0; q < 10; ++q) {
-                    row[q] = pp;
-                    pp *= sg;
+                    for (int q = 0; q < 10; ++q) {
+                        row[q] = pp;
+                        pp *= sg;
+                    }
                 }
             }
             __syncthreads();
@@ -1289,7 +1291,10 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
     const JointShape sh = joint_shape(R, NN);
     const int rg = 2 * sh.nrb, nt = sh.nrb * sh.cols;
     dim3 grid(nunits, (R + rg - 1) / rg, (NN + sh.cols - 1) / sh.cols);
-    const size_t smem = adj_joint_smem(sh.nrb, 2, sh.cols);
+    // 128-sample tiles (half the table barriers per sample: 9.85 against 9.93 ms at
+    // the one-year waveform) where their tables fit shared memory, else 64
+    const int tile = adj_joint_smem(sh.nrb, 2, sh.cols, 128) + 4096 <= 227 * 1024 ? 128 : 64;
+    const size_t smem = adj_joint_smem(sh.nrb, 2, sh.cols, tile);
     auto go = [&](auto kern) -> int {
         FEW_CUDA_TRY(ensure_smem_attr((const void *)kern, (int)smem));
         kern<<<grid, nt, smem, st>>>(a);
@@ -1297,14 +1302,25 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
         return FEW_OK;
     };
     int rc;
-    if (sh.nrb == 12)
-        rc = go(k_adj_joint<12, 2, 32, 2>);
-    else if (sh.nrb == 11)
-        rc = go(k_adj_joint<11, 2, 32, 2>);
-    else if (sh.nrb == 6)
-        rc = go(k_adj_joint<6, 2, 64, 2>);
-    else
-        rc = go(k_adj_joint<5, 2, 64, 2>);
+    if (tile == 64) {
+        if (sh.nrb == 12)
+            rc = go(k_adj_joint<12, 2, 32, 2, 64>);
+        else if (sh.nrb == 11)
+            rc = go(k_adj_joint<11, 2, 32, 2, 64>);
+        else if (sh.nrb == 6)
+            rc = go(k_adj_joint<6, 2, 64, 2, 64>);
+        else
+            rc = go(k_adj_joint<5, 2, 64, 2, 64>);
+    } else {
+        if (sh.nrb == 12)
+            rc = go(k_adj_joint<12, 2, 32, 2, 128>);
+        else if (sh.nrb == 11)
+            rc = go(k_adj_joint<11, 2, 32, 2, 128>);
+        else if (sh.nrb == 6)
+            rc = go(k_adj_joint<6, 2, 64, 2, 128>);
+        else
+            rc = go(k_adj_joint<5, 2, 64, 2, 128>);
+    }
     if (rc != FEW_OK) return rc;
     const int threads = 256;
     if (G) {
