@@ -635,7 +635,7 @@ class InterpolatedModeSum(SummationBase):
         return out
 
     @staticmethod
-    def _sum_streamed(run, seg, out, host_out, dev, parts: int = 4):
+    def _sum_streamed(run, seg, out, host_out, dev, parts: int = 8):
         """The sum in `parts` launches over consecutive units; after each, the
         samples it finished go to host_out on the download stream."""
         main = torch.cuda.current_stream(dev)
