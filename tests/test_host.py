@@ -203,3 +203,32 @@ def test_autotune_shape_search_and_cache(tmp_path, monkeypatch):
     assert choice["ctas_per_sm"] == 2 and choice["chunk"] == min(autotune.CHUNKS)
     assert len(choice["tried"]) == len(fp64)
     assert autotune.lookup("k")["ctas_per_sm"] == 2
+
+
+def test_balanced_work_units_tile_every_segment():
+    """The joint adjoint's work units: each segment's samples cut into
+    ceil(len / 1024) parts whose lengths differ by at most one, covering the
+    segment exactly once and in order; segments without samples get none."""
+    from fastemriwaveforms_b200.summation import _SegmentPlan
+
+    class Plan:
+        _device = "cpu"
+
+    rng = np.random.default_rng(3)
+    lens = np.concatenate([[0, 1, 1023, 1024, 1025, 3150], rng.integers(0, 5000, 40)])
+    plan = Plan()
+    plan.seg_start = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    plan.nseg = len(lens)
+    units, seg_units, total = _SegmentPlan.balanced_units(plan)
+    units = units.numpy().reshape(-1, 3)
+    seg_units = seg_units.numpy()
+    assert total == len(units) == seg_units[-1]
+    for s, n in enumerate(lens):
+        part = units[seg_units[s]: seg_units[s + 1]]
+        assert len(part) == -(-int(n) // 1024)
+        assert (part[:, 0] == s).all()
+        if len(part):
+            assert part[0, 1] == plan.seg_start[s] and part[-1, 2] == plan.seg_start[s + 1]
+            assert (part[1:, 1] == part[:-1, 2]).all()
+            sizes = part[:, 2] - part[:, 1]
+            assert sizes.max() - sizes.min() <= 1 and sizes.max() <= 1024 and sizes.min() >= 1
