@@ -12,6 +12,10 @@
 //   k_adj_G       per segment, G[key][c] = sum_i g_i x_i^c P_key(t_i): one CTA
 //                 per segment, per-sample phasor tables staged in shared memory,
 //                 each thread owning a few keys (deterministic, no atomics).
+//   k_adj_joint   both of the above from one pass: per key and work unit the
+//                 moments sum_i sigma_i^p g_i P_key(t_i), p = 0..10, from which
+//                 G and the phase-coefficient gradients follow (used when both
+//                 gradients are wanted); k_adj_joint_reduce(_G) add the units.
 //   k_unfold      the transpose of the fold: dL/da per mode and coefficient.
 //   k_spline_adjoint  the transpose of the spline build: solves with A^T, the
 //                 transposed not-a-knot matrix.  With M the row operations that
@@ -410,7 +414,8 @@ __global__ void __launch_bounds__(kGThreads, 1) k_adj_G(AdjGArgs a)
 // For key (r, n') let z_i = g_i u_r(t_i) v_n(t_i) (n = nlo + n') and let
 // sigma_i = x_i / w (x = t - t0, w the phase step of the segment).  The kernel
 // accumulates per key the eleven moments M_p = sum_i sigma_i^p z_i, p = 0..10,
-// over the segment's samples; both gradients are linear in them:
+// over the samples of a work unit (part of one segment); both gradients are
+// linear in them, so the units of a segment combine by plain sums:
 //   G[c] = w^c M_c  (c = 0..3), and
 //   dL/dcoef_{f,q} = sum_keys wt_f Im( sum_c W_c w^c sum_j beta_qj M_{j+c} ),
 // with wt_f = m', k' or n for the fields phi, theta, r, W_c the forward's folded
