@@ -464,7 +464,7 @@ constexpr size_t adj_joint_smem(int nrb, int rb, int cols, int tile)
 // samples added in order (deterministic).  The epilogue writes the unit's
 // share of G and reduces the keys' phase terms over the CTA into one row of 24
 // partials (field-major: phi, theta, r; 8 basis terms each).
-template <int NRB, int RB, int COLS, int UNR, int TILE>
+template <int NRB, int RB, int COLS, int UNR, int TILE, int NMOM>
 __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
 {
     constexpr int NT = NRB * COLS;  // threads; also the samples staged per phase batch
@@ -517,11 +517,14 @@ __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
             for (int j = 7; j >= 0; --j) b[j] = ga * b[j] + (j ? al * b[j - 1] : 0.0);
         }
     }
-    double2 acc[RB][kJMom];
+    // NMOM = 11 moments for both gradients, 5 for G alone (moments 0..3 used)
+    static_assert(NMOM == kJMom || NMOM == 5, "11 moments, or 5 for G alone");
+    constexpr bool PHASE = NMOM == kJMom;
+    double2 acc[RB][NMOM];
 #pragma unroll
     for (int q = 0; q < RB; ++q)
 #pragma unroll
-        for (int p = 0; p < kJMom; ++p) acc[q][p] = make_double2(0.0, 0.0);
+        for (int p = 0; p < NMOM; ++p) acc[q][p] = make_double2(0.0, 0.0);
 
     for (int p0 = lo; p0 < hi; p0 += NT) {
         const int np = min(NT, hi - p0);
@@ -614,7 +617,7 @@ __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
                     acc[q][0].y += z[q].y;
                 }
 #pragma unroll
-                for (int h = 0; h < 5; ++h) {
+                for (int h = 0; h < (NMOM - 1) / 2; ++h) {
                     const double2 sg = s_sig[j][h];
 #pragma unroll
                     for (int q = 0; q < RB; ++q) {
@@ -649,7 +652,7 @@ __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
             g[2] = make_double2(acc[q][2].x * w2, acc[q][2].y * w2);
             g[3] = make_double2(acc[q][3].x * w3, acc[q][3].y * w3);
         }
-        if (a.partial) {
+        if constexpr (PHASE) if (a.partial) {
             const double2 *Wk = a.W + key * 4;
             const double2 W0 = Wk[0], W1 = Wk[1], W2 = Wk[2], W3 = Wk[3];
             const double2 om[4] = {W0, make_double2(W1.x * w1, W1.y * w1), make_double2(W2.x * w2, W2.y * w2),
@@ -676,7 +679,7 @@ __global__ void __launch_bounds__(NRB * COLS, 1) k_adj_joint(AdjJointArgs a)
             }
         }
     }
-    if (!a.partial) return;
+    if (!PHASE || !a.partial) return;
     const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
     for (int f = 0; f < 3; ++f)
@@ -1293,6 +1296,17 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
     a.NN = NN;
     a.use_theta = use_theta;
     a.dt = dt;
+    if (!grad_pc) {
+        // G alone: five moments per key (0..3 used), 6 row blocks of 4 rows x 64
+        // columns, 64-sample tiles
+        dim3 grid(nunits, (R + 23) / 24, (NN + 63) / 64);
+        const size_t smem = adj_joint_smem(6, 4, 64, 64);
+        auto kern = k_adj_joint<6, 4, 64, 2, 64, 5>;
+        FEW_CUDA_TRY(ensure_smem_attr((const void *)kern, (int)smem));
+        kern<<<grid, 384, smem, st>>>(a);
+        FEW_LAUNCH_CHECK("k_adj_joint");
+        return launch_reduce_unit_G(Gpart, seg_units, nseg, (long long)R * NN * 4, G, st);
+    }
     const JointShape sh = joint_shape(R, NN);
     const int rg = 2 * sh.nrb, nt = sh.nrb * sh.cols;
     dim3 grid(nunits, (R + rg - 1) / rg, (NN + sh.cols - 1) / sh.cols);
@@ -1309,22 +1323,22 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
     int rc;
     if (tile == 64) {
         if (sh.nrb == 12)
-            rc = go(k_adj_joint<12, 2, 32, 2, 64>);
+            rc = go(k_adj_joint<12, 2, 32, 2, 64, kJMom>);
         else if (sh.nrb == 11)
-            rc = go(k_adj_joint<11, 2, 32, 2, 64>);
+            rc = go(k_adj_joint<11, 2, 32, 2, 64, kJMom>);
         else if (sh.nrb == 6)
-            rc = go(k_adj_joint<6, 2, 64, 2, 64>);
+            rc = go(k_adj_joint<6, 2, 64, 2, 64, kJMom>);
         else
-            rc = go(k_adj_joint<5, 2, 64, 2, 64>);
+            rc = go(k_adj_joint<5, 2, 64, 2, 64, kJMom>);
     } else {
         if (sh.nrb == 12)
-            rc = go(k_adj_joint<12, 2, 32, 2, 128>);
+            rc = go(k_adj_joint<12, 2, 32, 2, 128, kJMom>);
         else if (sh.nrb == 11)
-            rc = go(k_adj_joint<11, 2, 32, 2, 128>);
+            rc = go(k_adj_joint<11, 2, 32, 2, 128, kJMom>);
         else if (sh.nrb == 6)
-            rc = go(k_adj_joint<6, 2, 64, 2, 128>);
+            rc = go(k_adj_joint<6, 2, 64, 2, 128, kJMom>);
         else
-            rc = go(k_adj_joint<5, 2, 64, 2, 128>);
+            rc = go(k_adj_joint<5, 2, 64, 2, 128, kJMom>);
     }
     if (rc != FEW_OK) return rc;
     const int threads = 256;

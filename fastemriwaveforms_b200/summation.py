@@ -676,8 +676,8 @@ class InterpolatedModeSum(SummationBase):
         mixed = getattr(p, "bwd_mixed", False)
         if mixed and need_pc and fold.R > 64:
             raise ValueError("backward='mixed' supports at most 64 (m, k) rows for phase gradients")
-        if need_teuk and need_pc and not mixed:
-            return InterpolatedModeSum._joint_backward(p, grad)
+        if need_teuk and not mixed:
+            return InterpolatedModeSum._joint_backward(p, grad, need_pc)
         both = need_teuk and need_pc and concurrent
         main = torch.cuda.current_stream(dev)
         side = None
@@ -718,18 +718,19 @@ class InterpolatedModeSum(SummationBase):
         return g_teuk
 
     @staticmethod
-    def _joint_backward(p, grad):
-        """Both FP64 gradients from one pass (few_adjoint_joint): the per-key
-        moments give G and the phase-coefficient gradients together."""
+    def _joint_backward(p, grad, want_pc=True):
+        """FP64 gradients from one pass (few_adjoint_joint): the per-key moments
+        give G and, with want_pc, the phase-coefficient gradients together; G
+        alone takes the kernel's five-moment form."""
         fold, seg, N, st, dev = p.fold, p.seg, p.N, p.st, p.dev
         units, seg_units, nunits = seg.balanced_units()
         G = torch.empty((max(seg.nseg, 1), fold.R, fold.NN, 4), dtype=torch.complex128, device=dev)
-        g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev)
+        g_pc = torch.zeros((N - 1, 3, 8), dtype=torch.float64, device=dev) if want_pc else None
         nscratch = int(_lib.load().few_adjoint_joint_scratch(max(nunits, 1), fold.R, fold.NN))
         scratch = torch.empty(max(nscratch, 1), dtype=torch.float64, device=dev)
         _lib.call("few_adjoint_joint", _ptr(grad), _ptr(p.W), _ptr(p.pc), N, _ptr(seg.d_seg_info), _ptr(units),
                   nunits, _ptr(seg_units), seg.nseg, _ptr(fold.d_row_m), _ptr(fold.d_row_k), fold.R, fold.nlo,
-                  fold.NN, p.dt, fold.use_theta, _ptr(G), _ptr(g_pc), _ptr(scratch), st)
+                  fold.NN, p.dt, fold.use_theta, _ptr(G), _ptr(g_pc) if want_pc else 0, _ptr(scratch), st)
         return InterpolatedModeSum._amplitude_backward(p, G), g_pc
 
     @staticmethod

@@ -329,8 +329,9 @@ FEW_API int few_adjoint_G(const void *grad, const double *phase_coeffs, int N, c
  * null; grad_pc [device] (nseg, 3, 8) as few_adjoint_phase_reduce writes it,
  * or null (not both null); scratch [device] few_adjoint_joint_scratch(nunits,
  * R, NN) doubles (each unit's share of G and the CTAs' phase partials, summed
- * per segment in a fixed order).  Agrees with the two separate kernels to
- * rounding (the sums are regrouped). */
+ * per segment in a fixed order).  With grad_pc null the kernel keeps only the
+ * moments G needs (the form the amplitude-only backward uses).  Agrees with the
+ * two separate kernels to rounding (the sums are regrouped). */
 FEW_API long long few_adjoint_joint_scratch(int nunits, int R, int NN);
 FEW_API int few_adjoint_joint(const void *grad, const void *W, const double *phase_coeffs, int N,
                               const double *seg_info, const int *units, int nunits, const int *seg_units, int nseg,

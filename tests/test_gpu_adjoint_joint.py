@@ -97,8 +97,8 @@ def test_joint_adjoint_matches_separate_kernels(cuda, name):
 
 
 def test_joint_adjoint_single_outputs_and_determinism(cuda):
-    """G alone and the phase gradients alone equal the combined call's, and a
-    repeated call gives the same bits."""
+    """G alone (the five-moment form) and the phase gradients alone equal the
+    combined call's, and a repeated call gives the same bits."""
     p, grad = _plan(S.small_case(K=30, N=25, out_len=8000, seed=10, theta=True), cuda)
     G, pc = _joint(p, grad)
     G2, pc2 = _joint(p, grad)
@@ -126,3 +126,15 @@ def test_joint_adjoint_argument_errors(cuda):
     g_pc = torch.zeros((p.N - 1, 3, 8), dtype=torch.float64, device=cuda)
     with pytest.raises(ValueError, match="null pointer"):  # the scratch rows are required
         _lib.call("few_adjoint_joint", *common, 0, _ptr(g_pc), 0, p.st)
+
+
+@pytest.mark.parametrize("name", ["small_theta", "many_rows", "wide_n", "dense_knots"])
+def test_joint_G_alone_matches_G_kernel(cuda, name):
+    """G alone (five moments per key, used when only the amplitude gradient is
+    wanted) against few_adjoint_G."""
+    p, grad = _plan(CASES[name](), cuda)
+    G_ref, _ = _separate(p, grad)
+    G, _ = _joint(p, grad, want_pc=False)
+    assert np.isfinite(G).all()
+    assert np.abs(G - G_ref).max() <= TOL_G * np.abs(G_ref).max()
+
