@@ -1235,22 +1235,24 @@ int launch_adj_G(const double2 *grad, const double *pc, int N, const double *seg
     return FEW_OK;
 }
 
-// Shape of the joint adjoint's CTA: NRB row blocks of 2 rows by COLS columns,
+// Shape of the joint adjoint's CTA: NRB row blocks of RB rows by COLS columns,
 // the candidate that pads the (row, column) keys least, the first listed on a
 // tie.  With fewer columns per CTA the row and column tables cover fewer
 // entries per key (12 x 32: 24 + 32 per sample for 768 keys; 6 x 64: 12 + 64
-// for 768 keys).
+// for 768 keys).  Three rows per thread (7 x 3 rows x 32 columns, 224 threads,
+// no padding at R = 21) took 10.74 ms against 9.86 ms for 11 x 2 x 32: seven
+// warps per SM were too few.
 struct JointShape {
-    int nrb, cols;
+    int nrb, rb, cols;
 };
-constexpr JointShape kJointShapes[] = {{12, 32}, {11, 32}, {6, 64}, {5, 64}};
+constexpr JointShape kJointShapes[] = {{12, 2, 32}, {11, 2, 32}, {6, 2, 64}, {5, 2, 64}};
 
 static JointShape joint_shape(int R, int NN)
 {
     JointShape best = kJointShapes[0];
     long long best_keys = -1;
     for (const JointShape &c : kJointShapes) {
-        const int rg = 2 * c.nrb;
+        const int rg = c.rb * c.nrb;
         const long long keys = (long long)((R + rg - 1) / rg * rg) * ((NN + c.cols - 1) / c.cols * c.cols);
         if (best_keys < 0 || keys < best_keys) {
             best = c;
@@ -1263,7 +1265,8 @@ static JointShape joint_shape(int R, int NN)
 long long adj_joint_blocks(int R, int NN)
 {
     const JointShape sh = joint_shape(R, NN);
-    return (long long)((R + 2 * sh.nrb - 1) / (2 * sh.nrb)) * ((NN + sh.cols - 1) / sh.cols);
+    const int rg = sh.rb * sh.nrb;
+    return (long long)((R + rg - 1) / rg) * ((NN + sh.cols - 1) / sh.cols);
 }
 
 long long adj_joint_scratch(int nunits, int R, int NN)
@@ -1308,12 +1311,12 @@ int launch_adj_joint(const double2 *grad, const double2 *W, const double *pc, in
         return launch_reduce_unit_G(Gpart, seg_units, nseg, (long long)R * NN * 4, G, st);
     }
     const JointShape sh = joint_shape(R, NN);
-    const int rg = 2 * sh.nrb, nt = sh.nrb * sh.cols;
+    const int rg = sh.rb * sh.nrb, nt = sh.nrb * sh.cols;
     dim3 grid(nunits, (R + rg - 1) / rg, (NN + sh.cols - 1) / sh.cols);
     // 128-sample tiles (half the table barriers per sample: 9.85 against 9.93 ms at
     // the one-year waveform) where their tables fit shared memory, else 64
-    const int tile = adj_joint_smem(sh.nrb, 2, sh.cols, 128) + 4096 <= 227 * 1024 ? 128 : 64;
-    const size_t smem = adj_joint_smem(sh.nrb, 2, sh.cols, tile);
+    const int tile = adj_joint_smem(sh.nrb, sh.rb, sh.cols, 128) + 4096 <= 227 * 1024 ? 128 : 64;
+    const size_t smem = adj_joint_smem(sh.nrb, sh.rb, sh.cols, tile);
     auto go = [&](auto kern) -> int {
         FEW_CUDA_TRY(ensure_smem_attr((const void *)kern, (int)smem));
         kern<<<grid, nt, smem, st>>>(a);
